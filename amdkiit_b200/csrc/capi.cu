@@ -1,0 +1,978 @@
+// libamdk: device context and the extern "C" entry points of include/amdk.h.
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "amdk_internal.h"
+#include "fft.cuh"
+#include "kernels.cuh"
+
+namespace amdk {
+
+static thread_local std::string g_err;
+void set_error(const std::string &m) { g_err = m; }
+
+#define CK(x)                                                                                     \
+  do {                                                                                            \
+    cudaError_t e_ = (x);                                                                         \
+    if (e_ != cudaSuccess) {                                                                      \
+      set_error(std::string("CUDA: ") + cudaGetErrorString(e_) + " at " + __FILE__ + ":" +        \
+                std::to_string(__LINE__));                                                        \
+      return AMDK_ERR_CUDA;                                                                       \
+    }                                                                                             \
+  } while (0)
+#define CB(x)                                                                                     \
+  do {                                                                                            \
+    cublasStatus_t s_ = (x);                                                                      \
+    if (s_ != CUBLAS_STATUS_SUCCESS) {                                                            \
+      set_error(std::string("cuBLAS status ") + std::to_string((int)s_) + " at " + __FILE__ +    \
+                ":" + std::to_string(__LINE__));                                                  \
+      return AMDK_ERR_CUDA;                                                                       \
+    }                                                                                             \
+  } while (0)
+#define RC(x)                    \
+  do {                           \
+    int r_ = (x);                \
+    if (r_) return r_;           \
+  } while (0)
+
+template <typename T> static int dalloc(T **p, size_t n) {
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaMalloc failed: ") + cudaGetErrorString(e) + " (" + std::to_string(n * sizeof(T)) + " bytes)");
+    return AMDK_ERR_ALLOC;
+  }
+  return 0;
+}
+template <typename T> static int upload(T **p, const std::vector<T> &v) {
+  RC(dalloc(p, v.size()));
+  if (!v.empty()) CK(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+}  // namespace amdk
+
+using namespace amdk;
+
+struct amdk_ctx {
+  HostSetup hs;
+  int device = 0, precision = AMDK_FP64, batch = 4;
+  cudaStream_t st = nullptr;
+  cublasHandle_t cb = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0;
+  // geometry / FFT
+  Geom geom;
+  Plan<double2> pd[3];
+  Plan<float2> pf[3];
+  std::vector<void *> allocs;
+  int *d_gmap = nullptr, *d_posp = nullptr, *d_posm = nullptr, *d_zlist[2] = {}, *d_rayidx[2] = {};
+  int *d_inyh = nullptr;
+  double *d_hg = nullptr, *d_gvec = nullptr;
+  long rb_elems_pw = 0, sb_elems_pw = 0, rb_elems_rho = 0, sb_elems_rho = 0;
+  void *d_rb = nullptr, *d_sb = nullptr;
+  size_t fftbuf_bytes = 0;
+  // tables
+  double *d_vps = nullptr, *d_rhos = nullptr, *d_twnl = nullptr, *d_vpp = nullptr, *d_wsg = nullptr;
+  int *d_na = nullptr, *d_ngh = nullptr, *d_zv = nullptr;
+  double2 *d_evps = nullptr, *d_erhos = nullptr;
+  double *d_atarg = nullptr, *d_atco = nullptr;
+  int *d_isa_is = nullptr, *d_isa_ia = nullptr;
+  // projectors (compact list)
+  int nproj = 0;
+  std::vector<int> p_isa, p_is, p_iv, p_l;
+  int *d_pisa = nullptr, *d_pis = nullptr, *d_piv = nullptr, *d_pl = nullptr;
+  double2 *d_P = nullptr, *d_Q = nullptr;
+  double *d_H = nullptr, *d_nl = nullptr, *d_hn = nullptr, *d_D = nullptr, *d_dfnl = nullptr;
+  // electronic state
+  int nstate = 0, npairs = 0;
+  double *d_occ = nullptr, *d_wa = nullptr, *d_wb = nullptr;
+  double2 *d_c0 = nullptr, *d_c2 = nullptr, *d_cp = nullptr, *d_hnm1 = nullptr;
+  double *d_rho = nullptr, *d_vpot = nullptr;
+  double2 *d_rhog = nullptr, *d_vg = nullptr, *d_vxg = nullptr, *d_fp = nullptr, *d_fm = nullptr, *d_cgrid = nullptr;
+  double *d_gam = nullptr;
+  int *d_info = nullptr;
+  double *d_part = nullptr, *d_scal = nullptr, *d_force = nullptr, *d_esr = nullptr, *d_fsr = nullptr;
+  // host copies of scalars
+  double esr = 0, eself = 0;
+  bool tfor = false;
+  bool have_prev_g = false;
+
+  template <typename T> int alloc(T **p, size_t n) {
+    RC(dalloc(p, n));
+    allocs.push_back((void *)*p);
+    return 0;
+  }
+  template <typename T> int up(T **p, const std::vector<T> &v) {
+    RC(amdk::upload(p, v));
+    allocs.push_back((void *)*p);
+    return 0;
+  }
+};
+
+// scalar slots in d_scal
+enum { S_GG = 0, S_GGPREV, S_EH, S_ELOC, S_EXC, S_EKIN, S_ENL, S_GMAX, S_NSCAL = 16 };
+
+static int nblk(long n, int t = NTHR) { return (int)std::min<long>((n + t - 1) / t, 1L << 30); }
+
+template <typename C> static int make_plan(amdk_ctx *c, int n, Plan<C> &p) {
+  int m = n, nf = 0;
+  int f[MAXF];
+  while (m % 4 == 0) { f[nf++] = 4; m /= 4; }
+  while (m % 2 == 0) { f[nf++] = 2; m /= 2; }
+  while (m % 3 == 0) { f[nf++] = 3; m /= 3; }
+  while (m % 5 == 0) { f[nf++] = 5; m /= 5; }
+  if (m != 1 || nf > MAXF) {
+    set_error("FFT length " + std::to_string(n) + " is not 2,3,5-smooth");
+    return AMDK_ERR_UNSUPPORTED;
+  }
+  p.n = n;
+  p.nf = nf;
+  for (int i = 0; i < nf; i++) p.f[i] = f[i];
+  std::vector<C> w(n);
+  const double tp = 8.0 * std::atan(1.0);
+  for (int k = 0; k < n; k++) {
+    double a = -tp * (double)k / (double)n;
+    w[k].x = (decltype(w[k].x))std::cos(a);
+    w[k].y = (decltype(w[k].x))std::sin(a);
+  }
+  C *d;
+  RC(c->up(&d, w));
+  p.w = d;
+  return 0;
+}
+
+// ------------------------------------------------------------------ FFT driver
+template <typename C> static size_t x_smem(int n1) { return 2 * (size_t)n1 * (LX + 1) * sizeof(C); }
+template <typename C> static size_t yz_smem(int n) { return 2 * (size_t)n * TX * sizeof(C); }
+
+template <typename C> static void set_smem_attrs() {
+  int mx = 227 * 1024;
+  cudaFuncSetAttribute(k_x_bwd_pair<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_x_bwd_field<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_x_fwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_y<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_z<C, Z_TO_GRID>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_z<C, Z_FROM_GRID_REAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_z<C, Z_FROM_GRID_CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_z<C, Z_VPSI>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_z<C, Z_DENSITY>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+}
+
+template <typename C> static const Plan<C> &plan(amdk_ctx *c, int d);
+template <> const Plan<double2> &plan<double2>(amdk_ctx *c, int d) { return c->pd[d]; }
+template <> const Plan<float2> &plan<float2>(amdk_ctx *c, int d) { return c->pf[d]; }
+
+// strides of the FFT buffers for transforms of a sphere
+static long rstride(amdk_ctx *c, int sphere) { return (long)c->geom.nray[sphere] * c->geom.n1; }
+static long sstride(amdk_ctx *c, int sphere) { return (long)c->geom.nz[sphere] * c->geom.n2 * c->geom.n1; }
+
+template <typename C> static void y_pass(amdk_ctx *c, int sphere, int dir, int T) {
+  const Geom &g = c->geom;
+  dim3 grid((g.n1 + TX - 1) / TX, g.nz[sphere], T);
+  k_y<C><<<grid, NTHR, yz_smem<C>(g.n2), c->st>>>(sphere, dir, g, plan<C>(c, 1), (C *)c->d_rb, (C *)c->d_sb,
+                                                 rstride(c, sphere), sstride(c, sphere));
+}
+template <typename C, int MODE>
+static void z_pass(amdk_ctx *c, int sphere, int T, double2 *cg, const double *rg, int pair0 = 0) {
+  const Geom &g = c->geom;
+  dim3 grid((g.n1 + TX - 1) / TX, g.n2, MODE == Z_DENSITY ? 1 : T);
+  long gs = (long)g.n1 * g.n2 * g.n3;
+  k_z<C, MODE><<<grid, NTHR, yz_smem<C>(g.n3), c->st>>>(sphere, T, g, plan<C>(c, 2), (C *)c->d_sb, sstride(c, sphere),
+                                                        cg, rg, gs, c->d_vpot, c->d_rho, c->d_wa + pair0, c->d_wb + pair0);
+}
+template <typename C> static void x_fwd(amdk_ctx *c, int sphere, int T) {
+  const Geom &g = c->geom;
+  long lines = (long)T * g.nray[sphere];
+  k_x_fwd<C><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(sphere, T, g, plan<C>(c, 0), (C *)c->d_rb);
+}
+
+// T fields on the density sphere (fp at +G, fm at -G) -> real or complex grids
+static int field_to_grid(amdk_ctx *c, int T, const double2 *fp, const double2 *fm, double2 *cgrid) {
+  const Geom &g = c->geom;
+  long lines = (long)T * g.nray[1];
+  k_x_bwd_field<double2><<<nblk(lines, LX), NTHR, x_smem<double2>(g.n1), c->st>>>(fp, fm, g.ngrho, 1, T, g, c->pd[0],
+                                                                                  (double2 *)c->d_rb);
+  y_pass<double2>(c, 1, +1, T);
+  z_pass<double2, Z_TO_GRID>(c, 1, T, cgrid, nullptr);
+  return 0;
+}
+// T complex grids (or one real grid) -> forward transform left in the ray buffer
+static int grid_to_rays(amdk_ctx *c, int T, const double2 *cgrid, const double *rgrid) {
+  if (rgrid) z_pass<double2, Z_FROM_GRID_REAL>(c, 1, 1, nullptr, rgrid);
+  else z_pass<double2, Z_FROM_GRID_CPLX>(c, 1, T, (double2 *)cgrid, nullptr);
+  y_pass<double2>(c, 1, -1, T);
+  x_fwd<double2>(c, 1, T);
+  return 0;
+}
+
+// ------------------------------------------------------------------ routines
+static int finish_sums(amdk_ctx *c, int nk, int slot) {
+  k_finish_sum<<<nk, NTHR, 0, c->st>>>(c->d_part, RED_BLOCKS, c->d_scal + slot, nk);
+  return 0;
+}
+
+template <typename C> static int density_t(amdk_ctx *c) {
+  const HostSetup &h = c->hs;
+  const Geom &g = c->geom;
+  CK(cudaMemsetAsync(c->d_rho, 0, sizeof(double) * (size_t)g.n1 * g.n2 * g.n3, c->st));
+  for (int p0 = 0; p0 < c->npairs; p0 += c->batch) {
+    int T = std::min(c->batch, c->npairs - p0);
+    long lines = (long)T * g.nray[0];
+    k_x_bwd_pair<C><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(c->d_c0, h.ngpw, c->nstate, 2 * p0, T, g,
+                                                                      plan<C>(c, 0), (C *)c->d_rb);
+    y_pass<C>(c, 0, +1, T);
+    z_pass<C, Z_DENSITY>(c, 0, T, nullptr, nullptr, p0);
+  }
+  // rhor2g (density.f90:128-150)
+  RC(grid_to_rays(c, 1, nullptr, c->d_rho));
+  double scale = 1.0 / ((double)g.n1 * g.n2 * g.n3);
+  k_gather_p<double2><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_posp, (double2 *)c->d_rb, scale, c->d_rhog);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+static int do_density(amdk_ctx *c) {
+  if (c->precision == AMDK_MIXED) return density_t<float2>(c);
+  return density_t<double2>(c);
+}
+
+static int do_potential(amdk_ctx *c) {
+  const HostSetup &h = c->hs;
+  const Geom &g = c->geom;
+  long npt = (long)g.n1 * g.n2 * g.n3;
+  // eval_pot in G space and E_H, E_loc sums
+  k_vloc_g<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngrho, c->d_hg, h.tpiba2, c->d_rhog, c->d_erhos, c->d_evps, c->d_vg,
+                                           c->d_part);
+  RC(finish_sums(c, 2, S_EH));
+  int gga = (h.xc == AMDK_XC_PBE);
+  double2 *g0 = c->d_cgrid, *g1 = c->d_cgrid + npt;
+  if (gga) {
+    k_grad_fields<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_gvec, h.tpiba, c->d_rhog, c->d_fp, c->d_fm);
+    RC(field_to_grid(c, 2, c->d_fp, c->d_fm, c->d_cgrid));
+  }
+  k_xc<<<RED_BLOCKS, NTHR, 0, c->st>>>(npt, h.xc, c->d_rho, g0, g1, c->d_part);
+  RC(finish_sums(c, 1, S_EXC));
+  RC(grid_to_rays(c, gga ? 2 : 1, c->d_cgrid, nullptr));
+  double scale = 1.0 / (double)npt;
+  k_xc_combine<double2><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, gga, c->d_posp, c->d_posm, (double2 *)c->d_rb,
+                                                           rstride(c, 1), scale, c->d_gvec, h.tpiba, c->d_vg, c->d_vxg);
+  k_conj_field<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_vxg, c->d_fm);
+  RC(field_to_grid(c, 1, c->d_vxg, c->d_fm, c->d_cgrid));
+  // V(r) = Re of the backward transform (xc.f90:299-301)
+  CK(cudaMemcpy2DAsync(c->d_vpot, sizeof(double), c->d_cgrid, sizeof(double2), sizeof(double), npt,
+                       cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaGetLastError());
+  return 0;
+}
+
+template <typename C> static int apply_h_t(amdk_ctx *c) {
+  const HostSetup &h = c->hs;
+  const Geom &g = c->geom;
+  double scale = 1.0 / ((double)g.n1 * g.n2 * g.n3);
+  for (int p0 = 0; p0 < c->npairs; p0 += c->batch) {
+    int T = std::min(c->batch, c->npairs - p0);
+    long lines = (long)T * g.nray[0];
+    k_x_bwd_pair<C><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(c->d_c0, h.ngpw, c->nstate, 2 * p0, T, g,
+                                                                      plan<C>(c, 0), (C *)c->d_rb);
+    y_pass<C>(c, 0, +1, T);
+    z_pass<C, Z_VPSI>(c, 0, T, nullptr, nullptr);
+    y_pass<C>(c, 0, -1, T);
+    x_fwd<C>(c, 0, T);
+    dim3 gu(nblk(h.ngpw), T);
+    k_unpack_vpsi<C><<<gu, NTHR, 0, c->st>>>(h.ngpw, c->nstate, 2 * p0, T, c->d_posp, c->d_posm, (C *)c->d_rb,
+                                             rstride(c, 0), scale, c->d_hg, h.tpiba2, c->d_occ, c->d_c0, c->d_c2);
+  }
+  CK(cudaGetLastError());
+  return 0;
+}
+
+// fnl (pseudopotential.f90:164-226): nl = 2 P^T C0; hn = H nl
+static int do_fnl(amdk_ctx *c) {
+  const HostSetup &h = c->hs;
+  if (c->nproj == 0) return 0;
+  const double two = 2.0, one = 1.0, zero = 0.0;
+  int n = c->nstate, K = 2 * h.ngpw;
+  CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, c->nproj, n, K, &two, (const double *)c->d_P, K,
+                 (const double *)c->d_c0, K, &zero, c->d_nl, c->nproj));
+  CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, c->nproj, n, c->nproj, &one, c->d_H, c->nproj, c->d_nl, c->nproj, &zero,
+                 c->d_hn, c->nproj));
+  return 0;
+}
+
+static int do_energy(amdk_ctx *c, amdk_energies *e) {
+  const HostSetup &h = c->hs;
+  RC(do_fnl(c));
+  if (c->nproj) {
+    k_nl_energy_d<<<RED_BLOCKS, NTHR, 0, c->st>>>(c->nproj, c->nstate, c->d_nl, c->d_hn, c->d_occ, c->d_D, c->d_part);
+    RC(finish_sums(c, 1, S_ENL));
+  } else {
+    CK(cudaMemsetAsync(c->d_scal + S_ENL, 0, sizeof(double), c->st));
+  }
+  k_ekin<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngpw, c->nstate, c->d_c0, c->d_hg, c->d_occ, c->d_part);
+  RC(finish_sums(c, 1, S_EKIN));
+  if (e) {
+    double sc[S_NSCAL];
+    CK(cudaMemcpyAsync(sc, c->d_scal, sizeof sc, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    e->eh = sc[S_EH];
+    e->eloc = 2.0 * sc[S_ELOC] * h.omega;
+    e->eself = c->eself;
+    e->esr = c->esr;
+    e->estat = (sc[S_EH] * h.omega) + c->esr - c->eself;
+    e->eke = sc[S_EKIN] * h.tpiba2;
+    e->exc = h.omega / (double)(h.nr[0] * h.nr[1] * h.nr[2]) * sc[S_EXC];
+    e->enl = sc[S_ENL];
+    e->etotal = e->enl + e->eloc + e->eke + e->exc + e->estat;
+    if (!std::isfinite(e->etotal)) {
+      set_error("non-finite total energy");
+      return AMDK_ERR_NONFINITE;
+    }
+  }
+  return 0;
+}
+
+static int do_fnonloc(amdk_ctx *c) {
+  const HostSetup &h = c->hs;
+  if (c->nproj == 0) return 0;
+  const double one = 1.0;
+  int K = 2 * h.ngpw;
+  CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, K, c->nstate, c->nproj, &one, (const double *)c->d_P, K, c->d_D,
+                 c->nproj, &one, (double *)c->d_c2, K));
+  k_fnonloc_g0<<<nblk(c->nstate), NTHR, 0, c->st>>>(c->nproj, c->nstate, h.ngpw, c->d_P, c->d_D, c->d_c2);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+static int do_apply_h(amdk_ctx *c) {
+  if (c->precision == AMDK_MIXED) RC(apply_h_t<float2>(c));
+  else RC(apply_h_t<double2>(c));
+  return do_fnonloc(c);
+}
+
+// forces (gradient.f90:5-34) and eval_GMAX
+static int do_gradient(amdk_ctx *c) {
+  const HostSetup &h = c->hs;
+  int n = c->nstate, K = 2 * h.ngpw;
+  const double two = 2.0, one = 1.0, mone = -1.0, zero = 0.0;
+  CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, (const double *)c->d_c2, K, (const double *)c->d_c0, K,
+                 &zero, c->d_gam, n));
+  k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c2, c->d_c0, c->d_gam, c->d_occ, 1, 0);
+  CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &mone, (const double *)c->d_c0, K, c->d_gam, n, &one,
+                 (double *)c->d_c2, K));
+  k_zclean<<<nblk(n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c2);
+  int nocc = 0;
+  for (int i = 0; i < n; i++)
+    if (h.occ[i] > 1e-5) nocc++;
+  k_gmax<<<RED_BLOCKS, NTHR, 0, c->st>>>((long)nocc * h.ngpw, c->d_c2, c->d_part);
+  k_finish_max<<<1, NTHR, 0, c->st>>>(c->d_part, RED_BLOCKS, c->d_scal + S_GMAX);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+static int do_pcg(amdk_ctx *c, int istep) {
+  const HostSetup &h = c->hs;
+  int n = c->nstate, nocc = 0;
+  for (int i = 0; i < n; i++)
+    if (h.occ[i] > 1e-5) nocc++;
+  long tot = (long)h.ngpw * n;
+  k_precon<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngpw, n, nocc, c->d_vpp, c->d_occ, c->d_c2, c->d_cp, c->d_part);
+  RC(finish_sums(c, 1, S_GG));
+  k_pcg_update<<<RED_BLOCKS * 4, NTHR, 0, c->st>>>(tot, istep, c->d_scal, c->d_cp, c->d_hnm1, c->d_c0);
+  k_copy_scalar<<<1, 1, 0, c->st>>>(c->d_scal + S_GG, c->d_scal + S_GGPREV);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+static int do_ortho(amdk_ctx *c) {
+  const HostSetup &h = c->hs;
+  int n = c->nstate, K = 2 * h.ngpw;
+  const double two = 2.0, zero = 0.0, one = 1.0;
+  CB(cublasDsyrk(c->cb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, n, K, &two, (const double *)c->d_c0, K, &zero, c->d_gam, n));
+  k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c0, c->d_c0, c->d_gam, c->d_occ, 0, 1);
+  size_t sm = (size_t)n * n * sizeof(double);
+  if (sm > 200 * 1024) sm = 0;
+  k_cholesky_upper<<<1, 1024, sm, c->st>>>(n, c->d_gam, c->d_info);
+  int info = 0;
+  CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (info) {
+    set_error("overlap matrix not positive definite at leading minor " + std::to_string(info));
+    return AMDK_ERR_NOT_SPD;
+  }
+  CB(cublasDtrsm(c->cb, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, K, n, &one, c->d_gam,
+                 n, (double *)c->d_c0, K));
+  k_zclean<<<nblk(n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c0);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+// exp_igrxfactor and everything that depends on the positions: structure
+// factor sums, projector matrix, preconditioner, e_sr energy and forces.
+static int do_positions(amdk_ctx *c, const double *atco) {
+  HostSetup &h = c->hs;
+  h.atco.assign(atco, atco + 3L * h.na_max * h.nsp);
+  std::vector<double> arg(3L * h.nat);
+  for (int a = 0; a < h.nat; a++) {
+    const double *x = atco + 3 * (h.isa_ia[a] + (long)h.na_max * h.isa_is[a]);
+    for (int d = 1; d <= 3; d++) {
+      double sm = h.b_cell[0 + 3 * (d - 1)] * x[0];
+      sm = sm + h.b_cell[1 + 3 * (d - 1)] * x[1];
+      sm = sm + h.b_cell[2 + 3 * (d - 1)] * x[2];
+      arg[3 * a + d - 1] = h.tpiba * sm;
+    }
+  }
+  CK(cudaMemcpyAsync(c->d_atarg, arg.data(), sizeof(double) * arg.size(), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_atco, h.atco.data(), sizeof(double) * h.atco.size(), cudaMemcpyHostToDevice, c->st));
+  AtomArgs aa{c->d_atarg, c->d_isa_is};
+  int nh1 = h.nr[0] / 2 + 1, nh2 = h.nr[1] / 2 + 1, nh3 = h.nr[2] / 2 + 1;
+  k_sfac_sums<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, h.nat, c->d_inyh, nh1, nh2, nh3, aa, c->d_vps, c->d_rhos,
+                                                 c->d_evps, c->d_erhos);
+  if (c->nproj) {
+    ProjArgs pa{c->d_pisa, c->d_pis, c->d_piv, c->d_pl, h.nghmax};
+    k_projectors<<<dim3(nblk(h.ngpw), c->nproj), NTHR, 0, c->st>>>(h.ngpw, c->nproj, c->d_inyh, nh1, nh2, nh3, aa, pa,
+                                                                   c->d_twnl, c->d_P);
+  }
+  k_hess<<<nblk(h.ngpw), NTHR, 0, c->st>>>(h.ngpw, c->d_hg, h.tpiba2, c->d_evps, c->d_twnl, h.nsp, h.nghmax, c->d_na,
+                                           c->d_ngh, c->d_wsg, c->d_vpp);
+  k_esr<<<1, 32, 0, c->st>>>(h.nsp, c->d_na, h.na_max, c->d_zv, c->d_atco, h.alat, h.symmetry, 1, c->d_fsr, c->d_esr);
+  CK(cudaMemcpyAsync(&c->esr, c->d_esr, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaGetLastError());
+  return 0;
+}
+
+// e_sr + POTFOR + NLFOR (wfn_opt when tfor, do_opt.f90:98-106)
+static int do_ionic_forces(amdk_ctx *c) {
+  const HostSetup &h = c->hs;
+  size_t fb = sizeof(double) * 3 * h.na_max * h.nsp;
+  CK(cudaMemcpyAsync(c->d_force, c->d_fsr, fb, cudaMemcpyDeviceToDevice, c->st));
+  const int pnb = 64;
+  AtomArgs aa{c->d_atarg, c->d_isa_is};
+  int nh1 = h.nr[0] / 2 + 1, nh2 = h.nr[1] / 2 + 1, nh3 = h.nr[2] / 2 + 1;
+  double omtp = 2.0 * h.omega * h.tpiba;
+  k_potfor<<<dim3(pnb, h.nat), NTHR, 0, c->st>>>(h.ngrho, c->d_inyh, nh1, nh2, nh3, aa, c->d_hg, c->d_gvec, h.tpiba2,
+                                                 c->d_rhog, c->d_erhos, c->d_vps, c->d_rhos, omtp, c->d_part);
+  if (c->nproj) {
+    k_dproj<<<dim3(nblk(h.ngpw), c->nproj, 3), NTHR, 0, c->st>>>(h.ngpw, c->nproj, c->d_gvec, c->d_P, c->d_Q);
+    const double tfac = 2.0 * h.tpiba, zero = 0.0;
+    int K = 2 * h.ngpw;
+    CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, 3 * c->nproj, c->nstate, K, &tfac, (const double *)c->d_Q, K,
+                   (const double *)c->d_c0, K, &zero, c->d_dfnl, 3 * c->nproj));
+  }
+  k_force_total<<<h.nat, NTHR, 0, c->st>>>(h.nat, c->nproj, c->nstate, c->d_pisa, c->d_hn, c->d_dfnl, c->d_occ, c->d_part,
+                                           pnb, c->d_isa_is, c->d_isa_ia, h.na_max, c->d_force);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+// ------------------------------------------------------------------ setup
+static int build_device(amdk_ctx *c) {
+  HostSetup &h = c->hs;
+  Geom &g = c->geom;
+  g.n1 = h.nr[0];
+  g.n2 = h.nr[1];
+  g.n3 = h.nr[2];
+  g.ngpw = h.ngpw;
+  g.ngrho = h.ngrho;
+  g.nray[0] = h.ngrays;
+  g.nray[1] = h.nhrays;
+  int n1 = g.n1, n2 = g.n2, n3 = g.n3;
+  int nh1 = n1 / 2 + 1, nh2 = n2 / 2 + 1, nh3 = n3 / 2 + 1;
+  // ray coordinates from the reference's ray numbering
+  std::vector<int> ray_ky(h.nhrays), ray_kz(h.nhrays);
+  for (int r = 0; r < h.nhrays; r++) {
+    int m = h.msp[r] - 1;
+    int i = m % h.nrl[1] + 1, j = m / h.nrl[1] + 1;
+    int iy = i - nh2, iz = j - nh3;
+    ray_ky[r] = ((iy % n2) + n2) % n2;
+    ray_kz[r] = ((iz % n3) + n3) % n3;
+  }
+  std::vector<int> gmap((size_t)h.nhrays * n1, 0), posp(h.ngrho), posm(h.ngrho);
+  for (int ig = 0; ig < h.ngrho; ig++) {
+    int i1 = h.inyh[3L * ig], i2 = h.inyh[3L * ig + 1], i3 = h.inyh[3L * ig + 2];
+    int ix = i1 - nh1;
+    int rp = h.xrays[(i2 - 1) + (size_t)h.nrl[1] * (i3 - 1)] - 1;
+    int rm = h.xrays[(-i2 + 2 * nh2 - 1) + (size_t)h.nrl[1] * (-i3 + 2 * nh3 - 1)] - 1;
+    int kxp = ((ix % n1) + n1) % n1, kxm = ((-ix % n1) + n1) % n1;
+    posp[ig] = rp * n1 + kxp;
+    posm[ig] = rm * n1 + kxm;
+    if (ig != 0) gmap[(size_t)posm[ig]] = -(ig + 1);
+    gmap[(size_t)posp[ig]] = ig + 1;
+  }
+  RC(c->up(&c->d_gmap, gmap));
+  RC(c->up(&c->d_posp, posp));
+  RC(c->up(&c->d_posm, posm));
+  for (int S = 0; S < 2; S++) {
+    int R = g.nray[S];
+    std::vector<int> zi_of(n3, -1), zl;
+    for (int r = 0; r < R; r++) zi_of[ray_kz[r]] = 1;
+    for (int kz = 0; kz < n3; kz++)
+      if (zi_of[kz] > 0) {
+        zi_of[kz] = (int)zl.size();
+        zl.push_back(kz);
+      }
+    std::vector<int> ri(zl.size() * (size_t)n2, -1);
+    for (int r = 0; r < R; r++) ri[(size_t)zi_of[ray_kz[r]] * n2 + ray_ky[r]] = r;
+    g.nz[S] = (int)zl.size();
+    RC(c->up(&c->d_zlist[S], zl));
+    RC(c->up(&c->d_rayidx[S], ri));
+    g.zlist[S] = c->d_zlist[S];
+    g.rayidx[S] = c->d_rayidx[S];
+  }
+  g.gmap = c->d_gmap;
+  g.pos_p = c->d_posp;
+  g.pos_m = c->d_posm;
+  for (int d = 0; d < 3; d++) {
+    RC(make_plan<double2>(c, h.nr[d], c->pd[d]));
+    RC(make_plan<float2>(c, h.nr[d], c->pf[d]));
+  }
+  if (n3 * TX > 16 * NTHR) {
+    set_error("grid dimension above 256 is not supported");
+    return AMDK_ERR_UNSUPPORTED;
+  }
+  set_smem_attrs<double2>();
+  set_smem_attrs<float2>();
+  cudaFuncSetAttribute(k_cholesky_upper, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  // G vectors
+  RC(c->up(&c->d_inyh, h.inyh));
+  RC(c->up(&c->d_hg, h.hg));
+  RC(c->up(&c->d_gvec, h.gvec));
+  // electronic state
+  c->nstate = h.nstate;
+  c->npairs = (h.nstate + 1) / 2;
+  size_t cw = (size_t)h.ngpw * h.nstate;
+  RC(c->alloc(&c->d_c0, cw));
+  RC(c->alloc(&c->d_c2, cw));
+  RC(c->alloc(&c->d_cp, cw));
+  RC(c->alloc(&c->d_hnm1, cw));
+  CK(cudaMemset(c->d_c0, 0, cw * sizeof(double2)));
+  RC(c->up(&c->d_occ, h.occ));
+  {
+    // density weights per band pair (density.f90:51-62)
+    std::vector<double> wa(c->npairs), wb(c->npairs);
+    for (int p = 0; p < c->npairs; p++) {
+      wa[p] = h.occ[2 * p] / h.omega;
+      wb[p] = (2 * p + 1 < h.nstate) ? h.occ[2 * p + 1] / h.omega : 0.0;
+    }
+    RC(c->up(&c->d_wa, wa));
+    RC(c->up(&c->d_wb, wb));
+  }
+  long npt = (long)n1 * n2 * n3;
+  RC(c->alloc(&c->d_rho, npt));
+  RC(c->alloc(&c->d_vpot, npt));
+  RC(c->alloc(&c->d_cgrid, 2 * npt));
+  RC(c->alloc(&c->d_rhog, h.ngrho));
+  RC(c->alloc(&c->d_vg, h.ngrho));
+  RC(c->alloc(&c->d_vxg, h.ngrho));
+  RC(c->alloc(&c->d_fp, 2L * h.ngrho));
+  RC(c->alloc(&c->d_fm, 2L * h.ngrho));
+  RC(c->alloc(&c->d_gam, (size_t)h.nstate * h.nstate));
+  RC(c->alloc(&c->d_info, 1));
+  RC(c->alloc(&c->d_part, (size_t)RED_BLOCKS * 4 + 3L * 64 * h.nat + 64));
+  RC(c->alloc(&c->d_scal, S_NSCAL));
+  CK(cudaMemset(c->d_scal, 0, S_NSCAL * sizeof(double)));
+  // FFT buffers: pair batches (working precision) and up to 2 FP64 density fields
+  size_t csz = (c->precision == AMDK_MIXED) ? sizeof(float2) : sizeof(double2);
+  if (c->batch <= 0) c->batch = 8;
+  c->batch = std::max(1, std::min(c->batch, c->npairs));
+  size_t rb = std::max((size_t)c->batch * rstride(c, 0) * csz, 2 * (size_t)rstride(c, 1) * sizeof(double2));
+  size_t sb = std::max((size_t)c->batch * sstride(c, 0) * csz, 2 * (size_t)sstride(c, 1) * sizeof(double2));
+  RC(c->alloc((char **)&c->d_rb, rb));
+  RC(c->alloc((char **)&c->d_sb, sb));
+  c->fftbuf_bytes = rb + sb;
+  // pseudopotential tables on the device
+  RC(c->alloc(&c->d_vps, (size_t)h.nsp * h.ngrho));
+  RC(c->alloc(&c->d_rhos, (size_t)h.nsp * h.ngrho));
+  RC(c->alloc(&c->d_twnl, (size_t)h.nsp * h.nghmax * h.ngpw));
+  CK(cudaMemset(c->d_twnl, 0, sizeof(double) * (size_t)h.nsp * h.nghmax * h.ngpw));
+  {
+    double *xp, *yp, *hh, *sd;
+    std::vector<double> hv, sdd;
+    RC(c->alloc(&xp, NSPLN));
+    RC(c->alloc(&yp, NSPLN));
+    RC(c->alloc(&hh, NSPLN + 1));
+    RC(c->alloc(&sd, NSPLN + 1));
+    double vol = 1.0 / std::sqrt(h.omega);
+    for (int is = 0; is < h.nsp; is++) {
+      spline_coeffs(NSPLN, h.ggnh.data(), h.voo[is].data(), hv, sdd);
+      CK(cudaMemcpy(xp, h.ggnh.data(), sizeof(double) * NSPLN, cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(yp, h.voo[is].data(), sizeof(double) * NSPLN, cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(hh, hv.data(), sizeof(double) * (NSPLN + 1), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(sd, sdd.data(), sizeof(double) * (NSPLN + 1), cudaMemcpyHostToDevice));
+      k_vps_rhos<<<nblk(h.ngrho), NTHR>>>(h.ngrho, c->d_hg, xp, yp, hh, sd, NSPLN, (double)h.zv[is], h.omega, h.tpiba2,
+                                           c->d_vps + (size_t)is * h.ngrho, c->d_rhos + (size_t)is * h.ngrho);
+      CK(cudaDeviceSynchronize());
+      for (int iv = 0; iv < h.ngh[is]; iv++) {
+        const double *w = h.wns[is].data() + (size_t)iv * NSPLN;
+        double xx = 0;
+        for (int k = 0; k < NSPLN; k++) xx += std::fabs(w[k]);
+        if (!(xx > 1e-12)) continue;
+        spline_coeffs(NSPLN, h.ggng.data(), w, hv, sdd);
+        CK(cudaMemcpy(xp, h.ggng.data(), sizeof(double) * NSPLN, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(yp, w, sizeof(double) * NSPLN, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(hh, hv.data(), sizeof(double) * (NSPLN + 1), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(sd, sdd.data(), sizeof(double) * (NSPLN + 1), cudaMemcpyHostToDevice));
+        k_twnl<<<nblk(h.ngpw), NTHR>>>(h.ngpw, c->d_hg, c->d_gvec, xp, yp, hh, sd, NSPLN, h.lpval[is][iv], vol,
+                                        c->d_twnl + ((size_t)is * h.nghmax + iv) * h.ngpw);
+        CK(cudaDeviceSynchronize());
+      }
+    }
+  }
+  RC(c->alloc(&c->d_evps, h.ngrho));
+  RC(c->alloc(&c->d_erhos, h.ngrho));
+  RC(c->alloc(&c->d_vpp, h.ngpw));
+  RC(c->alloc(&c->d_atarg, 3L * h.nat));
+  RC(c->alloc(&c->d_atco, 3L * h.na_max * h.nsp));
+  RC(c->up(&c->d_isa_is, h.isa_is));
+  RC(c->up(&c->d_isa_ia, h.isa_ia));
+  std::vector<int> na(h.na, h.na + h.nsp), ngh(h.ngh, h.ngh + h.nsp), zv(h.zv, h.zv + h.nsp);
+  RC(c->up(&c->d_na, na));
+  RC(c->up(&c->d_ngh, ngh));
+  RC(c->up(&c->d_zv, zv));
+  std::vector<double> wsg((size_t)h.nsp * 120, 0.0);
+  for (int is = 0; is < h.nsp; is++)
+    for (int iv = 0; iv < MAXNGH; iv++) wsg[is * 120 + iv] = h.wsg[is][iv];
+  RC(c->up(&c->d_wsg, wsg));
+  RC(c->alloc(&c->d_force, 3L * h.na_max * h.nsp));
+  RC(c->alloc(&c->d_fsr, 3L * h.na_max * h.nsp));
+  RC(c->alloc(&c->d_esr, 1));
+  // projector list (isa-major within a species, as nl(isa,iv) of fnl)
+  int isa0 = 0;
+  for (int is = 0; is < h.nsp; is++) {
+    for (int iv = 0; iv < h.ngh[is]; iv++)
+      for (int ia = 0; ia < h.na[is]; ia++) {
+        c->p_isa.push_back(isa0 + ia);
+        c->p_is.push_back(is);
+        c->p_iv.push_back(iv);
+        c->p_l.push_back(h.nghtol[is][iv]);
+      }
+    isa0 += h.na[is];
+  }
+  c->nproj = (int)c->p_isa.size();
+  if (c->nproj) {
+    RC(c->up(&c->d_pisa, c->p_isa));
+    RC(c->up(&c->d_pis, c->p_is));
+    RC(c->up(&c->d_piv, c->p_iv));
+    RC(c->up(&c->d_pl, c->p_l));
+    RC(c->alloc(&c->d_P, (size_t)c->nproj * h.ngpw));
+    RC(c->alloc(&c->d_Q, 3 * (size_t)c->nproj * h.ngpw));
+    size_t pn = (size_t)c->nproj * h.nstate;
+    RC(c->alloc(&c->d_nl, pn));
+    RC(c->alloc(&c->d_hn, pn));
+    RC(c->alloc(&c->d_D, pn));
+    RC(c->alloc(&c->d_dfnl, 3 * pn));
+    // H: wsg on the diagonal (psp) or hlsg between projectors of equal l
+    // and m on the same atom (UPF): pseudopotential.f90:56-99
+    std::vector<double> H((size_t)c->nproj * c->nproj, 0.0);
+    for (int a = 0; a < c->nproj; a++)
+      for (int b = 0; b < c->nproj; b++) {
+        if (c->p_isa[a] != c->p_isa[b]) continue;
+        int is = c->p_is[a], iv = c->p_iv[a], jv = c->p_iv[b];
+        if (!h.upf) {
+          if (iv == jv) H[a + (size_t)c->nproj * b] = h.wsg[is][iv];
+        } else if (h.nghtol[is][iv] == h.nghtol[is][jv] && h.lpval[is][iv] == h.lpval[is][jv]) {
+          H[a + (size_t)c->nproj * b] = h.hlsg[is][h.nghtol[is][iv]][h.lfval[is][iv] - 1][h.lfval[is][jv] - 1];
+        }
+      }
+    RC(c->up(&c->d_H, H));
+  }
+  double es = 0.0;
+  for (int is = 0; is < h.nsp; is++) es = es + (double)h.na[is] * h.zv[is] * h.zv[is] / RAGGIO;
+  c->eself = es / std::sqrt(2.0 * (4.0 * std::atan(1.0)));
+  CK(cudaDeviceSynchronize());
+  return 0;
+}
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+const char *amdk_last_error(void) { return g_err.c_str(); }
+
+int amdk_create(const amdk_system *sys, const amdk_options *opt, amdk_ctx **out) {
+  if (!sys || !out) {
+    set_error("amdk_create: null argument");
+    return AMDK_ERR_BADARG;
+  }
+  *out = nullptr;
+  amdk_ctx *c = new amdk_ctx();
+  if (opt) {
+    c->device = opt->device;
+    c->precision = opt->precision;
+    c->batch = opt->pair_batch;
+  }
+  int rc = host_setup(sys, c->hs);
+  if (rc) {
+    delete c;
+    return rc;
+  }
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    delete c;
+    return AMDK_ERR_CUDA;
+  }
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cublasCreate(&c->cb) != CUBLAS_STATUS_SUCCESS || cublasSetStream(c->cb, c->st) != CUBLAS_STATUS_SUCCESS) {
+    set_error("stream / cuBLAS handle creation failed");
+    amdk_destroy(c);
+    return AMDK_ERR_CUDA;
+  }
+  cudaEventCreate(&c->ev0);
+  cudaEventCreate(&c->ev1);
+  rc = build_device(c);
+  if (!rc) rc = do_positions(c, sys->atco);
+  if (rc) {
+    amdk_destroy(c);
+    return rc;
+  }
+  *out = c;
+  return 0;
+}
+
+int amdk_destroy(amdk_ctx *c) {
+  if (!c) return 0;
+  cudaSetDevice(c->device);
+  if (c->st) cudaStreamSynchronize(c->st);
+  for (void *p : c->allocs) cudaFree(p);
+  if (c->cb) cublasDestroy(c->cb);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return 0;
+}
+
+int amdk_info_get(amdk_ctx *c, amdk_info *info) {
+  if (!c || !info) return AMDK_ERR_BADARG;
+  const HostSetup &h = c->hs;
+  for (int d = 0; d < 3; d++) info->nr[d] = h.nr[d];
+  info->ngpw = h.ngpw;
+  info->ngrho = h.ngrho;
+  info->ngrays = h.ngrays;
+  info->nhrays = h.nhrays;
+  info->nstate = h.nstate;
+  info->nat = h.nat;
+  info->nghmax = h.nghmax;
+  info->omega = h.omega;
+  return 0;
+}
+
+int amdk_get_gvectors(amdk_ctx *c, int *inyh, double *hg, double *gvec, int *map_p, int *map_m) {
+  if (!c) return AMDK_ERR_BADARG;
+  const HostSetup &h = c->hs;
+  if (inyh) std::memcpy(inyh, h.inyh.data(), sizeof(int) * h.inyh.size());
+  if (hg) std::memcpy(hg, h.hg.data(), sizeof(double) * h.hg.size());
+  if (gvec) std::memcpy(gvec, h.gvec.data(), sizeof(double) * h.gvec.size());
+  if (map_p) std::memcpy(map_p, h.mapp.data(), sizeof(int) * h.mapp.size());
+  if (map_m) std::memcpy(map_m, h.mapm.data(), sizeof(int) * h.mapm.size());
+  return 0;
+}
+
+int amdk_host_gvectors(const amdk_system *sys, amdk_info *info, int *inyh, double *hg, double *gvec, int *map_p,
+                       int *map_m) {
+  if (!sys || !info) {
+    set_error("amdk_host_gvectors: null argument");
+    return AMDK_ERR_BADARG;
+  }
+  HostSetup h;
+  int rc = host_setup(sys, h, true);
+  if (rc) return rc;
+  std::memset(info, 0, sizeof(*info));
+  for (int d = 0; d < 3; d++) info->nr[d] = h.nr[d];
+  info->ngpw = h.ngpw;
+  info->ngrho = h.ngrho;
+  info->ngrays = h.ngrays;
+  info->nhrays = h.nhrays;
+  info->nat = h.nat;
+  info->omega = h.omega;
+  if (inyh) std::memcpy(inyh, h.inyh.data(), sizeof(int) * h.inyh.size());
+  if (hg) std::memcpy(hg, h.hg.data(), sizeof(double) * h.hg.size());
+  if (gvec) std::memcpy(gvec, h.gvec.data(), sizeof(double) * h.gvec.size());
+  if (map_p) std::memcpy(map_p, h.mapp.data(), sizeof(int) * h.mapp.size());
+  if (map_m) std::memcpy(map_m, h.mapm.data(), sizeof(int) * h.mapm.size());
+  return 0;
+}
+
+int amdk_set_positions(amdk_ctx *c, const double *atco) {
+  if (!c || !atco) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  return do_positions(c, atco);
+}
+
+int amdk_set_wfn(amdk_ctx *c, const double *c0) {
+  if (!c || !c0) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  CK(cudaMemcpy(c->d_c0, c0, sizeof(double2) * (size_t)c->hs.ngpw * c->nstate, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int amdk_get_wfn(amdk_ctx *c, double *c0) {
+  if (!c || !c0) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaMemcpy(c0, c->d_c0, sizeof(double2) * (size_t)c->hs.ngpw * c->nstate, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int amdk_ortho(amdk_ctx *c) {
+  if (!c) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  return do_ortho(c);
+}
+int amdk_density(amdk_ctx *c) {
+  if (!c) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  return do_density(c);
+}
+int amdk_potential(amdk_ctx *c) {
+  if (!c) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  return do_potential(c);
+}
+int amdk_energy(amdk_ctx *c, amdk_energies *e) {
+  if (!c) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  return do_energy(c, e);
+}
+int amdk_apply_h(amdk_ctx *c) {
+  if (!c) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  CK(cudaMemsetAsync(c->d_c2, 0, sizeof(double2) * (size_t)c->hs.ngpw * c->nstate, c->st));
+  return do_apply_h(c);
+}
+int amdk_gradient(amdk_ctx *c, double *gemax) {
+  if (!c) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  RC(do_gradient(c));
+  if (gemax) {
+    CK(cudaMemcpyAsync(gemax, c->d_scal + S_GMAX, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  return 0;
+}
+int amdk_pcg(amdk_ctx *c, int istep) {
+  if (!c || istep < 1) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  return do_pcg(c, istep);
+}
+
+int amdk_scf_iteration(amdk_ctx *c, int istep, double gcut, amdk_energies *e, double *gemax, int *converged) {
+  if (!c || istep < 1) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  cudaEventRecord(c->ev0, c->st);
+  RC(do_density(c));
+  RC(do_potential(c));
+  amdk_energies en;
+  RC(do_energy(c, &en));
+  CK(cudaMemsetAsync(c->d_c2, 0, sizeof(double2) * (size_t)c->hs.ngpw * c->nstate, c->st));
+  RC(do_apply_h(c));
+  RC(do_gradient(c));
+  double gm = 0;
+  CK(cudaMemcpyAsync(&gm, c->d_scal + S_GMAX, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (!std::isfinite(gm)) {
+    set_error("non-finite wavefunction gradient");
+    return AMDK_ERR_NONFINITE;
+  }
+  // CHK_TFOR (gradient.f90:113-136)
+  if (istep == 1) c->tfor = false;
+  else if (gm < 3 * gcut) c->tfor = true;
+  if (c->tfor) RC(do_ionic_forces(c));
+  RC(do_pcg(c, istep));
+  RC(do_ortho(c));
+  cudaEventRecord(c->ev1, c->st);
+  CK(cudaEventSynchronize(c->ev1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  c->last_ms = ms;
+  if (e) *e = en;
+  if (gemax) *gemax = gm;
+  if (converged) *converged = gm < gcut;
+  return 0;
+}
+
+int amdk_ionic_forces(amdk_ctx *c, double *force) {
+  if (!c || !force) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  if (!c->tfor) {
+    // make sure nl/hn are for the current C0 (pp_energy) before NLFOR
+    RC(do_fnl(c));
+  }
+  RC(do_ionic_forces(c));
+  CK(cudaMemcpyAsync(force, c->d_force, sizeof(double) * 3 * c->hs.na_max * c->hs.nsp, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int amdk_get_array(amdk_ctx *c, const char *name, void *dst, size_t bytes) {
+  if (!c || !name || !dst) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  const HostSetup &h = c->hs;
+  long npt = (long)h.nr[0] * h.nr[1] * h.nr[2];
+  const void *src = nullptr;
+  size_t n = 0;
+  std::string k(name);
+  if (k == "rho") { src = c->d_rho; n = npt * sizeof(double); }
+  else if (k == "v_pot") { src = c->d_vpot; n = npt * sizeof(double); }
+  else if (k == "rho_g") { src = c->d_rhog; n = h.ngrho * sizeof(double2); }
+  else if (k == "c2") { src = c->d_c2; n = (size_t)h.ngpw * c->nstate * sizeof(double2); }
+  else if (k == "c0") { src = c->d_c0; n = (size_t)h.ngpw * c->nstate * sizeof(double2); }
+  else if (k == "nl") { src = c->d_nl; n = (size_t)c->nproj * c->nstate * sizeof(double); }
+  else if (k == "vps") { src = c->d_vps; n = (size_t)h.nsp * h.ngrho * sizeof(double); }
+  else if (k == "rhos") { src = c->d_rhos; n = (size_t)h.nsp * h.ngrho * sizeof(double); }
+  else if (k == "twnl") { src = c->d_twnl; n = (size_t)h.nsp * h.nghmax * h.ngpw * sizeof(double); }
+  else if (k == "eigrxvps") { src = c->d_evps; n = h.ngrho * sizeof(double2); }
+  else if (k == "eigrxrhos") { src = c->d_erhos; n = h.ngrho * sizeof(double2); }
+  else if (k == "vpp") { src = c->d_vpp; n = h.ngpw * sizeof(double); }
+  else if (k == "force") { src = c->d_force; n = 3 * h.na_max * h.nsp * sizeof(double); }
+  else {
+    set_error("amdk_get_array: unknown array " + k);
+    return AMDK_ERR_BADARG;
+  }
+  if (bytes < n) {
+    set_error("amdk_get_array: destination too small for " + k);
+    return AMDK_ERR_BADARG;
+  }
+  CK(cudaStreamSynchronize(c->st));
+  if (n && src) CK(cudaMemcpy(dst, src, n, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int amdk_fft_sphere(amdk_ctx *c, int sign, double *coef, double *grid) {
+  if (!c || !coef || !grid || (sign != 1 && sign != -1)) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  const HostSetup &h = c->hs;
+  long npt = (long)h.nr[0] * h.nr[1] * h.nr[2];
+  if (sign == -1) {
+    CK(cudaMemcpyAsync(c->d_vxg, coef, sizeof(double2) * h.ngrho, cudaMemcpyHostToDevice, c->st));
+    k_conj_field<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_vxg, c->d_fm);
+    RC(field_to_grid(c, 1, c->d_vxg, c->d_fm, c->d_cgrid));
+    CK(cudaMemcpyAsync(grid, c->d_cgrid, sizeof(double2) * npt, cudaMemcpyDeviceToHost, c->st));
+  } else {
+    CK(cudaMemcpyAsync(c->d_cgrid, grid, sizeof(double2) * npt, cudaMemcpyHostToDevice, c->st));
+    RC(grid_to_rays(c, 1, c->d_cgrid, nullptr));
+    k_gather_p<double2><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_posp, (double2 *)c->d_rb, 1.0 / (double)npt,
+                                                           c->d_vxg);
+    CK(cudaMemcpyAsync(coef, c->d_vxg, sizeof(double2) * h.ngrho, cudaMemcpyDeviceToHost, c->st));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int amdk_last_iteration_ms(amdk_ctx *c, double *ms) {
+  if (!c || !ms) return AMDK_ERR_BADARG;
+  *ms = c->last_ms;
+  return 0;
+}
+
+}  // extern "C"

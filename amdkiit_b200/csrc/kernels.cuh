@@ -1,0 +1,692 @@
+// Non-FFT kernels of libamdk (FP64 unless stated).  Each kernel names the
+// reference routine it implements (paths relative to the AMDKIIT project root).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "fft.cuh"
+
+namespace amdk {
+
+constexpr int RED_BLOCKS = 296;   // 2 x 148 SMs for grid-stride reductions
+constexpr int NTHR = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+// block sum in fixed order (deterministic for a fixed launch shape)
+__device__ double block_sum(double v, double *sh) {
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) r += sh[i];
+  return r;  // valid in thread 0
+}
+__device__ double block_max(double v, double *sh) {
+  v = warp_max(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double r = -1.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) r = fmax(r, sh[i]);
+  return r;
+}
+// sum partials[k*nb .. k*nb+nb) -> out[k], for k < nk (one block per k)
+__global__ void k_finish_sum(const double *part, int nb, double *out, int nk) {
+  __shared__ double sh[32];
+  const int k = blockIdx.x;
+  double v = 0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) v += part[(long)k * nb + i];
+  double r = block_sum(v, sh);
+  if (threadIdx.x == 0 && k < nk) out[k] = r;
+}
+
+// ---------------------------------------------------------------- tables
+// spline_inter (spline_inter.f90:1-36) evaluated at one point; the hunt is
+// spline_hunt's linear search done by bisection (same interval).  Points
+// beyond the last abscissa return 0, as the reference leaves them unset.
+__device__ double spline_at(const double *xp, const double *yp, const double *h, const double *sdd, int n, double x) {
+  if (x > xp[n - 1]) return 0.0;
+  int ig;
+  if (!(x < xp[n - 1])) ig = 1;
+  else {
+    int lo = 2, hi = n;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (x < xp[mid - 1]) hi = mid;
+      else lo = mid + 1;
+    }
+    ig = lo - 1;
+  }
+  const double *X = xp - 1, *Y = yp - 1;
+  double d1 = x - X[ig], d2 = X[ig + 1] - x;
+  double t1 = sdd[ig + 1] / 6.0 / h[ig] * (d1 * d1 * d1);
+  double t2 = sdd[ig] / 6.0 / h[ig] * (d2 * d2 * d2);
+  double t3 = (Y[ig + 1] / h[ig] - sdd[ig + 1] / 6.0 * h[ig]) * d1;
+  double t4 = (Y[ig] / h[ig] - h[ig] / 6.0 * sdd[ig]) * d2;
+  return t1 + t2 + t3 + t4;
+}
+
+// compute_yL (spherical_func.f90:158-206), real harmonics S,PX,PZ,PY,D...
+__device__ double ylm_dev(int L, double hg, const double *g) {
+  const double fp = 16.0 * atan(1.0);
+  if (fabs(hg) >= 1e-6) {
+    switch (L) {
+      case 1: return sqrt(1.0 / fp);
+      case 2: return sqrt(3.0 / fp) * g[0] / sqrt(hg);
+      case 3: return sqrt(3.0 / fp) * g[2] / sqrt(hg);
+      case 4: return sqrt(3.0 / fp) * g[1] / sqrt(hg);
+      case 5: return sqrt(15.0 / fp) * g[0] * g[1] / hg;
+      case 6: return sqrt(15.0 / fp) * g[0] * g[2] / hg;
+      case 7: return sqrt(5.0 / fp / 4.0) * (3.0 * (g[2] * g[2]) / hg - 1.0);
+      case 8: return sqrt(15.0 / fp) * g[1] * g[2] / hg;
+      case 9: return sqrt(15.0 / fp / 4.0) * (g[0] * g[0] - g[1] * g[1]) / hg;
+      default: return 0.0;
+    }
+  }
+  return L == 1 ? sqrt(1.0 / fp) : 0.0;
+}
+
+// vps (form_factor*, exp_igr.f90:190-206,273-285) and rhos per species and G
+__global__ void k_vps_rhos(int ngrho, const double *hg, const double *xp, const double *voo, const double *h,
+                           const double *sdd, int n, double zv, double omega, double tpiba2, double *vps, double *rhos) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngrho) return;
+  double x = hg[g];
+  vps[g] = (1.0 / omega) * spline_at(xp, voo, h, sdd, n, x);
+  if (g == 0) rhos[g] = -zv * (1.0 / omega);
+  else rhos[g] = -zv * exp(-(0.25 * (1.2 * 1.2) * x * tpiba2)) * (1.0 / omega);
+}
+
+// twnl (nlpro, pseudopotential.f90:108-162 / upf_nlpro :293-354)
+__global__ void k_twnl(int ngpw, const double *hg, const double *gvec, const double *xp, const double *wns,
+                       const double *h, const double *sdd, int n, int lp, double vol, double *tw) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngpw) return;
+  double x = hg[g];
+  tw[g] = ylm_dev(lp, x, gvec + 3L * g) * vol * spline_at(xp, wns, h, sdd, n, x);
+}
+
+// ---------------------------------------------------------------- geometry
+// exp_igrxfactor (exp_igr.f90:4-140): S_I(G) = exp(-i G.R_I).  The phase is
+// evaluated directly as sum_d n_d * arg_d (arg_d = tpiba b_d.R_I) instead of
+// the reference's recursive products of 1D phases.
+struct AtomArgs {
+  const double *arg;   // [nat*3]
+  const int *is;       // [nat]
+};
+__device__ __forceinline__ double2 eig_at(const int *inyh, int g, int nh1, int nh2, int nh3, const double *arg3) {
+  double ph = (double)(inyh[3 * g] - nh1) * arg3[0] + (double)(inyh[3 * g + 1] - nh2) * arg3[1] +
+              (double)(inyh[3 * g + 2] - nh3) * arg3[2];
+  double s, c;
+  sincos(ph, &s, &c);
+  return make_double2(c, -s);
+}
+// eigrxvps(G) = sum_I S_I vps, eigrxrhos(G) = sum_I S_I rhos  (exp_igr.f90:130-136)
+__global__ void k_sfac_sums(int ngrho, int nat, const int *inyh, int nh1, int nh2, int nh3, AtomArgs aa,
+                            const double *vps, const double *rhos, double2 *evps, double2 *erhos) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngrho) return;
+  double2 v = make_double2(0, 0), r = make_double2(0, 0);
+  for (int a = 0; a < nat; ++a) {
+    double2 e = eig_at(inyh, g, nh1, nh2, nh3, aa.arg + 3 * a);
+    int is = aa.is[a];
+    double pv = vps[(long)is * ngrho + g], pr = rhos[(long)is * ngrho + g];
+    v.x += e.x * pv; v.y += e.y * pv;
+    r.x += pr * e.x; r.y += pr * e.y;
+  }
+  evps[g] = v;
+  erhos[g] = r;
+}
+// Projector matrix P_j(G) = (-i)^l twnl(G) S_I(G), G=0 entry halved
+// (the scr arrays of fnl, pseudopotential.f90:179-209).
+struct ProjArgs {
+  const int *isa, *is, *iv, *l;   // [nproj]
+  int nghmax;
+};
+__global__ void k_projectors(int ngpw, int nproj, const int *inyh, int nh1, int nh2, int nh3, AtomArgs aa, ProjArgs pa,
+                             const double *twnl, double2 *P) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  if (g >= ngpw || j >= nproj) return;
+  int isa = pa.isa[j];
+  double2 e = eig_at(inyh, g, nh1, nh2, nh3, aa.arg + 3 * isa);
+  double t = twnl[((long)pa.is[j] * pa.nghmax + pa.iv[j]) * ngpw + g];
+  if (g == 0) t *= 0.5;
+  double2 v;
+  switch (pa.l[j] & 3) {
+    case 0: v = make_double2(t * e.x, t * e.y); break;
+    case 1: v = make_double2(t * e.y, -t * e.x); break;   // -i
+    case 2: v = make_double2(-t * e.x, -t * e.y); break;
+    default: v = make_double2(-t * e.y, t * e.x); break;  // +i
+  }
+  P[(long)j * ngpw + g] = v;
+}
+// hess (cg.f90:141-199): K(G) = 1/max(1/2 |G|^2 + V_loc(0) + sum n_s w twnl^2, 0.5)
+__global__ void k_hess(int ngpw, const double *hg, double tpiba2, const double2 *evps, const double *twnl, int nsp,
+                       int nghmax, const int *na, const int *ngh, const double *wsg, double *vpp) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngpw) return;
+  double v = evps[0].x;
+  for (int is = 0; is < nsp; ++is)
+    for (int iv = 0; iv < ngh[is]; ++iv) {
+      double t = twnl[((long)is * nghmax + iv) * ngpw + g];
+      v = v + na[is] * wsg[is * 120 + iv] * t * t;
+    }
+  v = 0.5 * tpiba2 * hg[g] + v;
+  if (v < 0.5) v = 0.5;
+  vpp[g] = 1.0 / v;
+}
+
+// ---------------------------------------------------------------- G-space
+// ray buffer (forward X done) -> F(+G)/N   (rhor2g, density.f90:143-145)
+template <typename C>
+__global__ void k_gather_p(int ng, const int *pos_p, const C *rb, double scale, double2 *out) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ng) return;
+  C v = rb[pos_p[g]];
+  out[g] = make_double2((double)v.x * scale, (double)v.y * scale);
+}
+
+// eval_pot (potential.f90:4-46) in G space + e_hartree / pp_energy E_loc
+// partial sums: part[0*nb+b] = Re sum 4pi/G^2 |rho+rho_ion|^2,
+// part[1*nb+b] = Re sum eigrxvps conj(rho) (G=0 weighted 1/2).
+__global__ void k_vloc_g(int ngrho, const double *hg, double tpiba2, const double2 *rhog, const double2 *erhos,
+                         const double2 *evps, double2 *vg, double *part) {
+  __shared__ double sh[32];
+  const double fp = 16.0 * atan(1.0);
+  double eh = 0, el = 0;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngrho; g += gridDim.x * blockDim.x) {
+    double2 rg = rhog[g], e = evps[g];
+    if (g == 0) {
+      vg[0] = make_double2(0.0, 0.0);
+      el += 0.5 * (e.x * rg.x + e.y * rg.y);
+    } else {
+      double f = fp / (tpiba2 * hg[g]);
+      double2 r = make_double2(rg.x + erhos[g].x, rg.y + erhos[g].y);
+      vg[g] = make_double2(f * r.x + e.x, f * r.y + e.y);
+      eh += f * (r.x * r.x + r.y * r.y);
+      el += e.x * rg.x + e.y * rg.y;
+    }
+  }
+  double a = block_sum(eh, sh);
+  double b = block_sum(el, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = a;
+    part[gridDim.x + blockIdx.x] = b;
+  }
+}
+
+// GRAD_CAL fields (xc.f90:471-487): t=0: rho + i d_x rho, t=1: d_y rho + i d_z rho
+__global__ void k_grad_fields(int ngrho, const double *gvec, double tpiba, const double2 *rhog, double2 *fp, double2 *fm) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngrho) return;
+  double2 r = rhog[g];
+  double gx = tpiba * gvec[3 * g], gy = gvec[3 * g + 1], gz = gvec[3 * g + 2];
+  fp[g] = make_double2(r.x - gx * r.x, r.y - gx * r.y);
+  fm[g] = make_double2(r.x + gx * r.x, -(r.y + gx * r.y));
+  // tpiba (i gy - gz) r  and tpiba (-i gy + gz) conj(r)
+  double ax = -tpiba * gz, ay = tpiba * gy;
+  fp[ngrho + g] = make_double2(ax * r.x - ay * r.y, ax * r.y + ay * r.x);
+  double bx = tpiba * gz, by = -tpiba * gy;
+  fm[ngrho + g] = make_double2(bx * r.x + by * r.y, by * r.x - bx * r.y);
+}
+__global__ void k_conj_field(int ng, const double2 *fp, double2 *fm) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ng) return;
+  fm[g] = make_double2(fp[g].x, -fp[g].y);
+}
+
+// ---------------------------------------------------------------- XC
+__device__ void xc_teter93(double rho, double &e, double &v) {
+  const double a0 = 0.4581652932831429, a1 = 2.217058676663745, a2 = 0.7405551735357053, a3 = 0.01968227878617998;
+  const double b1 = 1.0, b2 = 4.504130959426697, b3 = 1.110667363742916, b4 = 0.02359291751427506;
+  const double fp = 16.0 * atan(1.0);
+  double rs = cbrt(3.0 / (fp * rho));
+  double num = a0 + rs * (a1 + rs * (a2 + rs * a3));
+  double den = rs * (b1 + rs * (b2 + rs * (b3 + rs * b4)));
+  double dnum = a1 + rs * (2.0 * a2 + rs * 3.0 * a3);
+  double dden = b1 + rs * (2.0 * b2 + rs * (3.0 * b3 + rs * 4.0 * b4));
+  double eps = -num / den;
+  double deps = -(dnum * den - num * dden) / (den * den);
+  e = rho * eps;
+  v = eps - rs / 3.0 * deps;
+}
+__device__ void xc_pz(double rho, double &e, double &v) {
+  const double pi = 4.0 * atan(1.0), fp = 16.0 * atan(1.0);
+  double ex = -0.75 * cbrt(3.0 / pi) * cbrt(rho);
+  double rs = cbrt(3.0 / (fp * rho)), eps, deps;
+  if (rs >= 1.0) {
+    const double gg = -0.1423, b1 = 1.0529, b2 = 0.3334;
+    double sq = sqrt(rs), den = 1.0 + b1 * sq + b2 * rs;
+    eps = gg / den;
+    deps = -gg * (0.5 * b1 / sq + b2) / (den * den);
+  } else {
+    const double A = 0.0311, B = -0.048, Cc = 0.0020, D = -0.0116;
+    double lr = log(rs);
+    eps = A * lr + B + Cc * rs * lr + D * rs;
+    deps = A / rs + Cc * lr + Cc + D;
+  }
+  e = rho * ex + rho * eps;
+  v = 4.0 / 3.0 * ex + (eps - rs / 3.0 * deps);
+}
+__device__ void xc_pbe(double rho, double sigma, double &e, double &v, double &vs) {
+  const double pi = 4.0 * atan(1.0), fp = 16.0 * atan(1.0);
+  const double kappa = 0.804, mu = 0.2195149727645171, beta = 0.06672455060314922;
+  const double gamma = (1.0 - log(2.0)) / (pi * pi);
+  double kf = cbrt(3.0 * pi * pi * rho);
+  double exu = -3.0 / fp * kf * rho;
+  double s2 = sigma / (4.0 * kf * kf * rho * rho);
+  double den = 1.0 + mu * s2 / kappa;
+  double Fx = 1.0 + kappa - kappa / den, dF = mu / (den * den);
+  double ex = exu * Fx;
+  double vx = 4.0 / 3.0 * exu / rho * Fx + exu * dF * (-8.0 / 3.0 * s2 / rho);
+  double vsx = exu * dF / (4.0 * kf * kf * rho * rho);
+  double rs = cbrt(3.0 / (fp * rho));
+  const double A = 0.0310907, a1 = 0.21370, b1 = 7.5957, b2 = 3.5876, b3 = 1.6382, b4 = 0.49294;
+  double sq = sqrt(rs);
+  double q = 2.0 * A * (b1 * sq + b2 * rs + b3 * rs * sq + b4 * rs * rs);
+  double dq = 2.0 * A * (0.5 * b1 / sq + b2 + 1.5 * b3 * sq + 2.0 * b4 * rs);
+  double L = log(1.0 + 1.0 / q), dL = -dq / (q * q + q);
+  double ec = -2.0 * A * (1.0 + a1 * rs) * L;
+  double dec = -2.0 * A * a1 * L - 2.0 * A * (1.0 + a1 * rs) * dL;
+  double t2 = pi * sigma / (16.0 * kf * rho * rho);
+  double bg = beta / gamma, E = exp(-ec / gamma), AA = bg / (E - 1.0);
+  double At2 = AA * t2, num = 1.0 + At2, dd = 1.0 + At2 + At2 * At2;
+  double Q = t2 * num / dd;
+  double H = gamma * log(1.0 + bg * Q);
+  double dHdQ = beta / (1.0 + bg * Q);
+  double dQdt2 = (num + t2 * AA) / dd - t2 * num * (AA + 2.0 * AA * AA * t2) / (dd * dd);
+  double dQdA = (t2 * t2) / dd - t2 * num * (t2 + 2.0 * AA * t2 * t2) / (dd * dd);
+  double dAdec = bg * E / (gamma * (E - 1.0) * (E - 1.0));
+  double decdrho = dec * (-rs / (3.0 * rho));
+  double dt2drho = -7.0 / 3.0 * t2 / rho;
+  double vc = ec + H + rho * (decdrho + dHdQ * dQdA * dAdec * decdrho + dHdQ * dQdt2 * dt2drho);
+  double vsc = rho * dHdQ * dQdt2 * pi / (16.0 * kf * rho * rho);
+  e = ex + rho * (ec + H);
+  v = vx + vc;
+  vs = vsx + vsc;
+}
+
+// cal_vpot_ex pointwise part (xc.f90:66-131): smoothing below 4e-8, etxc
+// partial sums, and the two complex fields for the G-space assembly:
+// g0 <- v1 + i v2 d_x rho, g1 <- v2 d_y rho + i v2 d_z rho  (xc.f90:262-279)
+__global__ void k_xc(long npt, int xc, const double *rho, double2 *g0, double2 *g1, double *part) {
+  __shared__ double sh[32];
+  const double gc = 1.0e-8;
+  double sm = 0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < npt; i += (long)gridDim.x * blockDim.x) {
+    double r = rho[i];
+    double sigma = 0, dx = 0, dy = 0, dz = 0;
+    if (xc == 2) {
+      double2 a = g0[i], b = g1[i];
+      dx = a.y; dy = b.x; dz = b.y;
+      sigma = dx * dx + (dy * dy + dz * dz);
+    }
+    double e = 0, v = 0, vs = 0;
+    if (r > 1e-30) {
+      if (xc == 0) xc_teter93(r, e, v);
+      else if (xc == 1) xc_pz(r, e, v);
+      else xc_pbe(r, sigma, e, v, vs);
+    }
+    double rt = r > 0.0 ? r : 0.0, v1 = 0, v2 = 0;
+    if (rt > 0.1 * gc) {
+      double smoo, dsmoo;
+      if (rt > 4.0 * gc) { smoo = 1.0; dsmoo = 0.0; }
+      else {
+        double texp = exp(3.0 * (1.0 - rt / gc));
+        smoo = 1.0 / (1.0 + texp);
+        dsmoo = 3.0 / gc * texp * smoo * smoo;
+      }
+      sm += smoo * e;
+      v1 = dsmoo * e + smoo * v;
+      v2 = smoo * (2.0 * vs);
+    }
+    g0[i] = make_double2(v1, v2 * dx);
+    if (xc == 2) g1[i] = make_double2(v2 * dy, v2 * dz);
+  }
+  double s = block_sum(sm, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// G-space assembly of the XC potential (xc.f90:257-297): from the forward
+// transforms of g0 (and g1 for GGA) in the ray buffer (t stride) build
+// vpotg = V_H+V_loc + v1(G) - i G.(v2 grad rho)(G)
+template <typename C>
+__global__ void k_xc_combine(int ngrho, int gga, const int *pos_p, const int *pos_m, const C *rb, long rstride, double scale,
+                             const double *gvec, double tpiba, const double2 *vg, double2 *vout) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngrho) return;
+  double2 acc = vg[g];
+  for (int t = 0; t < (gga ? 2 : 1); ++t) {
+    C p = rb[t * rstride + pos_p[g]], m = rb[t * rstride + pos_m[g]];
+    double fax = ((double)p.x + (double)m.x) * scale, fay = ((double)p.y + (double)m.y) * scale;
+    double fbx = ((double)p.x - (double)m.x) * scale, fby = ((double)p.y - (double)m.y) * scale;
+    double2 vg1 = make_double2(0.5 * fax, 0.5 * fby), vg2 = make_double2(0.5 * fay, -0.5 * fbx);
+    if (t == 0) {
+      double vf = tpiba * gvec[3 * g];
+      acc.x = acc.x + vg1.x + vf * vg2.y;
+      acc.y = acc.y + vg1.y - vf * vg2.x;
+    } else {
+      double v2 = tpiba * gvec[3 * g + 1], v3 = tpiba * gvec[3 * g + 2];
+      acc.x = acc.x + v2 * vg1.y + v3 * vg2.y;
+      acc.y = acc.y - v2 * vg1.x - v3 * vg2.x;
+    }
+  }
+  vout[g] = acc;
+}
+
+// ---------------------------------------------------------------- vpsi unpack
+// (wfn_initialize.f90:342-361): FP = F(G)+F(-G), FM = F(G)-F(-G);
+// C2_a = -f_a/2 (tpiba2 hg c_a + (Re FP, Im FM)), C2_b = -f_b/2 (... + (Im FP, -Re FM))
+template <typename C>
+__global__ void k_unpack_vpsi(int ngpw, int nstate, int band0, int T, const int *pos_p, const int *pos_m, const C *rb,
+                              long rstride, double scale, const double *hg, double tpiba2, const double *occ,
+                              const double2 *c0, double2 *c2) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  int t = blockIdx.y;
+  if (g >= ngpw || t >= T) return;
+  const C *R = rb + (long)t * rstride;
+  C pp = R[pos_p[g]], pm = R[pos_m[g]];
+  double fpx = ((double)pp.x + (double)pm.x) * scale, fpy = ((double)pp.y + (double)pm.y) * scale;
+  double fmx = ((double)pp.x - (double)pm.x) * scale, fmy = ((double)pp.y - (double)pm.y) * scale;
+  double kin = tpiba2 * hg[g];
+  int ba = band0 + 2 * t, bb = ba + 1;
+  double fi = occ[ba] * 0.5;
+  if (fi == 0.0) fi = 1.0;
+  double2 ca = c0[(long)ba * ngpw + g];
+  c2[(long)ba * ngpw + g] = make_double2(-fi * (kin * ca.x + fpx), -fi * (kin * ca.y + fmy));
+  if (bb < nstate) {
+    double fb = occ[bb] * 0.5;
+    if (fb == 0.0) fb = 1.0;
+    double2 cb = c0[(long)bb * ngpw + g];
+    c2[(long)bb * ngpw + g] = make_double2(-fb * (kin * cb.x + fpy), -fb * (kin * cb.y - fmx));
+  }
+}
+
+// ---------------------------------------------------------------- bands
+// E_kin partial sums (total_energy.f90:38-61)
+__global__ void k_ekin(int ngpw, int nstate, const double2 *c0, const double *hg, const double *occ, double *part) {
+  __shared__ double sh[32];
+  double s = 0;
+  long tot = (long)ngpw * nstate;
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < tot; k += (long)gridDim.x * blockDim.x) {
+    int b = (int)(k / ngpw), g = (int)(k % ngpw);
+    double2 c = c0[k];
+    s += occ[b] * hg[g] * (c.x * c.x + c.y * c.y);
+  }
+  double r = block_sum(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = r;
+}
+// rank-1 G=0 correction and occupation mask of OVLAP_D / ortho_gs DGER
+// (wfn_initialize.f90:257,482): A(i,j) -= Re a_i(0) Re b_j(0); mask fsc
+__global__ void k_g0_correct(int n, int ngpw, const double2 *a, const double2 *b, double *A, const double *occ, int mask,
+                             int upper_only) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= n || j >= n) return;
+  if (upper_only && i > j) return;
+  double v = A[i + (long)n * j] - a[(long)i * ngpw].x * b[(long)j * ngpw].x;
+  if (mask) v *= (occ[i] == 0.0 ? 0.0 : 1.0) * (occ[j] == 0.0 ? 0.0 : 1.0);
+  A[i + (long)n * j] = v;
+}
+// ZCLEAN (wfn_initialize.f90:531-558)
+__global__ void k_zclean(int n, int ngpw, double2 *c) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) c[(long)i * ngpw].y = 0.0;
+}
+// eval_GMAX (gradient.f90:36-61): max |C2| over occupied bands
+__global__ void k_gmax(long tot, const double2 *c2, double *part) {
+  __shared__ double sh[32];
+  double m = -1.0;
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < tot; k += (long)gridDim.x * blockDim.x)
+    m = fmax(m, hypot(c2[k].x, c2[k].y));
+  double r = block_max(m, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = r;
+}
+__global__ void k_finish_max(const double *part, int nb, double *out) {
+  __shared__ double sh[32];
+  double m = -1.0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) m = fmax(m, part[i]);
+  double r = block_max(m, sh);
+  if (threadIdx.x == 0) *out = r;
+}
+
+// PRECON + GGNORM (cg.f90:239-245, 419-449): cp = fi K c2; partial DOTP sums
+__global__ void k_precon(int ngpw, int nstate, int nocc, const double *vpp, const double *occ, const double2 *c2,
+                         double2 *cp, double *part) {
+  __shared__ double sh[32];
+  double s = 0;
+  long tot = (long)ngpw * nstate;
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < tot; k += (long)gridDim.x * blockDim.x) {
+    int b = (int)(k / ngpw), g = (int)(k % ngpw);
+    double fi = occ[b] > 0.01 ? 1.0 / occ[b] : 1.0;
+    double f = fi * vpp[g];
+    double2 v = make_double2(f * c2[k].x, f * c2[k].y);
+    cp[k] = v;
+    if (b < nocc) s += (g == 0) ? v.x * v.x : 2.0 * (v.x * v.x + v.y * v.y);
+  }
+  double r = block_sum(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = r;
+}
+// PCG direction and step (cg.f90:247-281); scal[0] = ggnorm (new),
+// scal[1] = previous ggnorm; gamma = forget * new/prev
+__global__ void k_pcg_update(long tot, int istep, const double *scal, double2 *cp, double2 *hnm1, double2 *c0) {
+  double forget = istep <= 10 ? 0.60 : (istep <= 20 ? 0.91 : 0.95);
+  double gamma = (istep == 1) ? 0.0 : forget * (scal[0] / scal[1]);
+  const double dt = 5.0 * 5.0 / 400.0;
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < tot; k += (long)gridDim.x * blockDim.x) {
+    double2 d = cp[k];
+    if (istep > 1) {
+      d.x += gamma * hnm1[k].x;
+      d.y += gamma * hnm1[k].y;
+    }
+    hnm1[k] = d;
+    c0[k].x += dt * d.x;
+    c0[k].y += dt * d.y;
+  }
+}
+__global__ void k_copy_scalar(const double *src, double *dst) { *dst = *src; }
+
+// Cholesky S = U^T U of the upper triangle (DPOTRF('U'), UINV
+// wfn_initialize.f90:504-530), one block; A column-major n x n.  Sets *info
+// to j+1 if the leading minor j is not positive definite.
+__global__ void k_cholesky_upper(int n, double *A, int *info) {
+  extern __shared__ double shc[];
+  const bool in_smem = (size_t)n * n * sizeof(double) <= 200 * 1024;
+  double *M = in_smem ? shc : A;
+  if (in_smem)
+    for (long k = threadIdx.x; k < (long)n * n; k += blockDim.x) M[k] = A[k];
+  __shared__ double piv;
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    if (threadIdx.x == 0) {
+      double d = M[j + (long)n * j];
+      if (!(d > 0.0)) { bad = j + 1; piv = 1.0; }
+      else piv = sqrt(d);
+      M[j + (long)n * j] = piv;
+    }
+    __syncthreads();
+    if (bad) break;
+    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) M[j + (long)n * i] /= piv;
+    __syncthreads();
+    // trailing update of the upper triangle: M(a,b) -= U(j,a) U(j,b), j < a <= b
+    const int m = n - j - 1;
+    const long cnt = (long)m * m;
+    for (long k = threadIdx.x; k < cnt; k += blockDim.x) {
+      int a = j + 1 + (int)(k % m), b = j + 1 + (int)(k / m);
+      if (a <= b) M[a + (long)n * b] -= M[j + (long)n * a] * M[j + (long)n * b];
+    }
+    __syncthreads();
+  }
+  if (in_smem)
+    for (long k = threadIdx.x; k < (long)n * n; k += blockDim.x) A[k] = M[k];
+  if (threadIdx.x == 0) *info = bad;
+}
+
+// fnonloc G=0 row (P holds the halved G=0 entry): C2_b(0) += sum_j P_j(0) D(j,b)
+__global__ void k_fnonloc_g0(int nproj, int nstate, int ngpw, const double2 *P, const double *D, double2 *c2) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nstate) return;
+  double x = 0, y = 0;
+  for (int j = 0; j < nproj; ++j) {
+    double d = D[j + (long)nproj * b];
+    x += P[(long)j * ngpw].x * d;
+    y += P[(long)j * ngpw].y * d;
+  }
+  c2[(long)b * ngpw].x += x;
+  c2[(long)b * ngpw].y += y;
+}
+// D = -f' (H nl), f' = occ (1 when < 1e-5)   (FNONLOC T = -FFI*WSG, UPF DDIA)
+// and E_nl partial: sum_b occ_b sum_j nl(j,b) (H nl)(j,b)
+__global__ void k_nl_energy_d(int nproj, int nstate, const double *nl, const double *hn, const double *occ, double *D,
+                              double *part) {
+  __shared__ double sh[32];
+  double s = 0;
+  long tot = (long)nproj * nstate;
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < tot; k += (long)gridDim.x * blockDim.x) {
+    int b = (int)(k / nproj);
+    double f = occ[b] < 1e-5 ? 1.0 : occ[b];
+    D[k] = -f * hn[k];
+    s += occ[b] * nl[k] * hn[k];
+  }
+  double r = block_sum(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = r;
+}
+
+// ---------------------------------------------------------------- forces
+// e_sr (total_energy.f90:133-239) with minimum image (nlp = 0); one block.
+// F(3,na_max,nsp) zeroed first as in the reference; esr -> out[0].
+__global__ void k_esr(int nsp, const int *na, int na_max, const int *zv, const double *atco, double alat, int sym,
+                      int tfor, double *F, double *out) {
+  __shared__ double sh[32];
+  const double pi = 4.0 * atan(1.0);
+  const double rckj = sqrt(1.2 * 1.2 + 1.2 * 1.2);
+  double esr = 0;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3 * na_max * nsp; ++k) F[k] = 0.0;
+  __syncthreads();
+  // serial over pairs in thread 0 for the force accumulation order; the
+  // pair count is O(atoms^2) and small
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < nsp; ++k)
+      for (int j = k; j < nsp; ++j) {
+        double zv2 = (double)(zv[k] * zv[j]);
+        if (fabs(zv2) < 1e-10) continue;
+        for (int l = 0; l < na[k]; ++l)
+          for (int m = (k == j) ? l + 1 : 0; m < na[j]; ++m) {
+            const double *xl = atco + 3 * (l + (long)na_max * k), *xm = atco + 3 * (m + (long)na_max * j);
+            double x1 = xl[0] - xm[0], y1 = xl[1] - xm[1], z1 = xl[2] - xm[2], X, Y, Z;
+            if (sym == 1) {
+              double A = alat, h = A / 2.0;
+              X = fmod(x1, A); Y = fmod(y1, A); Z = fmod(z1, A);
+              X = X - A * trunc(X / h); Y = Y - A * trunc(Y / h); Z = Z - A * trunc(Z / h);
+            } else {
+              double ma = alat * sqrt(2.0) / 4.0, s2 = sqrt(2.0);
+              X = (x1 + y1) / s2; Y = (-x1 + y1) / s2;
+              X = fmod(X, 2.0 * ma); Y = fmod(Y, 2.0 * ma);
+              Z = fmod(z1, 2.0 * ma * s2);
+              X = X - 2.0 * ma * trunc(X / ma); Y = Y - 2.0 * ma * trunc(Y / ma);
+              Z = Z - 2.0 * ma * s2 * trunc(Z / (s2 * ma));
+              if (!(fabs(X) + fabs(Y) + s2 * fabs(Z) < 2.0 * ma)) {
+                X = X - copysign(ma, X); Y = Y - copysign(ma, Y); Z = Z - copysign(s2 * ma, Z);
+              }
+              double xt = (X - Y) / s2;
+              Y = (X + Y) / s2;
+              X = xt;
+            }
+            double e2 = X * X + Y * Y + Z * Z, r = sqrt(e2), arg = r / rckj;
+            if (arg <= 20.0) {
+              double add = zv2 * erfc(arg) / r;
+              esr += add;
+              if (tfor) {
+                double pre = (2.0 * zv2 / sqrt(pi)) * exp(-arg * arg) / rckj;
+                double rep = (add + pre) / e2;
+                double *fl = F + 3 * (l + (long)na_max * k), *fm = F + 3 * (m + (long)na_max * j);
+                fl[0] += rep * X; fl[1] += rep * Y; fl[2] += rep * Z;
+                fm[0] -= rep * X; fm[1] -= rep * Y; fm[2] -= rep * Z;
+              }
+            }
+          }
+      }
+    out[0] = esr;
+  }
+  (void)sh;
+}
+
+// POTFOR (nuclear_grad.f90:4-50): per atom and block partial sums of
+// Re[S_I(G) (rhos V_H(G)* + vps rho_e(G)*) i G] 2 Omega tpiba over G != 0
+__global__ void k_potfor(int ngrho, const int *inyh, int nh1, int nh2, int nh3, AtomArgs aa, const double *hg,
+                         const double *gvec, double tpiba2, const double2 *rhog, const double2 *erhos, const double *vps,
+                         const double *rhos, double omtp, double *part) {
+  __shared__ double sh[32];
+  const double fp = 16.0 * atan(1.0);
+  int a = blockIdx.y, is = aa.is[a];
+  double fx = 0, fy = 0, fz = 0;
+  for (int g = 1 + blockIdx.x * blockDim.x + threadIdx.x; g < ngrho; g += gridDim.x * blockDim.x) {
+    double2 rh = rhog[g], rp = erhos[g];
+    double rgx = rh.x + rp.x, rgy = rh.y + rp.y;
+    double f = fp / (tpiba2 * hg[g]);
+    double rs = rhos[(long)is * ngrho + g], vs = vps[(long)is * ngrho + g];
+    // base = rhos f conj(rho+rho_ion) + vps conj(rho)
+    double bx = rs * f * rgx + vs * rh.x, by = -(rs * f * rgy) - vs * rh.y;
+    double2 e = eig_at(inyh, g, nh1, nh2, nh3, aa.arg + 3 * a);
+    double im = e.x * by + e.y * bx;  // Im(e * base)
+    fx += -im * gvec[3 * g] * omtp;
+    fy += -im * gvec[3 * g + 1] * omtp;
+    fz += -im * gvec[3 * g + 2] * omtp;
+  }
+  double sx = block_sum(fx, sh), sy = block_sum(fy, sh), sz = block_sum(fz, sh);
+  if (threadIdx.x == 0) {
+    long o = ((long)a * 3) * gridDim.x + blockIdx.x;
+    part[o] = sx;
+    part[o + gridDim.x] = sy;
+    part[o + 2 * gridDim.x] = sz;
+  }
+}
+// Q_{k,j}(G) = -i G_k P_j(G) for the projector derivatives (D_FNL,
+// nuclear_grad.f90:330-357): rows ordered k*nproj + j
+__global__ void k_dproj(int ngpw, int nproj, const double *gvec, const double2 *P, double2 *Q) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (g >= ngpw) return;
+  double2 p = P[(long)j * ngpw + g];
+  double gk = gvec[3L * g + k];
+  Q[((long)k * nproj + j) * ngpw + g] = make_double2(gk * p.y, -gk * p.x);
+}
+// NLFOR / UPF_NLFOR (nuclear_grad.f90:51-89,153-199) plus POTFOR/e_sr sums:
+// F(isa) += potfor - sum_{j of isa} sum_b 2 occ_b (H nl)(j,b) dfnl_k(j,b)
+__global__ void k_force_total(int nat, int nproj, int nstate, const int *proj_isa, const double *hn, const double *dfnl,
+                              const double *occ, const double *potpart, int pnb, const int *isa_is, const int *isa_ia,
+                              int na_max, double *F) {
+  __shared__ double sh[32];
+  int a = blockIdx.x;
+  for (int k = 0; k < 3; ++k) {
+    double s = 0;
+    for (long q = threadIdx.x; q < (long)nproj * nstate; q += blockDim.x) {
+      int j = (int)(q % nproj), b = (int)(q / nproj);
+      if (proj_isa[j] != a) continue;
+      double w = occ[b];
+      if (!(fabs(w) > 1e-12)) continue;
+      s += 2.0 * w * hn[j + (long)nproj * b] * dfnl[(long)k * nproj + j + (long)3 * nproj * b];
+    }
+    double nlf = block_sum(s, sh);
+    double pf = 0;
+    for (int i = threadIdx.x; i < pnb; i += blockDim.x) pf += potpart[((long)a * 3 + k) * pnb + i];
+    double pfs = block_sum(pf, sh);
+    if (threadIdx.x == 0) F[3 * (isa_ia[a] + (long)na_max * isa_is[a]) + k] += pfs - nlf;
+    __syncthreads();
+  }
+}
+
+}  // namespace amdk

@@ -1,0 +1,306 @@
+"""ctypes binding of libamdk (include/amdk.h) and the driver loops.
+
+The driver loops restate AMDKIIT's outer loops, which stay outside the
+C-ABI in the reference design: wfn_opt (do_opt.f90:51-138) and the
+velocity-Verlet BOMD step (molecular_dynamics.f90:92-130).  Every
+numerical operation runs in libamdk on the GPU; there is no CPU fallback:
+constructing an Engine fails if the CUDA library cannot be loaded or the
+device cannot be initialised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from .inputs import System
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libamdk.so")
+MAXSP = 4
+
+FP64, MIXED = 0, 1
+
+
+class _Species(C.Structure):
+    _fields_ = [("type", C.c_int), ("z", C.c_int), ("zv", C.c_double), ("mesh", C.c_int),
+                ("rr", C.POINTER(C.c_double)), ("vr", C.POINTER(C.c_double)), ("rps", C.POINTER(C.c_double)),
+                ("lmax", C.c_int), ("l_local", C.c_int), ("skip", C.c_int), ("tkb", C.c_int),
+                ("rab", C.POINTER(C.c_double)), ("vloc", C.POINTER(C.c_double)), ("nbeta", C.c_int),
+                ("beta_l", C.POINTER(C.c_int)), ("beta", C.POINTER(C.c_double)), ("dij", C.POINTER(C.c_double)),
+                ("upf_lmax", C.c_int)]
+
+
+class _System(C.Structure):
+    _fields_ = [("a_cell", C.c_double * 9), ("alat", C.c_double), ("symmetry", C.c_int), ("ecut", C.c_double),
+                ("nsp", C.c_int), ("na", C.c_int * MAXSP), ("na_max", C.c_int), ("atco", C.POINTER(C.c_double)),
+                ("xc", C.c_int), ("nstate", C.c_int), ("sp", _Species * MAXSP)]
+
+
+class _Options(C.Structure):
+    _fields_ = [("device", C.c_int), ("precision", C.c_int), ("pair_batch", C.c_int), ("reserved", C.c_int * 8)]
+
+
+class _Info(C.Structure):
+    _fields_ = [("nr", C.c_int * 3), ("ngpw", C.c_int), ("ngrho", C.c_int), ("ngrays", C.c_int), ("nhrays", C.c_int),
+                ("nstate", C.c_int), ("nat", C.c_int), ("nghmax", C.c_int), ("omega", C.c_double)]
+
+
+class Energies(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("etotal", "eke", "estat", "eself", "esr", "eloc", "enl", "exc", "eh")]
+
+    def asdict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class AmdkError(RuntimeError):
+    pass
+
+
+_LIB = None
+
+
+def load_library(path: str = LIBPATH):
+    """Load libamdk.so (building it first when the sources are newer)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    from . import build as _build
+    if _build.needs_build():
+        _build.build()
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    lib.amdk_last_error.restype = C.c_char_p
+    lib.amdk_create.argtypes = [C.POINTER(_System), C.POINTER(_Options), C.POINTER(P)]
+    lib.amdk_destroy.argtypes = [P]
+    lib.amdk_info_get.argtypes = [P, C.POINTER(_Info)]
+    lib.amdk_get_gvectors.argtypes = [P, P, P, P, P, P]
+    lib.amdk_host_gvectors.argtypes = [C.POINTER(_System), C.POINTER(_Info), P, P, P, P, P]
+    lib.amdk_set_positions.argtypes = [P, C.POINTER(C.c_double)]
+    lib.amdk_set_wfn.argtypes = [P, C.POINTER(C.c_double)]
+    lib.amdk_get_wfn.argtypes = [P, C.POINTER(C.c_double)]
+    for f in ("amdk_ortho", "amdk_density", "amdk_potential", "amdk_apply_h"):
+        getattr(lib, f).argtypes = [P]
+    lib.amdk_energy.argtypes = [P, C.POINTER(Energies)]
+    lib.amdk_gradient.argtypes = [P, C.POINTER(C.c_double)]
+    lib.amdk_pcg.argtypes = [P, C.c_int]
+    lib.amdk_scf_iteration.argtypes = [P, C.c_int, C.c_double, C.POINTER(Energies), C.POINTER(C.c_double),
+                                       C.POINTER(C.c_int)]
+    lib.amdk_ionic_forces.argtypes = [P, C.POINTER(C.c_double)]
+    lib.amdk_get_array.argtypes = [P, C.c_char_p, P, C.c_size_t]
+    lib.amdk_fft_sphere.argtypes = [P, C.c_int, P, P]
+    lib.amdk_last_iteration_ms.argtypes = [P, C.POINTER(C.c_double)]
+    _LIB = lib
+    return lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def system_struct(system: System):
+    """Fill the amdk_system struct; returns (struct, keep-alive list)."""
+    keep = []
+    s = _System()
+    a = np.asarray(system.a_cell, dtype=np.float64).flatten(order="F")
+    for k in range(9):
+        s.a_cell[k] = a[k]
+    s.alat = system.alat
+    s.symmetry = system.symmetry
+    s.ecut = system.ecut
+    s.nsp = len(system.species)
+    for i, n in enumerate(system.na):
+        s.na[i] = n
+    s.na_max = system.na_max
+    atco = system.atco()
+    keep.append(atco)
+    s.atco = _dp(atco)
+    s.xc = system.xc
+    s.nstate = system.nstate
+    for i, sp in enumerate(system.species):
+        o = s.sp[i]
+        o.type, o.z, o.zv, o.mesh = sp.kind, sp.z, sp.zv, sp.mesh
+        for name in ("rr", "vr", "rps", "rab", "vloc", "beta", "dij"):
+            v = getattr(sp, name)
+            if v is not None:
+                v = np.ascontiguousarray(v, dtype=np.float64)
+                keep.append(v)
+                setattr(o, name, _dp(v))
+        o.lmax, o.l_local, o.skip, o.tkb = sp.lmax, sp.l_local, sp.skip, int(sp.tkb)
+        o.nbeta = sp.nbeta
+        if sp.beta_l is not None and sp.nbeta:
+            bl = np.ascontiguousarray(sp.beta_l, dtype=np.int32)
+            keep.append(bl)
+            o.beta_l = bl.ctypes.data_as(C.POINTER(C.c_int))
+        o.upf_lmax = sp.upf_lmax
+    return s, keep
+
+
+def _check(rc, what=""):
+    if rc != 0:
+        msg = load_library().amdk_last_error().decode()
+        raise AmdkError(f"{what} failed ({rc}): {msg}")
+
+
+def host_gvectors(system: System) -> dict:
+    """The G half-sphere and ray maps from the library's host setup (no GPU)."""
+    lib = load_library()
+    s, keep = system_struct(system)
+    info = _Info()
+    _check(lib.amdk_host_gvectors(C.byref(s), C.byref(info), None, None, None, None, None), "amdk_host_gvectors")
+    ng = info.ngrho
+    inyh = np.zeros((ng, 3), np.int32)
+    hg = np.zeros(ng)
+    gvec = np.zeros((ng, 3))
+    mp = np.zeros(ng, np.int32)
+    mm = np.zeros(ng, np.int32)
+    _check(lib.amdk_host_gvectors(C.byref(s), C.byref(info), inyh.ctypes.data, hg.ctypes.data, gvec.ctypes.data,
+                                  mp.ctypes.data, mm.ctypes.data), "amdk_host_gvectors")
+    return dict(inyh=inyh, hg=hg, gvec=gvec, mapp=mp, mapm=mm, ngpw=info.ngpw, ngrho=ng, ngrays=info.ngrays,
+                nhrays=info.nhrays, nr=tuple(info.nr))
+
+
+class Engine:
+    """One system resident on one GPU."""
+
+    def __init__(self, system: System, precision: int = FP64, pair_batch: int = 0, device: int = 0):
+        self.lib = load_library()
+        self.system = system
+        s, self._keep = system_struct(system)
+        opt = _Options()
+        opt.device, opt.precision, opt.pair_batch = device, precision, pair_batch
+        h = C.c_void_p()
+        _check(self.lib.amdk_create(C.byref(s), C.byref(opt), C.byref(h)), "amdk_create")
+        self.h = h
+        info = _Info()
+        _check(self.lib.amdk_info_get(self.h, C.byref(info)), "amdk_info_get")
+        self.info = info
+        self.ngpw, self.ngrho, self.nstate = info.ngpw, info.ngrho, info.nstate
+        self.nr = tuple(info.nr)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.amdk_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --------------------------------------------------------------- data
+    def gvectors(self) -> dict:
+        ng = self.ngrho
+        inyh = np.zeros((ng, 3), np.int32)
+        hg = np.zeros(ng)
+        gvec = np.zeros((ng, 3))
+        mp = np.zeros(ng, np.int32)
+        mm = np.zeros(ng, np.int32)
+        _check(self.lib.amdk_get_gvectors(self.h, inyh.ctypes.data, hg.ctypes.data, gvec.ctypes.data, mp.ctypes.data,
+                                          mm.ctypes.data))
+        return dict(inyh=inyh, hg=hg, gvec=gvec, mapp=mp, mapm=mm)
+
+    def set_wfn(self, c0: np.ndarray):
+        c = np.ascontiguousarray(c0, dtype=np.complex128)
+        assert c.shape == (self.nstate, self.ngpw)
+        _check(self.lib.amdk_set_wfn(self.h, c.ctypes.data_as(C.POINTER(C.c_double))), "amdk_set_wfn")
+
+    def get_wfn(self) -> np.ndarray:
+        c = np.zeros((self.nstate, self.ngpw), np.complex128)
+        _check(self.lib.amdk_get_wfn(self.h, c.ctypes.data_as(C.POINTER(C.c_double))), "amdk_get_wfn")
+        return c
+
+    def set_positions(self, atco: np.ndarray):
+        a = np.ascontiguousarray(atco, dtype=np.float64)
+        _check(self.lib.amdk_set_positions(self.h, _dp(a)), "amdk_set_positions")
+
+    def get(self, name: str) -> np.ndarray:
+        n1, n2, n3 = self.nr
+        nsp = len(self.system.species)
+        nproj = sum(n * 0 for n in self.system.na)
+        shapes = {
+            "rho": ((n3, n2, n1), np.float64), "v_pot": ((n3, n2, n1), np.float64),
+            "rho_g": ((self.ngrho,), np.complex128), "c2": ((self.nstate, self.ngpw), np.complex128),
+            "c0": ((self.nstate, self.ngpw), np.complex128),
+            "vps": ((nsp, self.ngrho), np.float64), "rhos": ((nsp, self.ngrho), np.float64),
+            "twnl": ((nsp, self.info.nghmax, self.ngpw), np.float64),
+            "eigrxvps": ((self.ngrho,), np.complex128), "eigrxrhos": ((self.ngrho,), np.complex128),
+            "vpp": ((self.ngpw,), np.float64),
+            "force": ((nsp, self.system.na_max, 3), np.float64),
+        }
+        del nproj
+        shape, dt = shapes[name]
+        a = np.zeros(shape, dt)
+        _check(self.lib.amdk_get_array(self.h, name.encode(), a.ctypes.data, a.nbytes), f"amdk_get_array({name})")
+        return a
+
+    # ----------------------------------------------------------- routines
+    def ortho(self):
+        _check(self.lib.amdk_ortho(self.h), "amdk_ortho")
+
+    def density(self):
+        _check(self.lib.amdk_density(self.h), "amdk_density")
+
+    def potential(self):
+        _check(self.lib.amdk_potential(self.h), "amdk_potential")
+
+    def energy(self) -> dict:
+        e = Energies()
+        _check(self.lib.amdk_energy(self.h, C.byref(e)), "amdk_energy")
+        return e.asdict()
+
+    def apply_h(self):
+        _check(self.lib.amdk_apply_h(self.h), "amdk_apply_h")
+
+    def gradient(self) -> float:
+        g = C.c_double()
+        _check(self.lib.amdk_gradient(self.h, C.byref(g)), "amdk_gradient")
+        return g.value
+
+    def pcg(self, istep: int):
+        _check(self.lib.amdk_pcg(self.h, istep), "amdk_pcg")
+
+    def scf_iteration(self, istep: int, gcut: float):
+        e = Energies()
+        g = C.c_double()
+        conv = C.c_int()
+        _check(self.lib.amdk_scf_iteration(self.h, istep, gcut, C.byref(e), C.byref(g), C.byref(conv)),
+               "amdk_scf_iteration")
+        return e.asdict(), g.value, bool(conv.value)
+
+    def last_iteration_ms(self) -> float:
+        m = C.c_double()
+        self.lib.amdk_last_iteration_ms(self.h, C.byref(m))
+        return m.value
+
+    def ionic_forces(self) -> np.ndarray:
+        s = self.system
+        f = np.zeros((len(s.species), s.na_max, 3))
+        _check(self.lib.amdk_ionic_forces(self.h, _dp(f)), "amdk_ionic_forces")
+        return f
+
+    def fft_sphere(self, sign: int, coef: Optional[np.ndarray] = None, grid: Optional[np.ndarray] = None):
+        n1, n2, n3 = self.nr
+        if coef is None:
+            coef = np.zeros(self.ngrho, np.complex128)
+        if grid is None:
+            grid = np.zeros((n3, n2, n1), np.complex128)
+        coef = np.ascontiguousarray(coef, dtype=np.complex128)
+        grid = np.ascontiguousarray(grid, dtype=np.complex128)
+        _check(self.lib.amdk_fft_sphere(self.h, sign, coef.ctypes.data, grid.ctypes.data), "amdk_fft_sphere")
+        return coef, grid
+
+    # ------------------------------------------------------------ drivers
+    def wfn_opt(self, max_step: int = 800, gcut: float = 1e-7, callback=None):
+        """do_opt.f90:51-138: CG iterations until GEMAX < gcut."""
+        e = None
+        for i in range(1, max_step + 1):
+            e, g, conv = self.scf_iteration(i, gcut)
+            if callback:
+                callback(i, e, g)
+            if conv:
+                return i, e, g
+        return max_step, e, g

@@ -1,0 +1,169 @@
+/*
+ * amdk.h -- C-ABI of libamdk, the sm_100a implementation of AMDKIIT's
+ * wavefunction hot path (one GPU).
+ *
+ * The reference (AMDKIIT, Fortran) has no plugin API: its hot path is a set
+ * of argument-less subroutines that read and write module globals
+ * (source/system_data_types.f90:63-234).  Each entry point below replaces one
+ * of those subroutines (cited per function, paths relative to the AMDKIIT
+ * project root) and is callable from Fortran through iso_c_binding in the
+ * way the reference already binds C (source/yaml.f90:35-42 <-> yaml.cpp:168).
+ *
+ * Conventions
+ *  - every function returns 0 on success or a negative AMDK_ERR_* code;
+ *    amdk_last_error() returns a message for the calling thread;
+ *  - host arrays are caller-owned; Fortran column-major layouts are kept
+ *    (C0(ngpw,nstate) complex, atco(3,na_max,nsp), force(3,na_max,nsp));
+ *  - device state is owned by the context; one CUDA stream per context;
+ *    calls on one context are not re-entrant, separate contexts may be used
+ *    from separate host threads;
+ *  - there is no CPU fallback: if the CUDA kernels cannot run, calls fail.
+ */
+#ifndef AMDK_H
+#define AMDK_H
+#include <stddef.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AMDK_MAXSP 4
+
+enum {
+  AMDK_OK = 0,
+  AMDK_ERR_BADARG = -1,
+  AMDK_ERR_CUDA = -2,
+  AMDK_ERR_ALLOC = -3,
+  AMDK_ERR_NOT_SPD = -4,     /* overlap not positive definite (UINV STOP, wfn_initialize.f90:514-528) */
+  AMDK_ERR_NONFINITE = -5,   /* NaN/Inf in energy or gradient */
+  AMDK_ERR_TIMEOUT = -6,
+  AMDK_ERR_UNSUPPORTED = -7
+};
+
+enum { AMDK_PP_PSP = 0, AMDK_PP_UPF = 1 };
+enum { AMDK_XC_TETER93 = 0, AMDK_XC_PZ = 1, AMDK_XC_PBE = 2 };
+enum { AMDK_FP64 = 0, AMDK_MIXED = 1 };
+
+/* One species as held after read_psp (source/readpsp.f90:11-67) or
+ * read_upf (source/readupf.f90:19-85). Same meaning as orc_species. */
+typedef struct {
+  int type;               /* AMDK_PP_PSP or AMDK_PP_UPF */
+  int z;
+  double zv;
+  int mesh;
+  const double *rr;       /* radial mesh (PSP rr, UPF PP_R) */
+  const double *vr;       /* PSP: vr[l*mesh+ir], l < lmax, Hartree */
+  const double *rps;      /* PSP: rps[l*mesh+ir] */
+  int lmax, l_local, skip, tkb;   /* PSP, 1-based (yamlread.f90:300-314) */
+  const double *rab;      /* UPF PP_RAB */
+  const double *vloc;     /* UPF PP_LOCAL / 2 (Hartree) */
+  int nbeta;
+  const int *beta_l;
+  const double *beta;     /* beta[nb*mesh+ir] = r*beta_nb(r) */
+  const double *dij;      /* PP_DIJ as in the file (Ry) */
+  int upf_lmax;           /* header l_max + 1 */
+} amdk_species;
+
+/* The system after the reference's input stage (init_module.f90:3-113). */
+typedef struct {
+  double a_cell[9];       /* a_cell(3,3) column-major, bohr */
+  double alat;            /* a_lattice, bohr */
+  int symmetry;           /* 1 cubic, 2 fcc */
+  double ecut;            /* wavefunction cutoff, Ry (density cutoff = 4 ecut) */
+  int nsp;
+  int na[AMDK_MAXSP];
+  int na_max;
+  const double *atco;     /* atco(3,na_max,nsp), bohr */
+  int xc;                 /* AMDK_XC_* */
+  int nstate;             /* 0: from the valence charge (atomic_basis.f90:49-71) */
+  amdk_species sp[AMDK_MAXSP];
+} amdk_system;
+
+typedef struct {
+  int device;             /* CUDA device ordinal */
+  int precision;          /* AMDK_FP64 or AMDK_MIXED */
+  int pair_batch;         /* band pairs per FFT batch (0: automatic) */
+  int reserved[8];
+} amdk_options;
+
+typedef struct {
+  int nr[3];              /* FFT grid (set_cell.f90:177-211) */
+  int ngpw, ngrho;        /* wavefunction / density half-sphere sizes */
+  int ngrays, nhrays;     /* x-rays of the two spheres (fft_interface.f90:262-293) */
+  int nstate, nat, nghmax;
+  double omega;
+} amdk_info;
+
+typedef struct {
+  double etotal, eke, estat, eself, esr, eloc, enl, exc, eh;  /* total_energy.f90:4-36 */
+} amdk_energies;
+
+typedef struct amdk_ctx amdk_ctx;
+
+const char *amdk_last_error(void);
+
+/* Setup: init_module.f90:3-162 from the input stage on (grids, G vectors,
+ * ray maps, form factors, projector tables, structure factors), then
+ * uploads every immutable table to the device. */
+int amdk_create(const amdk_system *sys, const amdk_options *opt, amdk_ctx **out);
+int amdk_destroy(amdk_ctx *ctx);
+int amdk_info_get(amdk_ctx *ctx, amdk_info *info);
+
+/* G half-sphere in the reference's layout (gvectors.f90:111-341 and
+ * fft_interface.f90:151-363 with one rank): inyh(3,ngrho) 1-based grid
+ * indices, hg(ngrho), gvec(3,ngrho), map_grid1d_p/m(ngrho) 1-based into the
+ * ray-compressed x-line buffer of leading dimension nrlead(1).  Any pointer
+ * may be NULL. */
+int amdk_get_gvectors(amdk_ctx *ctx, int *inyh, double *hg, double *gvec, int *map_p, int *map_m);
+
+/* The same G half-sphere and maps from the host setup alone, without a GPU
+ * context (gvectors.f90 + prepare_fft for callers that only need the
+ * integer maps).  Call first with NULL arrays to get the sizes in *info. */
+int amdk_host_gvectors(const amdk_system *sys, amdk_info *info, int *inyh, double *hg, double *gvec, int *map_p,
+                       int *map_m);
+
+/* exp_igr.f90:4-140 exp_igrxfactor for new positions atco(3,na_max,nsp) */
+int amdk_set_positions(amdk_ctx *ctx, const double *atco);
+
+/* C_0(ngpw,nstate) complex as interleaved doubles (host memory) */
+int amdk_set_wfn(amdk_ctx *ctx, const double *c0);
+int amdk_get_wfn(amdk_ctx *ctx, double *c0);
+
+/* wfn_initialize.f90:448-499 ortho_gs (Cholesky of the overlap) */
+int amdk_ortho(amdk_ctx *ctx);
+/* density.f90:5-98 eval_density + density.f90:128-150 rhor2g */
+int amdk_density(amdk_ctx *ctx);
+/* potential.f90:4-46 eval_pot + xc.f90:4-434 cal_vpot_ex */
+int amdk_potential(amdk_ctx *ctx);
+/* pseudopotential.f90:3-103 pp_energy (fnl) + total_energy.f90:4-36 e_total */
+int amdk_energy(amdk_ctx *ctx, amdk_energies *out);
+/* wfn_initialize.f90:268-365 vpsi + :560-695 fnonloc/upf_fnonloc: C2 = -f H C0 */
+int amdk_apply_h(amdk_ctx *ctx);
+/* gradient.f90:5-61 forces (Lambda, C2 -= C0 Lambda, ZCLEAN) + eval_GMAX */
+int amdk_gradient(amdk_ctx *ctx, double *gemax);
+/* cg.f90:201-283 PCG (hess, precon, direction, C0 += 0.0625 d) */
+int amdk_pcg(amdk_ctx *ctx, int istep);
+/* One CG iteration of do_opt.f90:80-128 (density ... ortho_gs), ionic
+ * forces included once GEMAX < 3*gcut as in CHK_TFOR (gradient.f90:113-136). */
+int amdk_scf_iteration(amdk_ctx *ctx, int istep, double gcut, amdk_energies *e, double *gemax, int *converged);
+/* total_energy.f90:133-239 e_sr + nuclear_grad.f90:4-89 POTFOR, NLFOR
+ * (UPF_NLFOR :153-199) for the current C0 and density: force(3,na_max,nsp) */
+int amdk_ionic_forces(amdk_ctx *ctx, double *force);
+
+/* Copy a named device array to host memory (parity tests and drivers).
+ * Names: "rho","v_pot" (nr3*nr2*nr1 real, x fastest), "rho_g" (ngrho complex),
+ * "c2" (ngpw*nstate complex), "nl" (nat*nghmax*nstate), "vps","rhos"
+ * (nsp*ngrho), "twnl" (ngpw*nghmax*nsp), "eigrxvps","eigrxrhos" (ngrho complex). */
+int amdk_get_array(amdk_ctx *ctx, const char *name, void *dst, size_t bytes);
+
+/* Raw pruned 3D FFT on the density sphere (fft_interface.f90:6-29):
+ * sign=-1: coef(ngrho) complex (the +G half; -G taken as conj) -> grid
+ *          (nr3*nr2*nr1 complex); sign=+1: grid -> coef = F(+G)/N. */
+int amdk_fft_sphere(amdk_ctx *ctx, int sign, double *coef, double *grid);
+
+/* Elapsed device time of the last amdk_scf_iteration, milliseconds. */
+int amdk_last_iteration_ms(amdk_ctx *ctx, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

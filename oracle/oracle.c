@@ -23,6 +23,12 @@
 typedef double _Complex zc;
 
 static double PI_, TWOPI_, FOURPI_;
+/* constants.f90:3-5, set when the library is loaded */
+__attribute__((constructor)) static void init_constants(void) {
+  PI_ = 4.0 * atan(1.0);
+  TWOPI_ = 8.0 * atan(1.0);
+  FOURPI_ = 16.0 * atan(1.0);
+}
 static const double RAGGIO = 1.2;      /* system_data_types.f90:72 */
 static const double EPSGX = 1.0e-12;   /* gvectors.f90:125 */
 static const double HCUT = 0.5;        /* constants.f90:15 */

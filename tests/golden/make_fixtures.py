@@ -1,0 +1,79 @@
+"""Generate the golden fixtures from the reference's committed test runs.
+
+Reads AMDKIIT's tests/<case>/ directories (input.yaml, xyz, pseudopotential
+files and the amdkiit.out of the committed run) and writes, per case,
+  <case>.npz   the parsed system (cell, positions, pseudopotential tables)
+  golden.json  the energies the reference printed (eprint.f90:1-14) and the
+               per-rank G-vector tables summed over ranks (gvectors.f90:315-325)
+Run from the repository root:  python tests/golden/make_fixtures.py /path/to/AMDKIIT
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from amdkiit_b200.inputs import load_reference_input  # noqa: E402
+
+CASES = {
+    "water1_mt": "tests/1_water/wf_opt",
+    "water2_mt": "tests/2_water/wf_opt",
+    "water32_mt": "tests/32_water/wf_opt",
+    "si_fcc_mt": "tests/bulk_si/single_point",
+}
+KEYS = {"TOTAL ENERGY": "etotal", "KINETIC ENERGY": "eke", "ELECTROSTATIC ENERGY": "estat",
+        "SELF ENERGY CONTRIBUTION": "eself", "OVERLAP ENERGY CONTRIBUTION": "esr", "LOCAL PP ENERGY": "eloc",
+        "NON LOCAL PP ENERGY": "enl", "EXCHANGE CORRELATION ENERGY": "exc"}
+
+
+def parse_out(path):
+    txt = open(path).read()
+    e = {}
+    for k, v in KEYS.items():
+        m = re.findall(r"#\s+%s\s+=\s+([-0-9.]+)" % re.escape(k), txt)
+        if m:
+            e[v] = float(m[-1])
+    rows = re.findall(r"^\s+\d+\s+(\d+)\s+(\d+)\s+\d+\s+(\d+)\s+(\d+)\s+(\d+)\s+(\d+)\s+\d+\s*$", txt, re.M)
+    g = {}
+    if rows:
+        a = np.array(rows, dtype=np.int64)
+        g = dict(ngpw=int(a[:, 0].sum()), ngrho=int(a[:, 1].sum()), ny=int(a[0, 2]), nz=int(a[0, 3]),
+                 ngrays=int(a[:, 4].sum()), nhrays=int(a[:, 5].sum()))
+    iters = re.findall(r"^#\s+(\d+)\s+-?[0-9.]+\s", txt, re.M)
+    return e, g, (int(iters[-1]) if iters else None)
+
+
+def save_system(path, s):
+    d = dict(a_cell=s.a_cell, alat=s.alat, symmetry=s.symmetry, ecut=s.ecut, xc=s.xc, nsp=len(s.species))
+    for i, (sp, pos) in enumerate(zip(s.species, s.positions)):
+        d[f"pos{i}"] = pos
+        d[f"sp{i}_meta"] = np.array([sp.z, sp.zv, sp.kind, sp.lmax, sp.l_local, sp.skip, int(sp.tkb), sp.upf_lmax])
+        d[f"sp{i}_label"] = np.array(sp.label)
+        for k in ("rr", "vr", "rps", "rab", "vloc", "beta", "beta_l", "dij"):
+            v = getattr(sp, k)
+            if v is not None:
+                d[f"sp{i}_{k}"] = v
+    np.savez_compressed(path, **d)
+
+
+def main(root):
+    golden = {}
+    for name, rel in CASES.items():
+        d = os.path.join(root, rel)
+        s = load_reference_input(d)
+        save_system(os.path.join(HERE, name + ".npz"), s)
+        e, g, it = parse_out(os.path.join(d, "amdkiit.out"))
+        golden[name] = dict(energies=e, gvectors=g, iterations=it, source=rel + "/amdkiit.out")
+        print(name, e.get("etotal"), g)
+    with open(os.path.join(HERE, "golden.json"), "w") as f:
+        json.dump(golden, f, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

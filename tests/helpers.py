@@ -1,0 +1,38 @@
+"""Shared helpers for the tests: golden fixtures and paired oracle/engine runs."""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+
+from amdkiit_b200.guess import initial_coefficients
+from amdkiit_b200.inputs import Species, System
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def golden():
+    with open(os.path.join(GOLDEN, "golden.json")) as f:
+        return json.load(f)
+
+
+def load_fixture(name: str) -> System:
+    d = np.load(os.path.join(GOLDEN, name + ".npz"))
+    species, pos = [], []
+    for i in range(int(d["nsp"])):
+        z, zv, kind, lmax, l_local, skip, tkb, upf_lmax = d[f"sp{i}_meta"]
+        kw = {}
+        for k in ("rr", "vr", "rps", "rab", "vloc", "beta", "beta_l", "dij"):
+            if f"sp{i}_{k}" in d:
+                kw[k] = d[f"sp{i}_{k}"]
+        species.append(Species(label=str(d[f"sp{i}_label"]), z=int(z), zv=float(zv), kind=int(kind),
+                               lmax=int(lmax), l_local=int(l_local), skip=int(skip), tkb=bool(tkb),
+                               upf_lmax=int(upf_lmax), **kw))
+        pos.append(d[f"pos{i}"])
+    return System(a_cell=d["a_cell"], alat=float(d["alat"]), symmetry=int(d["symmetry"]), ecut=float(d["ecut"]),
+                  species=species, positions=pos, xc=int(d["xc"]), name=name)
+
+
+def start_coefficients(hg_pw: np.ndarray, tpiba: float, nstate: int, seed: int = 1234) -> np.ndarray:
+    return initial_coefficients(hg_pw * tpiba * tpiba, nstate, seed)

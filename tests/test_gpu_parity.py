@@ -1,0 +1,170 @@
+"""GPU parity: every stage of one CG iteration through the C-ABI against the
+CPU restatement on the same inputs, then whole SCF runs.
+
+Tolerances (FP64 path): the GPU FFTs and reductions round differently from
+the oracle's, so real-space and G-space arrays agree to ~1e-12 relative;
+we test 1e-10 relative to the array's max.  Energies: 1e-9 Ha per stage.
+After convergence: |dE| <= 1e-6 Ha/atom and |dF| <= 1e-4 Ha/bohr (the
+build's correctness bar), in practice far tighter."""
+import numpy as np
+import pytest
+
+from amdkiit_b200 import configs
+from amdkiit_b200.engine import FP64, Engine
+from amdkiit_b200.inputs import XC_PBE
+from oracle.oracle import Oracle
+from tests.helpers import golden, load_fixture, start_coefficients
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def pair(system, seed=1234, batch=0):
+    o = Oracle(system, 0)
+    e = Engine(system, FP64, pair_batch=batch)
+    g = o.gvectors()
+    c = start_coefficients(g["hg"][: o.ngpw], o.d("tpiba"), o.nstate, seed)
+    o.set_wfn(c)
+    e.set_wfn(c)
+    return o, e
+
+
+SYSTEMS = {
+    "small_water_pz": lambda: configs.small_water(),
+    "small_water_pbe": lambda: configs.small_water(xc=XC_PBE),
+    "si_fcc_mt": lambda: load_fixture("si_fcc_mt"),
+}
+
+
+@pytest.mark.parametrize("name", sorted(SYSTEMS))
+def test_one_iteration_stage_by_stage(name):
+    s = SYSTEMS[name]()
+    o, e = pair(s)
+    # tables built on the device
+    ng = e.ngrho
+    assert rel(e.get("vps")[:, :ng], o.arr("vps", (len(s.species), ng))) < 1e-12
+    assert rel(e.get("eigrxvps"), o.arr("eigrxvps", (ng,), np.complex128)) < 1e-11
+    assert rel(e.get("eigrxrhos"), o.arr("eigrxrhos", (ng,), np.complex128)) < 1e-11
+    # ortho_gs
+    assert o.ortho() == 0
+    e.ortho()
+    assert rel(e.get_wfn(), o.c0()) < 1e-11
+    # eval_density + rhor2g
+    o.call("eval_density")
+    o.call("rhor2g")
+    e.density()
+    assert rel(e.get("rho"), o.real_grid("rho")) < 1e-11
+    assert rel(e.get("rho_g"), o.arr("rho_g", (ng,), np.complex128)) < 1e-11
+    # eval_pot + cal_vpot_ex
+    o.call("eval_pot")
+    o.call("cal_vpot_ex")
+    e.potential()
+    assert rel(e.get("v_pot"), o.real_grid("v_pot")) < 1e-10
+    # pp_energy + e_total
+    o.call("pp_energy")
+    o.call("e_total")
+    en = e.energy()
+    eo = o.energies()
+    for k in ("etotal", "eke", "estat", "eloc", "enl", "exc", "esr", "eself"):
+        assert abs(en[k] - eo[k]) < 1e-9, (k, en[k], eo[k])
+    # vpsi + fnonloc
+    o.call("vpsi")
+    o.call("fnonloc")
+    e.apply_h()
+    assert rel(e.get("c2"), o.c2()) < 1e-10
+    # forces (Lambda) + GEMAX
+    o.call("forces")
+    gm = e.gradient()
+    assert rel(e.get("c2"), o.c2()) < 1e-10
+    c2o = o.c2()
+    nocc = int(np.sum(o.arr("occ", (o.nstate,)) > 1e-5))
+    assert abs(gm - np.abs(c2o[:nocc]).max()) < 1e-12 * max(gm, 1.0)
+    # PCG (first step) + ortho
+    o.call("pcg", 1)
+    e.pcg(1)
+    assert rel(e.get_wfn(), o.c0()) < 1e-10
+    assert o.ortho() == 0
+    e.ortho()
+    assert rel(e.get_wfn(), o.c0()) < 1e-10
+
+
+@pytest.mark.parametrize("name", sorted(SYSTEMS))
+def test_scf_iterations_track_oracle(name):
+    s = SYSTEMS[name]()
+    o, e = pair(s)
+    o.ortho()
+    e.ortho()
+    for it in range(1, 26):
+        ro = o.scf_iteration(it, 1e-7)
+        en, gm, conv = e.scf_iteration(it, 1e-7)
+        assert abs(en["etotal"] - o.d("etotal")) < 1e-8, it
+        assert abs(gm - o.d("gemax")) < 1e-8 * max(1.0, gm), it
+    assert rel(e.get_wfn(), o.c0()) < 1e-6
+
+
+@pytest.mark.parametrize("batch", [1, 3, 0])
+def test_pair_batch_does_not_change_results(batch):
+    s = configs.small_water()
+    o, e = pair(s, batch=batch)
+    e.ortho()
+    e.density()
+    ref = Engine(s, FP64, pair_batch=1)
+    ref.set_wfn(e.get_wfn())
+    ref.density()
+    assert rel(e.get("rho"), ref.get("rho")) < 1e-13
+
+
+def test_converged_energy_and_forces_match_oracle():
+    s = configs.small_water(xc=XC_PBE)
+    o, e = pair(s)
+    o.ortho()
+    e.ortho()
+    no = o.wfn_opt(400, 1e-7)
+    ne, en, gm = e.wfn_opt(400, 1e-7)
+    assert 0 < no < 400 and ne < 400
+    assert abs(en["etotal"] - o.d("etotal")) < 1e-6 * s.nat
+    fo = o.force()
+    fe = e.ionic_forces()
+    assert np.max(np.abs(fe - fo)) < 1e-4
+    # forces are present (tfor) and the net force is small for a free molecule
+    assert np.abs(fo).max() > 1e-3
+
+
+def test_fft_sphere_roundtrip_and_numpy():
+    s = configs.small_water()
+    e = Engine(s, FP64)
+    g = e.gvectors()
+    rng = np.random.default_rng(0)
+    coef = (rng.standard_normal(e.ngrho) + 1j * rng.standard_normal(e.ngrho)) / (1 + g["hg"])
+    coef[0] = coef[0].real
+    _, grid = e.fft_sphere(-1, coef=coef)
+    n1, n2, n3 = e.nr
+    nh = np.array([n1 // 2 + 1, n2 // 2 + 1, n3 // 2 + 1])
+    mil = g["inyh"] - nh[None, :]
+    full = np.zeros((n3, n2, n1), complex)
+    full[mil[:, 2] % n3, mil[:, 1] % n2, mil[:, 0] % n1] = coef
+    full[(-mil[:, 2]) % n3, (-mil[:, 1]) % n2, (-mil[:, 0]) % n1] = np.conj(coef)
+    full[0, 0, 0] = coef[0]
+    ref = np.fft.ifftn(full) * full.size
+    assert rel(grid, ref) < 1e-12
+    back, _ = e.fft_sphere(+1, grid=grid)
+    assert rel(back, coef) < 1e-12
+
+
+def test_reference_energy_on_gpu():
+    """The 1-water reference run (tests/1_water/wf_opt: MT psp, Teter93,
+    80 Ry, 108^3) through the GPU path: E_tot within 1e-6 Ha/atom."""
+    s = load_fixture("water1_mt")
+    e = Engine(s, FP64)
+    g = e.gvectors()
+    tp = 2 * np.pi / s.alat
+    e.set_wfn(start_coefficients(g["hg"][: e.ngpw], tp, e.nstate))
+    e.ortho()
+    n, en, gm = e.wfn_opt(600, 1e-7)
+    ref = golden()["water1_mt"]["energies"]
+    assert abs(en["etotal"] - ref["etotal"]) < 1e-6 * s.nat
+    assert abs(en["esr"] - ref["esr"]) < 1e-9 and abs(en["eself"] - ref["eself"]) < 1e-9
