@@ -101,6 +101,15 @@ struct amdk_ctx {
   double *d_gam = nullptr;
   int *d_info = nullptr;
   double *d_part = nullptr, *d_scal = nullptr, *d_force = nullptr, *d_esr = nullptr, *d_fsr = nullptr;
+  // live per-kernel timing (CUDA events on the context stream)
+  long nlaunch = 0;  // kernels of this library launched on the context stream
+  bool prof = false;
+  struct Rec { int kind; double bytes; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evpool;
+  size_t evused = 0;
+  long kt_count[8] = {0};
+  double kt_ms[8] = {0}, kt_bytes[8] = {0};
   // host copies of scalars
   double esr = 0, eself = 0;
   bool tfor = false;
@@ -117,6 +126,39 @@ struct amdk_ctx {
     return 0;
   }
 };
+
+// kernel classes timed in profiling mode
+enum { KT_ZVPSI = 0, KT_ZDENS, KT_Y, KT_X, KT_UNPACK, KT_DGEMM, KT_OTHER, KT_N };
+
+static void prof_begin(amdk_ctx *c, int kind, double bytes) {
+  if (!c->prof) return;
+  if (c->evused == c->evpool.size()) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    c->evpool.push_back({a, b});
+  }
+  auto &e = c->evpool[c->evused++];
+  cudaEventRecord(e.first, c->st);
+  c->recs.push_back({kind, bytes, e.first, e.second});
+}
+static void prof_end(amdk_ctx *c) {
+  if (!c->prof) return;
+  cudaEventRecord(c->recs.back().b, c->st);
+}
+// after a stream synchronisation: fold the recorded intervals into the totals
+static void prof_harvest(amdk_ctx *c) {
+  if (!c->prof) return;
+  for (auto &r : c->recs) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    c->kt_count[r.kind]++;
+    c->kt_ms[r.kind] += ms;
+    c->kt_bytes[r.kind] += r.bytes;
+  }
+  c->recs.clear();
+  c->evused = 0;
+}
 
 // scalar slots in d_scal
 enum { S_GG = 0, S_GGPREV, S_EH, S_ELOC, S_EXC, S_EKIN, S_ENL, S_GMAX, S_NSCAL = 16 };
@@ -178,27 +220,41 @@ static long sstride(amdk_ctx *c, int sphere) { return (long)c->geom.nz[sphere] *
 template <typename C> static void y_pass(amdk_ctx *c, int sphere, int dir, int T) {
   const Geom &g = c->geom;
   dim3 grid((g.n1 + TX - 1) / TX, g.nz[sphere], T);
+  prof_begin(c, KT_Y, (double)T * (rstride(c, sphere) + sstride(c, sphere)) * sizeof(C));
+  ++c->nlaunch;
   k_y<C><<<grid, NTHR, yz_smem<C>(g.n2), c->st>>>(sphere, dir, g, plan<C>(c, 1), (C *)c->d_rb, (C *)c->d_sb,
                                                  rstride(c, sphere), sstride(c, sphere));
+  prof_end(c);
 }
 template <typename C, int MODE>
 static void z_pass(amdk_ctx *c, int sphere, int T, double2 *cg, const double *rg, int pair0 = 0) {
   const Geom &g = c->geom;
   dim3 grid((g.n1 + TX - 1) / TX, g.n2, MODE == Z_DENSITY ? 1 : T);
   long gs = (long)g.n1 * g.n2 * g.n3;
+  // algorithmic bytes: slab planes in (and out for VPSI), V once, rho read+write once
+  double slab = (double)T * sstride(c, sphere) * sizeof(C);
+  if (MODE == Z_VPSI) prof_begin(c, KT_ZVPSI, 2.0 * slab + gs * 8.0);
+  else if (MODE == Z_DENSITY) prof_begin(c, KT_ZDENS, slab + 2.0 * gs * 8.0);
+  else prof_begin(c, KT_OTHER, 0.0);
+  ++c->nlaunch;
   k_z<C, MODE><<<grid, NTHR, yz_smem<C>(g.n3), c->st>>>(sphere, T, g, plan<C>(c, 2), (C *)c->d_sb, sstride(c, sphere),
                                                         cg, rg, gs, c->d_vpot, c->d_rho, c->d_wa + pair0, c->d_wb + pair0);
+  prof_end(c);
 }
 template <typename C> static void x_fwd(amdk_ctx *c, int sphere, int T) {
   const Geom &g = c->geom;
   long lines = (long)T * g.nray[sphere];
+  prof_begin(c, KT_X, 2.0 * lines * g.n1 * sizeof(C));
+  ++c->nlaunch;
   k_x_fwd<C><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(sphere, T, g, plan<C>(c, 0), (C *)c->d_rb);
+  prof_end(c);
 }
 
 // T fields on the density sphere (fp at +G, fm at -G) -> real or complex grids
 static int field_to_grid(amdk_ctx *c, int T, const double2 *fp, const double2 *fm, double2 *cgrid) {
   const Geom &g = c->geom;
   long lines = (long)T * g.nray[1];
+  ++c->nlaunch;
   k_x_bwd_field<double2><<<nblk(lines, LX), NTHR, x_smem<double2>(g.n1), c->st>>>(fp, fm, g.ngrho, 1, T, g, c->pd[0],
                                                                                   (double2 *)c->d_rb);
   y_pass<double2>(c, 1, +1, T);
@@ -216,6 +272,7 @@ static int grid_to_rays(amdk_ctx *c, int T, const double2 *cgrid, const double *
 
 // ------------------------------------------------------------------ routines
 static int finish_sums(amdk_ctx *c, int nk, int slot) {
+  ++c->nlaunch;
   k_finish_sum<<<nk, NTHR, 0, c->st>>>(c->d_part, RED_BLOCKS, c->d_scal + slot, nk);
   return 0;
 }
@@ -227,6 +284,7 @@ template <typename C> static int density_t(amdk_ctx *c) {
   for (int p0 = 0; p0 < c->npairs; p0 += c->batch) {
     int T = std::min(c->batch, c->npairs - p0);
     long lines = (long)T * g.nray[0];
+    ++c->nlaunch;
     k_x_bwd_pair<C><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(c->d_c0, h.ngpw, c->nstate, 2 * p0, T, g,
                                                                       plan<C>(c, 0), (C *)c->d_rb);
     y_pass<C>(c, 0, +1, T);
@@ -235,6 +293,7 @@ template <typename C> static int density_t(amdk_ctx *c) {
   // rhor2g (density.f90:128-150)
   RC(grid_to_rays(c, 1, nullptr, c->d_rho));
   double scale = 1.0 / ((double)g.n1 * g.n2 * g.n3);
+  ++c->nlaunch;
   k_gather_p<double2><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_posp, (double2 *)c->d_rb, scale, c->d_rhog);
   CK(cudaGetLastError());
   return 0;
@@ -250,21 +309,26 @@ static int do_potential(amdk_ctx *c) {
   const Geom &g = c->geom;
   long npt = (long)g.n1 * g.n2 * g.n3;
   // eval_pot in G space and E_H, E_loc sums
+  ++c->nlaunch;
   k_vloc_g<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngrho, c->d_hg, h.tpiba2, c->d_rhog, c->d_erhos, c->d_evps, c->d_vg,
                                            c->d_part);
   RC(finish_sums(c, 2, S_EH));
   int gga = (h.xc == AMDK_XC_PBE);
   double2 *g0 = c->d_cgrid, *g1 = c->d_cgrid + npt;
   if (gga) {
+    ++c->nlaunch;
     k_grad_fields<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_gvec, h.tpiba, c->d_rhog, c->d_fp, c->d_fm);
     RC(field_to_grid(c, 2, c->d_fp, c->d_fm, c->d_cgrid));
   }
+  ++c->nlaunch;
   k_xc<<<RED_BLOCKS, NTHR, 0, c->st>>>(npt, h.xc, c->d_rho, g0, g1, c->d_part);
   RC(finish_sums(c, 1, S_EXC));
   RC(grid_to_rays(c, gga ? 2 : 1, c->d_cgrid, nullptr));
   double scale = 1.0 / (double)npt;
+  ++c->nlaunch;
   k_xc_combine<double2><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, gga, c->d_posp, c->d_posm, (double2 *)c->d_rb,
                                                            rstride(c, 1), scale, c->d_gvec, h.tpiba, c->d_vg, c->d_vxg);
+  ++c->nlaunch;
   k_conj_field<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_vxg, c->d_fm);
   RC(field_to_grid(c, 1, c->d_vxg, c->d_fm, c->d_cgrid));
   // V(r) = Re of the backward transform (xc.f90:299-301)
@@ -281,6 +345,7 @@ template <typename C> static int apply_h_t(amdk_ctx *c) {
   for (int p0 = 0; p0 < c->npairs; p0 += c->batch) {
     int T = std::min(c->batch, c->npairs - p0);
     long lines = (long)T * g.nray[0];
+    ++c->nlaunch;
     k_x_bwd_pair<C><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(c->d_c0, h.ngpw, c->nstate, 2 * p0, T, g,
                                                                       plan<C>(c, 0), (C *)c->d_rb);
     y_pass<C>(c, 0, +1, T);
@@ -288,6 +353,7 @@ template <typename C> static int apply_h_t(amdk_ctx *c) {
     y_pass<C>(c, 0, -1, T);
     x_fwd<C>(c, 0, T);
     dim3 gu(nblk(h.ngpw), T);
+    ++c->nlaunch;
     k_unpack_vpsi<C><<<gu, NTHR, 0, c->st>>>(h.ngpw, c->nstate, 2 * p0, T, c->d_posp, c->d_posm, (C *)c->d_rb,
                                              rstride(c, 0), scale, c->d_hg, h.tpiba2, c->d_occ, c->d_c0, c->d_c2);
   }
@@ -312,11 +378,13 @@ static int do_energy(amdk_ctx *c, amdk_energies *e) {
   const HostSetup &h = c->hs;
   RC(do_fnl(c));
   if (c->nproj) {
+    ++c->nlaunch;
     k_nl_energy_d<<<RED_BLOCKS, NTHR, 0, c->st>>>(c->nproj, c->nstate, c->d_nl, c->d_hn, c->d_occ, c->d_D, c->d_part);
     RC(finish_sums(c, 1, S_ENL));
   } else {
     CK(cudaMemsetAsync(c->d_scal + S_ENL, 0, sizeof(double), c->st));
   }
+  ++c->nlaunch;
   k_ekin<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngpw, c->nstate, c->d_c0, c->d_hg, c->d_occ, c->d_part);
   RC(finish_sums(c, 1, S_EKIN));
   if (e) {
@@ -347,6 +415,7 @@ static int do_fnonloc(amdk_ctx *c) {
   int K = 2 * h.ngpw;
   CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, K, c->nstate, c->nproj, &one, (const double *)c->d_P, K, c->d_D,
                  c->nproj, &one, (double *)c->d_c2, K));
+  ++c->nlaunch;
   k_fnonloc_g0<<<nblk(c->nstate), NTHR, 0, c->st>>>(c->nproj, c->nstate, h.ngpw, c->d_P, c->d_D, c->d_c2);
   CK(cudaGetLastError());
   return 0;
@@ -365,14 +434,18 @@ static int do_gradient(amdk_ctx *c) {
   const double two = 2.0, one = 1.0, mone = -1.0, zero = 0.0;
   CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, (const double *)c->d_c2, K, (const double *)c->d_c0, K,
                  &zero, c->d_gam, n));
+  ++c->nlaunch;
   k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c2, c->d_c0, c->d_gam, c->d_occ, 1, 0);
   CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &mone, (const double *)c->d_c0, K, c->d_gam, n, &one,
                  (double *)c->d_c2, K));
+  ++c->nlaunch;
   k_zclean<<<nblk(n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c2);
   int nocc = 0;
   for (int i = 0; i < n; i++)
     if (h.occ[i] > 1e-5) nocc++;
+  ++c->nlaunch;
   k_gmax<<<RED_BLOCKS, NTHR, 0, c->st>>>((long)nocc * h.ngpw, c->d_c2, c->d_part);
+  ++c->nlaunch;
   k_finish_max<<<1, NTHR, 0, c->st>>>(c->d_part, RED_BLOCKS, c->d_scal + S_GMAX);
   CK(cudaGetLastError());
   return 0;
@@ -384,9 +457,12 @@ static int do_pcg(amdk_ctx *c, int istep) {
   for (int i = 0; i < n; i++)
     if (h.occ[i] > 1e-5) nocc++;
   long tot = (long)h.ngpw * n;
+  ++c->nlaunch;
   k_precon<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngpw, n, nocc, c->d_vpp, c->d_occ, c->d_c2, c->d_cp, c->d_part);
   RC(finish_sums(c, 1, S_GG));
+  ++c->nlaunch;
   k_pcg_update<<<RED_BLOCKS * 4, NTHR, 0, c->st>>>(tot, istep, c->d_scal, c->d_cp, c->d_hnm1, c->d_c0);
+  ++c->nlaunch;
   k_copy_scalar<<<1, 1, 0, c->st>>>(c->d_scal + S_GG, c->d_scal + S_GGPREV);
   CK(cudaGetLastError());
   return 0;
@@ -397,9 +473,11 @@ static int do_ortho(amdk_ctx *c) {
   int n = c->nstate, K = 2 * h.ngpw;
   const double two = 2.0, zero = 0.0, one = 1.0;
   CB(cublasDsyrk(c->cb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, n, K, &two, (const double *)c->d_c0, K, &zero, c->d_gam, n));
+  ++c->nlaunch;
   k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c0, c->d_c0, c->d_gam, c->d_occ, 0, 1);
   size_t sm = (size_t)n * n * sizeof(double);
   if (sm > 200 * 1024) sm = 0;
+  ++c->nlaunch;
   k_cholesky_upper<<<1, 1024, sm, c->st>>>(n, c->d_gam, c->d_info);
   int info = 0;
   CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
@@ -410,6 +488,7 @@ static int do_ortho(amdk_ctx *c) {
   }
   CB(cublasDtrsm(c->cb, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, K, n, &one, c->d_gam,
                  n, (double *)c->d_c0, K));
+  ++c->nlaunch;
   k_zclean<<<nblk(n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c0);
   CK(cudaGetLastError());
   return 0;
@@ -434,15 +513,19 @@ static int do_positions(amdk_ctx *c, const double *atco) {
   CK(cudaMemcpyAsync(c->d_atco, h.atco.data(), sizeof(double) * h.atco.size(), cudaMemcpyHostToDevice, c->st));
   AtomArgs aa{c->d_atarg, c->d_isa_is};
   int nh1 = h.nr[0] / 2 + 1, nh2 = h.nr[1] / 2 + 1, nh3 = h.nr[2] / 2 + 1;
+  ++c->nlaunch;
   k_sfac_sums<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, h.nat, c->d_inyh, nh1, nh2, nh3, aa, c->d_vps, c->d_rhos,
                                                  c->d_evps, c->d_erhos);
   if (c->nproj) {
     ProjArgs pa{c->d_pisa, c->d_pis, c->d_piv, c->d_pl, h.nghmax};
+    ++c->nlaunch;
     k_projectors<<<dim3(nblk(h.ngpw), c->nproj), NTHR, 0, c->st>>>(h.ngpw, c->nproj, c->d_inyh, nh1, nh2, nh3, aa, pa,
                                                                    c->d_twnl, c->d_P);
   }
+  ++c->nlaunch;
   k_hess<<<nblk(h.ngpw), NTHR, 0, c->st>>>(h.ngpw, c->d_hg, h.tpiba2, c->d_evps, c->d_twnl, h.nsp, h.nghmax, c->d_na,
                                            c->d_ngh, c->d_wsg, c->d_vpp);
+  ++c->nlaunch;
   k_esr<<<1, 32, 0, c->st>>>(h.nsp, c->d_na, h.na_max, c->d_zv, c->d_atco, h.alat, h.symmetry, 1, c->d_fsr, c->d_esr);
   CK(cudaMemcpyAsync(&c->esr, c->d_esr, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -459,15 +542,18 @@ static int do_ionic_forces(amdk_ctx *c) {
   AtomArgs aa{c->d_atarg, c->d_isa_is};
   int nh1 = h.nr[0] / 2 + 1, nh2 = h.nr[1] / 2 + 1, nh3 = h.nr[2] / 2 + 1;
   double omtp = 2.0 * h.omega * h.tpiba;
+  ++c->nlaunch;
   k_potfor<<<dim3(pnb, h.nat), NTHR, 0, c->st>>>(h.ngrho, c->d_inyh, nh1, nh2, nh3, aa, c->d_hg, c->d_gvec, h.tpiba2,
                                                  c->d_rhog, c->d_erhos, c->d_vps, c->d_rhos, omtp, c->d_part);
   if (c->nproj) {
+    ++c->nlaunch;
     k_dproj<<<dim3(nblk(h.ngpw), c->nproj, 3), NTHR, 0, c->st>>>(h.ngpw, c->nproj, c->d_gvec, c->d_P, c->d_Q);
     const double tfac = 2.0 * h.tpiba, zero = 0.0;
     int K = 2 * h.ngpw;
     CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, 3 * c->nproj, c->nstate, K, &tfac, (const double *)c->d_Q, K,
                    (const double *)c->d_c0, K, &zero, c->d_dfnl, 3 * c->nproj));
   }
+  ++c->nlaunch;
   k_force_total<<<h.nat, NTHR, 0, c->st>>>(h.nat, c->nproj, c->nstate, c->d_pisa, c->d_hn, c->d_dfnl, c->d_occ, c->d_part,
                                            pnb, c->d_isa_is, c->d_isa_ia, h.na_max, c->d_force);
   CK(cudaGetLastError());
@@ -608,6 +694,7 @@ static int build_device(amdk_ctx *c) {
       CK(cudaMemcpy(yp, h.voo[is].data(), sizeof(double) * NSPLN, cudaMemcpyHostToDevice));
       CK(cudaMemcpy(hh, hv.data(), sizeof(double) * (NSPLN + 1), cudaMemcpyHostToDevice));
       CK(cudaMemcpy(sd, sdd.data(), sizeof(double) * (NSPLN + 1), cudaMemcpyHostToDevice));
+      ++c->nlaunch;
       k_vps_rhos<<<nblk(h.ngrho), NTHR>>>(h.ngrho, c->d_hg, xp, yp, hh, sd, NSPLN, (double)h.zv[is], h.omega, h.tpiba2,
                                            c->d_vps + (size_t)is * h.ngrho, c->d_rhos + (size_t)is * h.ngrho);
       CK(cudaDeviceSynchronize());
@@ -621,6 +708,7 @@ static int build_device(amdk_ctx *c) {
         CK(cudaMemcpy(yp, w, sizeof(double) * NSPLN, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(hh, hv.data(), sizeof(double) * (NSPLN + 1), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(sd, sdd.data(), sizeof(double) * (NSPLN + 1), cudaMemcpyHostToDevice));
+        ++c->nlaunch;
         k_twnl<<<nblk(h.ngpw), NTHR>>>(h.ngpw, c->d_hg, c->d_gvec, xp, yp, hh, sd, NSPLN, h.lpval[is][iv], vol,
                                         c->d_twnl + ((size_t)is * h.nghmax + iv) * h.ngpw);
         CK(cudaDeviceSynchronize());
@@ -743,6 +831,10 @@ int amdk_destroy(amdk_ctx *c) {
   cudaSetDevice(c->device);
   if (c->st) cudaStreamSynchronize(c->st);
   for (void *p : c->allocs) cudaFree(p);
+  for (auto &e : c->evpool) {
+    cudaEventDestroy(e.first);
+    cudaEventDestroy(e.second);
+  }
   if (c->cb) cublasDestroy(c->cb);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
@@ -894,6 +986,7 @@ int amdk_scf_iteration(amdk_ctx *c, int istep, double gcut, amdk_energies *e, do
   float ms = 0;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
   c->last_ms = ms;
+  prof_harvest(c);
   if (e) *e = en;
   if (gemax) *gemax = gm;
   if (converged) *converged = gm < gcut;
@@ -954,18 +1047,51 @@ int amdk_fft_sphere(amdk_ctx *c, int sign, double *coef, double *grid) {
   long npt = (long)h.nr[0] * h.nr[1] * h.nr[2];
   if (sign == -1) {
     CK(cudaMemcpyAsync(c->d_vxg, coef, sizeof(double2) * h.ngrho, cudaMemcpyHostToDevice, c->st));
+    ++c->nlaunch;
     k_conj_field<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_vxg, c->d_fm);
     RC(field_to_grid(c, 1, c->d_vxg, c->d_fm, c->d_cgrid));
     CK(cudaMemcpyAsync(grid, c->d_cgrid, sizeof(double2) * npt, cudaMemcpyDeviceToHost, c->st));
   } else {
     CK(cudaMemcpyAsync(c->d_cgrid, grid, sizeof(double2) * npt, cudaMemcpyHostToDevice, c->st));
     RC(grid_to_rays(c, 1, c->d_cgrid, nullptr));
+    ++c->nlaunch;
     k_gather_p<double2><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_posp, (double2 *)c->d_rb, 1.0 / (double)npt,
                                                            c->d_vxg);
     CK(cudaMemcpyAsync(coef, c->d_vxg, sizeof(double2) * h.ngrho, cudaMemcpyDeviceToHost, c->st));
   }
   CK(cudaStreamSynchronize(c->st));
   CK(cudaGetLastError());
+  return 0;
+}
+
+int amdk_profile(amdk_ctx *c, int enable) {
+  if (!c) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  CK(cudaStreamSynchronize(c->st));
+  prof_harvest(c);
+  c->prof = enable != 0;
+  for (int k = 0; k < KT_N; k++) {
+    c->kt_count[k] = 0;
+    c->kt_ms[k] = 0;
+    c->kt_bytes[k] = 0;
+  }
+  return 0;
+}
+
+int amdk_profile_get(amdk_ctx *c, int kind, long *launches, double *total_ms, double *bytes) {
+  if (!c || kind < 0 || kind >= KT_N) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  CK(cudaStreamSynchronize(c->st));
+  prof_harvest(c);
+  if (launches) *launches = c->kt_count[kind];
+  if (total_ms) *total_ms = c->kt_ms[kind];
+  if (bytes) *bytes = c->kt_bytes[kind];
+  return 0;
+}
+
+int amdk_launch_count(amdk_ctx *c, long *n) {
+  if (!c || !n) return AMDK_ERR_BADARG;
+  *n = c->nlaunch;
   return 0;
 }
 

@@ -92,6 +92,9 @@ def load_library(path: str = LIBPATH):
     lib.amdk_get_array.argtypes = [P, C.c_char_p, P, C.c_size_t]
     lib.amdk_fft_sphere.argtypes = [P, C.c_int, P, P]
     lib.amdk_last_iteration_ms.argtypes = [P, C.POINTER(C.c_double)]
+    lib.amdk_profile.argtypes = [P, C.c_int]
+    lib.amdk_launch_count.argtypes = [P, C.POINTER(C.c_long)]
+    lib.amdk_profile_get.argtypes = [P, C.c_int, C.POINTER(C.c_long), C.POINTER(C.c_double), C.POINTER(C.c_double)]
     _LIB = lib
     return lib
 
@@ -275,6 +278,21 @@ class Engine:
         m = C.c_double()
         self.lib.amdk_last_iteration_ms(self.h, C.byref(m))
         return m.value
+
+    KERNELS = {0: "z_vpsi", 1: "z_density", 2: "y_pass", 3: "x_fwd"}
+
+    def launch_count(self) -> int:
+        n = C.c_long()
+        _check(self.lib.amdk_launch_count(self.h, C.byref(n)), "amdk_launch_count")
+        return n.value
+
+    def profile(self, enable: bool):
+        _check(self.lib.amdk_profile(self.h, int(enable)), "amdk_profile")
+
+    def profile_get(self, kind: int):
+        n, ms, b = C.c_long(), C.c_double(), C.c_double()
+        _check(self.lib.amdk_profile_get(self.h, kind, C.byref(n), C.byref(ms), C.byref(b)), "amdk_profile_get")
+        return n.value, ms.value, b.value
 
     def ionic_forces(self) -> np.ndarray:
         s = self.system

@@ -160,6 +160,18 @@ int amdk_get_array(amdk_ctx *ctx, const char *name, void *dst, size_t bytes);
  *          (nr3*nr2*nr1 complex); sign=+1: grid -> coef = F(+G)/N. */
 int amdk_fft_sphere(amdk_ctx *ctx, int sign, double *coef, double *grid);
 
+/* Live kernel timing with CUDA events on the context stream (no
+ * counterpart in the reference, whose only tracing is cpu_time per CG
+ * iteration, do_opt.f90:81,118).  kind: 0 fused z pass of H|psi>, 1 fused
+ * z pass of the density, 2 y passes, 3 forward x passes.  bytes = the
+ * algorithmic bytes of the timed launches. */
+int amdk_profile(amdk_ctx *ctx, int enable);
+int amdk_profile_get(amdk_ctx *ctx, int kind, long *launches, double *total_ms, double *bytes);
+
+/* Number of this library's kernels launched so far on the context (cuBLAS
+ * kernels are not counted). */
+int amdk_launch_count(amdk_ctx *ctx, long *n);
+
 /* Elapsed device time of the last amdk_scf_iteration, milliseconds. */
 int amdk_last_iteration_ms(amdk_ctx *ctx, double *ms);
 
