@@ -1089,6 +1089,96 @@ int amdk_profile_get(amdk_ctx *c, int kind, long *launches, double *total_ms, do
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// amdk_fft_sphere_noalloc: the density-sphere FFT for callers that cannot
+// allocate device memory.  Its scratch (the ray buffer, the slab buffer and
+// the -G field of one FP64 transform) lives in this file-scope array, which
+// every GPU that loads the library holds until the process exits.  Host code
+// must not pass the array's name to a kernel: on the host that name is only a
+// stand-in, so the device address is looked up once per device with
+// cudaGetSymbolAddress and cached.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = (size_t)24 << 20;  // 24 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+static std::mutex g_noalloc_mu;
+constexpr int kNoAllocMaxDevices = 128;
+static void *g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on `device` (which must be current).
+static int noalloc_scratch(int device, unsigned char **out) {
+  if (device < 0 || device >= kNoAllocMaxDevices) {
+    set_error("amdk_fft_sphere_noalloc: device ordinal out of range");
+    return AMDK_ERR_BADARG;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      set_error(std::string("amdk_fft_sphere_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+      return AMDK_ERR_CUDA;
+    }
+    g_noalloc_addr[device] = p;
+  }
+  *out = (unsigned char *)g_noalloc_addr[device];
+  return 0;
+}
+
+int amdk_fft_sphere_noalloc(amdk_ctx *c, int sign, double *coef, double *grid) {
+  if (!c || !coef || !grid || (sign != 1 && sign != -1)) {
+    set_error("amdk_fft_sphere_noalloc: null pointer or sign not +-1");
+    return AMDK_ERR_BADARG;
+  }
+  CK(cudaSetDevice(c->device));
+  const HostSetup &h = c->hs;
+  const Geom &g = c->geom;
+  auto round256 = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t rbytes = round256((size_t)rstride(c, 1) * sizeof(double2));
+  const size_t sbytes = round256((size_t)sstride(c, 1) * sizeof(double2));
+  const size_t fbytes = round256((size_t)h.ngrho * sizeof(double2));
+  if (rbytes + sbytes + fbytes > kNoAllocScratchBytes) {
+    set_error("amdk_fft_sphere_noalloc: this grid needs " + std::to_string(rbytes + sbytes + fbytes) +
+              " bytes of scratch; the fixed maximum is " + std::to_string(kNoAllocScratchBytes) +
+              " bytes (use amdk_fft_sphere)");
+    return AMDK_ERR_UNSUPPORTED;
+  }
+  unsigned char *base = nullptr;
+  RC(noalloc_scratch(c->device, &base));
+  double2 *R = (double2 *)base;
+  double2 *S = (double2 *)(base + rbytes);
+  double2 *FM = (double2 *)(base + rbytes + sbytes);
+  const long npt = (long)g.n1 * g.n2 * g.n3;
+  const long lines = (long)g.nray[1];
+  const dim3 gy((g.n1 + TX - 1) / TX, g.nz[1], 1), gz((g.n1 + TX - 1) / TX, g.n2, 1);
+  if (sign == -1) {
+    // coef (+G half) -> complex grid; the -G values are conj(coef)
+    ++c->nlaunch;
+    k_conj_field<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, (const double2 *)coef, FM);
+    ++c->nlaunch;
+    k_x_bwd_field<double2><<<nblk(lines, LX), NTHR, x_smem<double2>(g.n1), c->st>>>(
+        (const double2 *)coef, FM, g.ngrho, 1, 1, g, c->pd[0], R);
+    ++c->nlaunch;
+    k_y<double2><<<gy, NTHR, yz_smem<double2>(g.n2), c->st>>>(1, +1, g, c->pd[1], R, S, rstride(c, 1), sstride(c, 1));
+    ++c->nlaunch;
+    k_z<double2, Z_TO_GRID><<<gz, NTHR, yz_smem<double2>(g.n3), c->st>>>(
+        1, 1, g, c->pd[2], S, sstride(c, 1), (double2 *)grid, nullptr, npt, nullptr, nullptr, nullptr, nullptr);
+  } else {
+    // complex grid -> coef = F(+G)/N
+    ++c->nlaunch;
+    k_z<double2, Z_FROM_GRID_CPLX><<<gz, NTHR, yz_smem<double2>(g.n3), c->st>>>(
+        1, 1, g, c->pd[2], S, sstride(c, 1), (double2 *)grid, nullptr, npt, nullptr, nullptr, nullptr, nullptr);
+    ++c->nlaunch;
+    k_y<double2><<<gy, NTHR, yz_smem<double2>(g.n2), c->st>>>(1, -1, g, c->pd[1], R, S, rstride(c, 1), sstride(c, 1));
+    ++c->nlaunch;
+    k_x_fwd<double2><<<nblk(lines, LX), NTHR, x_smem<double2>(g.n1), c->st>>>(1, 1, g, c->pd[0], R);
+    ++c->nlaunch;
+    k_gather_p<double2><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_posp, R, 1.0 / (double)npt, (double2 *)coef);
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
 int amdk_launch_count(amdk_ctx *c, long *n) {
   if (!c || !n) return AMDK_ERR_BADARG;
   *n = c->nlaunch;

@@ -172,6 +172,20 @@ int amdk_profile_get(amdk_ctx *ctx, int kind, long *launches, double *total_ms, 
  * kernels are not counted). */
 int amdk_launch_count(amdk_ctx *ctx, long *n);
 
+/* amdk_fft_sphere for callers that cannot allocate device memory (an
+ * application that hands every device allocation to its own pool, or a
+ * Fortran code whose device memory is managed by OpenACC/OpenMP runtimes):
+ * no counterpart in the reference.  coef (ngrho complex) and grid
+ * (nr3*nr2*nr1 complex) are DEVICE pointers owned by the caller; the call
+ * allocates nothing.  Its scratch is one fixed 24 MiB device array inside the
+ * library (held by every GPU that loads it), which limits it to grids whose
+ * density-sphere transform fits (about 90^3); larger grids return
+ * AMDK_ERR_UNSUPPORTED.  The first call on a device looks up the array's
+ * device address, so make that first call before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU (several contexts or
+ * threads at once) race.  Returns after the transform has finished. */
+int amdk_fft_sphere_noalloc(amdk_ctx *ctx, int sign, double *coef, double *grid);
+
 /* Elapsed device time of the last amdk_scf_iteration, milliseconds. */
 int amdk_last_iteration_ms(amdk_ctx *ctx, double *ms);
 
