@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -98,7 +99,7 @@ struct amdk_ctx {
   double2 *d_c0 = nullptr, *d_c2 = nullptr, *d_cp = nullptr, *d_hnm1 = nullptr;
   double *d_rho = nullptr, *d_vpot = nullptr;
   double2 *d_rhog = nullptr, *d_vg = nullptr, *d_vxg = nullptr, *d_fp = nullptr, *d_fm = nullptr, *d_cgrid = nullptr;
-  double *d_gam = nullptr;
+  double *d_gam = nullptr, *d_uinv = nullptr;
   int *d_info = nullptr;
   double *d_part = nullptr, *d_scal = nullptr, *d_force = nullptr, *d_esr = nullptr, *d_fsr = nullptr;
   // live per-kernel timing (CUDA events on the context stream)
@@ -193,8 +194,31 @@ template <typename C> static int make_plan(amdk_ctx *c, int n, Plan<C> &p) {
 }
 
 // ------------------------------------------------------------------ FFT driver
-template <typename C> static size_t x_smem(int n1) { return 2 * (size_t)n1 * (LX + 1) * sizeof(C); }
-template <typename C> static size_t yz_smem(int n) { return 2 * (size_t)n * TX * sizeof(C); }
+// FFT lengths with compile-time specialised kernels (the grid sizes of the
+// reference's set_r_grids for the configurations of interest); any other
+// 2,3,5-smooth length runs the run-time-length kernels.
+template <typename F> static void with_n(int n, F &&f) {
+  switch (n) {
+#define AMDK_NCASE(v) \
+  case v: f(std::integral_constant<int, v>{}); break;
+    AMDK_NCASE(36) AMDK_NCASE(48) AMDK_NCASE(64) AMDK_NCASE(72) AMDK_NCASE(80) AMDK_NCASE(90) AMDK_NCASE(96)
+    AMDK_NCASE(100) AMDK_NCASE(108) AMDK_NCASE(120) AMDK_NCASE(128) AMDK_NCASE(144) AMDK_NCASE(160)
+#undef AMDK_NCASE
+    default: f(std::integral_constant<int, 0>{}); break;
+  }
+}
+// opt every kernel instantiation into the large dynamic shared memory once
+// (one flag per kernel: the kernel itself is the template argument)
+template <auto K> static void smem_opt_in() {
+  static bool done = []() {
+    cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    return true;
+  }();
+  (void)done;
+}
+
+template <typename C> static size_t x_smem(int n1) { return 2 * (size_t)n1 * (LX + 1) * sizeof(C) + n1 * sizeof(C); }
+template <typename C> static size_t yz_smem(int n) { return 2 * (size_t)n * TX * sizeof(C) + n * sizeof(C); }
 
 template <typename C> static void set_smem_attrs() {
   int mx = 227 * 1024;
@@ -222,8 +246,12 @@ template <typename C> static void y_pass(amdk_ctx *c, int sphere, int dir, int T
   dim3 grid((g.n1 + TX - 1) / TX, g.nz[sphere], T);
   prof_begin(c, KT_Y, (double)T * (rstride(c, sphere) + sstride(c, sphere)) * sizeof(C));
   ++c->nlaunch;
-  k_y<C><<<grid, NTHR, yz_smem<C>(g.n2), c->st>>>(sphere, dir, g, plan<C>(c, 1), (C *)c->d_rb, (C *)c->d_sb,
-                                                 rstride(c, sphere), sstride(c, sphere));
+  with_n(g.n2, [&](auto NC) {
+    constexpr int N = decltype(NC)::value;
+    smem_opt_in<k_y<C, N>>();
+    k_y<C, N><<<grid, NTHR, yz_smem<C>(g.n2), c->st>>>(sphere, dir, g, plan<C>(c, 1), (C *)c->d_rb, (C *)c->d_sb,
+                                                      rstride(c, sphere), sstride(c, sphere));
+  });
   prof_end(c);
 }
 template <typename C, int MODE>
@@ -237,8 +265,13 @@ static void z_pass(amdk_ctx *c, int sphere, int T, double2 *cg, const double *rg
   else if (MODE == Z_DENSITY) prof_begin(c, KT_ZDENS, slab + 2.0 * gs * 8.0);
   else prof_begin(c, KT_OTHER, 0.0);
   ++c->nlaunch;
-  k_z<C, MODE><<<grid, NTHR, yz_smem<C>(g.n3), c->st>>>(sphere, T, g, plan<C>(c, 2), (C *)c->d_sb, sstride(c, sphere),
-                                                        cg, rg, gs, c->d_vpot, c->d_rho, c->d_wa + pair0, c->d_wb + pair0);
+  with_n(g.n3, [&](auto NC) {
+    constexpr int N = decltype(NC)::value;
+    smem_opt_in<k_z<C, MODE, N>>();
+    k_z<C, MODE, N><<<grid, NTHR, yz_smem<C>(g.n3), c->st>>>(sphere, T, g, plan<C>(c, 2), (C *)c->d_sb,
+                                                             sstride(c, sphere), cg, rg, gs, c->d_vpot, c->d_rho,
+                                                             c->d_wa + pair0, c->d_wb + pair0);
+  });
   prof_end(c);
 }
 template <typename C> static void x_fwd(amdk_ctx *c, int sphere, int T) {
@@ -246,7 +279,11 @@ template <typename C> static void x_fwd(amdk_ctx *c, int sphere, int T) {
   long lines = (long)T * g.nray[sphere];
   prof_begin(c, KT_X, 2.0 * lines * g.n1 * sizeof(C));
   ++c->nlaunch;
-  k_x_fwd<C><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(sphere, T, g, plan<C>(c, 0), (C *)c->d_rb);
+  with_n(g.n1, [&](auto NC) {
+    constexpr int N = decltype(NC)::value;
+    smem_opt_in<k_x_fwd<C, N>>();
+    k_x_fwd<C, N><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(sphere, T, g, plan<C>(c, 0), (C *)c->d_rb);
+  });
   prof_end(c);
 }
 
@@ -255,8 +292,12 @@ static int field_to_grid(amdk_ctx *c, int T, const double2 *fp, const double2 *f
   const Geom &g = c->geom;
   long lines = (long)T * g.nray[1];
   ++c->nlaunch;
-  k_x_bwd_field<double2><<<nblk(lines, LX), NTHR, x_smem<double2>(g.n1), c->st>>>(fp, fm, g.ngrho, 1, T, g, c->pd[0],
-                                                                                  (double2 *)c->d_rb);
+  with_n(g.n1, [&](auto NC) {
+    constexpr int N = decltype(NC)::value;
+    smem_opt_in<k_x_bwd_field<double2, N>>();
+    k_x_bwd_field<double2, N><<<nblk(lines, LX), NTHR, x_smem<double2>(g.n1), c->st>>>(fp, fm, g.ngrho, 1, T, g,
+                                                                                        c->pd[0], (double2 *)c->d_rb);
+  });
   y_pass<double2>(c, 1, +1, T);
   z_pass<double2, Z_TO_GRID>(c, 1, T, cgrid, nullptr);
   return 0;
@@ -285,8 +326,12 @@ template <typename C> static int density_t(amdk_ctx *c) {
     int T = std::min(c->batch, c->npairs - p0);
     long lines = (long)T * g.nray[0];
     ++c->nlaunch;
-    k_x_bwd_pair<C><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(c->d_c0, h.ngpw, c->nstate, 2 * p0, T, g,
-                                                                      plan<C>(c, 0), (C *)c->d_rb);
+    with_n(g.n1, [&](auto NC) {
+      constexpr int N = decltype(NC)::value;
+      smem_opt_in<k_x_bwd_pair<C, N>>();
+      k_x_bwd_pair<C, N><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(c->d_c0, h.ngpw, c->nstate, 2 * p0, T, g,
+                                                                           plan<C>(c, 0), (C *)c->d_rb);
+    });
     y_pass<C>(c, 0, +1, T);
     z_pass<C, Z_DENSITY>(c, 0, T, nullptr, nullptr, p0);
   }
@@ -346,8 +391,12 @@ template <typename C> static int apply_h_t(amdk_ctx *c) {
     int T = std::min(c->batch, c->npairs - p0);
     long lines = (long)T * g.nray[0];
     ++c->nlaunch;
-    k_x_bwd_pair<C><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(c->d_c0, h.ngpw, c->nstate, 2 * p0, T, g,
-                                                                      plan<C>(c, 0), (C *)c->d_rb);
+    with_n(g.n1, [&](auto NC) {
+      constexpr int N = decltype(NC)::value;
+      smem_opt_in<k_x_bwd_pair<C, N>>();
+      k_x_bwd_pair<C, N><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(c->d_c0, h.ngpw, c->nstate, 2 * p0, T, g,
+                                                                           plan<C>(c, 0), (C *)c->d_rb);
+    });
     y_pass<C>(c, 0, +1, T);
     z_pass<C, Z_VPSI>(c, 0, T, nullptr, nullptr);
     y_pass<C>(c, 0, -1, T);
@@ -472,13 +521,15 @@ static int do_ortho(amdk_ctx *c) {
   const HostSetup &h = c->hs;
   int n = c->nstate, K = 2 * h.ngpw;
   const double two = 2.0, zero = 0.0, one = 1.0;
-  CB(cublasDsyrk(c->cb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, n, K, &two, (const double *)c->d_c0, K, &zero, c->d_gam, n));
+  // S = 2 Re C0^T C0 - Re c0(0) Re c0(0)^T  (DSYRK + DGER, wfn_initialize.f90:481-482)
+  CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, (const double *)c->d_c0, K, (const double *)c->d_c0, K,
+                 &zero, c->d_gam, n));
   ++c->nlaunch;
   k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c0, c->d_c0, c->d_gam, c->d_occ, 0, 1);
   size_t sm = (size_t)n * n * sizeof(double);
   if (sm > 200 * 1024) sm = 0;
   ++c->nlaunch;
-  k_cholesky_upper<<<1, 1024, sm, c->st>>>(n, c->d_gam, c->d_info);
+  k_chol_inv<<<1, 1024, sm, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
   int info = 0;
   CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -486,8 +537,11 @@ static int do_ortho(amdk_ctx *c) {
     set_error("overlap matrix not positive definite at leading minor " + std::to_string(info));
     return AMDK_ERR_NOT_SPD;
   }
-  CB(cublasDtrsm(c->cb, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, K, n, &one, c->d_gam,
-                 n, (double *)c->d_c0, K));
+  // C0 <- C0 U^{-1} (DTRMM, wfn_initialize.f90:485) as a GEMM into the spare
+  // buffer, then swap the buffers
+  CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, (const double *)c->d_c0, K, c->d_uinv, n, &zero,
+                 (double *)c->d_cp, K));
+  std::swap(c->d_c0, c->d_cp);
   ++c->nlaunch;
   k_zclean<<<nblk(n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c0);
   CK(cudaGetLastError());
@@ -526,7 +580,8 @@ static int do_positions(amdk_ctx *c, const double *atco) {
   k_hess<<<nblk(h.ngpw), NTHR, 0, c->st>>>(h.ngpw, c->d_hg, h.tpiba2, c->d_evps, c->d_twnl, h.nsp, h.nghmax, c->d_na,
                                            c->d_ngh, c->d_wsg, c->d_vpp);
   ++c->nlaunch;
-  k_esr<<<1, 32, 0, c->st>>>(h.nsp, c->d_na, h.na_max, c->d_zv, c->d_atco, h.alat, h.symmetry, 1, c->d_fsr, c->d_esr);
+  k_esr_par<<<1, NTHR, 0, c->st>>>(h.nat, c->d_isa_is, c->d_isa_ia, h.na_max, c->d_zv, c->d_atco, h.alat, h.symmetry,
+                                   c->d_fsr, c->d_esr);
   CK(cudaMemcpyAsync(&c->esr, c->d_esr, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   CK(cudaGetLastError());
@@ -628,6 +683,7 @@ static int build_device(amdk_ctx *c) {
   set_smem_attrs<double2>();
   set_smem_attrs<float2>();
   cudaFuncSetAttribute(k_cholesky_upper, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   // G vectors
   RC(c->up(&c->d_inyh, h.inyh));
   RC(c->up(&c->d_hg, h.hg));
@@ -662,6 +718,7 @@ static int build_device(amdk_ctx *c) {
   RC(c->alloc(&c->d_fp, 2L * h.ngrho));
   RC(c->alloc(&c->d_fm, 2L * h.ngrho));
   RC(c->alloc(&c->d_gam, (size_t)h.nstate * h.nstate));
+  RC(c->alloc(&c->d_uinv, (size_t)h.nstate * h.nstate));
   RC(c->alloc(&c->d_info, 1));
   RC(c->alloc(&c->d_part, (size_t)RED_BLOCKS * 4 + 3L * 64 * h.nat + 64));
   RC(c->alloc(&c->d_scal, S_NSCAL));
@@ -732,6 +789,7 @@ static int build_device(amdk_ctx *c) {
   RC(c->up(&c->d_wsg, wsg));
   RC(c->alloc(&c->d_force, 3L * h.na_max * h.nsp));
   RC(c->alloc(&c->d_fsr, 3L * h.na_max * h.nsp));
+  CK(cudaMemset(c->d_fsr, 0, sizeof(double) * 3L * h.na_max * h.nsp));
   RC(c->alloc(&c->d_esr, 1));
   // projector list (isa-major within a species, as nl(isa,iv) of fnl)
   int isa0 = 0;

@@ -142,6 +142,82 @@ __device__ C *smem_fft(C *a, C *b, int L, int es, const Plan<C> &p, int sg) {
   return a;
 }
 
+// ---------------------------------------------------------------- compile-time FFT
+// The same Stockham schedule with the length known at compile time: every
+// stride, radix and index division is a constant, the radix butterflies live
+// in registers and the twiddles are read from a shared-memory copy.
+__host__ __device__ constexpr int ct_radix(int n) {
+  return (n % 4 == 0) ? 4 : (n % 2 == 0) ? 2 : (n % 3 == 0) ? 3 : (n % 5 == 0) ? 5 : 0;
+}
+__host__ __device__ constexpr int ct_prefix(int n, int st) {
+  int s = 1, m = n;
+  for (int i = 0; i < st; ++i) {
+    const int r = ct_radix(m);
+    s *= r;
+    m /= r;
+  }
+  return s;
+}
+__host__ __device__ constexpr int ct_nstages(int n) {
+  int c = 0;
+  while (n > 1) {
+    n /= ct_radix(n);
+    ++c;
+  }
+  return c;
+}
+
+template <typename C, int N, int L, int ES, int SG, int ST>
+struct CtStage {
+  static __device__ __forceinline__ C *run(C *a, C *b, const C *tw) {
+    if constexpr (ST == ct_nstages(N)) {
+      return a;
+    } else {
+      constexpr int S = ct_prefix(N, ST);
+      constexpr int R = ct_radix(N / S);
+      constexpr int M = N / (S * R);
+      constexpr int NBF = L * (N / R);
+      for (int idx = threadIdx.x; idx < NBF; idx += blockDim.x) {
+        const int l = idx % L;
+        const int bf = idx / L;
+        const int k = bf % S;
+        const int j = bf / S;
+        C v[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = a[(k + S * j + S * M * q) * ES + l];
+        dft_r(v, R, SG);
+        b[(k + S * R * j) * ES + l] = v[0];
+#pragma unroll
+        for (int q = 1; q < R; ++q) {
+          C w = tw[S * j * q];   // S*j*q < S*M*R = N
+          if (SG > 0) w.y = -w.y;
+          b[(k + S * q + S * R * j) * ES + l] = cmul(v[q], w);
+        }
+      }
+      __syncthreads();
+      return CtStage<C, N, L, ES, SG, ST + 1>::run(b, a, tw);
+    }
+  }
+};
+
+// FFT of a tile of L lines (element k of line l at buf[k*ES + l]); N = 0 is
+// the run-time-length path.  tw: shared copy of p.w (compile-time path).
+template <typename C, int N, int L, int ES>
+__device__ __forceinline__ C *fft_tile(C *a, C *b, const Plan<C> &p, const C *tw, int sg) {
+  if constexpr (N == 0) {
+    return smem_fft(a, b, L, ES, p, sg);
+  } else {
+    if (sg > 0) return CtStage<C, N, L, ES, 1, 0>::run(a, b, tw);
+    return CtStage<C, N, L, ES, -1, 0>::run(a, b, tw);
+  }
+}
+// copy the twiddles of the compile-time path into shared memory
+template <typename C, int N> __device__ __forceinline__ void load_tw(C *tw, const Plan<C> &p) {
+  if constexpr (N > 0) {
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = p.w[i];
+  }
+}
+
 // ---------------------------------------------------------------- geometry
 struct Geom {
   int n1, n2, n3;
@@ -161,7 +237,7 @@ constexpr int LX = 8;     // lines per X-pass block
 // ---------------------------------------------------------------- X pass
 // Backward X pass with the band-pair pack fused (vpsi/eval_density pack,
 // wfn_initialize.f90:286-308, density.f90:26-47): psi_a + i psi_b.
-template <typename C>
+template <typename C, int N = 0>
 __global__ void __launch_bounds__(256) k_x_bwd_pair(const double2 *__restrict__ c0, int ngpw, int nstate, int band0, int T,
                                                     Geom g, Plan<C> p, C *__restrict__ rb) {
   extern __shared__ unsigned char smraw[];
@@ -169,6 +245,8 @@ __global__ void __launch_bounds__(256) k_x_bwd_pair(const double2 *__restrict__ 
   const int n1 = g.n1, R = g.nray[0];
   const int es = LX + 1;
   C *sb = sa + n1 * es;
+  C *tw = sb + n1 * es;
+  load_tw<C, N>(tw, p);
   const long line0 = (long)blockIdx.x * LX;
   const long nlines = (long)T * R;
   for (int idx = threadIdx.x; idx < LX * n1; idx += blockDim.x) {
@@ -190,7 +268,7 @@ __global__ void __launch_bounds__(256) k_x_bwd_pair(const double2 *__restrict__ 
     sa[k * es + l] = v;
   }
   __syncthreads();
-  C *res = smem_fft(sa, sb, LX, es, p, +1);
+  C *res = fft_tile<C, N, LX, LX + 1>(sa, sb, p, tw, +1);
   for (int idx = threadIdx.x; idx < LX * n1; idx += blockDim.x) {
     const int l = idx / n1, k = idx % n1;
     const long line = line0 + l;
@@ -200,7 +278,7 @@ __global__ void __launch_bounds__(256) k_x_bwd_pair(const double2 *__restrict__ 
 
 // Backward X pass from a G field given at +G (fp) and -G (fm), t-th field at
 // fp + t*ngrho (eval_pot / rhog2r / GRAD_CAL packs).
-template <typename C>
+template <typename C, int N = 0>
 __global__ void __launch_bounds__(256) k_x_bwd_field(const double2 *__restrict__ fp, const double2 *__restrict__ fm, int ngmax,
                                                      int sphere, int T, Geom g, Plan<C> p, C *__restrict__ rb) {
   extern __shared__ unsigned char smraw[];
@@ -208,6 +286,8 @@ __global__ void __launch_bounds__(256) k_x_bwd_field(const double2 *__restrict__
   const int n1 = g.n1, R = g.nray[sphere];
   const int es = LX + 1;
   C *sb = sa + n1 * es;
+  C *tw = sb + n1 * es;
+  load_tw<C, N>(tw, p);
   const long line0 = (long)blockIdx.x * LX;
   const long nlines = (long)T * R;
   for (int idx = threadIdx.x; idx < LX * n1; idx += blockDim.x) {
@@ -226,7 +306,7 @@ __global__ void __launch_bounds__(256) k_x_bwd_field(const double2 *__restrict__
     sa[k * es + l] = v;
   }
   __syncthreads();
-  C *res = smem_fft(sa, sb, LX, es, p, +1);
+  C *res = fft_tile<C, N, LX, LX + 1>(sa, sb, p, tw, +1);
   for (int idx = threadIdx.x; idx < LX * n1; idx += blockDim.x) {
     const int l = idx / n1, k = idx % n1;
     const long line = line0 + l;
@@ -235,13 +315,15 @@ __global__ void __launch_bounds__(256) k_x_bwd_field(const double2 *__restrict__
 }
 
 // Forward X pass in place on the ray buffer.
-template <typename C>
+template <typename C, int N = 0>
 __global__ void __launch_bounds__(256) k_x_fwd(int sphere, int T, Geom g, Plan<C> p, C *__restrict__ rb) {
   extern __shared__ unsigned char smraw[];
   C *sa = reinterpret_cast<C *>(smraw);
   const int n1 = g.n1, R = g.nray[sphere];
   const int es = LX + 1;
   C *sb = sa + n1 * es;
+  C *tw = sb + n1 * es;
+  load_tw<C, N>(tw, p);
   const long line0 = (long)blockIdx.x * LX;
   const long nlines = (long)T * R;
   for (int idx = threadIdx.x; idx < LX * n1; idx += blockDim.x) {
@@ -250,7 +332,7 @@ __global__ void __launch_bounds__(256) k_x_fwd(int sphere, int T, Geom g, Plan<C
     sa[k * es + l] = (line < nlines) ? rb[line * n1 + k] : czero<C>();
   }
   __syncthreads();
-  C *res = smem_fft(sa, sb, LX, es, p, -1);
+  C *res = fft_tile<C, N, LX, LX + 1>(sa, sb, p, tw, -1);
   for (int idx = threadIdx.x; idx < LX * n1; idx += blockDim.x) {
     const int l = idx / n1, k = idx % n1;
     const long line = line0 + l;
@@ -261,13 +343,15 @@ __global__ void __launch_bounds__(256) k_x_fwd(int sphere, int T, Geom g, Plan<C
 // ---------------------------------------------------------------- Y pass
 // grid: (ceil(n1/TX), nz[sphere], T).  dir=+1 backward (rays -> slab),
 // dir=-1 forward (slab -> rays).
-template <typename C>
+template <typename C, int N = 0>
 __global__ void __launch_bounds__(256) k_y(int sphere, int dir, Geom g, Plan<C> p, C *__restrict__ rb, C *__restrict__ sbuf,
                                            long rstride, long sstride) {
   extern __shared__ unsigned char smraw[];
   C *sa = reinterpret_cast<C *>(smraw);
   const int n1 = g.n1, n2 = g.n2, nz = g.nz[sphere];
   C *sb = sa + n2 * TX;
+  C *tw = sb + n2 * TX;
+  load_tw<C, N>(tw, p);
   const int kx0 = blockIdx.x * TX, zi = blockIdx.y, t = blockIdx.z;
   const int *ri = g.rayidx[sphere] + (long)zi * n2;
   C *R = rb + (long)t * rstride;
@@ -286,7 +370,7 @@ __global__ void __launch_bounds__(256) k_y(int sphere, int dir, Geom g, Plan<C> 
     sa[ky * TX + tx] = v;
   }
   __syncthreads();
-  C *res = smem_fft(sa, sb, TX, TX, p, dir);
+  C *res = fft_tile<C, N, TX, TX>(sa, sb, p, tw, dir);
   for (int idx = threadIdx.x; idx < TX * n2; idx += blockDim.x) {
     const int ky = idx / TX, tx = idx % TX, kx = kx0 + tx;
     if (kx >= n1) continue;
@@ -310,7 +394,7 @@ enum { Z_TO_GRID = 0, Z_FROM_GRID_REAL = 1, Z_FROM_GRID_CPLX = 2, Z_VPSI = 3, Z_
 //   FROM_GRID_CPLX   complex grid (double2) -> slab                    forward
 //   VPSI             slab -> (bwd) * V(r) -> (fwd) -> slab  (vpsi, wfn_initialize.f90:311-340)
 //   DENSITY          slab -> (bwd) -> rho += f_a/Omega Re^2 + f_b/Omega Im^2 (density.f90:49-86)
-template <typename C, int MODE>
+template <typename C, int MODE, int N = 0>
 __global__ void __launch_bounds__(256) k_z(int sphere, int T, Geom g, Plan<C> p, C *__restrict__ sbuf, long sstride,
                                            double2 *__restrict__ cgrid, const double *__restrict__ rgrid, long gstride,
                                            const double *__restrict__ vpot, double *__restrict__ rho,
@@ -320,6 +404,8 @@ __global__ void __launch_bounds__(256) k_z(int sphere, int T, Geom g, Plan<C> p,
   C *sa = reinterpret_cast<C *>(smraw);
   const int n1 = g.n1, n2 = g.n2, n3 = g.n3, nz = g.nz[sphere];
   C *sb = sa + n3 * TX;
+  C *tw = sb + n3 * TX;
+  load_tw<C, N>(tw, p);
   const int kx0 = blockIdx.x * TX, ky = blockIdx.y;
   const int *zl = g.zlist[sphere];
   const long plane = (long)n2 * n1;
@@ -338,7 +424,7 @@ __global__ void __launch_bounds__(256) k_z(int sphere, int T, Geom g, Plan<C> p,
         if (kx < n1) sa[zl[zi] * TX + tx] = S[(long)zi * plane + (long)ky * n1 + kx];
       }
       __syncthreads();
-      C *res = smem_fft(sa, sb, TX, TX, p, +1);
+      C *res = fft_tile<C, N, TX, TX>(sa, sb, p, tw, +1);
       if (MODE == Z_TO_GRID) {
         double2 *G = cgrid + (long)t * gstride;
         for (int idx = threadIdx.x; idx < TX * n3; idx += blockDim.x) {
@@ -366,7 +452,7 @@ __global__ void __launch_bounds__(256) k_z(int sphere, int T, Geom g, Plan<C> p,
           res[idx] = cscale(res[idx], v);
         }
         __syncthreads();
-        C *out = smem_fft(res, other, TX, TX, p, -1);
+        C *out = fft_tile<C, N, TX, TX>(res, other, p, tw, -1);
         for (int idx = threadIdx.x; idx < TX * nz; idx += blockDim.x) {
           const int zi = idx / TX, tx = idx % TX, kx = kx0 + tx;
           if (kx < n1) S[(long)zi * plane + (long)ky * n1 + kx] = out[zl[zi] * TX + tx];
@@ -385,7 +471,7 @@ __global__ void __launch_bounds__(256) k_z(int sphere, int T, Geom g, Plan<C> p,
         sa[idx] = v;
       }
       __syncthreads();
-      C *res = smem_fft(sa, sb, TX, TX, p, -1);
+      C *res = fft_tile<C, N, TX, TX>(sa, sb, p, tw, -1);
       for (int idx = threadIdx.x; idx < TX * nz; idx += blockDim.x) {
         const int zi = idx / TX, tx = idx % TX, kx = kx0 + tx;
         if (kx < n1) S[(long)zi * plane + (long)ky * n1 + kx] = res[zl[zi] * TX + tx];

@@ -535,6 +535,122 @@ __global__ void k_cholesky_upper(int n, double *A, int *info) {
   if (threadIdx.x == 0) *info = bad;
 }
 
+// Cholesky S = U^T U (upper, DPOTRF('U')) followed by U <- U^{-1} (DTRTRI),
+// UINV of wfn_initialize.f90:504-530, in one block.  Column step j subtracts
+// S(j,a) S(j,b) / S(j,j) from the trailing upper triangle (one barrier per
+// step); the rows are scaled by 1/sqrt(S(j,j)) at the end.  The inverse is
+// computed column by column (one thread per column, back substitution).
+// Output: Ui (n x n, column-major, zero below the diagonal).  *info = j+1 if
+// the leading minor j is not positive definite.
+__global__ void k_chol_inv(int n, double *A, double *Ui, int *info) {
+  extern __shared__ double shc[];
+  // small n: factor in shared memory; otherwise in place in A (scratch)
+  const bool in_smem = (size_t)n * n * sizeof(double) <= 200 * 1024;
+  double *M = in_smem ? shc : A;
+  if (in_smem)
+    for (long k = threadIdx.x; k < (long)n * n; k += blockDim.x) M[k] = A[k];
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    const double d = M[j + (long)n * j];
+    if (!(d > 0.0)) {
+      if (threadIdx.x == 0) bad = j + 1;
+      break;   // uniform: every thread read the same d
+    }
+    const double inv = 1.0 / d;
+    const int m = n - j - 1;
+    const long cnt = (long)m * m;
+    for (long k = threadIdx.x; k < cnt; k += blockDim.x) {
+      const int a = j + 1 + (int)(k % m), b = j + 1 + (int)(k / m);
+      if (a <= b) M[a + (long)n * b] -= M[j + (long)n * a] * M[j + (long)n * b] * inv;
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  if (bad) {
+    if (threadIdx.x == 0) *info = bad;
+    return;
+  }
+  // U(j,b) = M(j,b) / sqrt(M(j,j)) for b >= j
+  for (long k = threadIdx.x; k < (long)n * n; k += blockDim.x) {
+    const int a = (int)(k % n), b = (int)(k / n);
+    if (a < b) M[k] = M[k] / sqrt(M[a + (long)n * a]);
+  }
+  __syncthreads();
+  for (int a = threadIdx.x; a < n; a += blockDim.x) M[a + (long)n * a] = sqrt(M[a + (long)n * a]);
+  __syncthreads();
+  // inverse: column j of U^{-1} solves U x = e_j; x stored into Ui
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    double *x = Ui + (long)n * j;
+    for (int i = j + 1; i < n; ++i) x[i] = 0.0;
+    x[j] = 1.0 / M[j + (long)n * j];
+    for (int i = j - 1; i >= 0; --i) {
+      double t = 0.0;
+      for (int k = i + 1; k <= j; ++k) t += M[i + (long)n * k] * x[k];
+      x[i] = -t / M[i + (long)n * i];
+    }
+  }
+  if (threadIdx.x == 0) *info = 0;
+}
+
+// e_sr (total_energy.f90:133-239) with minimum image: one thread per atom
+// sums its pair forces over every other atom (deterministic order) and the
+// pair energies with the atoms after it.  Pair terms are those of the
+// reference loop; esr -> out[0], forces F(3,na_max,nsp).
+__device__ void pbc_min_image(int sym, double alat, double x1, double y1, double z1, double &X, double &Y, double &Z) {
+  if (sym == 1) {
+    double A = alat, h = A / 2.0;
+    X = fmod(x1, A); Y = fmod(y1, A); Z = fmod(z1, A);
+    X = X - A * trunc(X / h); Y = Y - A * trunc(Y / h); Z = Z - A * trunc(Z / h);
+  } else {
+    double ma = alat * sqrt(2.0) / 4.0, s2 = sqrt(2.0);
+    X = (x1 + y1) / s2; Y = (-x1 + y1) / s2;
+    X = fmod(X, 2.0 * ma); Y = fmod(Y, 2.0 * ma);
+    Z = fmod(z1, 2.0 * ma * s2);
+    X = X - 2.0 * ma * trunc(X / ma); Y = Y - 2.0 * ma * trunc(Y / ma);
+    Z = Z - 2.0 * ma * s2 * trunc(Z / (s2 * ma));
+    if (!(fabs(X) + fabs(Y) + s2 * fabs(Z) < 2.0 * ma)) {
+      X = X - copysign(ma, X); Y = Y - copysign(ma, Y); Z = Z - copysign(s2 * ma, Z);
+    }
+    double xt = (X - Y) / s2;
+    Y = (X + Y) / s2;
+    X = xt;
+  }
+}
+__global__ void k_esr_par(int nat, const int *isa_is, const int *isa_ia, int na_max, const int *zv, const double *atco,
+                          double alat, int sym, double *F, double *out) {
+  __shared__ double sh[32];
+  const double pi = 4.0 * atan(1.0), rckj = sqrt(1.2 * 1.2 + 1.2 * 1.2);
+  double esr = 0;
+  for (int l = threadIdx.x; l < nat; l += blockDim.x) {
+    const int kl = isa_is[l];
+    const double *xl = atco + 3 * (isa_ia[l] + (long)na_max * kl);
+    double fx = 0, fy = 0, fz = 0;
+    for (int m = 0; m < nat; ++m) {
+      if (m == l) continue;
+      const int km = isa_is[m];
+      const double zv2 = (double)(zv[kl] * zv[km]);
+      if (fabs(zv2) < 1e-10) continue;
+      const double *xm = atco + 3 * (isa_ia[m] + (long)na_max * km);
+      double X, Y, Z;
+      pbc_min_image(sym, alat, xl[0] - xm[0], xl[1] - xm[1], xl[2] - xm[2], X, Y, Z);
+      const double e2 = X * X + Y * Y + Z * Z, r = sqrt(e2), arg = r / rckj;
+      if (arg <= 20.0) {
+        const double add = zv2 * erfc(arg) / r;
+        if (m > l) esr += add;
+        const double pre = (2.0 * zv2 / sqrt(pi)) * exp(-arg * arg) / rckj;
+        const double rep = (add + pre) / e2;
+        fx += rep * X; fy += rep * Y; fz += rep * Z;
+      }
+    }
+    double *f = F + 3 * (isa_ia[l] + (long)na_max * kl);
+    f[0] = fx; f[1] = fy; f[2] = fz;
+  }
+  const double e = block_sum(esr, sh);
+  if (threadIdx.x == 0) out[0] = e;
+}
+
 // fnonloc G=0 row (P holds the halved G=0 entry): C2_b(0) += sum_j P_j(0) D(j,b)
 __global__ void k_fnonloc_g0(int nproj, int nstate, int ngpw, const double2 *P, const double *D, double2 *c2) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
