@@ -526,10 +526,12 @@ static int do_ortho(amdk_ctx *c) {
                  &zero, c->d_gam, n));
   ++c->nlaunch;
   k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c0, c->d_c0, c->d_gam, c->d_occ, 0, 1);
-  size_t sm = (size_t)n * n * sizeof(double);
-  if (sm > 200 * 1024) sm = 0;
+  const size_t sm = (size_t)n * n * sizeof(double);
   ++c->nlaunch;
-  k_chol_inv<<<1, 1024, sm, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
+  if (sm <= 200 * 1024 && n <= 1024)
+    k_chol_inv_s<<<1, 1024, sm, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
+  else
+    k_chol_inv<<<1, 1024, 0, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
   int info = 0;
   CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -684,6 +686,7 @@ static int build_device(amdk_ctx *c) {
   set_smem_attrs<float2>();
   cudaFuncSetAttribute(k_cholesky_upper, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_chol_inv_s, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   // G vectors
   RC(c->up(&c->d_inyh, h.inyh));
   RC(c->up(&c->d_hg, h.hg));
@@ -1054,13 +1057,38 @@ int amdk_scf_iteration(amdk_ctx *c, int istep, double gcut, amdk_energies *e, do
 int amdk_ionic_forces(amdk_ctx *c, double *force) {
   if (!c || !force) return AMDK_ERR_BADARG;
   cudaSetDevice(c->device);
-  if (!c->tfor) {
-    // make sure nl/hn are for the current C0 (pp_energy) before NLFOR
-    RC(do_fnl(c));
-  }
+  // forces of the current C0: density (for POTFOR) and projections (NLFOR)
+  RC(do_density(c));
+  RC(do_fnl(c));
   RC(do_ionic_forces(c));
   CK(cudaMemcpyAsync(force, c->d_force, sizeof(double) * 3 * c->hs.na_max * c->hs.nsp, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int amdk_backward(amdk_ctx *c, double *dE_dR, double *dE_dpsi) {
+  if (!c || (!dE_dR && !dE_dpsi)) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  const HostSetup &h = c->hs;
+  RC(do_density(c));
+  if (dE_dpsi) RC(do_potential(c));
+  RC(do_energy(c, nullptr));
+  if (dE_dR) {
+    RC(do_ionic_forces(c));
+    const size_t nf = 3 * (size_t)h.na_max * h.nsp;
+    std::vector<double> f(nf);
+    CK(cudaMemcpyAsync(f.data(), c->d_force, sizeof(double) * nf, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (size_t k = 0; k < nf; k++) dE_dR[k] = -f[k];
+  }
+  if (dE_dpsi) {
+    CK(cudaMemsetAsync(c->d_c2, 0, sizeof(double2) * (size_t)h.ngpw * c->nstate, c->st));
+    RC(do_apply_h(c));
+    const size_t nc = 2 * (size_t)h.ngpw * c->nstate;
+    CK(cudaMemcpyAsync(dE_dpsi, c->d_c2, sizeof(double) * nc, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (size_t k = 0; k < nc; k++) dE_dpsi[k] = -dE_dpsi[k];
+  }
   return 0;
 }
 

@@ -594,6 +594,77 @@ __global__ void k_chol_inv(int n, double *A, double *Ui, int *info) {
   if (threadIdx.x == 0) *info = 0;
 }
 
+// Shared-memory Cholesky + inverse for n with n*n doubles in shared memory.
+// Threads form groups of g (a power of two); group c owns columns
+// b = c, c + ncols, ...  In step j it applies S(a,b) -= S(j,a) S(j,b)/S(j,j)
+// for j < a <= b (its g threads split the rows a).  The inverse of the
+// upper factor is formed column by column in place (DTRTI2 order):
+// X(i,j) = -X(j,j) sum_{k=i}^{j-1} X(i,k) U(k,j), the g threads of row i
+// splitting the sum.  Same contract as k_chol_inv.
+__global__ void __launch_bounds__(1024) k_chol_inv_s(int n, const double *A, double *Ui, int *info) {
+  extern __shared__ double M[];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int k = tid; k < n * n; k += nt) M[k] = A[k];
+  int g = 1;
+  while (g < 32 && 2 * g * n <= nt) g *= 2;
+  const int sub = tid % g, grp = tid / g, ngrp = nt / g;
+  __shared__ int bad;
+  if (tid == 0) bad = 0;
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    const double d = M[j + n * j];
+    if (!(d > 0.0)) {
+      if (tid == 0) bad = j + 1;
+      break;  // uniform: every thread read the same d
+    }
+    const double inv = 1.0 / d;
+    for (int b = j + 1 + grp; b < n; b += ngrp) {
+      const double mjb = M[j + n * b] * inv;
+      for (int a = j + 1 + sub; a <= b; a += g) M[a + n * b] -= M[j + n * a] * mjb;
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  if (bad) {
+    if (tid == 0) *info = bad;
+    return;
+  }
+  // U(a,b) = S(a,b) / sqrt(S(a,a)) (a < b), then the diagonal
+  for (int k = tid; k < n * n; k += nt) {
+    const int a = k % n, b = k / n;
+    if (a < b) M[k] = M[k] / sqrt(M[a + n * a]);
+  }
+  __syncthreads();
+  for (int a = tid; a < n; a += nt) M[a + n * a] = sqrt(M[a + n * a]);
+  __syncthreads();
+  // in-place inverse of the upper factor, column by column
+  for (int j = 0; j < n; ++j) {
+    const double xjj = 1.0 / M[j + n * j];
+    const int nrow = (j + ngrp - 1) / ngrp;  // same for every thread: the shuffles below see full warps
+    double val[4];
+    for (int c = 0; c < nrow; ++c) {
+      const int i = grp + c * ngrp;
+      double t = 0.0;
+      if (i < j)
+        for (int k = i + sub; k < j; k += g) t += M[i + n * k] * M[k + n * j];
+      for (int o = g >> 1; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o, g);
+      if (c < 4) val[c] = -xjj * t;
+    }
+    __syncthreads();
+    for (int c = 0; c < nrow && c < 4; ++c) {
+      const int i = grp + c * ngrp;
+      if (i < j && sub == 0) M[i + n * j] = val[c];
+    }
+    if (tid == 0) M[j + n * j] = xjj;
+    __syncthreads();
+  }
+  for (int k = tid; k < n * n; k += nt) {
+    const int a = k % n, b = k / n;
+    Ui[k] = (a <= b) ? M[k] : 0.0;
+  }
+  if (tid == 0) *info = 0;
+}
+
 // e_sr (total_energy.f90:133-239) with minimum image: one thread per atom
 // sums its pair forces over every other atom (deterministic order) and the
 // pair energies with the atoms after it.  Pair terms are those of the

@@ -89,6 +89,7 @@ def load_library(path: str = LIBPATH):
     lib.amdk_scf_iteration.argtypes = [P, C.c_int, C.c_double, C.POINTER(Energies), C.POINTER(C.c_double),
                                        C.POINTER(C.c_int)]
     lib.amdk_ionic_forces.argtypes = [P, C.POINTER(C.c_double)]
+    lib.amdk_backward.argtypes = [P, P, P]
     lib.amdk_get_array.argtypes = [P, C.c_char_p, P, C.c_size_t]
     lib.amdk_fft_sphere.argtypes = [P, C.c_int, P, P]
     lib.amdk_last_iteration_ms.argtypes = [P, C.POINTER(C.c_double)]
@@ -299,6 +300,14 @@ class Engine:
         f = np.zeros((len(s.species), s.na_max, 3))
         _check(self.lib.amdk_ionic_forces(self.h, _dp(f)), "amdk_ionic_forces")
         return f
+
+    def backward(self, want_psi: bool = False):
+        """dE/dR (same layout as the forces), and f (H c) when want_psi."""
+        s = self.system
+        g = np.zeros((len(s.species), s.na_max, 3))
+        p = np.zeros((self.nstate, self.ngpw), np.complex128) if want_psi else None
+        _check(self.lib.amdk_backward(self.h, g.ctypes.data, p.ctypes.data if want_psi else None), "amdk_backward")
+        return (g, p) if want_psi else g
 
     def fft_sphere(self, sign: int, coef: Optional[np.ndarray] = None, grid: Optional[np.ndarray] = None):
         n1, n2, n3 = self.nr

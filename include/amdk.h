@@ -149,6 +149,15 @@ int amdk_scf_iteration(amdk_ctx *ctx, int istep, double gcut, amdk_energies *e, 
  * (UPF_NLFOR :153-199) for the current C0 and density: force(3,na_max,nsp) */
 int amdk_ionic_forces(amdk_ctx *ctx, double *force);
 
+/* Backward (adjoint) entry for the current C0 and positions:
+ * dE_dR(3,na_max,nsp) = dE_total/dR_I = -(e_sr + POTFOR + NLFOR forces), the
+ * derivative of the local-pseudopotential/structure-factor term, of the
+ * nonlocal projectors (D_FNL, nuclear_grad.f90:314-372) and of the Ewald sum;
+ * dE_dpsi(ngpw,nstate) complex = f_i (H c_i)(G), the unconstrained gradient
+ * of E with respect to the coefficients as vpsi + fnonloc build it (the
+ * reference's C2 negated).  Either pointer may be NULL. */
+int amdk_backward(amdk_ctx *ctx, double *dE_dR, double *dE_dpsi);
+
 /* Copy a named device array to host memory (parity tests and drivers).
  * Names: "rho","v_pot" (nr3*nr2*nr1 real, x fastest), "rho_g" (ngrho complex),
  * "c2" (ngpw*nstate complex), "nl" (nat*nghmax*nstate), "vps","rhos"

@@ -36,3 +36,28 @@ def load_fixture(name: str) -> System:
 
 def start_coefficients(hg_pw: np.ndarray, tpiba: float, nstate: int, seed: int = 1234) -> np.ndarray:
     return initial_coefficients(hg_pw * tpiba * tpiba, nstate, seed)
+
+
+class OracleEngine:
+    """The CPU restatement behind the small Engine interface BOMD uses."""
+
+    def __init__(self, system, seed: int = 1234):
+        from oracle.oracle import Oracle
+        self.system = system
+        self.o = Oracle(system, 0)
+        g = self.o.gvectors()
+        self.o.set_wfn(start_coefficients(g["hg"][: self.o.ngpw], self.o.d("tpiba"), self.o.nstate, seed))
+
+    def ortho(self):
+        assert self.o.ortho() == 0
+
+    def set_positions(self, atco):
+        self.o.set_positions(atco)
+
+    def wfn_opt(self, max_step, gcut):
+        n = self.o.wfn_opt(max_step, gcut)
+        return n, {"etotal": self.o.d("etotal")}, self.o.d("gemax")
+
+    def get(self, name):
+        assert name == "force"
+        return self.o.force()

@@ -37,6 +37,7 @@ SYSTEMS = {
     "small_water_pz": lambda: configs.small_water(),
     "small_water_pbe": lambda: configs.small_water(xc=XC_PBE),
     "si_fcc_mt": lambda: load_fixture("si_fcc_mt"),
+    "si64_low": lambda: configs.si64(ecut=12.0),
 }
 
 
