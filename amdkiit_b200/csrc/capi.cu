@@ -6,7 +6,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
+#include <map>
 #include <mutex>
+#include <queue>
 #include <type_traits>
 #include <string>
 #include <vector>
@@ -14,6 +17,7 @@
 #include "amdk_internal.h"
 #include "fft.cuh"
 #include "kernels.cuh"
+#include "pencil.cuh"
 
 namespace amdk {
 
@@ -102,6 +106,15 @@ struct amdk_ctx {
   double *d_gam = nullptr, *d_uinv = nullptr;
   int *d_info = nullptr;
   double *d_part = nullptr, *d_scal = nullptr, *d_force = nullptr, *d_esr = nullptr, *d_fsr = nullptr;
+  // pencil path (cubic grids with a specialised length): tables and buffers
+  bool pencil_vpsi = false, pencil_density = false;
+  int pencil_groups = 1;  // upper bound on the density pair groups
+  int nsm = 148;
+  std::map<int, int> pencil_grp_cache;
+  PencilGeom pg{};
+  int *d_rpos = nullptr, *d_zinv = nullptr, *d_postp = nullptr, *d_postm = nullptr;
+  double *d_rhopart = nullptr;
+  void *d_vt = nullptr;
   // live per-kernel timing (CUDA events on the context stream)
   long nlaunch = 0;  // kernels of this library launched on the context stream
   bool prof = false;
@@ -311,6 +324,120 @@ static int grid_to_rays(amdk_ctx *c, int T, const double2 *cgrid, const double *
   return 0;
 }
 
+// ------------------------------------------------------------------ pencil path
+template <typename C> static size_t pencil_smem(int n, int nz) {
+  return ((size_t)nz * (n + 1) + 2 * (size_t)PL * n + n) * sizeof(C);
+}
+static size_t pencil_acc_smem(int n) { return (size_t)n * (n + 1) * sizeof(double); }
+// 256 threads when two blocks fit on an SM, else 512
+static int pencil_threads(size_t smem) { return (2 * (smem + 1024) <= 228 * 1024) ? 256 : PNT; }
+// Pair groups of the density pencil kernel: each (x-plane, group) block sums
+// its group's pairs into its own partial grid.  Pick the group count whose
+// block list, scheduled greedily on the SMs, ends first; each group also
+// costs one partial grid written and read back.
+static int pencil_density_groups(int n1, int T, int nsm, int bps, int maxg) {
+  int best = 1;
+  double best_cost = 1e300;
+  for (int grp = 1; grp <= std::min(maxg, T); ++grp) {
+    const int per = (T + grp - 1) / grp;
+    if ((grp - 1) * per >= T) continue;  // an empty group
+    std::priority_queue<double, std::vector<double>, std::greater<double>> slots;
+    for (int i = 0; i < nsm * bps; ++i) slots.push(0.0);
+    double end = 0.0;
+    for (int gi = 0; gi < grp; ++gi) {
+      const int np = std::min(T, (gi + 1) * per) - gi * per;
+      for (int kx = 0; kx < n1; ++kx) {
+        double t0 = slots.top();
+        slots.pop();
+        double t1 = t0 + (np + 0.5) / bps;
+        end = std::max(end, t1);
+        slots.push(t1);
+      }
+    }
+    const double cost = end + 0.3 * grp;
+    if (cost < best_cost) {
+      best_cost = cost;
+      best = grp;
+    }
+  }
+  return best;
+}
+template <typename C> static size_t xt_smem(int n1) { return (2 * (size_t)n1 * 17 + n1) * sizeof(C); }
+
+template <typename C> static void xt_bwd_pair(amdk_ctx *c, int p0, int T) {
+  const Geom &g = c->geom;
+  long lines = (long)T * g.nray[0];
+  with_n(g.n1, [&](auto NC) {
+    constexpr int N = decltype(NC)::value;
+    if constexpr (N > 0) {
+      smem_opt_in<k_xt_bwd_pair<C, N>>();
+      ++c->nlaunch;
+      k_xt_bwd_pair<C, N><<<nblk(lines, 16), NTHR, xt_smem<C>(g.n1), c->st>>>(c->d_c0, c->hs.ngpw, c->nstate, 2 * p0, T,
+                                                                             g, plan<C>(c, 0), (C *)c->d_rb);
+    }
+  });
+}
+template <typename C> static void xt_fwd(amdk_ctx *c, int T) {
+  const Geom &g = c->geom;
+  long lines = (long)T * g.nray[0];
+  prof_begin(c, KT_X, 2.0 * lines * g.n1 * sizeof(C));
+  with_n(g.n1, [&](auto NC) {
+    constexpr int N = decltype(NC)::value;
+    if constexpr (N > 0) {
+      smem_opt_in<k_xt_fwd<C, N>>();
+      ++c->nlaunch;
+      k_xt_fwd<C, N><<<nblk(lines, 16), NTHR, xt_smem<C>(g.n1), c->st>>>(T, g, plan<C>(c, 0), (C *)c->d_rb);
+    }
+  });
+  prof_end(c);
+}
+template <typename C> static void pencil_vpsi(amdk_ctx *c, int T) {
+  const Geom &g = c->geom;
+  typedef decltype(C().x) Rl;
+  const double npt = (double)g.n1 * g.n2 * g.n3;
+  prof_begin(c, KT_ZVPSI, 2.0 * T * rstride(c, 0) * sizeof(C) + npt * sizeof(Rl));
+  with_n(g.n2, [&](auto NC) {
+    constexpr int N = decltype(NC)::value;
+    if constexpr (N > 0) {
+      smem_opt_in<k_pencil_vpsi<C, N>>();
+      ++c->nlaunch;
+      const size_t sm = pencil_smem<C>(N, c->pg.nz);
+      k_pencil_vpsi<C, N><<<dim3(g.n1, T), pencil_threads(sm), sm, c->st>>>(c->pg, plan<C>(c, 1), (C *)c->d_rb,
+                                                                            (const Rl *)c->d_vt);
+    }
+  });
+  prof_end(c);
+}
+template <typename C> static int density_groups(amdk_ctx *c, int T) {
+  const Geom &g = c->geom;
+  const size_t sm = pencil_acc_smem(g.n2) + pencil_smem<C>(g.n2, c->pg.nz);
+  auto it = c->pencil_grp_cache.find(T);
+  if (it == c->pencil_grp_cache.end())
+    it = c->pencil_grp_cache
+             .emplace(T, pencil_density_groups(g.n1, T, c->nsm, pencil_threads(sm) == PNT ? 1 : 2, c->pencil_groups))
+             .first;
+  return it->second;
+}
+template <typename C> static void pencil_density(amdk_ctx *c, int p0, int T) {
+  const Geom &g = c->geom;
+  const size_t sm = pencil_acc_smem(g.n2) + pencil_smem<C>(g.n2, c->pg.nz);
+  const int nt = pencil_threads(sm);
+  const int grp = density_groups<C>(c, T);
+  const int per = (T + grp - 1) / grp;
+  const double npt = (double)g.n1 * g.n2 * g.n3;
+  prof_begin(c, KT_ZDENS, (double)T * rstride(c, 0) * sizeof(C) + 2.0 * grp * npt * 8.0);
+  with_n(g.n2, [&](auto NC) {
+    constexpr int N = decltype(NC)::value;
+    if constexpr (N > 0) {
+      smem_opt_in<k_pencil_density<C, N>>();
+      ++c->nlaunch;
+      k_pencil_density<C, N><<<dim3(g.n1, grp), nt, sm, c->st>>>(c->pg, plan<C>(c, 1), (const C *)c->d_rb, T, per,
+                                                                 c->d_wa + p0, c->d_wb + p0, c->d_rhopart);
+    }
+  });
+  prof_end(c);
+}
+
 // ------------------------------------------------------------------ routines
 static int finish_sums(amdk_ctx *c, int nk, int slot) {
   ++c->nlaunch;
@@ -321,6 +448,21 @@ static int finish_sums(amdk_ctx *c, int nk, int slot) {
 template <typename C> static int density_t(amdk_ctx *c) {
   const HostSetup &h = c->hs;
   const Geom &g = c->geom;
+  if (c->pencil_density) {
+    // pencil path: transposed x pass, then one block per (x-plane, pair group)
+    int ng = density_groups<C>(c, c->batch);
+    if (c->npairs % c->batch) ng = std::max(ng, density_groups<C>(c, c->npairs % c->batch));
+    const size_t part = (size_t)ng * g.n1 * g.n2 * g.n3;
+    CK(cudaMemsetAsync(c->d_rhopart, 0, sizeof(double) * part, c->st));
+    for (int p0 = 0; p0 < c->npairs; p0 += c->batch) {
+      int T = std::min(c->batch, c->npairs - p0);
+      xt_bwd_pair<C>(c, p0, T);
+      pencil_density<C>(c, p0, T);
+    }
+    ++c->nlaunch;
+    k_rho_reduce_t<<<dim3((g.n3 + 31) / 32, (g.n1 + 31) / 32, g.n2), dim3(32, 8), 0, c->st>>>(
+        g.n1, g.n2, g.n3, ng, c->d_rhopart, c->d_rho);
+  } else {
   CK(cudaMemsetAsync(c->d_rho, 0, sizeof(double) * (size_t)g.n1 * g.n2 * g.n3, c->st));
   for (int p0 = 0; p0 < c->npairs; p0 += c->batch) {
     int T = std::min(c->batch, c->npairs - p0);
@@ -334,6 +476,7 @@ template <typename C> static int density_t(amdk_ctx *c) {
     });
     y_pass<C>(c, 0, +1, T);
     z_pass<C, Z_DENSITY>(c, 0, T, nullptr, nullptr, p0);
+  }
   }
   // rhor2g (density.f90:128-150)
   RC(grid_to_rays(c, 1, nullptr, c->d_rho));
@@ -379,6 +522,15 @@ static int do_potential(amdk_ctx *c) {
   // V(r) = Re of the backward transform (xc.f90:299-301)
   CK(cudaMemcpy2DAsync(c->d_vpot, sizeof(double), c->d_cgrid, sizeof(double2), sizeof(double), npt,
                        cudaMemcpyDeviceToDevice, c->st));
+  if (c->pencil_vpsi) {
+    // V in the x-plane-major layout the pencil kernel reads
+    dim3 gt((g.n1 + 31) / 32, (g.n3 + 31) / 32, g.n2);
+    ++c->nlaunch;
+    if (c->precision == AMDK_MIXED)
+      k_v_transpose<float><<<gt, dim3(32, 8), 0, c->st>>>(g.n1, g.n2, g.n3, c->d_vpot, (float *)c->d_vt);
+    else
+      k_v_transpose<double><<<gt, dim3(32, 8), 0, c->st>>>(g.n1, g.n2, g.n3, c->d_vpot, (double *)c->d_vt);
+  }
   CK(cudaGetLastError());
   return 0;
 }
@@ -387,6 +539,20 @@ template <typename C> static int apply_h_t(amdk_ctx *c) {
   const HostSetup &h = c->hs;
   const Geom &g = c->geom;
   double scale = 1.0 / ((double)g.n1 * g.n2 * g.n3);
+  if (c->pencil_vpsi) {
+    for (int p0 = 0; p0 < c->npairs; p0 += c->batch) {
+      int T = std::min(c->batch, c->npairs - p0);
+      xt_bwd_pair<C>(c, p0, T);
+      pencil_vpsi<C>(c, T);
+      xt_fwd<C>(c, T);
+      dim3 gu(nblk(h.ngpw), T);
+      ++c->nlaunch;
+      k_unpack_vpsi<C><<<gu, NTHR, 0, c->st>>>(h.ngpw, c->nstate, 2 * p0, T, c->d_postp, c->d_postm, (C *)c->d_rb,
+                                               rstride(c, 0), scale, c->d_hg, h.tpiba2, c->d_occ, c->d_c0, c->d_c2);
+    }
+    CK(cudaGetLastError());
+    return 0;
+  }
   for (int p0 = 0; p0 < c->npairs; p0 += c->batch) {
     int T = std::min(c->batch, c->npairs - p0);
     long lines = (long)T * g.nray[0];
@@ -726,15 +892,57 @@ static int build_device(amdk_ctx *c) {
   RC(c->alloc(&c->d_part, (size_t)RED_BLOCKS * 4 + 3L * 64 * h.nat + 64));
   RC(c->alloc(&c->d_scal, S_NSCAL));
   CK(cudaMemset(c->d_scal, 0, S_NSCAL * sizeof(double)));
-  // FFT buffers: pair batches (working precision) and up to 2 FP64 density fields
+  // Pencil path for the pair transforms (cubic grids with a specialised
+  // length whose slab plane fits in shared memory): V(r)psi and the density
+  // go plane by plane through shared memory with no slab buffer in HBM.
   size_t csz = (c->precision == AMDK_MIXED) ? sizeof(float2) : sizeof(double2);
-  if (c->batch <= 0) c->batch = 8;
+  {
+    bool known = false;
+    with_n(n1, [&](auto NC) { known = decltype(NC)::value > 0; });
+    const bool ok = (n1 == n2 && n2 == n3) && known;
+    const size_t lim = 227 * 1024;
+    const size_t vs = ((size_t)g.nz[0] * (n1 + 1) + 2 * (size_t)PL * n1 + n1) * csz;
+    c->pencil_vpsi = ok && vs <= lim;
+    c->pencil_density = ok && vs + pencil_acc_smem(n1) <= lim;
+    const char *env = getenv("AMDK_NO_PENCIL");
+    if (env && env[0] == '1') c->pencil_vpsi = c->pencil_density = false;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const bool pencil_all = c->pencil_vpsi && c->pencil_density;
+  // pair batch: all pairs at once on the pencil path, else 8
+  if (c->batch <= 0) c->batch = pencil_all ? c->npairs : 8;
   c->batch = std::max(1, std::min(c->batch, c->npairs));
   size_t rb = std::max((size_t)c->batch * rstride(c, 0) * csz, 2 * (size_t)rstride(c, 1) * sizeof(double2));
-  size_t sb = std::max((size_t)c->batch * sstride(c, 0) * csz, 2 * (size_t)sstride(c, 1) * sizeof(double2));
+  size_t sb = 2 * (size_t)sstride(c, 1) * sizeof(double2);
+  if (!pencil_all) sb = std::max(sb, (size_t)c->batch * sstride(c, 0) * csz);
   RC(c->alloc((char **)&c->d_rb, rb));
   RC(c->alloc((char **)&c->d_sb, sb));
   c->fftbuf_bytes = rb + sb;
+  if (c->pencil_vpsi || c->pencil_density) {
+    std::vector<int> rpos(h.ngrays), zinv(n3, -1), zl0(g.nz[0]), postp(h.ngpw), postm(h.ngpw);
+    CK(cudaMemcpy(zl0.data(), c->d_zlist[0], sizeof(int) * g.nz[0], cudaMemcpyDeviceToHost));
+    for (int zi = 0; zi < g.nz[0]; zi++) zinv[zl0[zi]] = zi;
+    for (int r = 0; r < h.ngrays; r++) rpos[r] = zinv[ray_kz[r]] * (n2 + 1) + ray_ky[r];
+    // G -> transposed ray buffer position kx*R + ray
+    for (int ig = 0; ig < h.ngpw; ig++) {
+      postp[ig] = (posp[ig] % n1) * h.ngrays + posp[ig] / n1;
+      postm[ig] = (posm[ig] % n1) * h.ngrays + posm[ig] / n1;
+    }
+    RC(c->up(&c->d_rpos, rpos));
+    RC(c->up(&c->d_zinv, zinv));
+    RC(c->up(&c->d_postp, postp));
+    RC(c->up(&c->d_postm, postm));
+    c->pg = PencilGeom{n1, n2, n3, h.ngrays, g.nz[0], c->d_rpos, c->d_zinv, c->d_zlist[0]};
+    c->pencil_groups = std::max(1, std::min(c->batch, 16));
+    if (c->pencil_density) RC(c->alloc(&c->d_rhopart, (size_t)c->pencil_groups * npt));
+    if (c->pencil_vpsi) {
+      char *vt;
+      RC(c->alloc(&vt, (size_t)npt * (c->precision == AMDK_MIXED ? sizeof(float) : sizeof(double))));
+      c->d_vt = vt;
+    }
+  }
   // pseudopotential tables on the device
   RC(c->alloc(&c->d_vps, (size_t)h.nsp * h.ngrho));
   RC(c->alloc(&c->d_rhos, (size_t)h.nsp * h.ngrho));
