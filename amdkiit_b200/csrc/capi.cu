@@ -109,10 +109,12 @@ struct amdk_ctx {
   // pencil path (cubic grids with a specialised length): tables and buffers
   bool pencil_vpsi = false, pencil_density = false;
   int pencil_groups = 1;  // upper bound on the density pair groups
+  int ct_vpsi = 0, ct_dens = 0;  // column tiles of the pencil kernels
+  int pn1 = 0, pn2 = 0;          // two-level split n = pn1 * pn2
   int nsm = 148;
   std::map<int, int> pencil_grp_cache;
   PencilGeom pg{};
-  int *d_rpos = nullptr, *d_zinv = nullptr, *d_postp = nullptr, *d_postm = nullptr;
+  int *d_rpos = nullptr, *d_gmapt = nullptr, *d_zinv = nullptr, *d_postp = nullptr, *d_postm = nullptr;
   double *d_rhopart = nullptr;
   void *d_vt = nullptr;
   // live per-kernel timing (CUDA events on the context stream)
@@ -325,12 +327,22 @@ static int grid_to_rays(amdk_ctx *c, int T, const double2 *cgrid, const double *
 }
 
 // ------------------------------------------------------------------ pencil path
-template <typename C> static size_t pencil_smem(int n, int nz) {
-  return ((size_t)nz * (n + 1) + 2 * (size_t)PL * n + n) * sizeof(C);
+// shared memory of a pencil block: slab plane, column tile of ct columns,
+// twiddles and the kz -> slab index table (+ the accumulator for the density)
+template <typename C> static size_t pencil_smem(int n, int nz, int ct) {
+  return ((size_t)(nz + ct) * (n + 1) + n) * sizeof(C) + n * sizeof(int);
 }
 static size_t pencil_acc_smem(int n) { return (size_t)n * (n + 1) * sizeof(double); }
-// 256 threads when two blocks fit on an SM, else 512
-static int pencil_threads(size_t smem) { return (2 * (smem + 1024) <= 228 * 1024) ? 256 : PNT; }
+// widest column tile with the block within `budget` bytes (0: none fits)
+template <typename C> static int pencil_tile(int n, int nz, size_t extra, size_t budget) {
+  const size_t base = pencil_smem<C>(n, nz, 0) + extra;
+  if (base >= budget) return 0;
+  const int widest = (int)std::min<size_t>(n, (budget - base) / ((n + 1) * sizeof(C)));
+  if (widest <= 0) return 0;
+  const int tiles = (n + widest - 1) / widest;  // equal tiles
+  return (n + tiles - 1) / tiles;
+}
+template <typename C> static size_t xt_smem(int n1) { return ((size_t)XL * (n1 + 1) + n1) * sizeof(C); }
 // Pair groups of the density pencil kernel: each (x-plane, group) block sums
 // its group's pairs into its own partial grid.  Pick the group count whose
 // block list, scheduled greedily on the SMs, ends first; each group also
@@ -362,7 +374,6 @@ static int pencil_density_groups(int n1, int T, int nsm, int bps, int maxg) {
   }
   return best;
 }
-template <typename C> static size_t xt_smem(int n1) { return (2 * (size_t)n1 * 17 + n1) * sizeof(C); }
 
 template <typename C> static void xt_bwd_pair(amdk_ctx *c, int p0, int T) {
   const Geom &g = c->geom;
@@ -372,8 +383,9 @@ template <typename C> static void xt_bwd_pair(amdk_ctx *c, int p0, int T) {
     if constexpr (N > 0) {
       smem_opt_in<k_xt_bwd_pair<C, N>>();
       ++c->nlaunch;
-      k_xt_bwd_pair<C, N><<<nblk(lines, 16), NTHR, xt_smem<C>(g.n1), c->st>>>(c->d_c0, c->hs.ngpw, c->nstate, 2 * p0, T,
-                                                                             g, plan<C>(c, 0), (C *)c->d_rb);
+      constexpr int N2 = N / fft_n1(N);
+      k_xt_bwd_pair<C, N><<<nblk(lines, XL), XL * N2, xt_smem<C>(N), c->st>>>(c->d_c0, c->hs.ngpw, c->nstate, 2 * p0, T,
+                                                                             c->pg, plan<C>(c, 0), (C *)c->d_rb);
     }
   });
 }
@@ -386,7 +398,8 @@ template <typename C> static void xt_fwd(amdk_ctx *c, int T) {
     if constexpr (N > 0) {
       smem_opt_in<k_xt_fwd<C, N>>();
       ++c->nlaunch;
-      k_xt_fwd<C, N><<<nblk(lines, 16), NTHR, xt_smem<C>(g.n1), c->st>>>(T, g, plan<C>(c, 0), (C *)c->d_rb);
+      constexpr int N2 = N / fft_n1(N);
+      k_xt_fwd<C, N><<<nblk(lines, XL), XL * N2, xt_smem<C>(N), c->st>>>(T, c->pg, plan<C>(c, 0), (C *)c->d_rb);
     }
   });
   prof_end(c);
@@ -401,27 +414,27 @@ template <typename C> static void pencil_vpsi(amdk_ctx *c, int T) {
     if constexpr (N > 0) {
       smem_opt_in<k_pencil_vpsi<C, N>>();
       ++c->nlaunch;
-      const size_t sm = pencil_smem<C>(N, c->pg.nz);
-      k_pencil_vpsi<C, N><<<dim3(g.n1, T), pencil_threads(sm), sm, c->st>>>(c->pg, plan<C>(c, 1), (C *)c->d_rb,
-                                                                            (const Rl *)c->d_vt);
+      const size_t sm = pencil_smem<C>(N, c->pg.nz, c->ct_vpsi);
+      k_pencil_vpsi<C, N><<<dim3(g.n1, T), PNT, sm, c->st>>>(c->pg, plan<C>(c, 1), (C *)c->d_rb, (const Rl *)c->d_vt,
+                                                             c->ct_vpsi);
     }
   });
   prof_end(c);
 }
 template <typename C> static int density_groups(amdk_ctx *c, int T) {
   const Geom &g = c->geom;
-  const size_t sm = pencil_acc_smem(g.n2) + pencil_smem<C>(g.n2, c->pg.nz);
+  const size_t sm = pencil_acc_smem(g.n2) + pencil_smem<C>(g.n2, c->pg.nz, c->ct_dens);
   auto it = c->pencil_grp_cache.find(T);
   if (it == c->pencil_grp_cache.end())
     it = c->pencil_grp_cache
-             .emplace(T, pencil_density_groups(g.n1, T, c->nsm, pencil_threads(sm) == PNT ? 1 : 2, c->pencil_groups))
+             .emplace(T, pencil_density_groups(g.n1, T, c->nsm, (int)std::max<size_t>(1, (228 * 1024) / (sm + 1024)),
+                                               c->pencil_groups))
              .first;
   return it->second;
 }
 template <typename C> static void pencil_density(amdk_ctx *c, int p0, int T) {
   const Geom &g = c->geom;
-  const size_t sm = pencil_acc_smem(g.n2) + pencil_smem<C>(g.n2, c->pg.nz);
-  const int nt = pencil_threads(sm);
+  const size_t sm = pencil_acc_smem(g.n2) + pencil_smem<C>(g.n2, c->pg.nz, c->ct_dens);
   const int grp = density_groups<C>(c, T);
   const int per = (T + grp - 1) / grp;
   const double npt = (double)g.n1 * g.n2 * g.n3;
@@ -431,8 +444,8 @@ template <typename C> static void pencil_density(amdk_ctx *c, int p0, int T) {
     if constexpr (N > 0) {
       smem_opt_in<k_pencil_density<C, N>>();
       ++c->nlaunch;
-      k_pencil_density<C, N><<<dim3(g.n1, grp), nt, sm, c->st>>>(c->pg, plan<C>(c, 1), (const C *)c->d_rb, T, per,
-                                                                 c->d_wa + p0, c->d_wb + p0, c->d_rhopart);
+      k_pencil_density<C, N><<<dim3(g.n1, grp), PNT, sm, c->st>>>(c->pg, plan<C>(c, 1), (const C *)c->d_rb, T, per,
+                                                                  c->d_wa + p0, c->d_wb + p0, c->d_rhopart, c->ct_dens);
     }
   });
   prof_end(c);
@@ -460,8 +473,8 @@ template <typename C> static int density_t(amdk_ctx *c) {
       pencil_density<C>(c, p0, T);
     }
     ++c->nlaunch;
-    k_rho_reduce_t<<<dim3((g.n3 + 31) / 32, (g.n1 + 31) / 32, g.n2), dim3(32, 8), 0, c->st>>>(
-        g.n1, g.n2, g.n3, ng, c->d_rhopart, c->d_rho);
+    k_rho_reduce_p<<<dim3((g.n1 + 31) / 32, (g.n1 + 31) / 32, g.n1), dim3(32, 8), 0, c->st>>>(
+        g.n1, c->pn1, c->pn2, ng, c->d_rhopart, c->d_rho);
   } else {
   CK(cudaMemsetAsync(c->d_rho, 0, sizeof(double) * (size_t)g.n1 * g.n2 * g.n3, c->st));
   for (int p0 = 0; p0 < c->npairs; p0 += c->batch) {
@@ -524,12 +537,12 @@ static int do_potential(amdk_ctx *c) {
                        cudaMemcpyDeviceToDevice, c->st));
   if (c->pencil_vpsi) {
     // V in the x-plane-major layout the pencil kernel reads
-    dim3 gt((g.n1 + 31) / 32, (g.n3 + 31) / 32, g.n2);
+    dim3 gt((g.n1 + 31) / 32, (g.n1 + 31) / 32, g.n1);
     ++c->nlaunch;
     if (c->precision == AMDK_MIXED)
-      k_v_transpose<float><<<gt, dim3(32, 8), 0, c->st>>>(g.n1, g.n2, g.n3, c->d_vpot, (float *)c->d_vt);
+      k_v_permute<float><<<gt, dim3(32, 8), 0, c->st>>>(g.n1, c->pn1, c->pn2, c->d_vpot, (float *)c->d_vt);
     else
-      k_v_transpose<double><<<gt, dim3(32, 8), 0, c->st>>>(g.n1, g.n2, g.n3, c->d_vpot, (double *)c->d_vt);
+      k_v_permute<double><<<gt, dim3(32, 8), 0, c->st>>>(g.n1, c->pn1, c->pn2, c->d_vpot, (double *)c->d_vt);
   }
   CK(cudaGetLastError());
   return 0;
@@ -692,10 +705,11 @@ static int do_ortho(amdk_ctx *c) {
                  &zero, c->d_gam, n));
   ++c->nlaunch;
   k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c0, c->d_c0, c->d_gam, c->d_occ, 0, 1);
-  const size_t sm = (size_t)n * n * sizeof(double);
+  const int np = (n + CHOL_B - 1) / CHOL_B * CHOL_B;
+  const size_t sm = ((size_t)np * (np + 1) + (size_t)CHOL_B * np) * sizeof(double);
   ++c->nlaunch;
-  if (sm <= 200 * 1024 && n <= 1024)
-    k_chol_inv_s<<<1, 1024, sm, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
+  if (n <= CHOL_NMAX)
+    k_chol_inv_s<<<1, CHOL_NT, sm, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
   else
     k_chol_inv<<<1, 1024, 0, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
   int info = 0;
@@ -705,10 +719,10 @@ static int do_ortho(amdk_ctx *c) {
     set_error("overlap matrix not positive definite at leading minor " + std::to_string(info));
     return AMDK_ERR_NOT_SPD;
   }
-  // C0 <- C0 U^{-1} (DTRMM, wfn_initialize.f90:485) as a GEMM into the spare
-  // buffer, then swap the buffers
-  CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, (const double *)c->d_c0, K, c->d_uinv, n, &zero,
-                 (double *)c->d_cp, K));
+  // C0 <- C0 U^{-1} (DTRMM, wfn_initialize.f90:485) out of place into the
+  // spare buffer, then swap the buffers
+  CB(cublasDtrmm(c->cb, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, K, n, &one,
+                 c->d_uinv, n, (const double *)c->d_c0, K, (double *)c->d_cp, K));
   std::swap(c->d_c0, c->d_cp);
   ++c->nlaunch;
   k_zclean<<<nblk(n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c0);
@@ -850,9 +864,21 @@ static int build_device(amdk_ctx *c) {
   }
   set_smem_attrs<double2>();
   set_smem_attrs<float2>();
-  cudaFuncSetAttribute(k_cholesky_upper, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_chol_inv_s, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  {
+    // constant twiddles of the register DFTs: W_R^m = exp(-2 pi i m/R), R = 2..16
+    std::vector<double2> twd(CTW_LEN);
+    std::vector<float2> twf(CTW_LEN);
+    for (int R = 2; R <= 16; ++R)
+      for (int m = 0; m < R; ++m) {
+        const double ang = 8.0 * std::atan(1.0) * m / R;
+        twd[ctw_off(R) + m] = make_double2(std::cos(ang), -std::sin(ang));
+        twf[ctw_off(R) + m] = make_float2((float)std::cos(ang), (float)-std::sin(ang));
+      }
+    CK(cudaMemcpyToSymbol(c_twd, twd.data(), sizeof(double2) * CTW_LEN));
+    CK(cudaMemcpyToSymbol(c_twf, twf.data(), sizeof(float2) * CTW_LEN));
+  }
+  CK(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  CK(cudaFuncSetAttribute(k_chol_inv_s, cudaFuncAttributeMaxDynamicSharedMemorySize, 216 * 1024));
   // G vectors
   RC(c->up(&c->d_inyh, h.inyh));
   RC(c->up(&c->d_hg, h.hg));
@@ -901,9 +927,21 @@ static int build_device(amdk_ctx *c) {
     with_n(n1, [&](auto NC) { known = decltype(NC)::value > 0; });
     const bool ok = (n1 == n2 && n2 == n3) && known;
     const size_t lim = 227 * 1024;
-    const size_t vs = ((size_t)g.nz[0] * (n1 + 1) + 2 * (size_t)PL * n1 + n1) * csz;
-    c->pencil_vpsi = ok && vs <= lim;
-    c->pencil_density = ok && vs + pencil_acc_smem(n1) <= lim;
+    const int nz0 = g.nz[0];
+    if (ok) {
+      c->pn1 = fft_n1(n1);
+      c->pn2 = n1 / c->pn1;
+      // V(r)psi: two blocks per SM when the tile can stay at least half the
+      // plane wide, else one; the density block carries its accumulator
+      const bool mixed = c->precision == AMDK_MIXED;
+      int ct2 = mixed ? pencil_tile<float2>(n1, nz0, 0, lim / 2) : pencil_tile<double2>(n1, nz0, 0, lim / 2);
+      int ct1 = mixed ? pencil_tile<float2>(n1, nz0, 0, lim) : pencil_tile<double2>(n1, nz0, 0, lim);
+      c->ct_vpsi = (2 * ct2 >= n1) ? ct2 : ct1;
+      c->ct_dens = mixed ? pencil_tile<float2>(n1, nz0, pencil_acc_smem(n1), lim)
+                         : pencil_tile<double2>(n1, nz0, pencil_acc_smem(n1), lim);
+    }
+    c->pencil_vpsi = ok && c->ct_vpsi >= 8;
+    c->pencil_density = ok && c->ct_dens >= 8;
     const char *env = getenv("AMDK_NO_PENCIL");
     if (env && env[0] == '1') c->pencil_vpsi = c->pencil_density = false;
     int dev = 0;
@@ -934,7 +972,11 @@ static int build_device(amdk_ctx *c) {
     RC(c->up(&c->d_zinv, zinv));
     RC(c->up(&c->d_postp, postp));
     RC(c->up(&c->d_postm, postm));
-    c->pg = PencilGeom{n1, n2, n3, h.ngrays, g.nz[0], c->d_rpos, c->d_zinv, c->d_zlist[0]};
+    std::vector<int> gmapt((size_t)n1 * h.ngrays);
+    for (int r = 0; r < h.ngrays; r++)
+      for (int k = 0; k < n1; k++) gmapt[(size_t)k * h.ngrays + r] = gmap[(size_t)r * n1 + k];
+    RC(c->up(&c->d_gmapt, gmapt));
+    c->pg = PencilGeom{n1, n2, n3, h.ngrays, g.nz[0], c->d_rpos, c->d_zinv, c->d_zlist[0], c->d_gmapt};
     c->pencil_groups = std::max(1, std::min(c->batch, 16));
     if (c->pencil_density) RC(c->alloc(&c->d_rhopart, (size_t)c->pencil_groups * npt));
     if (c->pencil_vpsi) {

@@ -218,6 +218,145 @@ template <typename C, int N> __device__ __forceinline__ void load_tw(C *tw, cons
   }
 }
 
+// ---------------------------------------------------------------- register FFT
+// Small DFTs held in registers (R <= 16 with factors 2, 3, 4, 5) and the
+// two-level line transform N = N1*N2 built on them: each thread loads the N1
+// (or N2) elements of one sub-transform, works in registers and writes back,
+// so a length-N line costs two shared-memory round trips.  Twiddles
+// W_R^m = exp(-2 pi i m/R) of the small DFTs (R = 2..16) sit in constant
+// memory at ctw_off(R) + m and are filled by the host.
+__host__ __device__ constexpr int ctw_off(int R) { return R * (R - 1) / 2 - 1; }
+constexpr int CTW_LEN = ctw_off(17);
+__constant__ double2 c_twd[CTW_LEN];
+__constant__ float2 c_twf[CTW_LEN];
+template <typename C> __device__ __forceinline__ C ctw(int i);
+template <> __device__ __forceinline__ double2 ctw<double2>(int i) { return c_twd[i]; }
+template <> __device__ __forceinline__ float2 ctw<float2>(int i) { return c_twf[i]; }
+
+__host__ __device__ constexpr int reg_radix(int r) { return (r % 4 == 0) ? 4 : (r % 2 == 0) ? 2 : (r % 3 == 0) ? 3 : 5; }
+// N = N1 * N2 with N1 <= N2 <= 16 and N1 as large as possible (0: none)
+__host__ __device__ constexpr int fft_n1(int n) {
+  int best = 0;
+  for (int d = 2; d <= 16; ++d)
+    if (n % d == 0 && n / d <= 16 && d <= n / d) best = d;
+  return best;
+}
+
+// y_k = sum_j v_j exp(SG 2 pi i jk/R), natural order in and out
+template <typename C, int R, int SG> struct Dft {
+  static __device__ __forceinline__ void run(C (&v)[R]) {
+    if constexpr (R == 2 || R == 3 || R == 4 || R == 5) {
+      dft_r(v, R, SG);
+    } else if constexpr (R > 5) {
+      constexpr int A = reg_radix(R), B = R / A;
+      // j = j2 + B*j1: DFT_A over j1, twiddle W_R^(j2 k1), DFT_B over j2
+#pragma unroll
+      for (int j2 = 0; j2 < B; ++j2) {
+        C a[A];
+#pragma unroll
+        for (int j1 = 0; j1 < A; ++j1) a[j1] = v[j2 + B * j1];
+        Dft<C, A, SG>::run(a);
+#pragma unroll
+        for (int k1 = 0; k1 < A; ++k1) {
+          if ((j2 * k1) % R == 0) {
+            v[j2 + B * k1] = a[k1];
+          } else {
+            C w = ctw<C>(ctw_off(R) + (j2 * k1) % R);
+            if (SG > 0) w.y = -w.y;
+            v[j2 + B * k1] = cmul(a[k1], w);
+          }
+        }
+      }
+      C o[R];
+#pragma unroll
+      for (int k1 = 0; k1 < A; ++k1) {
+        C b[B];
+#pragma unroll
+        for (int j2 = 0; j2 < B; ++j2) b[j2] = v[j2 + B * k1];
+        Dft<C, B, SG>::run(b);
+#pragma unroll
+        for (int k2 = 0; k2 < B; ++k2) o[k1 + A * k2] = b[k2];
+      }
+#pragma unroll
+      for (int k = 0; k < R; ++k) v[k] = o[k];
+    }
+  }
+};
+
+// v[k] *= W_N^(SG j k), k = 1..R-1, from the shared table tw[e] = exp(-2 pi i e/N)
+template <typename C, int N, int R, int SG>
+__device__ __forceinline__ void twiddle_n(C (&v)[R], int j, const C *tw) {
+  int e = 0;
+#pragma unroll
+  for (int k = 1; k < R; ++k) {
+    e += j;
+    if (e >= N) e -= N;
+    C w = tw[e];
+    if (SG > 0) w.y = -w.y;
+    v[k] = cmul(v[k], w);
+  }
+}
+
+// Length-N transforms of nrow rows (row r at P + r*stride), in place.
+// nat_to_perm: natural order in, X[k1 + N1*k2] left at position k1*N2 + k2.
+// perm_to_nat: that permuted order in, natural order out.  Each phase's
+// sub-transform reads and writes the same positions, so a phase needs no
+// barrier inside; the two phases are separated by one.
+template <typename C, int N, int SG>
+__device__ __forceinline__ void rows_nat_to_perm(C *P, int nrow, int stride, const C *tw) {
+  constexpr int N1 = fft_n1(N), N2 = N / N1;
+  for (int idx = threadIdx.x; idx < nrow * N2; idx += blockDim.x) {
+    const int r = idx % nrow, j2 = idx / nrow;
+    C *row = P + r * stride;
+    C v[N1];
+#pragma unroll
+    for (int j1 = 0; j1 < N1; ++j1) v[j1] = row[j2 + N2 * j1];
+    Dft<C, N1, SG>::run(v);
+    twiddle_n<C, N, N1, SG>(v, j2, tw);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) row[k1 * N2 + j2] = v[k1];
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < nrow * N1; idx += blockDim.x) {
+    const int r = idx % nrow, k1 = idx / nrow;
+    C *row = P + r * stride + k1 * N2;
+    C u[N2];
+#pragma unroll
+    for (int j2 = 0; j2 < N2; ++j2) u[j2] = row[j2];
+    Dft<C, N2, SG>::run(u);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) row[k2] = u[k2];
+  }
+  __syncthreads();
+}
+template <typename C, int N, int SG>
+__device__ __forceinline__ void rows_perm_to_nat(C *P, int nrow, int stride, const C *tw) {
+  constexpr int N1 = fft_n1(N), N2 = N / N1;
+  for (int idx = threadIdx.x; idx < nrow * N1; idx += blockDim.x) {
+    const int r = idx % nrow, k1 = idx / nrow;
+    C *row = P + r * stride + k1 * N2;
+    C u[N2];
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) u[k2] = row[k2];
+    Dft<C, N2, SG>::run(u);
+    twiddle_n<C, N, N2, SG>(u, k1, tw);
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) row[n2] = u[n2];
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < nrow * N2; idx += blockDim.x) {
+    const int r = idx % nrow, n2 = idx / nrow;
+    C *row = P + r * stride;
+    C w[N1];
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) w[k1] = row[k1 * N2 + n2];
+    Dft<C, N1, SG>::run(w);
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) row[n2 + N2 * n1] = w[n1];
+  }
+  __syncthreads();
+}
+
 // ---------------------------------------------------------------- geometry
 struct Geom {
   int n1, n2, n3;

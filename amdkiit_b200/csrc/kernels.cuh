@@ -497,44 +497,6 @@ __global__ void k_pcg_update(long tot, int istep, const double *scal, double2 *c
 }
 __global__ void k_copy_scalar(const double *src, double *dst) { *dst = *src; }
 
-// Cholesky S = U^T U of the upper triangle (DPOTRF('U'), UINV
-// wfn_initialize.f90:504-530), one block; A column-major n x n.  Sets *info
-// to j+1 if the leading minor j is not positive definite.
-__global__ void k_cholesky_upper(int n, double *A, int *info) {
-  extern __shared__ double shc[];
-  const bool in_smem = (size_t)n * n * sizeof(double) <= 200 * 1024;
-  double *M = in_smem ? shc : A;
-  if (in_smem)
-    for (long k = threadIdx.x; k < (long)n * n; k += blockDim.x) M[k] = A[k];
-  __shared__ double piv;
-  __shared__ int bad;
-  if (threadIdx.x == 0) bad = 0;
-  __syncthreads();
-  for (int j = 0; j < n; ++j) {
-    if (threadIdx.x == 0) {
-      double d = M[j + (long)n * j];
-      if (!(d > 0.0)) { bad = j + 1; piv = 1.0; }
-      else piv = sqrt(d);
-      M[j + (long)n * j] = piv;
-    }
-    __syncthreads();
-    if (bad) break;
-    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) M[j + (long)n * i] /= piv;
-    __syncthreads();
-    // trailing update of the upper triangle: M(a,b) -= U(j,a) U(j,b), j < a <= b
-    const int m = n - j - 1;
-    const long cnt = (long)m * m;
-    for (long k = threadIdx.x; k < cnt; k += blockDim.x) {
-      int a = j + 1 + (int)(k % m), b = j + 1 + (int)(k / m);
-      if (a <= b) M[a + (long)n * b] -= M[j + (long)n * a] * M[j + (long)n * b];
-    }
-    __syncthreads();
-  }
-  if (in_smem)
-    for (long k = threadIdx.x; k < (long)n * n; k += blockDim.x) A[k] = M[k];
-  if (threadIdx.x == 0) *info = bad;
-}
-
 // Cholesky S = U^T U (upper, DPOTRF('U')) followed by U <- U^{-1} (DTRTRI),
 // UINV of wfn_initialize.f90:504-530, in one block.  Column step j subtracts
 // S(j,a) S(j,b) / S(j,j) from the trailing upper triangle (one barrier per
@@ -594,74 +556,142 @@ __global__ void k_chol_inv(int n, double *A, double *Ui, int *info) {
   if (threadIdx.x == 0) *info = 0;
 }
 
-// Shared-memory Cholesky + inverse for n with n*n doubles in shared memory.
-// Threads form groups of g (a power of two); group c owns columns
-// b = c, c + ncols, ...  In step j it applies S(a,b) -= S(j,a) S(j,b)/S(j,j)
-// for j < a <= b (its g threads split the rows a).  The inverse of the
-// upper factor is formed column by column in place (DTRTI2 order):
-// X(i,j) = -X(j,j) sum_{k=i}^{j-1} X(i,k) U(k,j), the g threads of row i
-// splitting the sum.  Same contract as k_chol_inv.
-__global__ void __launch_bounds__(1024) k_chol_inv_s(int n, const double *A, double *Ui, int *info) {
-  extern __shared__ double M[];
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int k = tid; k < n * n; k += nt) M[k] = A[k];
-  int g = 1;
-  while (g < 32 && 2 * g * n <= nt) g *= 2;
-  const int sub = tid % g, grp = tid / g, ngrp = nt / g;
-  __shared__ int bad;
-  if (tid == 0) bad = 0;
-  __syncthreads();
-  for (int j = 0; j < n; ++j) {
-    const double d = M[j + n * j];
-    if (!(d > 0.0)) {
-      if (tid == 0) bad = j + 1;
-      break;  // uniform: every thread read the same d
+// Shared-memory blocked Cholesky + inverse for n <= CHOL_NMAX, one block of
+// CHOL_NT threads.  The matrix is padded to np = 16*ceil(n/16) with the
+// identity and held in shared memory with leading dimension np+1.  Per
+// 16-column block k (right-looking): one warp factors the diagonal block in
+// registers (lane l holds column l, rows of other lanes arrive by shuffles)
+// and inverts it in place (X_kk = U_kk^{-1}, back substitution per column);
+// all threads then form the panel U_k,c = X_kk^T S_k,c and update the
+// trailing upper triangle S_c,d -= U_k,c^T U_k,d.  The inverse is completed
+// by block back substitution, j = last ... 0: X_j,c = X_jj R_j,c (c > j),
+// then R_i,c -= U_i,j X_j,c (i < j, c >= j; the block c = j becomes
+// -U_i,j X_jj), with R = I to start.  A non-positive pivot sets *info to its
+// 1-based index.  Same contract as k_chol_inv.
+constexpr int CHOL_NMAX = 144;
+constexpr int CHOL_NT = 512;
+constexpr int CHOL_B = 16;
+__device__ __forceinline__ void warp_chol_inv16(double *D, int ld, int base, int *bad) {
+  const int l = threadIdx.x & 31;
+  const bool own = l < CHOL_B;
+  double col[CHOL_B];
+#pragma unroll
+  for (int r = 0; r < CHOL_B; ++r) col[r] = own ? D[r + ld * l] : 0.0;
+#pragma unroll
+  for (int j = 0; j < CHOL_B; ++j) {
+    const double d = __shfl_sync(0xffffffffu, col[j], j);
+    if (!(d > 0.0) && l == 0 && *bad == 0) *bad = base + j + 1;
+    const double inv = rsqrt(d);
+    if (l == j) col[j] = d * inv;
+    else if (l > j) col[j] *= inv;
+#pragma unroll
+    for (int a = j + 1; a < CHOL_B; ++a) {
+      const double uja = __shfl_sync(0xffffffffu, col[j], a);
+      if (l >= a) col[a] -= uja * col[j];
     }
-    const double inv = 1.0 / d;
-    for (int b = j + 1 + grp; b < n; b += ngrp) {
-      const double mjb = M[j + n * b] * inv;
-      for (int a = j + 1 + sub; a <= b; a += g) M[a + n * b] -= M[j + n * a] * mjb;
+  }
+  if (own) {
+#pragma unroll
+    for (int r = 0; r < CHOL_B; ++r)
+      if (r <= l) D[r + ld * l] = col[r];
+  }
+  __syncwarp();
+  double x[CHOL_B];
+#pragma unroll
+  for (int i = CHOL_B - 1; i >= 0; --i) {
+    double t = 0.0;
+#pragma unroll
+    for (int k = i + 1; k < CHOL_B; ++k) t += D[i + ld * k] * x[k];
+    const double di = 1.0 / D[i + ld * i];
+    x[i] = (i == l) ? di : ((i < l) ? -t * di : 0.0);
+  }
+  __syncwarp();
+  if (own) {
+#pragma unroll
+    for (int r = 0; r < CHOL_B; ++r)
+      if (r <= l) D[r + ld * l] = x[r];
+  }
+}
+
+__global__ void __launch_bounds__(CHOL_NT) k_chol_inv_s(int n, const double *A, double *Ui, int *info) {
+  extern __shared__ double M[];
+  __shared__ int bad;
+  const int np = (n + CHOL_B - 1) / CHOL_B * CHOL_B, ld = np + 1, nb = np / CHOL_B;
+  double *Ut = M + (size_t)np * ld;  // [CHOL_B][np]: a column block of U, rows above it
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
+  const int hr = lane & 15, hc = 2 * w + (lane >> 4);  // half-warp: row hr of column hc (+32p)
+  if (tid == 0) bad = 0;
+  for (int b = w; b < np; b += nw)
+    for (int a = lane; a < np; a += 32)
+      M[a + ld * b] = (a < n && b < n) ? A[a + (long)n * b] : (a == b ? 1.0 : 0.0);
+  __syncthreads();
+  for (int kb = 0; kb < nb; ++kb) {
+    const int k0 = CHOL_B * kb, c0 = k0 + CHOL_B;
+    if (w == 0) warp_chol_inv16(M + k0 + ld * k0, ld, k0, &bad);
+    __syncthreads();
+    if (bad) break;
+    // panel: U(k0+r, c) = sum_{s<=r} X(s,r) S(k0+s, c); column c lives in one half-warp
+    for (int p = 0; c0 + 32 * p < np; ++p) {
+      const int c = c0 + hc + 32 * p;
+      double t = 0.0;
+      if (c < np)
+        for (int s = 0; s <= hr; ++s) t += M[(k0 + s) + ld * (k0 + hr)] * M[(k0 + s) + ld * c];
+      __syncwarp();
+      if (c < np) M[(k0 + hr) + ld * c] = t;
+      __syncwarp();
+    }
+    __syncthreads();
+    // trailing update: warp per column c, lanes over rows r <= c
+    for (int c = c0 + w; c < np; c += nw) {
+      double uc[CHOL_B];
+#pragma unroll
+      for (int s = 0; s < CHOL_B; ++s) uc[s] = M[(k0 + s) + ld * c];
+      for (int r = c0 + lane; r <= c; r += 32) {
+        double t = 0.0;
+#pragma unroll
+        for (int s = 0; s < CHOL_B; ++s) t += M[(k0 + s) + ld * r] * uc[s];
+        M[r + ld * c] -= t;
+      }
     }
     __syncthreads();
   }
-  __syncthreads();
   if (bad) {
     if (tid == 0) *info = bad;
     return;
   }
-  // U(a,b) = S(a,b) / sqrt(S(a,a)) (a < b), then the diagonal
-  for (int k = tid; k < n * n; k += nt) {
-    const int a = k % n, b = k / n;
-    if (a < b) M[k] = M[k] / sqrt(M[a + n * a]);
-  }
-  __syncthreads();
-  for (int a = tid; a < n; a += nt) M[a + n * a] = sqrt(M[a + n * a]);
-  __syncthreads();
-  // in-place inverse of the upper factor, column by column
-  for (int j = 0; j < n; ++j) {
-    const double xjj = 1.0 / M[j + n * j];
-    const int nrow = (j + ngrp - 1) / ngrp;  // same for every thread: the shuffles below see full warps
-    double val[4];
-    for (int c = 0; c < nrow; ++c) {
-      const int i = grp + c * ngrp;
+  for (int jb = nb - 1; jb >= 0; --jb) {
+    const int k0 = CHOL_B * jb, c0 = k0 + CHOL_B;
+    // X_j,c = X_jj R_j,c, c >= c0
+    for (int p = 0; c0 + 32 * p < np; ++p) {
+      const int c = c0 + hc + 32 * p;
       double t = 0.0;
-      if (i < j)
-        for (int k = i + sub; k < j; k += g) t += M[i + n * k] * M[k + n * j];
-      for (int o = g >> 1; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o, g);
-      if (c < 4) val[c] = -xjj * t;
+      if (c < np)
+        for (int s = hr; s < CHOL_B; ++s) t += M[(k0 + hr) + ld * (k0 + s)] * M[(k0 + s) + ld * c];
+      __syncwarp();
+      if (c < np) M[(k0 + hr) + ld * c] = t;
+      __syncwarp();
+    }
+    if (k0 == 0) break;
+    // copy U_i,j (rows i < k0) aside, then R_i,c -= U_i,j X_j,c for c >= k0
+    for (int s = w; s < CHOL_B; s += nw)
+      for (int i = lane; i < k0; i += 32) Ut[s * np + i] = M[i + ld * (k0 + s)];
+    __syncthreads();
+    for (int c = k0 + w; c < np; c += nw) {
+      const int smax = (c < c0) ? c - k0 : CHOL_B - 1;  // X_jj is upper triangular
+      double xc[CHOL_B];
+#pragma unroll
+      for (int s = 0; s < CHOL_B; ++s) xc[s] = (s <= smax) ? M[(k0 + s) + ld * c] : 0.0;
+      for (int i = lane; i < k0; i += 32) {
+        double t = 0.0;
+#pragma unroll
+        for (int s = 0; s < CHOL_B; ++s) t += Ut[s * np + i] * xc[s];
+        M[i + ld * c] = (c < c0) ? -t : M[i + ld * c] - t;
+      }
     }
     __syncthreads();
-    for (int c = 0; c < nrow && c < 4; ++c) {
-      const int i = grp + c * ngrp;
-      if (i < j && sub == 0) M[i + n * j] = val[c];
-    }
-    if (tid == 0) M[j + n * j] = xjj;
-    __syncthreads();
   }
-  for (int k = tid; k < n * n; k += nt) {
-    const int a = k % n, b = k / n;
-    Ui[k] = (a <= b) ? M[k] : 0.0;
-  }
+  for (int b = w; b < n; b += nw)
+    for (int a = lane; a < n; a += 32) Ui[a + (long)n * b] = (a <= b) ? M[a + ld * b] : 0.0;
   if (tid == 0) *info = 0;
 }
 

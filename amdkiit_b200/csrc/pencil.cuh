@@ -4,9 +4,12 @@
 // The x pass writes the ray buffer transposed, RT[t][kx][ray], so that one
 // block can take one x-plane of one band pair: it scatters the plane's rays
 // into a shared-memory slab plane P[zi][ky] (only the z planes that carry
-// rays), runs the y FFTs, then per chunk of ky columns the z FFT, V(r)*psi
-// and the inverse z FFT (or the |psi|^2 accumulation), the inverse y FFTs,
-// and gathers the rays back.  No slab or grid buffer goes through HBM; the
+// rays), runs the y transforms of those rows, then per tile of columns the
+// z transform, V(r)*psi and the inverse z transform (or the |psi|^2
+// accumulation), the inverse y transforms, and gathers the rays back.  Every
+// line transform is the two-level register FFT of fft.cuh; the backward y
+// transform leaves its output in the permuted order the forward one takes,
+// so no pass reorders data.  No slab or grid buffer goes through HBM: the
 // only HBM traffic is the ray buffer (read and written once per pass), V
 // (L2 resident) and the coefficients.
 #pragma once
@@ -19,110 +22,127 @@ struct PencilGeom {
   const int *rpos;   // [nray] zi*(n2+1) + ky of the ray in the padded plane
   const int *zinv;   // [n3] slab index of kz, -1 outside the slab
   const int *zlist;  // [nz] kz of slab plane
+  const int *gmapt;  // [n1][nray] G code of (ray, kx): +(ig+1) at +G, -(ig+1) at -G, 0 empty
 };
 
-constexpr int PL = 16;    // lines per scratch tile in the pencil kernel
-constexpr int PNT = 512;  // maximum threads per pencil block
-// The plane P[zi][ky] is stored with row stride N+1 so that the y-tile
-// gathers (stride one row per line) hit distinct shared-memory banks.
+constexpr int PNT = 512;  // threads per pencil block
+// Shared-memory rows (slab plane P, column tile S, density accumulator) have
+// stride N+1 so that threads taking consecutive rows hit distinct banks.
 
-// Backward x pass with the pair pack, output transposed: RT[t][kx][r]
+constexpr int XL = 32;  // lines per x-pass block
+// Backward x pass with the band-pair pack (psi_a + i psi_b, the pack of
+// vpsi and eval_density), output transposed: RT[t][kx][r].  Block = XL lines
+// (consecutive rays) x N2 threads; thread (l, j2) gathers the N1 elements
+// kx = j2 + N2*j1 of its ray straight from the coefficients, the second
+// phase writes kx = k1 + N1*k2 back with consecutive threads on consecutive
+// rays.
 template <typename C, int N>
-__global__ void __launch_bounds__(256) k_xt_bwd_pair(const double2 *__restrict__ c0, int ngpw, int nstate, int band0,
-                                                     int T, Geom g, Plan<C> p, C *__restrict__ rt) {
+__global__ void __launch_bounds__(512) k_xt_bwd_pair(const double2 *__restrict__ c0, int ngpw, int nstate, int band0,
+                                                     int T, PencilGeom pg, Plan<C> p, C *__restrict__ rt) {
+  typedef decltype(C().x) Rl;
+  constexpr int N1 = fft_n1(N), N2 = N / N1, NP = N + 1;
   extern __shared__ unsigned char smraw[];
-  constexpr int L = 16, ES = L + 1;
-  C *sa = reinterpret_cast<C *>(smraw);
-  const int n1 = g.n1, R = g.nray[0];
-  C *sb = sa + n1 * ES;
-  C *tw = sb + n1 * ES;
+  C *S = reinterpret_cast<C *>(smraw);
+  C *tw = S + XL * NP;
   load_tw<C, N>(tw, p);
-  const long line0 = (long)blockIdx.x * L;
+  __syncthreads();
+  const int R = pg.nray;
+  const long line0 = (long)blockIdx.x * XL;
   const long nlines = (long)T * R;
-  for (int idx = threadIdx.x; idx < L * n1; idx += blockDim.x) {
-    const int l = idx / n1, k = idx % n1;
+  {
+    const int l = threadIdx.x % XL, j2 = threadIdx.x / XL;
     const long line = line0 + l;
-    C v = czero<C>();
+    C v[N1];
+#pragma unroll
+    for (int j1 = 0; j1 < N1; ++j1) v[j1] = czero<C>();
     if (line < nlines) {
       const int t = (int)(line / R), r = (int)(line % R);
-      const int code = g.gmap[(long)r * n1 + k];
-      const int ig = (code > 0 ? code : -code) - 1;
-      if (code != 0 && ig < ngpw) {
-        const int ba = band0 + 2 * t, bb = ba + 1;
-        double2 a = c0[(long)ba * ngpw + ig];
-        double2 b = (bb < nstate) ? c0[(long)bb * ngpw + ig] : make_double2(0.0, 0.0);
-        if (code > 0) v = mk((decltype(v.x))(a.x - b.y), (decltype(v.x))(a.y + b.x));
-        else v = mk((decltype(v.x))(a.x + b.y), (decltype(v.x))(-a.y + b.x));
+      const int ba = band0 + 2 * t, bb = ba + 1;
+      const double2 *ca = c0 + (long)ba * ngpw;
+      const double2 *cb = c0 + (long)bb * ngpw;
+      const bool hb = bb < nstate;
+#pragma unroll
+      for (int j1 = 0; j1 < N1; ++j1) {
+        const int code = pg.gmapt[(long)(j2 + N2 * j1) * R + r];
+        const int ig = (code > 0 ? code : -code) - 1;
+        if (code != 0 && ig < ngpw) {
+          const double2 a = ca[ig];
+          const double2 b = hb ? cb[ig] : make_double2(0.0, 0.0);
+          if (code > 0) v[j1] = mk((Rl)(a.x - b.y), (Rl)(a.y + b.x));
+          else v[j1] = mk((Rl)(a.x + b.y), (Rl)(-a.y + b.x));
+        }
       }
     }
-    sa[k * ES + l] = v;
+    Dft<C, N1, 1>::run(v);
+    twiddle_n<C, N, N1, 1>(v, j2, tw);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) S[l * NP + k1 * N2 + j2] = v[k1];
   }
   __syncthreads();
-  C *res = fft_tile<C, N, L, ES>(sa, sb, p, tw, +1);
-  // transposed store: consecutive threads take consecutive rays of one kx
-  for (int idx = threadIdx.x; idx < L * n1; idx += blockDim.x) {
-    const int k = idx / L, l = idx % L;
+  if (threadIdx.x < XL * N1) {
+    const int l = threadIdx.x % XL, k1 = threadIdx.x / XL;
     const long line = line0 + l;
+    C u[N2];
+#pragma unroll
+    for (int j2 = 0; j2 < N2; ++j2) u[j2] = S[l * NP + k1 * N2 + j2];
+    Dft<C, N2, 1>::run(u);
     if (line < nlines) {
       const int t = (int)(line / R), r = (int)(line % R);
-      rt[((long)t * n1 + k) * R + r] = res[k * ES + l];
+      C *o = rt + (long)t * pg.n1 * R + r;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) o[(long)(k1 + N1 * k2) * R] = u[k2];
     }
   }
 }
 
-// Forward x pass in place on the transposed ray buffer
+// Forward x pass in place on the transposed ray buffer (same blocking)
 template <typename C, int N>
-__global__ void __launch_bounds__(256) k_xt_fwd(int T, Geom g, Plan<C> p, C *__restrict__ rt) {
+__global__ void __launch_bounds__(512) k_xt_fwd(int T, PencilGeom pg, Plan<C> p, C *__restrict__ rt) {
+  constexpr int N1 = fft_n1(N), N2 = N / N1, NP = N + 1;
   extern __shared__ unsigned char smraw[];
-  constexpr int L = 16, ES = L + 1;
-  C *sa = reinterpret_cast<C *>(smraw);
-  const int n1 = g.n1, R = g.nray[0];
-  C *sb = sa + n1 * ES;
-  C *tw = sb + n1 * ES;
+  C *S = reinterpret_cast<C *>(smraw);
+  C *tw = S + XL * NP;
   load_tw<C, N>(tw, p);
-  const long line0 = (long)blockIdx.x * L;
+  __syncthreads();
+  const int R = pg.nray;
+  const long line0 = (long)blockIdx.x * XL;
   const long nlines = (long)T * R;
-  for (int idx = threadIdx.x; idx < L * n1; idx += blockDim.x) {
-    const int k = idx / L, l = idx % L;
+  {
+    const int l = threadIdx.x % XL, j2 = threadIdx.x / XL;
     const long line = line0 + l;
-    C v = czero<C>();
+    C v[N1];
     if (line < nlines) {
       const int t = (int)(line / R), r = (int)(line % R);
-      v = rt[((long)t * n1 + k) * R + r];
+      const C *in = rt + (long)t * pg.n1 * R + r;
+#pragma unroll
+      for (int j1 = 0; j1 < N1; ++j1) v[j1] = in[(long)(j2 + N2 * j1) * R];
+    } else {
+#pragma unroll
+      for (int j1 = 0; j1 < N1; ++j1) v[j1] = czero<C>();
     }
-    sa[k * ES + l] = v;
+    Dft<C, N1, -1>::run(v);
+    twiddle_n<C, N, N1, -1>(v, j2, tw);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) S[l * NP + k1 * N2 + j2] = v[k1];
   }
   __syncthreads();
-  C *res = fft_tile<C, N, L, ES>(sa, sb, p, tw, -1);
-  for (int idx = threadIdx.x; idx < L * n1; idx += blockDim.x) {
-    const int k = idx / L, l = idx % L;
+  if (threadIdx.x < XL * N1) {
+    const int l = threadIdx.x % XL, k1 = threadIdx.x / XL;
     const long line = line0 + l;
+    C u[N2];
+#pragma unroll
+    for (int j2 = 0; j2 < N2; ++j2) u[j2] = S[l * NP + k1 * N2 + j2];
+    Dft<C, N2, -1>::run(u);
     if (line < nlines) {
       const int t = (int)(line / R), r = (int)(line % R);
-      rt[((long)t * n1 + k) * R + r] = res[k * ES + l];
+      C *o = rt + (long)t * pg.n1 * R + r;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) o[(long)(k1 + N1 * k2) * R] = u[k2];
     }
   }
 }
 
-// y FFTs of the nz slab lines of the plane P[zi][ky] in tiles of PL lines
-template <typename C, int N>
-__device__ __forceinline__ void pencil_y(C *P, C *s0, C *s1, const Plan<C> &p, const C *tw, int nz, int sg) {
-  for (int z0 = 0; z0 < nz; z0 += PL) {
-    for (int idx = threadIdx.x; idx < PL * N; idx += blockDim.x) {
-      const int ky = idx / PL, l = idx % PL;
-      s0[idx] = (z0 + l < nz) ? P[(z0 + l) * (N + 1) + ky] : czero<C>();
-    }
-    __syncthreads();
-    C *res = fft_tile<C, N, PL, PL>(s0, s1, p, tw, sg);
-    for (int idx = threadIdx.x; idx < PL * N; idx += blockDim.x) {
-      const int ky = idx / PL, l = idx % PL;
-      if (z0 + l < nz) P[(z0 + l) * (N + 1) + ky] = res[idx];
-    }
-    __syncthreads();
-  }
-}
-
-// scatter the rays of plane kx of transform t into P (zero elsewhere)
+// scatter the rays of one x-plane into P (zero elsewhere)
 template <typename C, int N>
 __device__ __forceinline__ void pencil_scatter(C *P, const C *__restrict__ rt_plane, const PencilGeom &pg) {
   for (int idx = threadIdx.x; idx < pg.nz * (N + 1); idx += blockDim.x) P[idx] = czero<C>();
@@ -131,93 +151,133 @@ __device__ __forceinline__ void pencil_scatter(C *P, const C *__restrict__ rt_pl
   __syncthreads();
 }
 
-// One x-plane of one band pair through y, z, V(r), z, y (vpsi :311-340).
-// grid (n1, T); V_T[kx][ky][kz] in the working precision.
+// Backward z transform of the column tile q0 .. q0+ct-1 of P, first phase:
+// thread (column, j2) takes the slab planes at kz = j2 + N2*j1 (zero where
+// the slab has no plane) and leaves W_N^(j2 k1) DFT_N1 in S[col][k1*N2 + j2].
+template <typename C, int N>
+__device__ __forceinline__ void zcols_phase_a(const C *P, C *S, const int *zinv, int q0, int ct, const C *tw) {
+  constexpr int N1 = fft_n1(N), N2 = N / N1, NP = N + 1;
+  for (int idx = threadIdx.x; idx < ct * N2; idx += blockDim.x) {
+    const int qq = idx % ct, j2 = idx / ct;
+    C v[N1];
+#pragma unroll
+    for (int j1 = 0; j1 < N1; ++j1) {
+      const int zi = zinv[j2 + N2 * j1];
+      v[j1] = (zi >= 0) ? P[zi * NP + q0 + qq] : czero<C>();
+    }
+    Dft<C, N1, 1>::run(v);
+    twiddle_n<C, N, N1, 1>(v, j2, tw);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) S[qq * NP + k1 * N2 + j2] = v[k1];
+  }
+}
+
+// One x-plane of one band pair through y, z, V(r), z, y (vpsi,
+// wfn_initialize.f90:311-340).  grid (n1, T).  P[zi][q] holds the slab
+// plane (row stride N+1); after the backward y transform column q carries
+// ky = q/N2 + N1*(q%N2).  vp[kx][q][k'] is V at that ky and at
+// kz = k'/N2 + N1*(k'%N2), the order in which the z transform leaves psi.
 template <typename C, int N>
 __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C *__restrict__ rt,
-                                                     const decltype(C().x) *__restrict__ vt) {
+                                                     const decltype(C().x) *__restrict__ vp, int CTs) {
   typedef decltype(C().x) Rl;
+  constexpr int N1 = fft_n1(N), N2 = N / N1, NP = N + 1;
   extern __shared__ unsigned char smraw[];
   const int nz = pg.nz;
   C *P = reinterpret_cast<C *>(smraw);
-  C *s0 = P + nz * (N + 1);
-  C *s1 = s0 + PL * N;
-  C *tw = s1 + PL * N;
+  C *S = P + nz * NP;
+  C *tw = S + CTs * NP;
+  int *zinv = reinterpret_cast<int *>(tw + N);
   load_tw<C, N>(tw, p);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) zinv[i] = pg.zinv[i];
   const int kx = blockIdx.x, t = blockIdx.y;
   C *plane = rt + ((long)t * pg.n1 + kx) * pg.nray;
   pencil_scatter<C, N>(P, plane, pg);
-  pencil_y<C, N>(P, s0, s1, p, tw, nz, +1);
-  const Rl *V = vt + (long)kx * N * N;
-  for (int y0 = 0; y0 < N; y0 += PL) {
-    // column tile: element kz of column l (= ky - y0) at s0[kz*PL + l]
-    for (int idx = threadIdx.x; idx < PL * N; idx += blockDim.x) {
-      const int kz = idx / PL, l = idx % PL;
-      const int zi = pg.zinv[kz];
-      s0[idx] = (zi >= 0 && y0 + l < N) ? P[zi * (N + 1) + y0 + l] : czero<C>();
+  rows_nat_to_perm<C, N, 1>(P, nz, NP, tw);
+  const Rl *V = vp + (long)kx * N * N;
+  for (int q0 = 0; q0 < N; q0 += CTs) {
+    const int ct = min(CTs, N - q0);
+    zcols_phase_a<C, N>(P, S, zinv, q0, ct, tw);
+    __syncthreads();
+    // DFT_N2 -> psi(kz = k1 + N1*k2), times V, then the first phase of the
+    // forward z transform, in registers
+    for (int idx = threadIdx.x; idx < ct * N1; idx += blockDim.x) {
+      const int qq = idx % ct, k1 = idx / ct;
+      C *row = S + qq * NP + k1 * N2;
+      const Rl *vv = V + (long)(q0 + qq) * N + k1 * N2;
+      C u[N2];
+#pragma unroll
+      for (int j2 = 0; j2 < N2; ++j2) u[j2] = row[j2];
+      Dft<C, N2, 1>::run(u);
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) u[k2] = cscale(u[k2], vv[k2]);
+      Dft<C, N2, -1>::run(u);
+      twiddle_n<C, N, N2, -1>(u, k1, tw);
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) row[n2] = u[n2];
     }
     __syncthreads();
-    C *res = fft_tile<C, N, PL, PL>(s0, s1, p, tw, +1);
-    C *other = (res == s0) ? s1 : s0;
-    // V tile staged through the free buffer: coalesced along kz, row stride N+1
-    Rl *vs = reinterpret_cast<Rl *>(other);
-    for (int idx = threadIdx.x; idx < PL * N; idx += blockDim.x) {
-      const int l = idx / N, kz = idx % N;
-      vs[l * (N + 1) + kz] = (y0 + l < N) ? V[(long)(y0 + l) * N + kz] : (Rl)0;
-    }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < PL * N; idx += blockDim.x) {
-      const int kz = idx / PL, l = idx % PL;
-      res[idx] = cscale(res[idx], vs[l * (N + 1) + kz]);
-    }
-    __syncthreads();
-    C *out = fft_tile<C, N, PL, PL>(res, other, p, tw, -1);
-    for (int idx = threadIdx.x; idx < PL * nz; idx += blockDim.x) {
-      const int zi = idx / PL, l = idx % PL;
-      if (y0 + l < N) P[zi * (N + 1) + y0 + l] = out[pg.zlist[zi] * PL + l];
+    // second phase: x(kz = n2 + N2*n1), stored back for the slab planes only
+    for (int idx = threadIdx.x; idx < ct * N2; idx += blockDim.x) {
+      const int qq = idx % ct, n2 = idx / ct;
+      C w[N1];
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) w[k1] = S[qq * NP + k1 * N2 + n2];
+      Dft<C, N1, -1>::run(w);
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) {
+        const int zi = zinv[n2 + N2 * n1];
+        if (zi >= 0) P[zi * NP + q0 + qq] = w[n1];
+      }
     }
     __syncthreads();
   }
-  pencil_y<C, N>(P, s0, s1, p, tw, nz, -1);
+  rows_perm_to_nat<C, N, -1>(P, nz, NP, tw);
   for (int r = threadIdx.x; r < pg.nray; r += blockDim.x) plane[r] = P[pg.rpos[r]];
 }
 
-// Density: one x-plane for a group of band pairs; rho_part[grp][kx][ky][kz]
-// += sum_t wa_t Re^2 + wb_t Im^2 (density.f90:49-86).  grid (n1, ngroups).
+// Density: one x-plane for a group of band pairs (density.f90:49-86);
+// rho_part[grp][kx][q][k'] += wa_t Re^2 + wb_t Im^2 in the permuted (ky, kz)
+// order of the vpsi kernel.  grid (n1, ngroups).
 template <typename C, int N>
 __global__ void __launch_bounds__(PNT) k_pencil_density(PencilGeom pg, Plan<C> p, const C *__restrict__ rt, int T,
                                                         int per_group, const double *__restrict__ wa,
-                                                        const double *__restrict__ wb, double *__restrict__ rho_part) {
+                                                        const double *__restrict__ wb, double *__restrict__ rho_part,
+                                                        int CTs) {
+  constexpr int N1 = fft_n1(N), N2 = N / N1, NP = N + 1;
   extern __shared__ unsigned char smraw[];
   const int nz = pg.nz;
-  double *acc = reinterpret_cast<double *>(smraw);        // [ky][kz], row stride N+1
-  C *P = reinterpret_cast<C *>(acc + N * (N + 1));
-  C *s0 = P + nz * (N + 1);
-  C *s1 = s0 + PL * N;
-  C *tw = s1 + PL * N;
+  double *acc = reinterpret_cast<double *>(smraw);  // [q][k'], row stride N+1
+  C *P = reinterpret_cast<C *>(acc + N * NP);
+  C *S = P + nz * NP;
+  C *tw = S + CTs * NP;
+  int *zinv = reinterpret_cast<int *>(tw + N);
   load_tw<C, N>(tw, p);
-  for (int idx = threadIdx.x; idx < N * (N + 1); idx += blockDim.x) acc[idx] = 0.0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) zinv[i] = pg.zinv[i];
+  for (int idx = threadIdx.x; idx < N * NP; idx += blockDim.x) acc[idx] = 0.0;
   const int kx = blockIdx.x, grp = blockIdx.y;
   const int t0 = grp * per_group, t1 = min(T, t0 + per_group);
   for (int t = t0; t < t1; ++t) {
     const C *plane = rt + ((long)t * pg.n1 + kx) * pg.nray;
     pencil_scatter<C, N>(P, plane, pg);
-    pencil_y<C, N>(P, s0, s1, p, tw, nz, +1);
+    rows_nat_to_perm<C, N, 1>(P, nz, NP, tw);
     const double fa = wa[t], fb = wb[t];
-    for (int y0 = 0; y0 < N; y0 += PL) {
-      for (int idx = threadIdx.x; idx < PL * N; idx += blockDim.x) {
-        const int kz = idx / PL, l = idx % PL;
-        const int zi = pg.zinv[kz];
-        s0[idx] = (zi >= 0 && y0 + l < N) ? P[zi * (N + 1) + y0 + l] : czero<C>();
-      }
+    for (int q0 = 0; q0 < N; q0 += CTs) {
+      const int ct = min(CTs, N - q0);
+      zcols_phase_a<C, N>(P, S, zinv, q0, ct, tw);
       __syncthreads();
-      C *res = fft_tile<C, N, PL, PL>(s0, s1, p, tw, +1);
-      for (int idx = threadIdx.x; idx < PL * N; idx += blockDim.x) {
-        const int kz = idx / PL, l = idx % PL;
-        if (y0 + l < N) {
-          const C v = res[idx];
-          const double re = (double)v.x, im = (double)v.y;
-          acc[(y0 + l) * (N + 1) + kz] += fa * re * re + fb * im * im;
+      for (int idx = threadIdx.x; idx < ct * N1; idx += blockDim.x) {
+        const int qq = idx % ct, k1 = idx / ct;
+        const C *row = S + qq * NP + k1 * N2;
+        double *ar = acc + (q0 + qq) * NP + k1 * N2;
+        C u[N2];
+#pragma unroll
+        for (int j2 = 0; j2 < N2; ++j2) u[j2] = row[j2];
+        Dft<C, N2, 1>::run(u);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+          const double re = (double)u[k2].x, im = (double)u[k2].y;
+          ar[k2] += fa * re * re + fb * im * im;
         }
       }
       __syncthreads();
@@ -225,46 +285,52 @@ __global__ void __launch_bounds__(PNT) k_pencil_density(PencilGeom pg, Plan<C> p
   }
   double *out = rho_part + ((long)grp * pg.n1 + kx) * N * N;
   for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
-    const int ky = idx / N, kz = idx % N;
-    out[idx] += acc[ky * (N + 1) + kz];
+    const int q = idx / N, k = idx % N;
+    out[idx] += acc[q * NP + k];
   }
 }
 
-// rho[kz][ky][kx] = sum over groups of rho_part[g][kx][ky][kz]
-__global__ void k_rho_reduce_t(int n1, int n2, int n3, int ngroups, const double *__restrict__ part, double *__restrict__ rho) {
+// position <-> index of the permuted (ky, kz) order: position a*N2 + b holds
+// index a + N1*b
+__device__ __forceinline__ int perm_index(int pos, int n1f, int n2f) { return pos / n2f + n1f * (pos % n2f); }
+
+// rho[kz][ky][kx] = sum over groups of rho_part[g][kx][q][k']
+__global__ void k_rho_reduce_p(int n, int n1f, int n2f, int ngroups, const double *__restrict__ part,
+                               double *__restrict__ rho) {
   __shared__ double tile[32][33];
-  // tile over (kx, kz) at fixed ky: read along kz, write along kx
-  const int ky = blockIdx.z;
-  const int kz0 = blockIdx.x * 32, kx0 = blockIdx.y * 32;
-  const long gstride = (long)n1 * n2 * n3;
+  const int q = blockIdx.z;
+  const int k0 = blockIdx.x * 32, kx0 = blockIdx.y * 32;
+  const long gstride = (long)n * n * n;
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-    const int kx = kx0 + j, kz = kz0 + threadIdx.x;
+    const int kx = kx0 + j, k = k0 + threadIdx.x;
     double s = 0.0;
-    if (kx < n1 && kz < n3)
-      for (int g = 0; g < ngroups; ++g) s += part[g * gstride + ((long)kx * n2 + ky) * n3 + kz];
+    if (kx < n && k < n)
+      for (int g = 0; g < ngroups; ++g) s += part[g * gstride + ((long)kx * n + q) * n + k];
     tile[j][threadIdx.x] = s;
   }
   __syncthreads();
+  const int ky = perm_index(q, n1f, n2f);
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-    const int kz = kz0 + j, kx = kx0 + threadIdx.x;
-    if (kx < n1 && kz < n3) rho[((long)kz * n2 + ky) * n1 + kx] = tile[threadIdx.x][j];
+    const int k = k0 + j, kx = kx0 + threadIdx.x;
+    if (kx < n && k < n) rho[((long)perm_index(k, n1f, n2f) * n + ky) * n + kx] = tile[threadIdx.x][j];
   }
 }
 
-// V_T[kx][ky][kz] (working precision) from V[kz][ky][kx] (FP64)
+// vp[kx][q][k'] (working precision) from V[kz][ky][kx] (FP64), permuted order
 template <typename Rl>
-__global__ void k_v_transpose(int n1, int n2, int n3, const double *__restrict__ v, Rl *__restrict__ vt) {
+__global__ void k_v_permute(int n, int n1f, int n2f, const double *__restrict__ v, Rl *__restrict__ vp) {
   __shared__ double tile[32][33];
-  const int ky = blockIdx.z;
-  const int kx0 = blockIdx.x * 32, kz0 = blockIdx.y * 32;
+  const int q = blockIdx.z;
+  const int ky = perm_index(q, n1f, n2f);
+  const int kx0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-    const int kz = kz0 + j, kx = kx0 + threadIdx.x;
-    tile[j][threadIdx.x] = (kx < n1 && kz < n3) ? v[((long)kz * n2 + ky) * n1 + kx] : 0.0;
+    const int k = k0 + j, kx = kx0 + threadIdx.x;
+    tile[j][threadIdx.x] = (kx < n && k < n) ? v[((long)perm_index(k, n1f, n2f) * n + ky) * n + kx] : 0.0;
   }
   __syncthreads();
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-    const int kx = kx0 + j, kz = kz0 + threadIdx.x;
-    if (kx < n1 && kz < n3) vt[((long)kx * n2 + ky) * n3 + kz] = (Rl)tile[threadIdx.x][j];
+    const int kx = kx0 + j, k = k0 + threadIdx.x;
+    if (kx < n && k < n) vp[((long)kx * n + q) * n + k] = (Rl)tile[threadIdx.x][j];
   }
 }
 

@@ -212,8 +212,14 @@ class Engine:
         assert c.shape == (self.nstate, self.ngpw)
         _check(self.lib.amdk_set_wfn(self.h, c.ctypes.data_as(C.POINTER(C.c_double))), "amdk_set_wfn")
 
-    def get_wfn(self) -> np.ndarray:
-        c = np.zeros((self.nstate, self.ngpw), np.complex128)
+    def get_wfn(self, out: np.ndarray | None = None) -> np.ndarray:
+        """C0 as (nstate, ngpw) complex128; with `out` (C-contiguous, that
+        shape and dtype, e.g. a pinned host buffer) the copy lands there."""
+        c = out
+        if c is None:
+            c = np.empty((self.nstate, self.ngpw), np.complex128)
+        elif c.shape != (self.nstate, self.ngpw) or c.dtype != np.complex128 or not c.flags.c_contiguous:
+            raise ValueError("get_wfn: out must be C-contiguous complex128 of shape (nstate, ngpw)")
         _check(self.lib.amdk_get_wfn(self.h, c.ctypes.data_as(C.POINTER(C.c_double))), "amdk_get_wfn")
         return c
 
