@@ -109,7 +109,9 @@ struct amdk_ctx {
   // pencil path (cubic grids with a specialised length): tables and buffers
   bool pencil_vpsi = false, pencil_density = false;
   int pencil_groups = 1;  // upper bound on the density pair groups
-  int ct_vpsi = 0, ct_dens = 0;  // column tiles of the pencil kernels
+  int ct_vpsi = 0, ct_dens = 0;  // column tiles of the pencil kernels (current precision)
+  bool pv_p[2] = {false, false}, pd_p[2] = {false, false};  // per pair precision: FP64, mixed
+  int ctv_p[2] = {0, 0}, ctd_p[2] = {0, 0};
   int pn1 = 0, pn2 = 0;          // two-level split n = pn1 * pn2
   int nsm = 148;
   std::map<int, int> pencil_grp_cache;
@@ -424,10 +426,11 @@ template <typename C> static void pencil_vpsi(amdk_ctx *c, int T) {
 template <typename C> static int density_groups(amdk_ctx *c, int T) {
   const Geom &g = c->geom;
   const size_t sm = pencil_acc_smem(g.n2) + pencil_smem<C>(g.n2, c->pg.nz, c->ct_dens);
-  auto it = c->pencil_grp_cache.find(T);
+  const int key = 2 * T + (c->precision == AMDK_MIXED ? 1 : 0);
+  auto it = c->pencil_grp_cache.find(key);
   if (it == c->pencil_grp_cache.end())
     it = c->pencil_grp_cache
-             .emplace(T, pencil_density_groups(g.n1, T, c->nsm, (int)std::max<size_t>(1, (228 * 1024) / (sm + 1024)),
+             .emplace(key, pencil_density_groups(g.n1, T, c->nsm, (int)std::max<size_t>(1, (228 * 1024) / (sm + 1024)),
                                                c->pencil_groups))
              .first;
   return it->second;
@@ -798,6 +801,16 @@ static int do_ionic_forces(amdk_ctx *c) {
 }
 
 // ------------------------------------------------------------------ setup
+// pair-transform precision in use (FP32 band-pair FFTs for AMDK_MIXED)
+static void set_pair_precision(amdk_ctx *c, int prec) {
+  const int q = (prec == AMDK_MIXED) ? 1 : 0;
+  c->precision = prec;
+  c->pencil_vpsi = c->pv_p[q];
+  c->pencil_density = c->pd_p[q];
+  c->ct_vpsi = c->ctv_p[q];
+  c->ct_dens = c->ctd_p[q];
+}
+
 static int build_device(amdk_ctx *c) {
   HostSetup &h = c->hs;
   Geom &g = c->geom;
@@ -921,44 +934,51 @@ static int build_device(amdk_ctx *c) {
   // Pencil path for the pair transforms (cubic grids with a specialised
   // length whose slab plane fits in shared memory): V(r)psi and the density
   // go plane by plane through shared memory with no slab buffer in HBM.
-  size_t csz = (c->precision == AMDK_MIXED) ? sizeof(float2) : sizeof(double2);
+  // Decided for both pair precisions (index 0 FP64, 1 mixed) so that
+  // amdk_set_precision can switch between them; buffers are sized for FP64.
   {
     bool known = false;
     with_n(n1, [&](auto NC) { known = decltype(NC)::value > 0; });
     const bool ok = (n1 == n2 && n2 == n3) && known;
     const size_t lim = 227 * 1024;
     const int nz0 = g.nz[0];
+    const char *env = getenv("AMDK_NO_PENCIL");
+    const bool off = env && env[0] == '1';
     if (ok) {
       c->pn1 = fft_n1(n1);
       c->pn2 = n1 / c->pn1;
       // V(r)psi: two blocks per SM when the tile can stay at least half the
       // plane wide, else one; the density block carries its accumulator
-      const bool mixed = c->precision == AMDK_MIXED;
-      int ct2 = mixed ? pencil_tile<float2>(n1, nz0, 0, lim / 2) : pencil_tile<double2>(n1, nz0, 0, lim / 2);
-      int ct1 = mixed ? pencil_tile<float2>(n1, nz0, 0, lim) : pencil_tile<double2>(n1, nz0, 0, lim);
-      c->ct_vpsi = (2 * ct2 >= n1) ? ct2 : ct1;
-      c->ct_dens = mixed ? pencil_tile<float2>(n1, nz0, pencil_acc_smem(n1), lim)
-                         : pencil_tile<double2>(n1, nz0, pencil_acc_smem(n1), lim);
+      int ct2 = pencil_tile<double2>(n1, nz0, 0, lim / 2), ct1 = pencil_tile<double2>(n1, nz0, 0, lim);
+      c->ctv_p[0] = (2 * ct2 >= n1) ? ct2 : ct1;
+      c->ctd_p[0] = pencil_tile<double2>(n1, nz0, pencil_acc_smem(n1), lim);
+      ct2 = pencil_tile<float2>(n1, nz0, 0, lim / 2);
+      ct1 = pencil_tile<float2>(n1, nz0, 0, lim);
+      c->ctv_p[1] = (2 * ct2 >= n1) ? ct2 : ct1;
+      c->ctd_p[1] = pencil_tile<float2>(n1, nz0, pencil_acc_smem(n1), lim);
     }
-    c->pencil_vpsi = ok && c->ct_vpsi >= 8;
-    c->pencil_density = ok && c->ct_dens >= 8;
-    const char *env = getenv("AMDK_NO_PENCIL");
-    if (env && env[0] == '1') c->pencil_vpsi = c->pencil_density = false;
+    for (int q = 0; q < 2; ++q) {
+      c->pv_p[q] = ok && !off && c->ctv_p[q] >= 8;
+      c->pd_p[q] = ok && !off && c->ctd_p[q] >= 8;
+    }
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
   }
-  const bool pencil_all = c->pencil_vpsi && c->pencil_density;
+  const int q0 = (c->precision == AMDK_MIXED) ? 1 : 0;
+  const bool pencil_all = c->pv_p[q0] && c->pd_p[q0];
   // pair batch: all pairs at once on the pencil path, else 8
   if (c->batch <= 0) c->batch = pencil_all ? c->npairs : 8;
   c->batch = std::max(1, std::min(c->batch, c->npairs));
-  size_t rb = std::max((size_t)c->batch * rstride(c, 0) * csz, 2 * (size_t)rstride(c, 1) * sizeof(double2));
+  size_t rb = std::max((size_t)c->batch * rstride(c, 0) * sizeof(double2), 2 * (size_t)rstride(c, 1) * sizeof(double2));
   size_t sb = 2 * (size_t)sstride(c, 1) * sizeof(double2);
-  if (!pencil_all) sb = std::max(sb, (size_t)c->batch * sstride(c, 0) * csz);
+  if (!(c->pv_p[0] && c->pd_p[0] && c->pv_p[1] && c->pd_p[1]))
+    sb = std::max(sb, (size_t)c->batch * sstride(c, 0) * sizeof(double2));
   RC(c->alloc((char **)&c->d_rb, rb));
   RC(c->alloc((char **)&c->d_sb, sb));
   c->fftbuf_bytes = rb + sb;
-  if (c->pencil_vpsi || c->pencil_density) {
+  set_pair_precision(c, c->precision);
+  if (c->pv_p[0] || c->pv_p[1] || c->pd_p[0] || c->pd_p[1]) {
     std::vector<int> rpos(h.ngrays), zinv(n3, -1), zl0(g.nz[0]), postp(h.ngpw), postm(h.ngpw);
     CK(cudaMemcpy(zl0.data(), c->d_zlist[0], sizeof(int) * g.nz[0], cudaMemcpyDeviceToHost));
     for (int zi = 0; zi < g.nz[0]; zi++) zinv[zl0[zi]] = zi;
@@ -978,10 +998,10 @@ static int build_device(amdk_ctx *c) {
     RC(c->up(&c->d_gmapt, gmapt));
     c->pg = PencilGeom{n1, n2, n3, h.ngrays, g.nz[0], c->d_rpos, c->d_zinv, c->d_zlist[0], c->d_gmapt};
     c->pencil_groups = std::max(1, std::min(c->batch, 16));
-    if (c->pencil_density) RC(c->alloc(&c->d_rhopart, (size_t)c->pencil_groups * npt));
-    if (c->pencil_vpsi) {
+    if (c->pd_p[0] || c->pd_p[1]) RC(c->alloc(&c->d_rhopart, (size_t)c->pencil_groups * npt));
+    if (c->pv_p[0] || c->pv_p[1]) {
       char *vt;
-      RC(c->alloc(&vt, (size_t)npt * (c->precision == AMDK_MIXED ? sizeof(float) : sizeof(double))));
+      RC(c->alloc(&vt, (size_t)npt * sizeof(double)));
       c->d_vt = vt;
     }
   }
@@ -1202,6 +1222,12 @@ int amdk_host_gvectors(const amdk_system *sys, amdk_info *info, int *inyh, doubl
   if (gvec) std::memcpy(gvec, h.gvec.data(), sizeof(double) * h.gvec.size());
   if (map_p) std::memcpy(map_p, h.mapp.data(), sizeof(int) * h.mapp.size());
   if (map_m) std::memcpy(map_m, h.mapm.data(), sizeof(int) * h.mapm.size());
+  return 0;
+}
+
+int amdk_set_precision(amdk_ctx *c, int precision) {
+  if (!c || (precision != AMDK_FP64 && precision != AMDK_MIXED)) return AMDK_ERR_BADARG;
+  set_pair_precision(c, precision);
   return 0;
 }
 

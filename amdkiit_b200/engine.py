@@ -79,6 +79,7 @@ def load_library(path: str = LIBPATH):
     lib.amdk_get_gvectors.argtypes = [P, P, P, P, P, P]
     lib.amdk_host_gvectors.argtypes = [C.POINTER(_System), C.POINTER(_Info), P, P, P, P, P]
     lib.amdk_set_positions.argtypes = [P, C.POINTER(C.c_double)]
+    lib.amdk_set_precision.argtypes = [P, C.c_int]
     lib.amdk_set_wfn.argtypes = [P, C.POINTER(C.c_double)]
     lib.amdk_get_wfn.argtypes = [P, C.POINTER(C.c_double)]
     for f in ("amdk_ortho", "amdk_density", "amdk_potential", "amdk_apply_h"):
@@ -183,6 +184,13 @@ class Engine:
         self.info = info
         self.ngpw, self.ngrho, self.nstate = info.ngpw, info.ngrho, info.nstate
         self.nr = tuple(info.nr)
+        self.precision = precision      # precision the engine was created with
+        self.pair_precision = precision  # precision of the band-pair FFTs now
+
+    def set_precision(self, precision: int):
+        """Precision of the band-pair transforms from the next call on."""
+        _check(self.lib.amdk_set_precision(self.h, precision), "amdk_set_precision")
+        self.pair_precision = precision
 
     def close(self):
         if getattr(self, "h", None):
@@ -327,13 +335,28 @@ class Engine:
         return coef, grid
 
     # ------------------------------------------------------------ drivers
-    def wfn_opt(self, max_step: int = 800, gcut: float = 1e-7, callback=None):
-        """do_opt.f90:51-138: CG iterations until GEMAX < gcut."""
-        e = None
-        for i in range(1, max_step + 1):
-            e, g, conv = self.scf_iteration(i, gcut)
-            if callback:
-                callback(i, e, g)
-            if conv:
-                return i, e, g
-        return max_step, e, g
+    def wfn_opt(self, max_step: int = 800, gcut: float = 1e-7, callback=None, refine: bool = True):
+        """do_opt.f90:51-138: CG iterations until GEMAX < gcut.
+
+        On a mixed-precision engine with refine=True the iterations that
+        follow the first GEMAX < gcut run with FP64 band-pair transforms until
+        GEMAX < gcut holds there too, so the returned energy, gradient and
+        forces are those of the FP64 path at a converged wavefunction (the CG
+        history carries on; only the FFT precision changes)."""
+        e, g = None, None
+        refining = False
+        try:
+            for i in range(1, max_step + 1):
+                e, g, conv = self.scf_iteration(i, gcut)
+                if callback:
+                    callback(i, e, g)
+                if conv:
+                    if refine and self.pair_precision == MIXED and not refining:
+                        refining = True
+                        self.set_precision(FP64)
+                        continue
+                    return i, e, g
+            return max_step, e, g
+        finally:
+            if refining:
+                self.set_precision(self.precision)

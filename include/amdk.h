@@ -124,6 +124,12 @@ int amdk_host_gvectors(const amdk_system *sys, amdk_info *info, int *inyh, doubl
 /* exp_igr.f90:4-140 exp_igrxfactor for new positions atco(3,na_max,nsp) */
 int amdk_set_positions(amdk_ctx *ctx, const double *atco);
 
+/* Precision of the band-pair transforms (vpsi, eval_density) from the next
+ * call on: AMDK_FP64 or AMDK_MIXED (FP32 FFT data, FP64 everything else).
+ * Lets a driver converge in mixed precision and refine the last iterations
+ * in FP64 (no reference counterpart: the reference is FP64 only). */
+int amdk_set_precision(amdk_ctx *ctx, int precision);
+
 /* C_0(ngpw,nstate) complex as interleaved doubles (host memory) */
 int amdk_set_wfn(amdk_ctx *ctx, const double *c0);
 int amdk_get_wfn(amdk_ctx *ctx, double *c0);

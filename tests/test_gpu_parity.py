@@ -169,3 +169,45 @@ def test_reference_energy_on_gpu():
     ref = golden()["water1_mt"]["energies"]
     assert abs(en["etotal"] - ref["etotal"]) < 1e-6 * s.nat
     assert abs(en["esr"] - ref["esr"]) < 1e-9 and abs(en["eself"] - ref["eself"]) < 1e-9
+
+
+def test_set_precision_switches_pair_transforms():
+    """A mixed-precision engine switched to FP64 pair transforms reproduces
+    the FP64 engine's density; switched back it is FP32-accurate again."""
+    from amdkiit_b200.engine import MIXED
+    s = configs.small_water()
+    o, ref = pair(s)
+    ref.ortho()
+    c = ref.get_wfn()
+    ref.density()
+    rho64 = ref.get("rho")
+    e = Engine(s, MIXED)
+    e.set_wfn(c)
+    e.density()
+    rho_mx = e.get("rho")
+    assert 1e-12 < rel(rho_mx, rho64) < 1e-5
+    e.set_precision(FP64)
+    e.density()
+    assert rel(e.get("rho"), rho64) < 1e-12
+    e.set_precision(MIXED)
+    e.density()
+    assert rel(e.get("rho"), rho_mx) < 1e-14
+
+
+def test_mixed_with_fp64_refinement_matches_fp64_energy():
+    """wfn_opt on a mixed engine ends with FP64 pair transforms: its energy
+    and forces agree with the FP64 engine's at convergence far inside the
+    1e-6 Ha/atom and 1e-4 Ha/bohr bars."""
+    from amdkiit_b200.engine import MIXED
+    s = configs.small_water(xc=XC_PBE)
+    _, e64 = pair(s)
+    emx = Engine(s, MIXED)
+    emx.set_wfn(e64.get_wfn())
+    e64.ortho()
+    emx.ortho()
+    n64, en64, _ = e64.wfn_opt(400, 1e-7)
+    nmx, enmx, _ = emx.wfn_opt(400, 1e-7)
+    assert n64 < 400 and nmx < 400
+    assert emx.pair_precision == MIXED
+    assert abs(enmx["etotal"] - en64["etotal"]) < 1e-7 * s.nat
+    assert np.max(np.abs(emx.get("force") - e64.get("force"))) < 1e-5
