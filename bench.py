@@ -40,6 +40,12 @@ UNIT = "SCF iter/s"
 WORKLOAD = "water32: 32 H2O, PBE, 70 Ry, 100^3 grid, 128 bands, GTH, Gamma"
 
 
+# DRAM bytes (read + write) per launch of the dominant kernel classes, from
+# one `ncu --set full` capture of each on this workload (one launch inside
+# `bench.py --steps 3 --warmup 3 --md-steps 0`); None where none was taken.
+TRAFFIC = {("z_vpsi", "mixed"): 145.60e6, ("z_vpsi", "fp64"): 347.54e6, ("z_density", "mixed"): 142.22e6}
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -303,7 +309,8 @@ def main():
         "e2e": head["e2e"],
         "gpu_launches": head["launches"],
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": src, "traffic": None,
+                     "frac": achieved / peak, "peak_source": src,
+                     "traffic": TRAFFIC.get((dom, "mixed" if head is arms.get("mixed") else "fp64")),
                      "launches": n, "avg_launch_ms": ms / n if n else None},
         "kernels_ms": {k: round(v[1], 3) for k, v in kern.items()},
         "md": head["md"],
