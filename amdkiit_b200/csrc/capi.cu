@@ -334,7 +334,8 @@ static int grid_to_rays(amdk_ctx *c, int T, const double2 *cgrid, const double *
 template <typename C> static size_t pencil_smem(int n, int nz, int ct) {
   return ((size_t)(nz + ct) * (n + 1) + n) * sizeof(C) + n * sizeof(int);
 }
-static size_t pencil_acc_smem(int n) { return (size_t)n * (n + 1) * sizeof(double); }
+// density accumulator: FP32 for float2 data (the mixed path ends on FP64), FP64 otherwise
+template <typename C> static size_t pencil_acc_smem(int n) { return (size_t)n * (n + 1) * (sizeof(C) == 8 ? 4 : 8); }
 // widest column tile with the block within `budget` bytes (0: none fits)
 template <typename C> static int pencil_tile(int n, int nz, size_t extra, size_t budget) {
   const size_t base = pencil_smem<C>(n, nz, 0) + extra;
@@ -425,7 +426,7 @@ template <typename C> static void pencil_vpsi(amdk_ctx *c, int T) {
 }
 template <typename C> static int density_groups(amdk_ctx *c, int T) {
   const Geom &g = c->geom;
-  const size_t sm = pencil_acc_smem(g.n2) + pencil_smem<C>(g.n2, c->pg.nz, c->ct_dens);
+  const size_t sm = pencil_acc_smem<C>(g.n2) + pencil_smem<C>(g.n2, c->pg.nz, c->ct_dens);
   const int key = 2 * T + (c->precision == AMDK_MIXED ? 1 : 0);
   auto it = c->pencil_grp_cache.find(key);
   if (it == c->pencil_grp_cache.end())
@@ -437,7 +438,7 @@ template <typename C> static int density_groups(amdk_ctx *c, int T) {
 }
 template <typename C> static void pencil_density(amdk_ctx *c, int p0, int T) {
   const Geom &g = c->geom;
-  const size_t sm = pencil_acc_smem(g.n2) + pencil_smem<C>(g.n2, c->pg.nz, c->ct_dens);
+  const size_t sm = pencil_acc_smem<C>(g.n2) + pencil_smem<C>(g.n2, c->pg.nz, c->ct_dens);
   const int grp = density_groups<C>(c, T);
   const int per = (T + grp - 1) / grp;
   const double npt = (double)g.n1 * g.n2 * g.n3;
@@ -951,11 +952,14 @@ static int build_device(amdk_ctx *c) {
       // plane wide, else one; the density block carries its accumulator
       int ct2 = pencil_tile<double2>(n1, nz0, 0, lim / 2), ct1 = pencil_tile<double2>(n1, nz0, 0, lim);
       c->ctv_p[0] = (2 * ct2 >= n1) ? ct2 : ct1;
-      c->ctd_p[0] = pencil_tile<double2>(n1, nz0, pencil_acc_smem(n1), lim);
+      c->ctd_p[0] = pencil_tile<double2>(n1, nz0, pencil_acc_smem<double2>(n1), lim);
       ct2 = pencil_tile<float2>(n1, nz0, 0, lim / 2);
       ct1 = pencil_tile<float2>(n1, nz0, 0, lim);
       c->ctv_p[1] = (2 * ct2 >= n1) ? ct2 : ct1;
-      c->ctd_p[1] = pencil_tile<float2>(n1, nz0, pencil_acc_smem(n1), lim);
+      // density: two blocks per SM when that leaves at most four column tiles
+      ct2 = pencil_tile<float2>(n1, nz0, pencil_acc_smem<float2>(n1), lim / 2);
+      ct1 = pencil_tile<float2>(n1, nz0, pencil_acc_smem<float2>(n1), lim);
+      c->ctd_p[1] = (4 * ct2 >= n1) ? ct2 : ct1;
     }
     for (int q = 0; q < 2; ++q) {
       c->pv_p[q] = ok && !off && c->ctv_p[q] >= 8;

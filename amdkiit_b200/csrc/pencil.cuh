@@ -238,30 +238,33 @@ __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C
 
 // Density: one x-plane for a group of band pairs (density.f90:49-86);
 // rho_part[grp][kx][q][k'] += wa_t Re^2 + wb_t Im^2 in the permuted (ky, kz)
-// order of the vpsi kernel.  grid (n1, ngroups).
+// order of the vpsi kernel.  grid (n1, ngroups).  The group sum is kept in
+// shared memory in the data's precision (FP32 for float2), then added to the
+// FP64 partial grid.
 template <typename C, int N>
 __global__ void __launch_bounds__(PNT) k_pencil_density(PencilGeom pg, Plan<C> p, const C *__restrict__ rt, int T,
                                                         int per_group, const double *__restrict__ wa,
                                                         const double *__restrict__ wb, double *__restrict__ rho_part,
                                                         int CTs) {
+  typedef decltype(C().x) Rl;
   constexpr int N1 = fft_n1(N), N2 = N / N1, NP = N + 1;
   extern __shared__ unsigned char smraw[];
   const int nz = pg.nz;
-  double *acc = reinterpret_cast<double *>(smraw);  // [q][k'], row stride N+1
+  Rl *acc = reinterpret_cast<Rl *>(smraw);  // [q][k'], row stride N+1
   C *P = reinterpret_cast<C *>(acc + N * NP);
   C *S = P + nz * NP;
   C *tw = S + CTs * NP;
   int *zinv = reinterpret_cast<int *>(tw + N);
   load_tw<C, N>(tw, p);
   for (int i = threadIdx.x; i < N; i += blockDim.x) zinv[i] = pg.zinv[i];
-  for (int idx = threadIdx.x; idx < N * NP; idx += blockDim.x) acc[idx] = 0.0;
+  for (int idx = threadIdx.x; idx < N * NP; idx += blockDim.x) acc[idx] = (Rl)0;
   const int kx = blockIdx.x, grp = blockIdx.y;
   const int t0 = grp * per_group, t1 = min(T, t0 + per_group);
   for (int t = t0; t < t1; ++t) {
     const C *plane = rt + ((long)t * pg.n1 + kx) * pg.nray;
     pencil_scatter<C, N>(P, plane, pg);
     rows_nat_to_perm<C, N, 1>(P, nz, NP, tw);
-    const double fa = wa[t], fb = wb[t];
+    const Rl fa = (Rl)wa[t], fb = (Rl)wb[t];
     for (int q0 = 0; q0 < N; q0 += CTs) {
       const int ct = min(CTs, N - q0);
       zcols_phase_a<C, N>(P, S, zinv, q0, ct, tw);
@@ -269,14 +272,14 @@ __global__ void __launch_bounds__(PNT) k_pencil_density(PencilGeom pg, Plan<C> p
       for (int idx = threadIdx.x; idx < ct * N1; idx += blockDim.x) {
         const int qq = idx % ct, k1 = idx / ct;
         const C *row = S + qq * NP + k1 * N2;
-        double *ar = acc + (q0 + qq) * NP + k1 * N2;
+        Rl *ar = acc + (q0 + qq) * NP + k1 * N2;
         C u[N2];
 #pragma unroll
         for (int j2 = 0; j2 < N2; ++j2) u[j2] = row[j2];
         Dft<C, N2, 1>::run(u);
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2) {
-          const double re = (double)u[k2].x, im = (double)u[k2].y;
+          const Rl re = u[k2].x, im = u[k2].y;
           ar[k2] += fa * re * re + fb * im * im;
         }
       }
@@ -286,7 +289,7 @@ __global__ void __launch_bounds__(PNT) k_pencil_density(PencilGeom pg, Plan<C> p
   double *out = rho_part + ((long)grp * pg.n1 + kx) * N * N;
   for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
     const int q = idx / N, k = idx % N;
-    out[idx] += acc[q * NP + k];
+    out[idx] += (double)acc[q * NP + k];
   }
 }
 
