@@ -108,6 +108,8 @@ struct amdk_ctx {
   double *d_part = nullptr, *d_scal = nullptr, *d_force = nullptr, *d_esr = nullptr, *d_fsr = nullptr;
   // pencil path (cubic grids with a specialised length): tables and buffers
   bool pencil_vpsi = false, pencil_density = false;
+  double *h_pin = nullptr;  // pinned: scalar slots [S_NSCAL], GEMAX
+  int *h_info = nullptr;    // pinned: Cholesky status
   int pencil_groups = 1;  // upper bound on the density pair groups
   int ct_vpsi = 0, ct_dens = 0;  // column tiles of the pencil kernels (current precision)
   bool pv_p[2] = {false, false}, pd_p[2] = {false, false};  // per pair precision: FP64, mixed
@@ -606,6 +608,28 @@ static int do_fnl(amdk_ctx *c) {
   return 0;
 }
 
+// energies from the device scalar slots (copied to the host)
+static int fill_energies(amdk_ctx *c, const double *sc, amdk_energies *e) {
+  const HostSetup &h = c->hs;
+  e->eh = sc[S_EH];
+  e->eloc = 2.0 * sc[S_ELOC] * h.omega;
+  e->eself = c->eself;
+  e->esr = c->esr;
+  e->estat = (sc[S_EH] * h.omega) + c->esr - c->eself;
+  e->eke = sc[S_EKIN] * h.tpiba2;
+  e->exc = h.omega / (double)(h.nr[0] * h.nr[1] * h.nr[2]) * sc[S_EXC];
+  e->enl = sc[S_ENL];
+  e->etotal = e->enl + e->eloc + e->eke + e->exc + e->estat;
+  if (!std::isfinite(e->etotal)) {
+    set_error("non-finite total energy");
+    return AMDK_ERR_NONFINITE;
+  }
+  return 0;
+}
+
+// pp_energy + e_total.  With e the energies are read back now (one stream
+// synchronisation); without, the scalar slots are copied to the pinned host
+// buffer in stream order for fill_energies after the caller's own sync.
 static int do_energy(amdk_ctx *c, amdk_energies *e) {
   const HostSetup &h = c->hs;
   RC(do_fnl(c));
@@ -619,23 +643,10 @@ static int do_energy(amdk_ctx *c, amdk_energies *e) {
   ++c->nlaunch;
   k_ekin<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngpw, c->nstate, c->d_c0, c->d_hg, c->d_occ, c->d_part);
   RC(finish_sums(c, 1, S_EKIN));
+  CK(cudaMemcpyAsync(c->h_pin, c->d_scal, sizeof(double) * S_NSCAL, cudaMemcpyDeviceToHost, c->st));
   if (e) {
-    double sc[S_NSCAL];
-    CK(cudaMemcpyAsync(sc, c->d_scal, sizeof sc, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
-    e->eh = sc[S_EH];
-    e->eloc = 2.0 * sc[S_ELOC] * h.omega;
-    e->eself = c->eself;
-    e->esr = c->esr;
-    e->estat = (sc[S_EH] * h.omega) + c->esr - c->eself;
-    e->eke = sc[S_EKIN] * h.tpiba2;
-    e->exc = h.omega / (double)(h.nr[0] * h.nr[1] * h.nr[2]) * sc[S_EXC];
-    e->enl = sc[S_ENL];
-    e->etotal = e->enl + e->eloc + e->eke + e->exc + e->estat;
-    if (!std::isfinite(e->etotal)) {
-      set_error("non-finite total energy");
-      return AMDK_ERR_NONFINITE;
-    }
+    RC(fill_energies(c, c->h_pin, e));
   }
   return 0;
 }
@@ -700,7 +711,18 @@ static int do_pcg(amdk_ctx *c, int istep) {
   return 0;
 }
 
-static int do_ortho(amdk_ctx *c) {
+// ortho_gs.  With check the Cholesky status is read back now; without, it is
+// copied to the pinned host buffer in stream order (checked by the caller
+// after its own sync with check_ortho).
+static int check_ortho(amdk_ctx *c) {
+  const int info = c->h_info[0];
+  if (info) {
+    set_error("overlap matrix not positive definite at leading minor " + std::to_string(info));
+    return AMDK_ERR_NOT_SPD;
+  }
+  return 0;
+}
+static int do_ortho(amdk_ctx *c, bool check = true) {
   const HostSetup &h = c->hs;
   int n = c->nstate, K = 2 * h.ngpw;
   const double two = 2.0, zero = 0.0, one = 1.0;
@@ -716,12 +738,10 @@ static int do_ortho(amdk_ctx *c) {
     k_chol_inv_s<<<1, CHOL_NT, sm, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
   else
     k_chol_inv<<<1, 1024, 0, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
-  int info = 0;
-  CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
-  if (info) {
-    set_error("overlap matrix not positive definite at leading minor " + std::to_string(info));
-    return AMDK_ERR_NOT_SPD;
+  CK(cudaMemcpyAsync(c->h_info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  if (check) {
+    CK(cudaStreamSynchronize(c->st));
+    RC(check_ortho(c));
   }
   // C0 <- C0 U^{-1} (DTRMM, wfn_initialize.f90:485) out of place into the
   // spare buffer, then swap the buffers
@@ -931,6 +951,9 @@ static int build_device(amdk_ctx *c) {
   RC(c->alloc(&c->d_info, 1));
   RC(c->alloc(&c->d_part, (size_t)RED_BLOCKS * 4 + 3L * 64 * h.nat + 64));
   RC(c->alloc(&c->d_scal, S_NSCAL));
+  CK(cudaMallocHost(&c->h_pin, sizeof(double) * (S_NSCAL + 8)));
+  CK(cudaMallocHost(&c->h_info, sizeof(int) * 4));
+  c->h_info[0] = 0;
   CK(cudaMemset(c->d_scal, 0, S_NSCAL * sizeof(double)));
   // Pencil path for the pair transforms (cubic grids with a specialised
   // length whose slab plane fits in shared memory): V(r)psi and the density
@@ -1166,6 +1189,8 @@ int amdk_destroy(amdk_ctx *c) {
   cudaSetDevice(c->device);
   if (c->st) cudaStreamSynchronize(c->st);
   for (void *p : c->allocs) cudaFree(p);
+  if (c->h_pin) cudaFreeHost(c->h_pin);
+  if (c->h_info) cudaFreeHost(c->h_info);
   for (auto &e : c->evpool) {
     cudaEventDestroy(e.first);
     cudaEventDestroy(e.second);
@@ -1304,14 +1329,15 @@ int amdk_scf_iteration(amdk_ctx *c, int istep, double gcut, amdk_energies *e, do
   cudaEventRecord(c->ev0, c->st);
   RC(do_density(c));
   RC(do_potential(c));
-  amdk_energies en;
-  RC(do_energy(c, &en));
+  RC(do_energy(c, nullptr));  // energies read after the end-of-iteration sync
   CK(cudaMemsetAsync(c->d_c2, 0, sizeof(double2) * (size_t)c->hs.ngpw * c->nstate, c->st));
   RC(do_apply_h(c));
   RC(do_gradient(c));
-  double gm = 0;
-  CK(cudaMemcpyAsync(&gm, c->d_scal + S_GMAX, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  // GEMAX decides CHK_TFOR (forces or not) before PCG: the one host sync
+  // inside the iteration
+  CK(cudaMemcpyAsync(c->h_pin + S_NSCAL, c->d_scal + S_GMAX, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  const double gm = c->h_pin[S_NSCAL];
   if (!std::isfinite(gm)) {
     set_error("non-finite wavefunction gradient");
     return AMDK_ERR_NONFINITE;
@@ -1321,13 +1347,16 @@ int amdk_scf_iteration(amdk_ctx *c, int istep, double gcut, amdk_energies *e, do
   else if (gm < 3 * gcut) c->tfor = true;
   if (c->tfor) RC(do_ionic_forces(c));
   RC(do_pcg(c, istep));
-  RC(do_ortho(c));
+  RC(do_ortho(c, false));
   cudaEventRecord(c->ev1, c->st);
   CK(cudaEventSynchronize(c->ev1));
   float ms = 0;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
   c->last_ms = ms;
   prof_harvest(c);
+  RC(check_ortho(c));
+  amdk_energies en;
+  RC(fill_energies(c, c->h_pin, &en));
   if (e) *e = en;
   if (gemax) *gemax = gm;
   if (converged) *converged = gm < gcut;

@@ -10,10 +10,13 @@
 //   Y pass : the z planes that contain rays (the slab), layout S[t][zi][ky][kx]
 //   Z pass : every (kx,ky) column of the full grid
 // Each pass loads a tile of lines into shared memory (x-fastest global tiles,
-// coalesced), runs a Stockham mixed-radix (4,2,3,5) FFT in shared memory and
+// coalesced), transforms it (the two-level register FFT for the specialised
+// lengths, a shared-memory Stockham mixed-radix (4,2,3,5) FFT otherwise) and
 // stores the tile.  The Z pass carries the fused consumers: |psi|^2 density
 // accumulation, and V(r)*psi between the backward and forward z transforms
-// (the full grid is never written for H|psi>).
+// (the full grid is never written for H|psi>).  The band-pair transforms of
+// cubic grids take the pencil path of pencil.cuh instead; these kernels
+// serve the density-sphere fields and the other grids.
 //
 // Index convention: grid index k = (Miller index) mod N, x fastest.  The
 // backward transform is sum_G c(G) exp(+iG.r) (FFTW_BACKWARD, unscaled); the
@@ -142,75 +145,6 @@ __device__ C *smem_fft(C *a, C *b, int L, int es, const Plan<C> &p, int sg) {
   return a;
 }
 
-// ---------------------------------------------------------------- compile-time FFT
-// The same Stockham schedule with the length known at compile time: every
-// stride, radix and index division is a constant, the radix butterflies live
-// in registers and the twiddles are read from a shared-memory copy.
-__host__ __device__ constexpr int ct_radix(int n) {
-  return (n % 4 == 0) ? 4 : (n % 2 == 0) ? 2 : (n % 3 == 0) ? 3 : (n % 5 == 0) ? 5 : 0;
-}
-__host__ __device__ constexpr int ct_prefix(int n, int st) {
-  int s = 1, m = n;
-  for (int i = 0; i < st; ++i) {
-    const int r = ct_radix(m);
-    s *= r;
-    m /= r;
-  }
-  return s;
-}
-__host__ __device__ constexpr int ct_nstages(int n) {
-  int c = 0;
-  while (n > 1) {
-    n /= ct_radix(n);
-    ++c;
-  }
-  return c;
-}
-
-template <typename C, int N, int L, int ES, int SG, int ST>
-struct CtStage {
-  static __device__ __forceinline__ C *run(C *a, C *b, const C *tw) {
-    if constexpr (ST == ct_nstages(N)) {
-      return a;
-    } else {
-      constexpr int S = ct_prefix(N, ST);
-      constexpr int R = ct_radix(N / S);
-      constexpr int M = N / (S * R);
-      constexpr int NBF = L * (N / R);
-      for (int idx = threadIdx.x; idx < NBF; idx += blockDim.x) {
-        const int l = idx % L;
-        const int bf = idx / L;
-        const int k = bf % S;
-        const int j = bf / S;
-        C v[R];
-#pragma unroll
-        for (int q = 0; q < R; ++q) v[q] = a[(k + S * j + S * M * q) * ES + l];
-        dft_r(v, R, SG);
-        b[(k + S * R * j) * ES + l] = v[0];
-#pragma unroll
-        for (int q = 1; q < R; ++q) {
-          C w = tw[S * j * q];   // S*j*q < S*M*R = N
-          if (SG > 0) w.y = -w.y;
-          b[(k + S * q + S * R * j) * ES + l] = cmul(v[q], w);
-        }
-      }
-      __syncthreads();
-      return CtStage<C, N, L, ES, SG, ST + 1>::run(b, a, tw);
-    }
-  }
-};
-
-// FFT of a tile of L lines (element k of line l at buf[k*ES + l]); N = 0 is
-// the run-time-length path.  tw: shared copy of p.w (compile-time path).
-template <typename C, int N, int L, int ES>
-__device__ __forceinline__ C *fft_tile(C *a, C *b, const Plan<C> &p, const C *tw, int sg) {
-  if constexpr (N == 0) {
-    return smem_fft(a, b, L, ES, p, sg);
-  } else {
-    if (sg > 0) return CtStage<C, N, L, ES, 1, 0>::run(a, b, tw);
-    return CtStage<C, N, L, ES, -1, 0>::run(a, b, tw);
-  }
-}
 // copy the twiddles of the compile-time path into shared memory
 template <typename C, int N> __device__ __forceinline__ void load_tw(C *tw, const Plan<C> &p) {
   if constexpr (N > 0) {
@@ -355,6 +289,51 @@ __device__ __forceinline__ void rows_perm_to_nat(C *P, int nrow, int stride, con
     for (int n1 = 0; n1 < N1; ++n1) row[n2 + N2 * n1] = w[n1];
   }
   __syncthreads();
+}
+
+// Two-level register FFT of a tile of L lines (element k of line l at
+// a[k*ES + l]), natural order in a, natural order out in b: phase A in place
+// in a (thread (l, j2): DFT_N1 of elements j2 + N2*j1, twiddle, back to
+// k1*N2 + j2), phase B from a to b (thread (l, k1): DFT_N2 of the N2
+// contiguous elements, out to k1 + N1*k2).
+template <typename C, int N, int L, int ES, int SG>
+__device__ __forceinline__ void tile_reg_fft(C *a, C *b, const C *tw) {
+  constexpr int N1 = fft_n1(N), N2 = N / N1;
+  for (int idx = threadIdx.x; idx < L * N2; idx += blockDim.x) {
+    const int l = idx % L, j2 = idx / L;
+    C v[N1];
+#pragma unroll
+    for (int j1 = 0; j1 < N1; ++j1) v[j1] = a[(j2 + N2 * j1) * ES + l];
+    Dft<C, N1, SG>::run(v);
+    twiddle_n<C, N, N1, SG>(v, j2, tw);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) a[(k1 * N2 + j2) * ES + l] = v[k1];
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < L * N1; idx += blockDim.x) {
+    const int l = idx % L, k1 = idx / L;
+    C u[N2];
+#pragma unroll
+    for (int j2 = 0; j2 < N2; ++j2) u[j2] = a[(k1 * N2 + j2) * ES + l];
+    Dft<C, N2, SG>::run(u);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) b[(k1 + N1 * k2) * ES + l] = u[k2];
+  }
+  __syncthreads();
+}
+
+// FFT of a tile of L lines (element k of line l at buf[k*ES + l]); returns
+// the buffer that holds the result.  N = 0 is the run-time-length Stockham
+// path; a specialised N uses the register FFT (tw: shared copy of p.w).
+template <typename C, int N, int L, int ES>
+__device__ __forceinline__ C *fft_tile(C *a, C *b, const Plan<C> &p, const C *tw, int sg) {
+  if constexpr (N == 0) {
+    return smem_fft(a, b, L, ES, p, sg);
+  } else {
+    if (sg > 0) tile_reg_fft<C, N, L, ES, 1>(a, b, tw);
+    else tile_reg_fft<C, N, L, ES, -1>(a, b, tw);
+    return b;
+  }
 }
 
 // ---------------------------------------------------------------- geometry

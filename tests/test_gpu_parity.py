@@ -211,3 +211,27 @@ def test_mixed_with_fp64_refinement_matches_fp64_energy():
     assert emx.pair_precision == MIXED
     assert abs(enmx["etotal"] - en64["etotal"]) < 1e-7 * s.nat
     assert np.max(np.abs(emx.get("force") - e64.get("force"))) < 1e-5
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_slab_path_matches_pencil_path(prec, monkeypatch):
+    """The slab transforms (used for grids the pencil kernels do not take)
+    give the pencil path's density and H|psi> on the same wavefunction."""
+    from amdkiit_b200.engine import MIXED
+    p = FP64 if prec == "fp64" else MIXED
+    tol = 1e-12 if prec == "fp64" else 1e-5
+    s = configs.small_water(xc=XC_PBE)
+    o, ref = pair(s)
+    ref.ortho()
+    c = ref.get_wfn()
+    a = Engine(s, p)
+    monkeypatch.setenv("AMDK_NO_PENCIL", "1")
+    b = Engine(s, p)
+    for e in (a, b):
+        e.set_wfn(c)
+        e.density()
+        e.potential()
+        e.energy()
+        e.apply_h()
+    assert rel(b.get("rho"), a.get("rho")) < tol
+    assert rel(b.get("c2"), a.get("c2")) < tol
