@@ -416,14 +416,39 @@ __global__ void k_unpack_vpsi(int ngpw, int nstate, int band0, int T, const int 
 
 // ---------------------------------------------------------------- bands
 // E_kin partial sums (total_energy.f90:38-61)
+// Band-major [nstate][ngpw] arrays in fixed contiguous chunks per block
+// (deterministic partials): thread t walks k = k0 + t, k0 + t + blockDim...,
+// tracking (band, g) incrementally (blockDim < ngpw), four loads in flight.
+struct BandWalk {
+  long k, k1;
+  int b, g;
+  __device__ BandWalk(long tot, int ngpw) {
+    const long per = (tot + gridDim.x - 1) / gridDim.x;
+    const long chunk = (per + blockDim.x - 1) / blockDim.x * blockDim.x;
+    const long k0 = blockIdx.x * chunk;
+    k1 = min(tot, k0 + chunk);
+    k = k0 + threadIdx.x;
+    b = (int)(k / ngpw);
+    g = (int)(k % ngpw);
+  }
+  __device__ __forceinline__ void next(int ngpw) {
+    k += blockDim.x;
+    g += blockDim.x;
+    if (g >= ngpw) {
+      g -= ngpw;
+      ++b;
+    }
+  }
+};
+
 __global__ void k_ekin(int ngpw, int nstate, const double2 *c0, const double *hg, const double *occ, double *part) {
   __shared__ double sh[32];
   double s = 0;
-  long tot = (long)ngpw * nstate;
-  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < tot; k += (long)gridDim.x * blockDim.x) {
-    int b = (int)(k / ngpw), g = (int)(k % ngpw);
-    double2 c = c0[k];
-    s += occ[b] * hg[g] * (c.x * c.x + c.y * c.y);
+  BandWalk w((long)ngpw * nstate, ngpw);
+#pragma unroll 4
+  for (; w.k < w.k1; w.next(ngpw)) {
+    const double2 c = c0[w.k];
+    s += occ[w.b] * hg[w.g] * (c.x * c.x + c.y * c.y);
   }
   double r = block_sum(s, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = r;
@@ -445,11 +470,18 @@ __global__ void k_zclean(int n, int ngpw, double2 *c) {
   if (i < n) c[(long)i * ngpw].y = 0.0;
 }
 // eval_GMAX (gradient.f90:36-61): max |C2| over occupied bands
+// max |c2|^2 per block (the square root is taken once, in k_finish_max)
 __global__ void k_gmax(long tot, const double2 *c2, double *part) {
   __shared__ double sh[32];
   double m = -1.0;
-  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < tot; k += (long)gridDim.x * blockDim.x)
-    m = fmax(m, hypot(c2[k].x, c2[k].y));
+  const long stride = (long)gridDim.x * blockDim.x;
+  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  for (; k + 3 * stride < tot; k += 4 * stride) {
+    const double2 a = c2[k], b = c2[k + stride], c = c2[k + 2 * stride], d = c2[k + 3 * stride];
+    m = fmax(fmax(m, fmax(a.x * a.x + a.y * a.y, b.x * b.x + b.y * b.y)),
+             fmax(c.x * c.x + c.y * c.y, d.x * d.x + d.y * d.y));
+  }
+  for (; k < tot; k += stride) m = fmax(m, c2[k].x * c2[k].x + c2[k].y * c2[k].y);
   double r = block_max(m, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = r;
 }
@@ -458,7 +490,7 @@ __global__ void k_finish_max(const double *part, int nb, double *out) {
   double m = -1.0;
   for (int i = threadIdx.x; i < nb; i += blockDim.x) m = fmax(m, part[i]);
   double r = block_max(m, sh);
-  if (threadIdx.x == 0) *out = r;
+  if (threadIdx.x == 0) *out = sqrt(fmax(r, 0.0));  // partials hold |c2|^2
 }
 
 // PRECON + GGNORM (cg.f90:239-245, 419-449): cp = fi K c2; partial DOTP sums
@@ -466,13 +498,20 @@ __global__ void k_precon(int ngpw, int nstate, int nocc, const double *vpp, cons
                          double2 *cp, double *part) {
   __shared__ double sh[32];
   double s = 0;
-  long tot = (long)ngpw * nstate;
-  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < tot; k += (long)gridDim.x * blockDim.x) {
-    int b = (int)(k / ngpw), g = (int)(k % ngpw);
-    double fi = occ[b] > 0.01 ? 1.0 / occ[b] : 1.0;
-    double f = fi * vpp[g];
-    double2 v = make_double2(f * c2[k].x, f * c2[k].y);
-    cp[k] = v;
+  BandWalk w((long)ngpw * nstate, ngpw);
+  int bf = -1;
+  double fi = 1.0;
+#pragma unroll 4
+  for (; w.k < w.k1; w.next(ngpw)) {
+    const int b = w.b, g = w.g;
+    if (b != bf) {  // 1/f_i once per band
+      bf = b;
+      fi = occ[b] > 0.01 ? 1.0 / occ[b] : 1.0;
+    }
+    const double f = fi * vpp[g];
+    const double2 c = c2[w.k];
+    const double2 v = make_double2(f * c.x, f * c.y);
+    cp[w.k] = v;
     if (b < nocc) s += (g == 0) ? v.x * v.x : 2.0 * (v.x * v.x + v.y * v.y);
   }
   double r = block_sum(s, sh);
