@@ -7,7 +7,7 @@
 
 namespace amdk {
 
-constexpr int RED_BLOCKS = 296;   // 2 x 148 SMs for grid-stride reductions
+constexpr int RED_BLOCKS = 1184;  // 8 x 148 SMs: enough loads in flight for the streaming reductions
 constexpr int NTHR = 256;
 
 __device__ __forceinline__ double warp_sum(double v) {
