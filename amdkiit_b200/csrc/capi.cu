@@ -306,27 +306,30 @@ template <typename C> static void x_fwd(amdk_ctx *c, int sphere, int T) {
   prof_end(c);
 }
 
-// T fields on the density sphere (fp at +G, fm at -G) -> real or complex grids
+// T fields on the density sphere (fp at +G, fm at -G) -> real or complex
+// grids (FP64 in and out; C is the precision of the transform itself)
+template <typename C = double2>
 static int field_to_grid(amdk_ctx *c, int T, const double2 *fp, const double2 *fm, double2 *cgrid) {
   const Geom &g = c->geom;
   long lines = (long)T * g.nray[1];
   ++c->nlaunch;
   with_n(g.n1, [&](auto NC) {
     constexpr int N = decltype(NC)::value;
-    smem_opt_in<k_x_bwd_field<double2, N>>();
-    k_x_bwd_field<double2, N><<<nblk(lines, LX), NTHR, x_smem<double2>(g.n1), c->st>>>(fp, fm, g.ngrho, 1, T, g,
-                                                                                        c->pd[0], (double2 *)c->d_rb);
+    smem_opt_in<k_x_bwd_field<C, N>>();
+    k_x_bwd_field<C, N><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(fp, fm, g.ngrho, 1, T, g, plan<C>(c, 0),
+                                                                         (C *)c->d_rb);
   });
-  y_pass<double2>(c, 1, +1, T);
-  z_pass<double2, Z_TO_GRID>(c, 1, T, cgrid, nullptr);
+  y_pass<C>(c, 1, +1, T);
+  z_pass<C, Z_TO_GRID>(c, 1, T, cgrid, nullptr);
   return 0;
 }
 // T complex grids (or one real grid) -> forward transform left in the ray buffer
+template <typename C = double2>
 static int grid_to_rays(amdk_ctx *c, int T, const double2 *cgrid, const double *rgrid) {
-  if (rgrid) z_pass<double2, Z_FROM_GRID_REAL>(c, 1, 1, nullptr, rgrid);
-  else z_pass<double2, Z_FROM_GRID_CPLX>(c, 1, T, (double2 *)cgrid, nullptr);
-  y_pass<double2>(c, 1, -1, T);
-  x_fwd<double2>(c, 1, T);
+  if (rgrid) z_pass<C, Z_FROM_GRID_REAL>(c, 1, 1, nullptr, rgrid);
+  else z_pass<C, Z_FROM_GRID_CPLX>(c, 1, T, (double2 *)cgrid, nullptr);
+  y_pass<C>(c, 1, -1, T);
+  x_fwd<C>(c, 1, T);
   return 0;
 }
 
@@ -497,11 +500,11 @@ template <typename C> static int density_t(amdk_ctx *c) {
     z_pass<C, Z_DENSITY>(c, 0, T, nullptr, nullptr, p0);
   }
   }
-  // rhor2g (density.f90:128-150)
-  RC(grid_to_rays(c, 1, nullptr, c->d_rho));
+  // rhor2g (density.f90:128-150), in the pair transforms' precision
+  RC(grid_to_rays<C>(c, 1, nullptr, c->d_rho));
   double scale = 1.0 / ((double)g.n1 * g.n2 * g.n3);
   ++c->nlaunch;
-  k_gather_p<double2><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_posp, (double2 *)c->d_rb, scale, c->d_rhog);
+  k_gather_p<C><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_posp, (C *)c->d_rb, scale, c->d_rhog);
   CK(cudaGetLastError());
   return 0;
 }
@@ -511,7 +514,9 @@ static int do_density(amdk_ctx *c) {
   return density_t<double2>(c);
 }
 
-static int do_potential(amdk_ctx *c) {
+// eval_pot + cal_vpot_ex; the density-sphere transforms run in the pair
+// transforms' precision (FP32 on the mixed path, which ends on FP64)
+template <typename C> static int potential_t(amdk_ctx *c) {
   const HostSetup &h = c->hs;
   const Geom &g = c->geom;
   long npt = (long)g.n1 * g.n2 * g.n3;
@@ -525,19 +530,19 @@ static int do_potential(amdk_ctx *c) {
   if (gga) {
     ++c->nlaunch;
     k_grad_fields<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_gvec, h.tpiba, c->d_rhog, c->d_fp, c->d_fm);
-    RC(field_to_grid(c, 2, c->d_fp, c->d_fm, c->d_cgrid));
+    RC(field_to_grid<C>(c, 2, c->d_fp, c->d_fm, c->d_cgrid));
   }
   ++c->nlaunch;
   k_xc<<<RED_BLOCKS, NTHR, 0, c->st>>>(npt, h.xc, c->d_rho, g0, g1, c->d_part);
   RC(finish_sums(c, 1, S_EXC));
-  RC(grid_to_rays(c, gga ? 2 : 1, c->d_cgrid, nullptr));
+  RC(grid_to_rays<C>(c, gga ? 2 : 1, c->d_cgrid, nullptr));
   double scale = 1.0 / (double)npt;
   ++c->nlaunch;
-  k_xc_combine<double2><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, gga, c->d_posp, c->d_posm, (double2 *)c->d_rb,
-                                                           rstride(c, 1), scale, c->d_gvec, h.tpiba, c->d_vg, c->d_vxg);
+  k_xc_combine<C><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, gga, c->d_posp, c->d_posm, (C *)c->d_rb, rstride(c, 1),
+                                                     scale, c->d_gvec, h.tpiba, c->d_vg, c->d_vxg);
   ++c->nlaunch;
   k_conj_field<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_vxg, c->d_fm);
-  RC(field_to_grid(c, 1, c->d_vxg, c->d_fm, c->d_cgrid));
+  RC(field_to_grid<C>(c, 1, c->d_vxg, c->d_fm, c->d_cgrid));
   // V(r) = Re of the backward transform (xc.f90:299-301)
   CK(cudaMemcpy2DAsync(c->d_vpot, sizeof(double), c->d_cgrid, sizeof(double2), sizeof(double), npt,
                        cudaMemcpyDeviceToDevice, c->st));
@@ -552,6 +557,10 @@ static int do_potential(amdk_ctx *c) {
   }
   CK(cudaGetLastError());
   return 0;
+}
+static int do_potential(amdk_ctx *c) {
+  if (c->precision == AMDK_MIXED) return potential_t<float2>(c);
+  return potential_t<double2>(c);
 }
 
 template <typename C> static int apply_h_t(amdk_ctx *c) {
