@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -67,6 +68,13 @@ template <typename T> static int upload(T **p, const std::vector<T> &v) {
 
 using namespace amdk;
 
+// one profiled interval: kernel class, algorithmic bytes, events around it
+struct ProfRec {
+  int kind;
+  double bytes;
+  cudaEvent_t a, b;
+};
+
 struct amdk_ctx {
   HostSetup hs;
   int device = 0, precision = AMDK_FP64, batch = 4;
@@ -108,7 +116,21 @@ struct amdk_ctx {
   double *d_part = nullptr, *d_scal = nullptr, *d_force = nullptr, *d_esr = nullptr, *d_fsr = nullptr;
   // pencil path (cubic grids with a specialised length): tables and buffers
   bool pencil_vpsi = false, pencil_density = false;
-  double *h_pin = nullptr;  // pinned: scalar slots [S_NSCAL], GEMAX
+  double *h_pin = nullptr;  // pinned: scalar slots [S_NSCAL], GEMAX, CG step
+  // CUDA graphs of the CG iteration's two segments (before and after the
+  // GEMAX read), keyed by segment, precision/forces flag, which buffer holds
+  // C0, and profiling
+  struct SegGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<ProfRec> recs;
+    size_t nevents = 0;
+    long nlaunch = 0;
+  };
+  std::map<std::array<int, 4>, SegGraph> graphs;
+  bool use_graphs = true;
+  bool warm[2] = {false, false};  // an eager iteration has run at this pair precision
+  void *c0_first = nullptr;       // the buffer that held C0 at creation
+  void *cb_ws = nullptr;          // cuBLAS workspace (fixed, for capture)
   int *h_info = nullptr;    // pinned: Cholesky status
   int pencil_groups = 1;  // upper bound on the density pair groups
   int ct_vpsi = 0, ct_dens = 0;  // column tiles of the pencil kernels (current precision)
@@ -124,7 +146,7 @@ struct amdk_ctx {
   // live per-kernel timing (CUDA events on the context stream)
   long nlaunch = 0;  // kernels of this library launched on the context stream
   bool prof = false;
-  struct Rec { int kind; double bytes; cudaEvent_t a, b; };
+  typedef ProfRec Rec;
   std::vector<Rec> recs;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evpool;
   size_t evused = 0;
@@ -150,6 +172,14 @@ struct amdk_ctx {
 // kernel classes timed in profiling mode
 enum { KT_ZVPSI = 0, KT_ZDENS, KT_Y, KT_X, KT_UNPACK, KT_DGEMM, KT_OTHER, KT_N };
 
+// an event record that is also a node of a graph being captured (a plain
+// record inside a capture is only a dependency marker)
+static void prof_record(amdk_ctx *c, cudaEvent_t ev) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(c->st, &st);
+  if (st == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(ev, c->st, cudaEventRecordExternal);
+  else cudaEventRecord(ev, c->st);
+}
 static void prof_begin(amdk_ctx *c, int kind, double bytes) {
   if (!c->prof) return;
   if (c->evused == c->evpool.size()) {
@@ -159,19 +189,22 @@ static void prof_begin(amdk_ctx *c, int kind, double bytes) {
     c->evpool.push_back({a, b});
   }
   auto &e = c->evpool[c->evused++];
-  cudaEventRecord(e.first, c->st);
+  prof_record(c, e.first);
   c->recs.push_back({kind, bytes, e.first, e.second});
 }
 static void prof_end(amdk_ctx *c) {
   if (!c->prof) return;
-  cudaEventRecord(c->recs.back().b, c->st);
+  prof_record(c, c->recs.back().b);
 }
 // after a stream synchronisation: fold the recorded intervals into the totals
 static void prof_harvest(amdk_ctx *c) {
   if (!c->prof) return;
   for (auto &r : c->recs) {
     float ms = 0;
-    cudaEventElapsedTime(&ms, r.a, r.b);
+    if (cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess) {
+      cudaGetLastError();  // a failed interval is dropped, not left as a sticky error
+      continue;
+    }
     c->kt_count[r.kind]++;
     c->kt_ms[r.kind] += ms;
     c->kt_bytes[r.kind] += r.bytes;
@@ -181,7 +214,7 @@ static void prof_harvest(amdk_ctx *c) {
 }
 
 // scalar slots in d_scal
-enum { S_GG = 0, S_GGPREV, S_EH, S_ELOC, S_EXC, S_EKIN, S_ENL, S_GMAX, S_NSCAL = 16 };
+enum { S_GG = 0, S_GGPREV, S_EH, S_ELOC, S_EXC, S_EKIN, S_ENL, S_GMAX, S_ISTEP, S_NSCAL = 16 };
 
 static int nblk(long n, int t = NTHR) { return (int)std::min<long>((n + t - 1) / t, 1L << 30); }
 
@@ -703,8 +736,12 @@ static int do_gradient(amdk_ctx *c) {
   return 0;
 }
 
+// PCG; the step number goes through pinned host memory and the S_ISTEP slot
+// so that a captured graph of this step reads the current one
 static int do_pcg(amdk_ctx *c, int istep) {
   const HostSetup &h = c->hs;
+  c->h_pin[S_NSCAL + 1] = (double)istep;
+  CK(cudaMemcpyAsync(c->d_scal + S_ISTEP, c->h_pin + S_NSCAL + 1, sizeof(double), cudaMemcpyHostToDevice, c->st));
   int n = c->nstate, nocc = 0;
   for (int i = 0; i < n; i++)
     if (h.occ[i] > 1e-5) nocc++;
@@ -713,7 +750,7 @@ static int do_pcg(amdk_ctx *c, int istep) {
   k_precon<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngpw, n, nocc, c->d_vpp, c->d_occ, c->d_c2, c->d_cp, c->d_part);
   RC(finish_sums(c, 1, S_GG));
   ++c->nlaunch;
-  k_pcg_update<<<RED_BLOCKS * 4, NTHR, 0, c->st>>>(tot, istep, c->d_scal, c->d_cp, c->d_hnm1, c->d_c0);
+  k_pcg_update<<<RED_BLOCKS * 4, NTHR, 0, c->st>>>(tot, c->d_scal, c->d_cp, c->d_hnm1, c->d_c0);
   ++c->nlaunch;
   k_copy_scalar<<<1, 1, 0, c->st>>>(c->d_scal + S_GG, c->d_scal + S_GGPREV);
   CK(cudaGetLastError());
@@ -731,7 +768,7 @@ static int check_ortho(amdk_ctx *c) {
   }
   return 0;
 }
-static int do_ortho(amdk_ctx *c, bool check = true) {
+static int do_ortho(amdk_ctx *c, bool check = true, bool swap = true) {
   const HostSetup &h = c->hs;
   int n = c->nstate, K = 2 * h.ngpw;
   const double two = 2.0, zero = 0.0, one = 1.0;
@@ -753,12 +790,12 @@ static int do_ortho(amdk_ctx *c, bool check = true) {
     RC(check_ortho(c));
   }
   // C0 <- C0 U^{-1} (DTRMM, wfn_initialize.f90:485) out of place into the
-  // spare buffer, then swap the buffers
+  // spare buffer (ZCLEAN there), then the buffers swap roles
   CB(cublasDtrmm(c->cb, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, K, n, &one,
                  c->d_uinv, n, (const double *)c->d_c0, K, (double *)c->d_cp, K));
-  std::swap(c->d_c0, c->d_cp);
   ++c->nlaunch;
-  k_zclean<<<nblk(n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c0);
+  k_zclean<<<nblk(n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_cp);
+  if (swap) std::swap(c->d_c0, c->d_cp);
   CK(cudaGetLastError());
   return 0;
 }
@@ -935,6 +972,20 @@ static int build_device(amdk_ctx *c) {
   RC(c->alloc(&c->d_cp, cw));
   RC(c->alloc(&c->d_hnm1, cw));
   CK(cudaMemset(c->d_c0, 0, cw * sizeof(double2)));
+  c->c0_first = c->d_c0;
+  {
+    // fixed cuBLAS workspace so that captured GEMMs allocate nothing
+    const size_t ws = 32u << 20;
+    char *w;
+    RC(c->alloc(&w, ws));
+    c->cb_ws = w;
+    if (cublasSetWorkspace(c->cb, c->cb_ws, ws) != CUBLAS_STATUS_SUCCESS) {
+      set_error("cublasSetWorkspace failed");
+      return AMDK_ERR_CUDA;
+    }
+    const char *env = getenv("AMDK_NO_GRAPHS");
+    c->use_graphs = !(env && env[0] == '1');
+  }
   RC(c->up(&c->d_occ, h.occ));
   {
     // density weights per band pair (density.f90:51-62)
@@ -1148,6 +1199,47 @@ static int build_device(amdk_ctx *c) {
 }
 
 // ------------------------------------------------------------------ C ABI
+// Run one segment of the CG iteration: captured into a CUDA graph the first
+// time its key is seen, replayed afterwards.  body() only enqueues work on
+// the context stream (no host synchronisation, no host-side state change the
+// replay would miss).  A capture that fails turns graphs off and runs eagerly.
+template <typename F> static int run_segment(amdk_ctx *c, const std::array<int, 4> &key, F &&body) {
+  auto it = c->graphs.find(key);
+  if (it == c->graphs.end()) {
+    const size_t rec0 = c->recs.size(), ev0 = c->evused;
+    const long nl0 = c->nlaunch;
+    if (cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      c->use_graphs = false;
+      return body();
+    }
+    const int rc = body();
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(c->st, &g);
+    amdk_ctx::SegGraph sg;
+    const bool ok = rc == 0 && ce == cudaSuccess && g && cudaGraphInstantiate(&sg.exec, g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+    sg.recs.assign(c->recs.begin() + rec0, c->recs.end());
+    sg.nevents = c->evused - ev0;
+    sg.nlaunch = c->nlaunch - nl0;
+    c->recs.resize(rec0);
+    c->evused = ev0;
+    c->nlaunch = nl0;
+    if (!ok) {
+      cudaGetLastError();
+      if (sg.exec) cudaGraphExecDestroy(sg.exec);
+      c->use_graphs = false;
+      return rc ? rc : body();
+    }
+    it = c->graphs.emplace(key, std::move(sg)).first;
+  }
+  CK(cudaGraphLaunch(it->second.exec, c->st));
+  c->recs.insert(c->recs.end(), it->second.recs.begin(), it->second.recs.end());
+  c->evused += it->second.nevents;
+  c->nlaunch += it->second.nlaunch;
+  return 0;
+}
+
 extern "C" {
 
 const char *amdk_last_error(void) { return g_err.c_str(); }
@@ -1198,6 +1290,8 @@ int amdk_destroy(amdk_ctx *c) {
   cudaSetDevice(c->device);
   if (c->st) cudaStreamSynchronize(c->st);
   for (void *p : c->allocs) cudaFree(p);
+  for (auto &kv : c->graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   if (c->h_pin) cudaFreeHost(c->h_pin);
   if (c->h_info) cudaFreeHost(c->h_info);
   for (auto &e : c->evpool) {
@@ -1335,16 +1429,26 @@ int amdk_pcg(amdk_ctx *c, int istep) {
 int amdk_scf_iteration(amdk_ctx *c, int istep, double gcut, amdk_energies *e, double *gemax, int *converged) {
   if (!c || istep < 1) return AMDK_ERR_BADARG;
   cudaSetDevice(c->device);
+  const int q = (c->precision == AMDK_MIXED) ? 1 : 0;
+  // graphs from the second iteration on, once this precision has run eagerly
+  // (first-call setup of kernels and cuBLAS stays out of the capture)
+  const bool graph = c->use_graphs && istep > 1 && c->warm[q];
+  const int parity = (c->d_c0 == c->c0_first) ? 0 : 1;
   cudaEventRecord(c->ev0, c->st);
-  RC(do_density(c));
-  RC(do_potential(c));
-  RC(do_energy(c, nullptr));  // energies read after the end-of-iteration sync
-  CK(cudaMemsetAsync(c->d_c2, 0, sizeof(double2) * (size_t)c->hs.ngpw * c->nstate, c->st));
-  RC(do_apply_h(c));
-  RC(do_gradient(c));
+  auto seg_a = [&]() -> int {
+    RC(do_density(c));
+    RC(do_potential(c));
+    RC(do_energy(c, nullptr));  // energies read after the end-of-iteration sync
+    CK(cudaMemsetAsync(c->d_c2, 0, sizeof(double2) * (size_t)c->hs.ngpw * c->nstate, c->st));
+    RC(do_apply_h(c));
+    RC(do_gradient(c));
+    CK(cudaMemcpyAsync(c->h_pin + S_NSCAL, c->d_scal + S_GMAX, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    return 0;
+  };
+  if (graph) RC(run_segment(c, {0, q, parity, c->prof ? 1 : 0}, seg_a));
+  else RC(seg_a());
   // GEMAX decides CHK_TFOR (forces or not) before PCG: the one host sync
   // inside the iteration
-  CK(cudaMemcpyAsync(c->h_pin + S_NSCAL, c->d_scal + S_GMAX, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   const double gm = c->h_pin[S_NSCAL];
   if (!std::isfinite(gm)) {
@@ -1354,15 +1458,24 @@ int amdk_scf_iteration(amdk_ctx *c, int istep, double gcut, amdk_energies *e, do
   // CHK_TFOR (gradient.f90:113-136)
   if (istep == 1) c->tfor = false;
   else if (gm < 3 * gcut) c->tfor = true;
-  if (c->tfor) RC(do_ionic_forces(c));
-  RC(do_pcg(c, istep));
-  RC(do_ortho(c, false));
+  const bool tfor = c->tfor;
+  c->h_pin[S_NSCAL + 1] = (double)istep;
+  auto seg_b = [&]() -> int {
+    if (tfor) RC(do_ionic_forces(c));
+    RC(do_pcg(c, istep));
+    RC(do_ortho(c, false, false));
+    return 0;
+  };
+  if (graph) RC(run_segment(c, {1, tfor ? 1 : 0, parity, c->prof ? 1 : 0}, seg_b));
+  else RC(seg_b());
+  std::swap(c->d_c0, c->d_cp);  // ortho's output buffer holds C0 now
   cudaEventRecord(c->ev1, c->st);
   CK(cudaEventSynchronize(c->ev1));
   float ms = 0;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
   c->last_ms = ms;
   prof_harvest(c);
+  c->warm[q] = true;
   RC(check_ortho(c));
   amdk_energies en;
   RC(fill_energies(c, c->h_pin, &en));

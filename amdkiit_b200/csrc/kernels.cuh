@@ -518,8 +518,10 @@ __global__ void k_precon(int ngpw, int nstate, int nocc, const double *vpp, cons
   if (threadIdx.x == 0) part[blockIdx.x] = r;
 }
 // PCG direction and step (cg.f90:247-281); scal[0] = ggnorm (new),
-// scal[1] = previous ggnorm; gamma = forget * new/prev
-__global__ void k_pcg_update(long tot, int istep, const double *scal, double2 *cp, double2 *hnm1, double2 *c0) {
+// scal[1] = previous ggnorm, scal[8] = the CG step number;
+// gamma = forget * new/prev
+__global__ void k_pcg_update(long tot, const double *scal, double2 *cp, double2 *hnm1, double2 *c0) {
+  const int istep = (int)scal[8];
   double forget = istep <= 10 ? 0.60 : (istep <= 20 ? 0.91 : 0.95);
   double gamma = (istep == 1) ? 0.0 : forget * (scal[0] / scal[1]);
   const double dt = 5.0 * 5.0 / 400.0;

@@ -235,3 +235,40 @@ def test_slab_path_matches_pencil_path(prec, monkeypatch):
         e.apply_h()
     assert rel(b.get("rho"), a.get("rho")) < tol
     assert rel(b.get("c2"), a.get("c2")) < tol
+
+
+def test_graph_replay_matches_eager(monkeypatch):
+    """CG iterations replayed from CUDA graphs (the default from the second
+    iteration on) give the eager launches' energies, gradients and C0, with
+    and without the ionic forces segment."""
+    s = configs.small_water(xc=XC_PBE)
+    o, ref = pair(s)
+    c = ref.get_wfn()
+    monkeypatch.setenv("AMDK_NO_GRAPHS", "1")
+    eager = Engine(s, FP64)
+    monkeypatch.delenv("AMDK_NO_GRAPHS")
+    for e in (ref, eager):
+        e.set_wfn(c)
+        e.ortho()
+    for it in range(1, 9):
+        # a loose cutoff turns the forces segment on after a few iterations
+        a = ref.scf_iteration(it, 5e-2)
+        b = eager.scf_iteration(it, 5e-2)
+        assert a[0]["etotal"] == b[0]["etotal"] and a[1] == b[1], it
+    assert np.array_equal(ref.get_wfn(), eager.get_wfn())
+    assert np.array_equal(ref.get("force"), eager.get("force"))
+
+
+def test_graph_replay_with_profiling():
+    """Profiled intervals recorded inside captured graphs are timed."""
+    s = configs.small_water()
+    o, e = pair(s)
+    e.ortho()
+    e.scf_iteration(1, 1e-7)
+    e.profile(True)
+    for it in range(2, 6):
+        e.scf_iteration(it, 1e-7)
+        assert e.last_iteration_ms() > 0
+    got = [e.profile_get(k) for k in e.KERNELS]
+    e.profile(False)
+    assert all(n >= 4 and ms > 0 for n, ms, _ in got), got
