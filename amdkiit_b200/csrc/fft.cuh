@@ -59,6 +59,45 @@ template <typename C> __device__ __forceinline__ C cimul(C a, int sg) {
   return r;
 }
 template <typename C> __device__ __forceinline__ C czero() { C r; r.x = 0; r.y = 0; return r; }
+// a*s + b, s real
+template <typename C, typename R> __device__ __forceinline__ C cfmas(C a, R s, C b) {
+  b.x += a.x * s;
+  b.y += a.y * s;
+  return b;
+}
+
+// float2 arithmetic on the packed FP32x2 instructions of sm_100 (one
+// instruction for both components)
+__device__ __forceinline__ unsigned long long f2pack(float2 v) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(v.x), "f"(v.y));
+  return r;
+}
+__device__ __forceinline__ float2 f2unpack(unsigned long long u) {
+  float2 v;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(u));
+  return v;
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2pack(a)), "l"(f2pack(b)));
+  return f2unpack(r);
+}
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2pack(a)), "l"(f2pack(b)));
+  return f2unpack(r);
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2pack(a)), "l"(f2pack(make_float2(s, s))));
+  return f2unpack(r);
+}
+__device__ __forceinline__ float2 cfmas(float2 a, float s, float2 b) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(f2pack(a)), "l"(f2pack(make_float2(s, s))), "l"(f2pack(b)));
+  return f2unpack(r);
+}
 
 // ---------------------------------------------------------------- plans
 constexpr int MAXF = 8;
@@ -85,7 +124,7 @@ template <typename C> __device__ __forceinline__ void dft_r(C *a, int r, int sg)
   } else if (r == 3) {
     const R c3 = (R)-0.5, s3 = (R)0.86602540378443864676;
     C t1 = cadd(a[1], a[2]), t2 = cimul(cscale(csub(a[1], a[2]), s3), sg);
-    C m = cadd(a[0], cscale(t1, c3));
+    C m = cfmas(t1, c3, a[0]);
     a[0] = cadd(a[0], t1);
     a[1] = cadd(m, t2);
     a[2] = csub(m, t2);
@@ -94,10 +133,10 @@ template <typename C> __device__ __forceinline__ void dft_r(C *a, int r, int sg)
     const R s1 = (R)0.95105651629515357212, s2 = (R)0.58778525229247312917;
     C t1 = cadd(a[1], a[4]), t2 = cadd(a[2], a[3]);
     C t3 = csub(a[1], a[4]), t4 = csub(a[2], a[3]);
-    C m1 = cadd(a[0], cadd(cscale(t1, c1), cscale(t2, c2)));
-    C m2 = cadd(a[0], cadd(cscale(t1, c2), cscale(t2, c1)));
-    C n1 = cimul(cadd(cscale(t3, s1), cscale(t4, s2)), sg);
-    C n2 = cimul(csub(cscale(t3, s2), cscale(t4, s1)), sg);
+    C m1 = cfmas(t2, c2, cfmas(t1, c1, a[0]));
+    C m2 = cfmas(t2, c1, cfmas(t1, c2, a[0]));
+    C n1 = cimul(cfmas(t4, s2, cscale(t3, s1)), sg);
+    C n2 = cimul(cfmas(t4, -s1, cscale(t3, s2)), sg);
     a[0] = cadd(a[0], cadd(t1, t2));
     a[1] = cadd(m1, n1);
     a[4] = csub(m1, n1);
