@@ -48,7 +48,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         subprocess.check_call(cmd)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    cmd = [_nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcublas"]
+    cmd = [_nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcublas", "-lcusolver"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)

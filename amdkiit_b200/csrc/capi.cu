@@ -1,5 +1,6 @@
 // libamdk: device context and the extern "C" entry points of include/amdk.h.
 #include <cublas_v2.h>
+#include <cusolverDn.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -80,6 +81,13 @@ struct amdk_ctx {
   int device = 0, precision = AMDK_FP64, batch = 4;
   cudaStream_t st = nullptr;
   cublasHandle_t cb = nullptr;
+  // cuSOLVER for the Cholesky/inverse of overlaps too large for one SM
+  cusolverDnHandle_t cs = nullptr;
+  double *d_potrf_ws = nullptr;
+  int potrf_lw = 0;
+  void *d_trtri_ws = nullptr, *h_trtri_ws = nullptr;
+  size_t trtri_dws = 0, trtri_hws = 0;
+  int *d_info2 = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
   // geometry / FFT
@@ -780,10 +788,20 @@ static int do_ortho(amdk_ctx *c, bool check = true, bool swap = true) {
   const int np = (n + CHOL_B - 1) / CHOL_B * CHOL_B;
   const size_t sm = ((size_t)np * (np + 1) + (size_t)CHOL_B * np) * sizeof(double);
   ++c->nlaunch;
-  if (n <= CHOL_NMAX)
+  if (n <= CHOL_NMAX) {
     k_chol_inv_s<<<1, CHOL_NT, sm, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
-  else
-    k_chol_inv<<<1, 1024, 0, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
+  } else {
+    // DPOTRF + DTRTRI as the reference (wfn_initialize.f90:513,524), in place
+    // in a copy of S (the lower triangle is never read by the DTRMM below)
+    CK(cudaMemcpyAsync(c->d_uinv, c->d_gam, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, c->st));
+    if (cusolverDnDpotrf(c->cs, CUBLAS_FILL_MODE_UPPER, n, c->d_uinv, n, c->d_potrf_ws, c->potrf_lw, c->d_info) !=
+            CUSOLVER_STATUS_SUCCESS ||
+        cusolverDnXtrtri(c->cs, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, n, CUDA_R_64F, c->d_uinv, n,
+                         c->d_trtri_ws, c->trtri_dws, c->h_trtri_ws, c->trtri_hws, c->d_info2) != CUSOLVER_STATUS_SUCCESS) {
+      set_error("cuSOLVER Cholesky/inverse failed");
+      return AMDK_ERR_CUDA;
+    }
+  }
   CK(cudaMemcpyAsync(c->h_info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   if (check) {
     CK(cudaStreamSynchronize(c->st));
@@ -957,7 +975,6 @@ static int build_device(amdk_ctx *c) {
     CK(cudaMemcpyToSymbol(c_twd, twd.data(), sizeof(double2) * CTW_LEN));
     CK(cudaMemcpyToSymbol(c_twf, twf.data(), sizeof(float2) * CTW_LEN));
   }
-  CK(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(k_chol_inv_s, cudaFuncAttributeMaxDynamicSharedMemorySize, 216 * 1024));
   // G vectors
   RC(c->up(&c->d_inyh, h.inyh));
@@ -985,6 +1002,30 @@ static int build_device(amdk_ctx *c) {
     }
     const char *env = getenv("AMDK_NO_GRAPHS");
     c->use_graphs = !(env && env[0] == '1');
+  }
+  if (h.nstate > CHOL_NMAX) {
+    // large overlaps: cuSOLVER (its DTRTRI keeps a host workspace, so the
+    // iteration is not graph-captured)
+    if (cusolverDnCreate(&c->cs) != CUSOLVER_STATUS_SUCCESS || cusolverDnSetStream(c->cs, c->st) != CUSOLVER_STATUS_SUCCESS) {
+      set_error("cusolverDnCreate failed");
+      return AMDK_ERR_CUDA;
+    }
+    const int n = h.nstate;
+    double *tmp;
+    RC(c->alloc(&tmp, (size_t)n * n));
+    if (cusolverDnDpotrf_bufferSize(c->cs, CUBLAS_FILL_MODE_UPPER, n, tmp, n, &c->potrf_lw) != CUSOLVER_STATUS_SUCCESS ||
+        cusolverDnXtrtri_bufferSize(c->cs, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, n, CUDA_R_64F, tmp, n,
+                                    &c->trtri_dws, &c->trtri_hws) != CUSOLVER_STATUS_SUCCESS) {
+      set_error("cuSOLVER workspace query failed");
+      return AMDK_ERR_CUDA;
+    }
+    RC(c->alloc(&c->d_potrf_ws, (size_t)std::max(c->potrf_lw, 1)));
+    char *tw;
+    RC(c->alloc(&tw, std::max<size_t>(c->trtri_dws, 16)));
+    c->d_trtri_ws = tw;
+    c->h_trtri_ws = std::malloc(std::max<size_t>(c->trtri_hws, 16));
+    RC(c->alloc(&c->d_info2, 4));
+    c->use_graphs = false;
   }
   RC(c->up(&c->d_occ, h.occ));
   {
@@ -1293,6 +1334,8 @@ int amdk_destroy(amdk_ctx *c) {
   for (auto &kv : c->graphs)
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   if (c->h_pin) cudaFreeHost(c->h_pin);
+  if (c->cs) cusolverDnDestroy(c->cs);
+  if (c->h_trtri_ws) std::free(c->h_trtri_ws);
   if (c->h_info) cudaFreeHost(c->h_info);
   for (auto &e : c->evpool) {
     cudaEventDestroy(e.first);

@@ -538,65 +538,6 @@ __global__ void k_pcg_update(long tot, const double *scal, double2 *cp, double2 
 }
 __global__ void k_copy_scalar(const double *src, double *dst) { *dst = *src; }
 
-// Cholesky S = U^T U (upper, DPOTRF('U')) followed by U <- U^{-1} (DTRTRI),
-// UINV of wfn_initialize.f90:504-530, in one block.  Column step j subtracts
-// S(j,a) S(j,b) / S(j,j) from the trailing upper triangle (one barrier per
-// step); the rows are scaled by 1/sqrt(S(j,j)) at the end.  The inverse is
-// computed column by column (one thread per column, back substitution).
-// Output: Ui (n x n, column-major, zero below the diagonal).  *info = j+1 if
-// the leading minor j is not positive definite.
-__global__ void k_chol_inv(int n, double *A, double *Ui, int *info) {
-  extern __shared__ double shc[];
-  // small n: factor in shared memory; otherwise in place in A (scratch)
-  const bool in_smem = (size_t)n * n * sizeof(double) <= 200 * 1024;
-  double *M = in_smem ? shc : A;
-  if (in_smem)
-    for (long k = threadIdx.x; k < (long)n * n; k += blockDim.x) M[k] = A[k];
-  __shared__ int bad;
-  if (threadIdx.x == 0) bad = 0;
-  __syncthreads();
-  for (int j = 0; j < n; ++j) {
-    const double d = M[j + (long)n * j];
-    if (!(d > 0.0)) {
-      if (threadIdx.x == 0) bad = j + 1;
-      break;   // uniform: every thread read the same d
-    }
-    const double inv = 1.0 / d;
-    const int m = n - j - 1;
-    const long cnt = (long)m * m;
-    for (long k = threadIdx.x; k < cnt; k += blockDim.x) {
-      const int a = j + 1 + (int)(k % m), b = j + 1 + (int)(k / m);
-      if (a <= b) M[a + (long)n * b] -= M[j + (long)n * a] * M[j + (long)n * b] * inv;
-    }
-    __syncthreads();
-  }
-  __syncthreads();
-  if (bad) {
-    if (threadIdx.x == 0) *info = bad;
-    return;
-  }
-  // U(j,b) = M(j,b) / sqrt(M(j,j)) for b >= j
-  for (long k = threadIdx.x; k < (long)n * n; k += blockDim.x) {
-    const int a = (int)(k % n), b = (int)(k / n);
-    if (a < b) M[k] = M[k] / sqrt(M[a + (long)n * a]);
-  }
-  __syncthreads();
-  for (int a = threadIdx.x; a < n; a += blockDim.x) M[a + (long)n * a] = sqrt(M[a + (long)n * a]);
-  __syncthreads();
-  // inverse: column j of U^{-1} solves U x = e_j; x stored into Ui
-  for (int j = threadIdx.x; j < n; j += blockDim.x) {
-    double *x = Ui + (long)n * j;
-    for (int i = j + 1; i < n; ++i) x[i] = 0.0;
-    x[j] = 1.0 / M[j + (long)n * j];
-    for (int i = j - 1; i >= 0; --i) {
-      double t = 0.0;
-      for (int k = i + 1; k <= j; ++k) t += M[i + (long)n * k] * x[k];
-      x[i] = -t / M[i + (long)n * i];
-    }
-  }
-  if (threadIdx.x == 0) *info = 0;
-}
-
 // Shared-memory blocked Cholesky + inverse for n <= CHOL_NMAX, one block of
 // CHOL_NT threads.  The matrix is padded to np = 16*ceil(n/16) with the
 // identity and held in shared memory with leading dimension np+1.  Per
@@ -608,7 +549,7 @@ __global__ void k_chol_inv(int n, double *A, double *Ui, int *info) {
 // by block back substitution, j = last ... 0: X_j,c = X_jj R_j,c (c > j),
 // then R_i,c -= U_i,j X_j,c (i < j, c >= j; the block c = j becomes
 // -U_i,j X_jj), with R = I to start.  A non-positive pivot sets *info to its
-// 1-based index.  Same contract as k_chol_inv.
+// 1-based index; Ui gets U^{-1} (upper, zero below).
 constexpr int CHOL_NMAX = 144;
 constexpr int CHOL_NT = 512;
 constexpr int CHOL_B = 16;
@@ -731,6 +672,7 @@ __global__ void __launch_bounds__(CHOL_NT) k_chol_inv_s(int n, const double *A, 
     }
     __syncthreads();
   }
+  __syncthreads();  // the last block row (jb = 0) left the loop right after its writes
   for (int b = w; b < n; b += nw)
     for (int a = lane; a < n; a += 32) Ui[a + (long)n * b] = (a <= b) ? M[a + ld * b] : 0.0;
   if (tid == 0) *info = 0;

@@ -259,6 +259,89 @@ def run_arm(prec, args, local, dist, world):
     return out
 
 
+def config_report(args, local):
+    """The other benchmark configurations (one JSON line): SCF iter/s of the
+    FP64 and mixed paths, and the converged energy and force differences of
+    the two (mixed with its FP64 refinement) from the same start."""
+    import threading
+    from amdkiit_b200 import configs
+    from amdkiit_b200.engine import FP64, MIXED, Engine
+    from amdkiit_b200.guess import initial_coefficients
+
+    def start(e, s):
+        g = e.gvectors()
+        tp = 2.0 * np.pi / s.alat
+        return initial_coefficients(g["hg"][: e.ngpw] * tp * tp, e.nstate)
+
+    def timed(e, n):
+        for i in range(1, 4):
+            e.scf_iteration(i, 1e-6)
+        ms = 0.0
+        for i in range(4, 4 + n):
+            e.scf_iteration(i, 1e-6)
+            ms += e.last_iteration_ms()
+        return n / (ms / 1000.0)
+
+    def one(name, s, steps):
+        row = {"config": name, "grid": None, "nstate": s.nstate, "atoms": s.nat}
+        res = {}
+        for pname, prec in (("fp64", FP64), ("mixed", MIXED)):
+            e = Engine(s, precision=prec, device=local)
+            row["grid"] = list(e.nr)
+            c0 = start(e, s)
+            e.set_wfn(c0)
+            e.ortho()
+            row[pname + "_scf_iter_per_s"] = timed(e, steps)
+            e.set_wfn(c0)
+            e.ortho()
+            n, en, gm = e.wfn_opt(1500, 1e-6)
+            res[pname] = (en["etotal"], e.get("force") if n > 1 else e.ionic_forces(), n)
+            e.close()
+        row["scf_speedup"] = row["mixed_scf_iter_per_s"] / row["fp64_scf_iter_per_s"]
+        row["dE_Ha_per_atom"] = abs(res["mixed"][0] - res["fp64"][0]) / s.nat
+        row["dF_max_Ha_per_bohr"] = float(np.max(np.abs(res["mixed"][1] - res["fp64"][1])))
+        row["iterations_to_1e-6"] = {"fp64": res["fp64"][2], "mixed": res["mixed"][2]}
+        return row
+
+    rows = [one("cfg0 water1 (64^3, 4 bands)", configs.water1(), args.steps),
+            one("cfg1 si64 (72^3, 128 bands)", configs.si64(), args.steps),
+            one("cfg4 water128 (160^3, 512 bands)", configs.water128(), max(3, args.steps // 10))]
+    # cfg2: 16 independent clusters at once, one engine (stream) and host
+    # thread each; value = SCF iterations of all systems / wall time
+    ens = configs.ensemble()
+    for pname, prec in (("fp64", FP64), ("mixed", MIXED)):
+        engines = []
+        for s in ens:
+            e = Engine(s, precision=prec, device=local)
+            e.set_wfn(start(e, s))
+            e.ortho()
+            for i in range(1, 4):
+                e.scf_iteration(i, 1e-6)
+            engines.append(e)
+
+        def work(e):
+            for i in range(4, 4 + args.steps):
+                e.scf_iteration(i, 1e-6)
+        th = [threading.Thread(target=work, args=(e,)) for e in engines]
+        t0 = time.perf_counter()
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        wall = time.perf_counter() - t0
+        if pname == "fp64":
+            ens_row = {"config": "cfg2 ensemble of 16 clusters (concurrent, one stream each)",
+                       "systems": len(ens), "grids": sorted({tuple(e.nr) for e in engines})}
+        ens_row[pname + "_scf_iter_per_s"] = len(ens) * args.steps / wall
+        ens_row["timing"] = "host wall clock over all systems"
+        for e in engines:
+            e.close()
+    ens_row["scf_speedup"] = ens_row["mixed_scf_iter_per_s"] / ens_row["fp64_scf_iter_per_s"]
+    rows.append(ens_row)
+    print(json.dumps({"metric": METRIC, "report": "other configurations", "unit": UNIT, "rows": rows}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -269,6 +352,8 @@ def main():
                     help="both: mixed precision is the headline value, FP64 is measured beside it")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--md-steps", type=int, default=3)
+    ap.add_argument("--configs", action="store_true",
+                    help="report configurations 0, 1, 2 and 4 instead of the headline line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -276,6 +361,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.configs:
+        return config_report(args, local) if rank == 0 else 0
 
     import torch
     dist = None

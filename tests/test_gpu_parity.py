@@ -272,3 +272,14 @@ def test_graph_replay_with_profiling():
     got = [e.profile_get(k) for k in e.KERNELS]
     e.profile(False)
     assert all(n >= 4 and ms > 0 for n, ms, _ in got), got
+
+
+@pytest.mark.parametrize("nmol", [2, 5, 7, 8, 12])
+def test_ortho_matches_oracle_across_band_counts(nmol):
+    """ortho_gs for band counts that are and are not multiples of the
+    Cholesky kernel's 16-column blocks (8 to 48 bands)."""
+    s = configs.cluster(nmol, 18.0, 900 + nmol, ecut=20.0)
+    o, e = pair(s)
+    assert o.ortho() == 0
+    e.ortho()
+    assert rel(e.get_wfn(), o.c0()) < 1e-11
