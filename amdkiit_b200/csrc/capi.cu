@@ -139,6 +139,8 @@ struct amdk_ctx {
   bool warm[2] = {false, false};  // an eager iteration has run at this pair precision
   void *c0_first = nullptr;       // the buffer that held C0 at creation
   void *cb_ws = nullptr;          // cuBLAS workspace (fixed, for capture)
+  double2 *d_hist = nullptr;      // C0 of the previous MD step (predictor)
+  bool have_hist = false;
   int *h_info = nullptr;    // pinned: Cholesky status
   int pencil_groups = 1;  // upper bound on the density pair groups
   int ct_vpsi = 0, ct_dens = 0;  // column tiles of the pencil kernels (current precision)
@@ -1537,6 +1539,39 @@ int amdk_ionic_forces(amdk_ctx *c, double *force) {
   RC(do_ionic_forces(c));
   CK(cudaMemcpyAsync(force, c->d_force, sizeof(double) * 3 * c->hs.na_max * c->hs.nsp, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int amdk_wfn_extrapolate(amdk_ctx *c) {
+  if (!c) return AMDK_ERR_BADARG;
+  cudaSetDevice(c->device);
+  const HostSetup &h = c->hs;
+  const size_t cw = (size_t)h.ngpw * c->nstate;
+  if (!c->d_hist) RC(c->alloc(&c->d_hist, cw));
+  if (c->have_hist) {
+    const int n = c->nstate, K = 2 * h.ngpw;
+    const double two = 2.0, one = 1.0, zero = 0.0;
+    // M = 2 Re C_prev^T C0 - Re c_prev(0) Re c0(0)^T, then cp = C_prev M
+    CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, (const double *)c->d_hist, K,
+                   (const double *)c->d_c0, K, &zero, c->d_gam, n));
+    ++c->nlaunch;
+    k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_hist, c->d_c0, c->d_gam, c->d_occ, 0, 0);
+    CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, (const double *)c->d_hist, K, c->d_gam, n, &zero,
+                   (double *)c->d_cp, K));
+    ++c->nlaunch;
+    k_two_a_minus<<<RED_BLOCKS * 4, NTHR, 0, c->st>>>((long)cw, c->d_c0, c->d_cp);
+    CK(cudaMemcpyAsync(c->d_hist, c->d_c0, sizeof(double2) * cw, cudaMemcpyDeviceToDevice, c->st));
+    std::swap(c->d_c0, c->d_cp);
+  } else {
+    CK(cudaMemcpyAsync(c->d_hist, c->d_c0, sizeof(double2) * cw, cudaMemcpyDeviceToDevice, c->st));
+    c->have_hist = true;
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+int amdk_wfn_history_clear(amdk_ctx *c) {
+  if (!c) return AMDK_ERR_BADARG;
+  c->have_hist = false;
   return 0;
 }
 

@@ -453,6 +453,13 @@ __global__ void k_ekin(int ngpw, int nstate, const double2 *c0, const double *hg
   double r = block_sum(s, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = r;
 }
+// c = 2 a - c (wavefunction predictor)
+__global__ void k_two_a_minus(long n, const double2 *__restrict__ a, double2 *__restrict__ c) {
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+    const double2 x = a[k], y = c[k];
+    c[k] = make_double2(2.0 * x.x - y.x, 2.0 * x.y - y.y);
+  }
+}
 // rank-1 G=0 correction and occupation mask of OVLAP_D / ortho_gs DGER
 // (wfn_initialize.f90:257,482): A(i,j) -= Re a_i(0) Re b_j(0); mask fsc
 __global__ void k_g0_correct(int n, int ngpw, const double2 *a, const double2 *b, double *A, const double *occ, int mask,

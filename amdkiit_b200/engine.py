@@ -80,6 +80,8 @@ def load_library(path: str = LIBPATH):
     lib.amdk_host_gvectors.argtypes = [C.POINTER(_System), C.POINTER(_Info), P, P, P, P, P]
     lib.amdk_set_positions.argtypes = [P, C.POINTER(C.c_double)]
     lib.amdk_set_precision.argtypes = [P, C.c_int]
+    lib.amdk_wfn_extrapolate.argtypes = [P]
+    lib.amdk_wfn_history_clear.argtypes = [P]
     lib.amdk_set_wfn.argtypes = [P, C.POINTER(C.c_double)]
     lib.amdk_get_wfn.argtypes = [P, C.POINTER(C.c_double)]
     for f in ("amdk_ortho", "amdk_density", "amdk_potential", "amdk_apply_h"):
@@ -186,6 +188,14 @@ class Engine:
         self.nr = tuple(info.nr)
         self.precision = precision      # precision the engine was created with
         self.pair_precision = precision  # precision of the band-pair FFTs now
+
+    def extrapolate(self):
+        """BOMD predictor: C0 <- 2 C0(t) - C0(t-dt) [C0(t-dt)^T C0(t)] once a
+        previous step is stored (stores C0(t)); orthonormalise afterwards."""
+        _check(self.lib.amdk_wfn_extrapolate(self.h), "amdk_wfn_extrapolate")
+
+    def clear_history(self):
+        _check(self.lib.amdk_wfn_history_clear(self.h), "amdk_wfn_history_clear")
 
     def set_precision(self, precision: int):
         """Precision of the band-pair transforms from the next call on."""

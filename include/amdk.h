@@ -164,6 +164,16 @@ int amdk_ionic_forces(amdk_ctx *ctx, double *force);
  * reference's C2 negated).  Either pointer may be NULL. */
 int amdk_backward(amdk_ctx *ctx, double *dE_dR, double *dE_dpsi);
 
+/* Wavefunction predictor for BOMD (no reference counterpart: the reference
+ * restarts each step from the previous C0, molecular_dynamics.f90:106-109).
+ * With a previous step's C0 stored, C0 <- 2 C0(t) - C0(t-dt) M with
+ * M = C0(t-dt)^T C0(t) (the overlap in the Gamma convention, aligning the
+ * previous occupied subspace with the current one); C0(t) is then stored.
+ * The caller orthonormalises afterwards (amdk_ortho), as after a geometry
+ * update.  amdk_wfn_history_clear forgets the stored C0. */
+int amdk_wfn_extrapolate(amdk_ctx *ctx);
+int amdk_wfn_history_clear(amdk_ctx *ctx);
+
 /* Copy a named device array to host memory (parity tests and drivers).
  * Names: "rho","v_pot" (nr3*nr2*nr1 real, x fastest), "rho_g" (ngrho complex),
  * "c2" (ngpw*nstate complex), "nl" (nat*nghmax*nstate), "vps","rhos"

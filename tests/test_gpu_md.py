@@ -88,3 +88,20 @@ def test_bomd_energy_error_scales_with_timestep():
         drift.append(worst)
     assert drift[1] < 0.5 * drift[0]
     assert drift[0] < 1e-3
+
+
+def test_bomd_predictor_keeps_trajectory_and_saves_iterations():
+    """The wavefunction predictor (an option outside the reference driver)
+    reaches the same states to the SCF tolerance in fewer iterations."""
+    s = configs.small_water()
+    runs = {}
+    for x in (False, True):
+        e = _engine(s)
+        md = BOMD(e, temperature=300.0, dt_fs=0.5, seed=3, gcut=1e-7, extrapolate=x)
+        md.start()
+        for _ in range(6):
+            md.step()
+        runs[x] = md
+    assert np.max(np.abs(runs[True].pos - runs[False].pos)) < 1e-6
+    assert abs(runs[True].total_energy() - runs[False].total_energy()) < 1e-7
+    assert np.mean(runs[True].scf_iterations[3:]) < np.mean(runs[False].scf_iterations[3:])
