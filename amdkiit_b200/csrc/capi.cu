@@ -136,6 +136,7 @@ struct amdk_ctx {
   };
   std::map<std::array<int, 4>, SegGraph> graphs;
   bool use_graphs = true;
+  bool tune = true;  // measure launch shapes at first use (AMDK_NO_TUNE=1: model only)
   bool warm[2] = {false, false};  // an eager iteration has run at this pair precision
   void *c0_first = nullptr;       // the buffer that held C0 at creation
   void *cb_ws = nullptr;          // cuBLAS workspace (fixed, for capture)
@@ -472,25 +473,10 @@ template <typename C> static void pencil_vpsi(amdk_ctx *c, int T) {
   });
   prof_end(c);
 }
-template <typename C> static int density_groups(amdk_ctx *c, int T) {
+template <typename C> static void launch_pencil_density(amdk_ctx *c, int p0, int T, int grp) {
   const Geom &g = c->geom;
   const size_t sm = pencil_acc_smem<C>(g.n2) + pencil_smem<C>(g.n2, c->pg.nz, c->ct_dens);
-  const int key = 2 * T + (c->precision == AMDK_MIXED ? 1 : 0);
-  auto it = c->pencil_grp_cache.find(key);
-  if (it == c->pencil_grp_cache.end())
-    it = c->pencil_grp_cache
-             .emplace(key, pencil_density_groups(g.n1, T, c->nsm, (int)std::max<size_t>(1, (228 * 1024) / (sm + 1024)),
-                                               c->pencil_groups))
-             .first;
-  return it->second;
-}
-template <typename C> static void pencil_density(amdk_ctx *c, int p0, int T) {
-  const Geom &g = c->geom;
-  const size_t sm = pencil_acc_smem<C>(g.n2) + pencil_smem<C>(g.n2, c->pg.nz, c->ct_dens);
-  const int grp = density_groups<C>(c, T);
   const int per = (T + grp - 1) / grp;
-  const double npt = (double)g.n1 * g.n2 * g.n3;
-  prof_begin(c, KT_ZDENS, (double)T * rstride(c, 0) * sizeof(C) + 2.0 * grp * npt * 8.0);
   with_n(g.n2, [&](auto NC) {
     constexpr int N = decltype(NC)::value;
     if constexpr (N > 0) {
@@ -500,6 +486,57 @@ template <typename C> static void pencil_density(amdk_ctx *c, int p0, int T) {
                                                                   c->d_wa + p0, c->d_wb + p0, c->d_rhopart, c->ct_dens);
     }
   });
+}
+// Pair groups of the density pencil kernel for T pairs at the current
+// precision: measured once (every candidate launched on the current buffers,
+// whose contents do not matter for the timing; the partial grids are cleared
+// before use), then cached.  Inside a graph capture the schedule model's
+// choice is used instead.
+template <typename C> static int density_groups(amdk_ctx *c, int T) {
+  const Geom &g = c->geom;
+  const size_t sm = pencil_acc_smem<C>(g.n2) + pencil_smem<C>(g.n2, c->pg.nz, c->ct_dens);
+  const int key = 2 * T + (c->precision == AMDK_MIXED ? 1 : 0);
+  auto it = c->pencil_grp_cache.find(key);
+  if (it != c->pencil_grp_cache.end()) return it->second;
+  int best = pencil_density_groups(g.n1, T, c->nsm, (int)std::max<size_t>(1, (228 * 1024) / (sm + 1024)),
+                                   c->pencil_groups);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(c->st, &cap);
+  if (cap == cudaStreamCaptureStatusNone && c->tune) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const long nl = c->nlaunch;
+    float best_ms = 1e30f;
+    const int cands[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16};
+    for (int grp : cands) {
+      if (grp > c->pencil_groups || grp > T || (grp - 1) * ((T + grp - 1) / grp) >= T) continue;  // no empty group
+      launch_pencil_density<C>(c, 0, T, grp);  // warm
+      cudaEventRecord(e0, c->st);
+      launch_pencil_density<C>(c, 0, T, grp);
+      launch_pencil_density<C>(c, 0, T, grp);
+      cudaEventRecord(e1, c->st);
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = grp;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->nlaunch = nl;  // tuning launches are not part of the work
+  }
+  c->pencil_grp_cache.emplace(key, best);
+  return best;
+}
+template <typename C> static void pencil_density(amdk_ctx *c, int p0, int T) {
+  const Geom &g = c->geom;
+  const int grp = density_groups<C>(c, T);
+  const double npt = (double)g.n1 * g.n2 * g.n3;
+  prof_begin(c, KT_ZDENS, (double)T * rstride(c, 0) * sizeof(C) + 2.0 * grp * npt * 8.0);
+  launch_pencil_density<C>(c, p0, T, grp);
   prof_end(c);
 }
 
@@ -1004,6 +1041,8 @@ static int build_device(amdk_ctx *c) {
     }
     const char *env = getenv("AMDK_NO_GRAPHS");
     c->use_graphs = !(env && env[0] == '1');
+    const char *nt = getenv("AMDK_NO_TUNE");
+    c->tune = !(nt && nt[0] == '1');
   }
   if (h.nstate > CHOL_NMAX) {
     // large overlaps: cuSOLVER (its DTRTRI keeps a host workspace, so the

@@ -286,6 +286,7 @@ __global__ void __launch_bounds__(PNT) k_pencil_density(PencilGeom pg, Plan<C> p
       __syncthreads();
     }
   }
+  __syncthreads();  // a group without pairs has seen no barrier since the clearing
   double *out = rho_part + ((long)grp * pg.n1 + kx) * N * N;
   for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
     const int q = idx / N, k = idx % N;

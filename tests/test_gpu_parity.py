@@ -242,6 +242,9 @@ def test_graph_replay_matches_eager(monkeypatch):
     iteration on) give the eager launches' energies, gradients and C0, with
     and without the ionic forces segment."""
     s = configs.small_water(xc=XC_PBE)
+    # measured launch shapes could differ between the two engines and change
+    # the summation order; the model's choice is deterministic
+    monkeypatch.setenv("AMDK_NO_TUNE", "1")
     o, ref = pair(s)
     c = ref.get_wfn()
     monkeypatch.setenv("AMDK_NO_GRAPHS", "1")
@@ -283,3 +286,20 @@ def test_ortho_matches_oracle_across_band_counts(nmol):
     assert o.ortho() == 0
     e.ortho()
     assert rel(e.get_wfn(), o.c0()) < 1e-11
+
+
+def test_density_independent_of_measured_launch_shape(monkeypatch):
+    """The density pair-group count is measured at first use; whatever it
+    picks, the density equals the model choice's to rounding."""
+    s = configs.water32()
+    monkeypatch.setenv("AMDK_NO_TUNE", "1")
+    ref = Engine(s, FP64)
+    monkeypatch.delenv("AMDK_NO_TUNE")
+    e = Engine(s, FP64)
+    g = ref.gvectors()
+    c = start_coefficients(g["hg"][: ref.ngpw], 2 * np.pi / s.alat, ref.nstate, 7)
+    for x in (ref, e):
+        x.set_wfn(c)
+        x.ortho()
+        x.density()
+    assert rel(e.get("rho"), ref.get("rho")) < 1e-13
