@@ -100,6 +100,13 @@ struct amdk_ctx {
   double *d_hg = nullptr, *d_gvec = nullptr;
   long rb_elems_pw = 0, sb_elems_pw = 0, rb_elems_rho = 0, sb_elems_rho = 0;
   void *d_rb = nullptr, *d_sb = nullptr;
+  void *d_rbf = nullptr;  // ray buffer of the density-sphere fields
+  // side stream for the work that needs only C0 (projections, E_kin, the
+  // x pass of H|psi>), overlapped with the density and the potential
+  cudaStream_t st2 = nullptr;
+  cublasHandle_t cb2 = nullptr;
+  double *d_part2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_rt_free = nullptr, ev_side_done = nullptr;
   size_t fftbuf_bytes = 0;
   // tables
   double *d_vps = nullptr, *d_rhos = nullptr, *d_twnl = nullptr, *d_vpp = nullptr, *d_wsg = nullptr;
@@ -137,6 +144,7 @@ struct amdk_ctx {
   std::map<std::array<int, 4>, SegGraph> graphs;
   bool use_graphs = true;
   bool tune = true;  // measure launch shapes at first use (AMDK_NO_TUNE=1: model only)
+  bool overlap = true;  // C0-only work on the side stream (AMDK_NO_OVERLAP=1: one stream)
   bool warm[2] = {false, false};  // an eager iteration has run at this pair precision
   void *c0_first = nullptr;       // the buffer that held C0 at creation
   void *cb_ws = nullptr;          // cuBLAS workspace (fixed, for capture)
@@ -300,6 +308,9 @@ template <typename C> static const Plan<C> &plan(amdk_ctx *c, int d);
 template <> const Plan<double2> &plan<double2>(amdk_ctx *c, int d) { return c->pd[d]; }
 template <> const Plan<float2> &plan<float2>(amdk_ctx *c, int d) { return c->pf[d]; }
 
+// ray buffer of a sphere: band pairs (0) or density-sphere fields (1)
+static void *rays(amdk_ctx *c, int sphere) { return sphere ? c->d_rbf : c->d_rb; }
+
 // strides of the FFT buffers for transforms of a sphere
 static long rstride(amdk_ctx *c, int sphere) { return (long)c->geom.nray[sphere] * c->geom.n1; }
 static long sstride(amdk_ctx *c, int sphere) { return (long)c->geom.nz[sphere] * c->geom.n2 * c->geom.n1; }
@@ -312,7 +323,7 @@ template <typename C> static void y_pass(amdk_ctx *c, int sphere, int dir, int T
   with_n(g.n2, [&](auto NC) {
     constexpr int N = decltype(NC)::value;
     smem_opt_in<k_y<C, N>>();
-    k_y<C, N><<<grid, NTHR, yz_smem<C>(g.n2), c->st>>>(sphere, dir, g, plan<C>(c, 1), (C *)c->d_rb, (C *)c->d_sb,
+    k_y<C, N><<<grid, NTHR, yz_smem<C>(g.n2), c->st>>>(sphere, dir, g, plan<C>(c, 1), (C *)rays(c, sphere), (C *)c->d_sb,
                                                       rstride(c, sphere), sstride(c, sphere));
   });
   prof_end(c);
@@ -345,7 +356,7 @@ template <typename C> static void x_fwd(amdk_ctx *c, int sphere, int T) {
   with_n(g.n1, [&](auto NC) {
     constexpr int N = decltype(NC)::value;
     smem_opt_in<k_x_fwd<C, N>>();
-    k_x_fwd<C, N><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(sphere, T, g, plan<C>(c, 0), (C *)c->d_rb);
+    k_x_fwd<C, N><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(sphere, T, g, plan<C>(c, 0), (C *)rays(c, sphere));
   });
   prof_end(c);
 }
@@ -361,7 +372,7 @@ static int field_to_grid(amdk_ctx *c, int T, const double2 *fp, const double2 *f
     constexpr int N = decltype(NC)::value;
     smem_opt_in<k_x_bwd_field<C, N>>();
     k_x_bwd_field<C, N><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(fp, fm, g.ngrho, 1, T, g, plan<C>(c, 0),
-                                                                         (C *)c->d_rb);
+                                                                         (C *)c->d_rbf);
   });
   y_pass<C>(c, 1, +1, T);
   z_pass<C, Z_TO_GRID>(c, 1, T, cgrid, nullptr);
@@ -547,7 +558,7 @@ static int finish_sums(amdk_ctx *c, int nk, int slot) {
   return 0;
 }
 
-template <typename C> static int density_t(amdk_ctx *c) {
+template <typename C> static int density_pairs_t(amdk_ctx *c) {
   const HostSetup &h = c->hs;
   const Geom &g = c->geom;
   if (c->pencil_density) {
@@ -580,15 +591,25 @@ template <typename C> static int density_t(amdk_ctx *c) {
     z_pass<C, Z_DENSITY>(c, 0, T, nullptr, nullptr, p0);
   }
   }
-  // rhor2g (density.f90:128-150), in the pair transforms' precision
+  CK(cudaGetLastError());
+  return 0;
+}
+// rhor2g (density.f90:128-150), in the pair transforms' precision
+template <typename C> static int rhor2g_t(amdk_ctx *c) {
+  const HostSetup &h = c->hs;
+  const Geom &g = c->geom;
   RC(grid_to_rays<C>(c, 1, nullptr, c->d_rho));
   double scale = 1.0 / ((double)g.n1 * g.n2 * g.n3);
   ++c->nlaunch;
-  k_gather_p<C><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_posp, (C *)c->d_rb, scale, c->d_rhog);
+  k_gather_p<C><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_posp, (C *)c->d_rbf, scale, c->d_rhog);
   CK(cudaGetLastError());
   return 0;
 }
 
+template <typename C> static int density_t(amdk_ctx *c) {
+  RC(density_pairs_t<C>(c));
+  return rhor2g_t<C>(c);
+}
 static int do_density(amdk_ctx *c) {
   if (c->precision == AMDK_MIXED) return density_t<float2>(c);
   return density_t<double2>(c);
@@ -618,7 +639,7 @@ template <typename C> static int potential_t(amdk_ctx *c) {
   RC(grid_to_rays<C>(c, gga ? 2 : 1, c->d_cgrid, nullptr));
   double scale = 1.0 / (double)npt;
   ++c->nlaunch;
-  k_xc_combine<C><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, gga, c->d_posp, c->d_posm, (C *)c->d_rb, rstride(c, 1),
+  k_xc_combine<C><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, gga, c->d_posp, c->d_posm, (C *)c->d_rbf, rstride(c, 1),
                                                      scale, c->d_gvec, h.tpiba, c->d_vg, c->d_vxg);
   ++c->nlaunch;
   k_conj_field<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_vxg, c->d_fm);
@@ -719,7 +740,8 @@ static int fill_energies(amdk_ctx *c, const double *sc, amdk_energies *e) {
 // pp_energy + e_total.  With e the energies are read back now (one stream
 // synchronisation); without, the scalar slots are copied to the pinned host
 // buffer in stream order for fill_energies after the caller's own sync.
-static int do_energy(amdk_ctx *c, amdk_energies *e) {
+// the C0-only part of pp_energy/e_total: projections, E_nl, E_kin
+static int energy_c0_terms(amdk_ctx *c) {
   const HostSetup &h = c->hs;
   RC(do_fnl(c));
   if (c->nproj) {
@@ -732,6 +754,10 @@ static int do_energy(amdk_ctx *c, amdk_energies *e) {
   ++c->nlaunch;
   k_ekin<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngpw, c->nstate, c->d_c0, c->d_hg, c->d_occ, c->d_part);
   RC(finish_sums(c, 1, S_EKIN));
+  return 0;
+}
+static int do_energy(amdk_ctx *c, amdk_energies *e) {
+  RC(energy_c0_terms(c));
   CK(cudaMemcpyAsync(c->h_pin, c->d_scal, sizeof(double) * S_NSCAL, cudaMemcpyDeviceToHost, c->st));
   if (e) {
     CK(cudaStreamSynchronize(c->st));
@@ -1035,14 +1061,20 @@ static int build_device(amdk_ctx *c) {
     char *w;
     RC(c->alloc(&w, ws));
     c->cb_ws = w;
-    if (cublasSetWorkspace(c->cb, c->cb_ws, ws) != CUBLAS_STATUS_SUCCESS) {
+    char *w2;
+    RC(c->alloc(&w2, ws));
+    if (cublasSetWorkspace(c->cb, c->cb_ws, ws) != CUBLAS_STATUS_SUCCESS ||
+        cublasSetWorkspace(c->cb2, w2, ws) != CUBLAS_STATUS_SUCCESS) {
       set_error("cublasSetWorkspace failed");
       return AMDK_ERR_CUDA;
     }
+    RC(c->alloc(&c->d_part2, (size_t)RED_BLOCKS * 4));
     const char *env = getenv("AMDK_NO_GRAPHS");
     c->use_graphs = !(env && env[0] == '1');
     const char *nt = getenv("AMDK_NO_TUNE");
     c->tune = !(nt && nt[0] == '1');
+    const char *no = getenv("AMDK_NO_OVERLAP");
+    c->overlap = !(no && no[0] == '1');
   }
   if (h.nstate > CHOL_NMAX) {
     // large overlaps: cuSOLVER (its DTRTRI keeps a host workspace, so the
@@ -1139,13 +1171,15 @@ static int build_device(amdk_ctx *c) {
   // pair batch: all pairs at once on the pencil path, else 8
   if (c->batch <= 0) c->batch = pencil_all ? c->npairs : 8;
   c->batch = std::max(1, std::min(c->batch, c->npairs));
-  size_t rb = std::max((size_t)c->batch * rstride(c, 0) * sizeof(double2), 2 * (size_t)rstride(c, 1) * sizeof(double2));
+  size_t rb = (size_t)c->batch * rstride(c, 0) * sizeof(double2);
+  const size_t rbf = 2 * (size_t)rstride(c, 1) * sizeof(double2);
   size_t sb = 2 * (size_t)sstride(c, 1) * sizeof(double2);
   if (!(c->pv_p[0] && c->pd_p[0] && c->pv_p[1] && c->pd_p[1]))
     sb = std::max(sb, (size_t)c->batch * sstride(c, 0) * sizeof(double2));
   RC(c->alloc((char **)&c->d_rb, rb));
+  RC(c->alloc((char **)&c->d_rbf, rbf));
   RC(c->alloc((char **)&c->d_sb, sb));
-  c->fftbuf_bytes = rb + sb;
+  c->fftbuf_bytes = rb + rbf + sb;
   set_pair_precision(c, c->precision);
   if (c->pv_p[0] || c->pv_p[1] || c->pd_p[0] || c->pd_p[1]) {
     std::vector<int> rpos(h.ngrays), zinv(n3, -1), zl0(g.nz[0]), postp(h.ngpw), postm(h.ngpw);
@@ -1281,6 +1315,67 @@ static int build_device(amdk_ctx *c) {
 }
 
 // ------------------------------------------------------------------ C ABI
+// Launches inside its scope go to the side stream, with the side stream's
+// cuBLAS handle and reduction partials.
+struct OnSideStream {
+  amdk_ctx *c;
+  cudaStream_t s;
+  cublasHandle_t b;
+  double *p;
+  explicit OnSideStream(amdk_ctx *cc) : c(cc), s(cc->st), b(cc->cb), p(cc->d_part) {
+    c->st = c->st2;
+    c->cb = c->cb2;
+    c->d_part = c->d_part2;
+  }
+  ~OnSideStream() {
+    c->st = s;
+    c->cb = b;
+    c->d_part = p;
+  }
+};
+
+// Segment A of the CG iteration with the C0-only work on the side stream:
+// projections + E_nl + E_kin and the clearing of C2 from the start, the x
+// pass of H|psi> once the density kernel has released the ray buffer; the
+// context stream runs the density, rho(G), the potential, then (after the
+// join) V(r)psi, fnonloc and the gradient.  Same kernels and results as the
+// sequential order; used on the pencil path with all pairs in one batch.
+template <typename C> static int seg_a_overlap(amdk_ctx *c) {
+  const HostSetup &h = c->hs;
+  const Geom &g = c->geom;
+  const int T = c->npairs;
+  CK(cudaEventRecord(c->ev_fork, c->st));
+  CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
+  {
+    OnSideStream side(c);
+    RC(energy_c0_terms(c));
+    CK(cudaMemsetAsync(c->d_c2, 0, sizeof(double2) * (size_t)h.ngpw * c->nstate, c->st));
+  }
+  RC(density_pairs_t<C>(c));
+  CK(cudaEventRecord(c->ev_rt_free, c->st));
+  {
+    OnSideStream side(c);
+    CK(cudaStreamWaitEvent(c->st, c->ev_rt_free, 0));
+    xt_bwd_pair<C>(c, 0, T);
+    CK(cudaEventRecord(c->ev_side_done, c->st));
+  }
+  RC(rhor2g_t<C>(c));
+  RC(potential_t<C>(c));
+  CK(cudaStreamWaitEvent(c->st, c->ev_side_done, 0));
+  CK(cudaMemcpyAsync(c->h_pin, c->d_scal, sizeof(double) * S_NSCAL, cudaMemcpyDeviceToHost, c->st));
+  pencil_vpsi<C>(c, T);
+  xt_fwd<C>(c, T);
+  dim3 gu(nblk(h.ngpw), T);
+  ++c->nlaunch;
+  k_unpack_vpsi<C><<<gu, NTHR, 0, c->st>>>(h.ngpw, c->nstate, 0, T, c->d_postp, c->d_postm, (C *)c->d_rb, rstride(c, 0),
+                                           1.0 / ((double)g.n1 * g.n2 * g.n3), c->d_hg, h.tpiba2, c->d_occ, c->d_c0,
+                                           c->d_c2);
+  RC(do_fnonloc(c));
+  RC(do_gradient(c));
+  CK(cudaMemcpyAsync(c->h_pin + S_NSCAL, c->d_scal + S_GMAX, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  return 0;
+}
+
 // Run one segment of the CG iteration: captured into a CUDA graph the first
 // time its key is seen, replayed afterwards.  body() only enqueues work on
 // the context stream (no host synchronisation, no host-side state change the
@@ -1357,6 +1452,15 @@ int amdk_create(const amdk_system *sys, const amdk_options *opt, amdk_ctx **out)
   }
   cudaEventCreate(&c->ev0);
   cudaEventCreate(&c->ev1);
+  if (cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess ||
+      cublasCreate(&c->cb2) != CUBLAS_STATUS_SUCCESS || cublasSetStream(c->cb2, c->st2) != CUBLAS_STATUS_SUCCESS ||
+      cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_rt_free, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_side_done, cudaEventDisableTiming) != cudaSuccess) {
+    set_error("side stream / cuBLAS handle creation failed");
+    amdk_destroy(c);
+    return AMDK_ERR_CUDA;
+  }
   rc = build_device(c);
   if (!rc) rc = do_positions(c, sys->atco);
   if (rc) {
@@ -1383,6 +1487,13 @@ int amdk_destroy(amdk_ctx *c) {
     cudaEventDestroy(e.second);
   }
   if (c->cb) cublasDestroy(c->cb);
+  if (c->cb2) cublasDestroy(c->cb2);
+  if (c->st2) {
+    cudaStreamSynchronize(c->st2);
+    cudaStreamDestroy(c->st2);
+  }
+  for (cudaEvent_t e : {c->ev_fork, c->ev_rt_free, c->ev_side_done})
+    if (e) cudaEventDestroy(e);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->st) cudaStreamDestroy(c->st);
@@ -1519,7 +1630,9 @@ int amdk_scf_iteration(amdk_ctx *c, int istep, double gcut, amdk_energies *e, do
   const bool graph = c->use_graphs && istep > 1 && c->warm[q];
   const int parity = (c->d_c0 == c->c0_first) ? 0 : 1;
   cudaEventRecord(c->ev0, c->st);
+  const bool overlap = c->overlap && c->pencil_vpsi && c->pencil_density && c->batch == c->npairs;
   auto seg_a = [&]() -> int {
+    if (overlap) return q ? seg_a_overlap<float2>(c) : seg_a_overlap<double2>(c);
     RC(do_density(c));
     RC(do_potential(c));
     RC(do_energy(c, nullptr));  // energies read after the end-of-iteration sync
@@ -1689,7 +1802,7 @@ int amdk_fft_sphere(amdk_ctx *c, int sign, double *coef, double *grid) {
     CK(cudaMemcpyAsync(c->d_cgrid, grid, sizeof(double2) * npt, cudaMemcpyHostToDevice, c->st));
     RC(grid_to_rays(c, 1, c->d_cgrid, nullptr));
     ++c->nlaunch;
-    k_gather_p<double2><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_posp, (double2 *)c->d_rb, 1.0 / (double)npt,
+    k_gather_p<double2><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_posp, (double2 *)c->d_rbf, 1.0 / (double)npt,
                                                            c->d_vxg);
     CK(cudaMemcpyAsync(coef, c->d_vxg, sizeof(double2) * h.ngrho, cudaMemcpyDeviceToHost, c->st));
   }

@@ -303,3 +303,23 @@ def test_density_independent_of_measured_launch_shape(monkeypatch):
         x.ortho()
         x.density()
     assert rel(e.get("rho"), ref.get("rho")) < 1e-13
+
+
+def test_side_stream_overlap_matches_single_stream(monkeypatch):
+    """The C0-only work on the side stream (the default) leaves every result
+    of the iteration unchanged."""
+    monkeypatch.setenv("AMDK_NO_TUNE", "1")
+    s = configs.small_water(xc=XC_PBE)
+    o, a = pair(s)
+    c = a.get_wfn()
+    monkeypatch.setenv("AMDK_NO_OVERLAP", "1")
+    b = Engine(s, FP64)
+    monkeypatch.delenv("AMDK_NO_OVERLAP")
+    for e in (a, b):
+        e.set_wfn(c)
+        e.ortho()
+    for it in range(1, 7):
+        ra = a.scf_iteration(it, 1e-7)
+        rb = b.scf_iteration(it, 1e-7)
+        assert ra[0] == rb[0] and ra[1] == rb[1], it
+    assert np.array_equal(a.get_wfn(), b.get_wfn())
