@@ -101,12 +101,12 @@ struct amdk_ctx {
   long rb_elems_pw = 0, sb_elems_pw = 0, rb_elems_rho = 0, sb_elems_rho = 0;
   void *d_rb = nullptr, *d_sb = nullptr;
   void *d_rbf = nullptr;  // ray buffer of the density-sphere fields
-  // side stream for the work that needs only C0 (projections, E_kin, the
-  // x pass of H|psi>), overlapped with the density and the potential
+  // side stream for the work that needs only C0 (projections, E_kin, C2
+  // clearing), overlapped with the density and the potential
   cudaStream_t st2 = nullptr;
   cublasHandle_t cb2 = nullptr;
   double *d_part2 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_rt_free = nullptr, ev_side_done = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_side_done = nullptr;
   size_t fftbuf_bytes = 0;
   // tables
   double *d_vps = nullptr, *d_rhos = nullptr, *d_twnl = nullptr, *d_vpp = nullptr, *d_wsg = nullptr;
@@ -1334,11 +1334,12 @@ struct OnSideStream {
   }
 };
 
-// Segment A of the CG iteration with the C0-only work on the side stream:
-// projections + E_nl + E_kin and the clearing of C2 from the start, the x
-// pass of H|psi> once the density kernel has released the ray buffer; the
-// context stream runs the density, rho(G), the potential, then (after the
-// join) V(r)psi, fnonloc and the gradient.  Same kernels and results as the
+// Segment A of the CG iteration with the C0-only work (projections, E_nl,
+// E_kin, the clearing of C2) on the side stream; the context stream runs the
+// density, rho(G), the potential, then (after the join) V(r)psi, fnonloc
+// and the gradient.  The x pass of H|psi> is the density's: the density
+// kernel only reads the transposed ray buffer, and the field transforms have
+// their own, so V(r)psi starts from it as it is.  Same results as the
 // sequential order; used on the pencil path with all pairs in one batch.
 template <typename C> static int seg_a_overlap(amdk_ctx *c) {
   const HostSetup &h = c->hs;
@@ -1350,15 +1351,9 @@ template <typename C> static int seg_a_overlap(amdk_ctx *c) {
     OnSideStream side(c);
     RC(energy_c0_terms(c));
     CK(cudaMemsetAsync(c->d_c2, 0, sizeof(double2) * (size_t)h.ngpw * c->nstate, c->st));
-  }
-  RC(density_pairs_t<C>(c));
-  CK(cudaEventRecord(c->ev_rt_free, c->st));
-  {
-    OnSideStream side(c);
-    CK(cudaStreamWaitEvent(c->st, c->ev_rt_free, 0));
-    xt_bwd_pair<C>(c, 0, T);
     CK(cudaEventRecord(c->ev_side_done, c->st));
   }
+  RC(density_pairs_t<C>(c));
   RC(rhor2g_t<C>(c));
   RC(potential_t<C>(c));
   CK(cudaStreamWaitEvent(c->st, c->ev_side_done, 0));
@@ -1455,7 +1450,6 @@ int amdk_create(const amdk_system *sys, const amdk_options *opt, amdk_ctx **out)
   if (cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess ||
       cublasCreate(&c->cb2) != CUBLAS_STATUS_SUCCESS || cublasSetStream(c->cb2, c->st2) != CUBLAS_STATUS_SUCCESS ||
       cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&c->ev_rt_free, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_side_done, cudaEventDisableTiming) != cudaSuccess) {
     set_error("side stream / cuBLAS handle creation failed");
     amdk_destroy(c);
@@ -1492,7 +1486,7 @@ int amdk_destroy(amdk_ctx *c) {
     cudaStreamSynchronize(c->st2);
     cudaStreamDestroy(c->st2);
   }
-  for (cudaEvent_t e : {c->ev_fork, c->ev_rt_free, c->ev_side_done})
+  for (cudaEvent_t e : {c->ev_fork, c->ev_side_done})
     if (e) cudaEventDestroy(e);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
