@@ -20,6 +20,9 @@
 #include "fft.cuh"
 #include "kernels.cuh"
 #include "pencil.cuh"
+#include "slicegemm.cuh"
+
+#include <cudaTypedefs.h>
 
 namespace amdk {
 
@@ -145,11 +148,27 @@ struct amdk_ctx {
   bool use_graphs = true;
   bool tune = true;  // measure launch shapes at first use (AMDK_NO_TUNE=1: model only)
   bool overlap = true;  // C0-only work on the side stream (AMDK_NO_OVERLAP=1: one stream)
+  bool chol_regs = true;  // register Cholesky up to 128 bands (AMDK_CHOL_SHARED=1: blocked shared-memory kernel)
+  // integer-slice tensor-core GEMMs of the mixed path (<= 128 bands;
+  // AMDK_SLICE=1 turns them on, else DGEMM/DTRMM as the FP64 path)
+  bool slice_gemm = false, sg_ready = false;
+  int8_t *d_plA = nullptr, *d_plB = nullptr, *d_plS = nullptr;  // C0, C2, small-matrix digit planes
+  double *d_sgA = nullptr, *d_sgB = nullptr, *d_sgS = nullptr;  // their row (column) scales
+  double *d_sgpart = nullptr;
+  int *d_sgerr = nullptr;
+  long sg_kpad = 0;
+  int sg_ktiles = 0, sg_per = 0, sg_chunks = 0, sg_mtiles = 0;
+  CUtensorMap tm_a_tn, tm_b_tn, tm_a_nn, tm_s_nn;
   bool warm[2] = {false, false};  // an eager iteration has run at this pair precision
   void *c0_first = nullptr;       // the buffer that held C0 at creation
   void *cb_ws = nullptr;          // cuBLAS workspace (fixed, for capture)
-  double2 *d_hist = nullptr;      // C0 of the previous MD step (predictor)
-  bool have_hist = false;
+  // BOMD predictor: converged C0 of earlier steps, most recent first
+  static constexpr int MAX_PRED = 8;
+  double2 *d_hist[MAX_PRED] = {};
+  int nhist = 0;                                  // steps stored
+  int pred_npts = 2;                              // points per prediction, C0(t) included
+  double pred_coef[MAX_PRED] = {2.0, -1.0};       // weights of C0(t), C0(t-dt), ...
+  bool pred_user = false;                         // coefficients given by the caller
   int *h_info = nullptr;    // pinned: Cholesky status
   int pencil_groups = 1;  // upper bound on the density pair groups
   int ct_vpsi = 0, ct_dens = 0;  // column tiles of the pencil kernels (current precision)
@@ -484,7 +503,7 @@ template <typename C> static void pencil_vpsi(amdk_ctx *c, int T) {
   });
   prof_end(c);
 }
-template <typename C> static void launch_pencil_density(amdk_ctx *c, int p0, int T, int grp) {
+template <typename C> static void launch_pencil_density(amdk_ctx *c, int p0, int T, int grp, int add) {
   const Geom &g = c->geom;
   const size_t sm = pencil_acc_smem<C>(g.n2) + pencil_smem<C>(g.n2, c->pg.nz, c->ct_dens);
   const int per = (T + grp - 1) / grp;
@@ -494,7 +513,8 @@ template <typename C> static void launch_pencil_density(amdk_ctx *c, int p0, int
       smem_opt_in<k_pencil_density<C, N>>();
       ++c->nlaunch;
       k_pencil_density<C, N><<<dim3(g.n1, grp), PNT, sm, c->st>>>(c->pg, plan<C>(c, 1), (const C *)c->d_rb, T, per,
-                                                                  c->d_wa + p0, c->d_wb + p0, c->d_rhopart, c->ct_dens);
+                                                                  c->d_wa + p0, c->d_wb + p0, c->d_rhopart, c->ct_dens,
+                                                                  add);
     }
   });
 }
@@ -522,10 +542,10 @@ template <typename C> static int density_groups(amdk_ctx *c, int T) {
     const int cands[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16};
     for (int grp : cands) {
       if (grp > c->pencil_groups || grp > T || (grp - 1) * ((T + grp - 1) / grp) >= T) continue;  // no empty group
-      launch_pencil_density<C>(c, 0, T, grp);  // warm
+      launch_pencil_density<C>(c, 0, T, grp, 0);  // warm
       cudaEventRecord(e0, c->st);
-      launch_pencil_density<C>(c, 0, T, grp);
-      launch_pencil_density<C>(c, 0, T, grp);
+      launch_pencil_density<C>(c, 0, T, grp, 0);
+      launch_pencil_density<C>(c, 0, T, grp, 0);
       cudaEventRecord(e1, c->st);
       cudaEventSynchronize(e1);
       float ms = 0;
@@ -546,8 +566,9 @@ template <typename C> static void pencil_density(amdk_ctx *c, int p0, int T) {
   const Geom &g = c->geom;
   const int grp = density_groups<C>(c, T);
   const double npt = (double)g.n1 * g.n2 * g.n3;
-  prof_begin(c, KT_ZDENS, (double)T * rstride(c, 0) * sizeof(C) + 2.0 * grp * npt * 8.0);
-  launch_pencil_density<C>(c, p0, T, grp);
+  const int add = p0 > 0;
+  prof_begin(c, KT_ZDENS, (double)T * rstride(c, 0) * sizeof(C) + (1.0 + add) * grp * npt * 8.0);
+  launch_pencil_density<C>(c, p0, T, grp, add);
   prof_end(c);
 }
 
@@ -563,10 +584,15 @@ template <typename C> static int density_pairs_t(amdk_ctx *c) {
   const Geom &g = c->geom;
   if (c->pencil_density) {
     // pencil path: transposed x pass, then one block per (x-plane, pair group)
-    int ng = density_groups<C>(c, c->batch);
-    if (c->npairs % c->batch) ng = std::max(ng, density_groups<C>(c, c->npairs % c->batch));
-    const size_t part = (size_t)ng * g.n1 * g.n2 * g.n3;
-    CK(cudaMemsetAsync(c->d_rhopart, 0, sizeof(double) * part, c->st));
+    // the first batch stores its groups' partial grids, later batches add;
+    // groups that only later batches use are cleared first
+    const int ng_full = density_groups<C>(c, c->batch);
+    const int ng_rem = (c->npairs % c->batch) ? density_groups<C>(c, c->npairs % c->batch) : 0;
+    const int ng = std::max(ng_full, ng_rem);
+    const int ng_first = c->npairs < c->batch ? ng_rem : ng_full;
+    const size_t npt = (size_t)g.n1 * g.n2 * g.n3;
+    if (ng > ng_first)
+      CK(cudaMemsetAsync(c->d_rhopart + (size_t)ng_first * npt, 0, sizeof(double) * (ng - ng_first) * npt, c->st));
     for (int p0 = 0; p0 < c->npairs; p0 += c->batch) {
       int T = std::min(c->batch, c->npairs - p0);
       xt_bwd_pair<C>(c, p0, T);
@@ -786,16 +812,109 @@ static int do_apply_h(amdk_ctx *c) {
 }
 
 // forces (gradient.f90:5-34) and eval_GMAX
+// ------------------------------------------------- integer-slice GEMMs
+// Mixed path with at most 128 bands: Lambda, S, C2 -= C0 Lambda and C0 U^{-1}
+// on the int8 tensor cores (slicegemm.cuh) instead of DGEMM/DTRMM.
+static bool use_slice(const amdk_ctx *c) { return c->sg_ready && c->slice_gemm && c->precision == AMDK_MIXED; }
+// 2D map of S digit planes (kdim bytes per row, S*128 rows): box box_x x 128
+static int sg_encode(CUtensorMap *m, void *base, long kdim, int box_x, CUtensorMapSwizzle sw) {
+  static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+  if (!enc) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+      set_error("cuTensorMapEncodeTiled not available");
+      return AMDK_ERR_CUDA;
+    }
+    enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  }
+  cuuint64_t dims[2] = {(cuuint64_t)kdim, (cuuint64_t)SG_S * SG_M};
+  cuuint64_t strides[1] = {(cuuint64_t)kdim};
+  cuuint32_t box[2] = {(cuuint32_t)box_x, (cuuint32_t)SG_M};
+  cuuint32_t es[2] = {1, 1};
+  if (enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed");
+    return AMDK_ERR_CUDA;
+  }
+  return 0;
+}
+static int sg_setup(amdk_ctx *c) {
+  const HostSetup &h = c->hs;
+  const char *ns = getenv("AMDK_SLICE");
+  c->slice_gemm = ns && ns[0] == '1';
+  if (h.nstate > SG_M) return 0;
+  const long K = 2L * h.ngpw;
+  c->sg_kpad = (K + SG_M - 1) / SG_M * SG_M;
+  c->sg_ktiles = (int)(c->sg_kpad / SG_TN_KT);
+  c->sg_per = (c->sg_ktiles + c->nsm - 1) / c->nsm;
+  c->sg_chunks = (c->sg_ktiles + c->sg_per - 1) / c->sg_per;
+  c->sg_mtiles = (int)(c->sg_kpad / SG_M);
+  const size_t pl = (size_t)SG_S * SG_M * c->sg_kpad;
+  RC(c->alloc(&c->d_plA, pl));
+  RC(c->alloc(&c->d_plB, pl));
+  RC(c->alloc(&c->d_plS, (size_t)SG_S * SG_M * SG_M));
+  RC(c->alloc(&c->d_sgA, SG_M));
+  RC(c->alloc(&c->d_sgB, SG_M));
+  RC(c->alloc(&c->d_sgS, SG_M));
+  RC(c->alloc(&c->d_sgpart, (size_t)c->sg_chunks * SG_M * SG_M));
+  c->d_sgerr = c->d_info + 1;
+  RC(sg_encode(&c->tm_a_tn, c->d_plA, c->sg_kpad, SG_TN_KT, CU_TENSOR_MAP_SWIZZLE_64B));
+  RC(sg_encode(&c->tm_b_tn, c->d_plB, c->sg_kpad, SG_TN_KT, CU_TENSOR_MAP_SWIZZLE_64B));
+  RC(sg_encode(&c->tm_a_nn, c->d_plA, c->sg_kpad, SG_M, CU_TENSOR_MAP_SWIZZLE_128B));
+  RC(sg_encode(&c->tm_s_nn, c->d_plS, SG_M, SG_M, CU_TENSOR_MAP_SWIZZLE_128B));
+  CK(cudaFuncSetAttribute(k_sgemm_tn<SG_S>, cudaFuncAttributeMaxDynamicSharedMemorySize, SgTn<SG_S>::SMEM));
+  CK(cudaFuncSetAttribute(k_sgemm_nn<SG_S>, cudaFuncAttributeMaxDynamicSharedMemorySize, SgNn<SG_S>::SMEM));
+  c->sg_ready = true;
+  return 0;
+}
+// digit planes and row scales of the bands of x (C0 or C2)
+static void sg_slice(amdk_ctx *c, const double2 *x, int8_t *planes, double *scale) {
+  const long K = 2L * c->hs.ngpw;
+  ++c->nlaunch;
+  k_slice_rows<SG_S><<<SG_M, 512, 0, c->st>>>((const double *)x, K, K, c->nstate, planes, c->sg_kpad, scale);
+}
+// out (n x n) = alpha diag(sa) A B^T diag(sb), the product over the real index
+static void sg_tn(amdk_ctx *c, const CUtensorMap &ta, const CUtensorMap &tb, int same, const double *sa,
+                  const double *sb, double alpha, double *out) {
+  const int n = c->nstate;
+  c->nlaunch += 2;
+  k_sgemm_tn<SG_S><<<c->sg_chunks, 128, SgTn<SG_S>::SMEM, c->st>>>(ta, tb, same, c->sg_ktiles, c->sg_per, c->d_sgpart,
+                                                                     c->d_sgerr);
+  k_sgemm_reduce<<<n, SG_M, 0, c->st>>>(c->sg_chunks, c->d_sgpart, n, sa, sb, alpha, out, n);
+}
+// out (the real view, 2 ngpw x n) = (or -=, sub) C0 B for B n x n, with C0's
+// planes and scales in d_plA / d_sgA
+static void sg_nn(amdk_ctx *c, const double *B, double2 *out, int sub) {
+  const int n = c->nstate;
+  const long K = 2L * c->hs.ngpw;
+  c->nlaunch += 2;
+  k_slice_small<SG_S><<<SG_M, SG_M, 0, c->st>>>(B, n, n, n, c->d_sgA, c->d_plS, c->d_sgS);
+  k_sgemm_nn<SG_S><<<std::min(c->sg_mtiles, c->nsm), 192, SgNn<SG_S>::SMEM, c->st>>>(
+      c->tm_a_nn, c->tm_s_nn, c->sg_mtiles, K, (double *)out, K, n, c->d_sgS, sub, c->d_sgerr);
+}
+
 static int do_gradient(amdk_ctx *c) {
   const HostSetup &h = c->hs;
   int n = c->nstate, K = 2 * h.ngpw;
   const double two = 2.0, one = 1.0, mone = -1.0, zero = 0.0;
-  CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, (const double *)c->d_c2, K, (const double *)c->d_c0, K,
-                 &zero, c->d_gam, n));
+  const bool sl = use_slice(c);
+  if (sl) {
+    sg_slice(c, c->d_c2, c->d_plB, c->d_sgB);
+    sg_slice(c, c->d_c0, c->d_plA, c->d_sgA);
+    sg_tn(c, c->tm_b_tn, c->tm_a_tn, 0, c->d_sgB, c->d_sgA, 2.0, c->d_gam);
+  } else {
+    CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, (const double *)c->d_c2, K,
+                   (const double *)c->d_c0, K, &zero, c->d_gam, n));
+  }
   ++c->nlaunch;
   k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c2, c->d_c0, c->d_gam, c->d_occ, 1, 0);
-  CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &mone, (const double *)c->d_c0, K, c->d_gam, n, &one,
-                 (double *)c->d_c2, K));
+  if (sl)
+    sg_nn(c, c->d_gam, c->d_c2, 1);
+  else
+    CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &mone, (const double *)c->d_c0, K, c->d_gam, n, &one,
+                   (double *)c->d_c2, K));
   ++c->nlaunch;
   k_zclean<<<nblk(n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c2);
   int nocc = 0;
@@ -839,6 +958,10 @@ static int check_ortho(amdk_ctx *c) {
     set_error("overlap matrix not positive definite at leading minor " + std::to_string(info));
     return AMDK_ERR_NOT_SPD;
   }
+  if (c->h_info[1]) {
+    set_error("tensor-core slice GEMM: a pipeline wait expired (code " + std::to_string(c->h_info[1]) + ")");
+    return AMDK_ERR_TIMEOUT;
+  }
   return 0;
 }
 static int do_ortho(amdk_ctx *c, bool check = true, bool swap = true) {
@@ -846,14 +969,26 @@ static int do_ortho(amdk_ctx *c, bool check = true, bool swap = true) {
   int n = c->nstate, K = 2 * h.ngpw;
   const double two = 2.0, zero = 0.0, one = 1.0;
   // S = 2 Re C0^T C0 - Re c0(0) Re c0(0)^T  (DSYRK + DGER, wfn_initialize.f90:481-482)
-  CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, (const double *)c->d_c0, K, (const double *)c->d_c0, K,
-                 &zero, c->d_gam, n));
+  const bool sl = use_slice(c);
+  if (sl) {
+    sg_slice(c, c->d_c0, c->d_plA, c->d_sgA);
+    sg_tn(c, c->tm_a_tn, c->tm_a_tn, 1, c->d_sgA, c->d_sgA, 2.0, c->d_gam);
+  } else {
+    CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, (const double *)c->d_c0, K,
+                   (const double *)c->d_c0, K, &zero, c->d_gam, n));
+  }
   ++c->nlaunch;
   k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c0, c->d_c0, c->d_gam, c->d_occ, 0, 1);
   const int np = (n + CHOL_B - 1) / CHOL_B * CHOL_B;
   const size_t sm = ((size_t)np * (np + 1) + (size_t)CHOL_B * np) * sizeof(double);
   ++c->nlaunch;
-  if (n <= CHOL_NMAX) {
+  if (n <= 32 && c->chol_regs) {
+    k_chol_inv_r<32><<<1, CHR_NT, sizeof(double) * 32 * ChR<32>::LD, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
+  } else if (n <= 64 && c->chol_regs) {
+    k_chol_inv_r<64><<<1, CHR_NT, sizeof(double) * 64 * ChR<64>::LD, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
+  } else if (n <= 128 && c->chol_regs) {
+    k_chol_inv_r<128><<<1, CHR_NT, sizeof(double) * 128 * ChR<128>::LD, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
+  } else if (n <= CHOL_NMAX) {
     k_chol_inv_s<<<1, CHOL_NT, sm, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
   } else {
     // DPOTRF + DTRTRI as the reference (wfn_initialize.f90:513,524), in place
@@ -867,15 +1002,18 @@ static int do_ortho(amdk_ctx *c, bool check = true, bool swap = true) {
       return AMDK_ERR_CUDA;
     }
   }
-  CK(cudaMemcpyAsync(c->h_info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(c->h_info, c->d_info, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
   if (check) {
     CK(cudaStreamSynchronize(c->st));
     RC(check_ortho(c));
   }
   // C0 <- C0 U^{-1} (DTRMM, wfn_initialize.f90:485) out of place into the
   // spare buffer (ZCLEAN there), then the buffers swap roles
-  CB(cublasDtrmm(c->cb, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, K, n, &one,
-                 c->d_uinv, n, (const double *)c->d_c0, K, (double *)c->d_cp, K));
+  if (sl)
+    sg_nn(c, c->d_uinv, c->d_cp, 0);
+  else
+    CB(cublasDtrmm(c->cb, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, K, n, &one,
+                   c->d_uinv, n, (const double *)c->d_c0, K, (double *)c->d_cp, K));
   ++c->nlaunch;
   k_zclean<<<nblk(n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_cp);
   if (swap) std::swap(c->d_c0, c->d_cp);
@@ -1041,6 +1179,8 @@ static int build_device(amdk_ctx *c) {
     CK(cudaMemcpyToSymbol(c_twf, twf.data(), sizeof(float2) * CTW_LEN));
   }
   CK(cudaFuncSetAttribute(k_chol_inv_s, cudaFuncAttributeMaxDynamicSharedMemorySize, 216 * 1024));
+  CK(cudaFuncSetAttribute(k_chol_inv_r<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)(sizeof(double) * 128 * ChR<128>::LD)));
   // G vectors
   RC(c->up(&c->d_inyh, h.inyh));
   RC(c->up(&c->d_hg, h.hg));
@@ -1075,6 +1215,8 @@ static int build_device(amdk_ctx *c) {
     c->tune = !(nt && nt[0] == '1');
     const char *no = getenv("AMDK_NO_OVERLAP");
     c->overlap = !(no && no[0] == '1');
+    const char *cs = getenv("AMDK_CHOL_SHARED");
+    c->chol_regs = !(cs && cs[0] == '1');
   }
   if (h.nstate > CHOL_NMAX) {
     // large overlaps: cuSOLVER (its DTRTRI keeps a host workspace, so the
@@ -1122,12 +1264,13 @@ static int build_device(amdk_ctx *c) {
   RC(c->alloc(&c->d_fm, 2L * h.ngrho));
   RC(c->alloc(&c->d_gam, (size_t)h.nstate * h.nstate));
   RC(c->alloc(&c->d_uinv, (size_t)h.nstate * h.nstate));
-  RC(c->alloc(&c->d_info, 1));
+  RC(c->alloc(&c->d_info, 2));  // [0] Cholesky status, [1] slice-GEMM wait status
+  CK(cudaMemset(c->d_info, 0, 2 * sizeof(int)));
   RC(c->alloc(&c->d_part, (size_t)RED_BLOCKS * 4 + 3L * 64 * h.nat + 64));
   RC(c->alloc(&c->d_scal, S_NSCAL));
   CK(cudaMallocHost(&c->h_pin, sizeof(double) * (S_NSCAL + 8)));
   CK(cudaMallocHost(&c->h_info, sizeof(int) * 4));
-  c->h_info[0] = 0;
+  c->h_info[0] = c->h_info[1] = 0;
   CK(cudaMemset(c->d_scal, 0, S_NSCAL * sizeof(double)));
   // Pencil path for the pair transforms (cubic grids with a specialised
   // length whose slab plane fits in shared memory): V(r)psi and the density
@@ -1166,6 +1309,7 @@ static int build_device(amdk_ctx *c) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
   }
+  RC(sg_setup(c));
   const int q0 = (c->precision == AMDK_MIXED) ? 1 : 0;
   const bool pencil_all = c->pv_p[q0] && c->pd_p[q0];
   // pair batch: all pairs at once on the pencil path, else 8
@@ -1688,36 +1832,66 @@ int amdk_ionic_forces(amdk_ctx *c, double *force) {
   return 0;
 }
 
+int amdk_wfn_set_predictor(amdk_ctx *c, int npoints, const double *coef) {
+  if (!c || npoints < 1 || npoints > amdk_ctx::MAX_PRED) return AMDK_ERR_BADARG;
+  c->pred_npts = npoints;
+  c->pred_user = coef != nullptr;
+  if (coef)
+    for (int j = 0; j < npoints; ++j) c->pred_coef[j] = coef[j];
+  else
+    amdk::aspc_coefficients(npoints, c->pred_coef);
+  if (c->nhist > npoints - 1) c->nhist = npoints - 1;
+  return 0;
+}
+
 int amdk_wfn_extrapolate(amdk_ctx *c) {
   if (!c) return AMDK_ERR_BADARG;
   cudaSetDevice(c->device);
   const HostSetup &h = c->hs;
   const size_t cw = (size_t)h.ngpw * c->nstate;
-  if (!c->d_hist) RC(c->alloc(&c->d_hist, cw));
-  if (c->have_hist) {
+  const int keep = c->pred_npts - 1;  // earlier steps the predictor uses
+  // points of this prediction: all configured ones once enough steps are
+  // stored, else the always-stable weights of the points there are
+  const int np = std::min(c->pred_npts, c->nhist + 1);
+  double w[amdk_ctx::MAX_PRED];
+  if (np == c->pred_npts)
+    for (int j = 0; j < np; ++j) w[j] = c->pred_coef[j];
+  else
+    amdk::aspc_coefficients(np, w);
+  if (np > 1) {
     const int n = c->nstate, K = 2 * h.ngpw;
     const double two = 2.0, one = 1.0, zero = 0.0;
-    // M = 2 Re C_prev^T C0 - Re c_prev(0) Re c0(0)^T, then cp = C_prev M
-    CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, (const double *)c->d_hist, K,
-                   (const double *)c->d_c0, K, &zero, c->d_gam, n));
+    for (int j = 1; j < np; ++j) {
+      const double2 *hj = c->d_hist[j - 1];
+      // M = 2 Re C_j^T C0 - Re c_j(0) Re c0(0)^T aligns step j's occupied
+      // subspace with the current one; cp (+)= w_j C_j M
+      CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, (const double *)hj, K, (const double *)c->d_c0, K,
+                     &zero, c->d_gam, n));
+      ++c->nlaunch;
+      k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, hj, c->d_c0, c->d_gam, c->d_occ, 0, 0);
+      CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &w[j], (const double *)hj, K, c->d_gam, n,
+                     j == 1 ? &zero : &one, (double *)c->d_cp, K));
+    }
     ++c->nlaunch;
-    k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_hist, c->d_c0, c->d_gam, c->d_occ, 0, 0);
-    CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, (const double *)c->d_hist, K, c->d_gam, n, &zero,
-                   (double *)c->d_cp, K));
-    ++c->nlaunch;
-    k_two_a_minus<<<RED_BLOCKS * 4, NTHR, 0, c->st>>>((long)cw, c->d_c0, c->d_cp);
-    CK(cudaMemcpyAsync(c->d_hist, c->d_c0, sizeof(double2) * cw, cudaMemcpyDeviceToDevice, c->st));
-    std::swap(c->d_c0, c->d_cp);
-  } else {
-    CK(cudaMemcpyAsync(c->d_hist, c->d_c0, sizeof(double2) * cw, cudaMemcpyDeviceToDevice, c->st));
-    c->have_hist = true;
+    k_axpy_c<<<RED_BLOCKS * 4, NTHR, 0, c->st>>>((long)cw, w[0], c->d_c0, c->d_cp);
   }
+  if (keep > 0) {
+    // store C0(t) as the most recent step: it takes the oldest slot
+    const int slots = std::min(c->nhist + 1, keep);
+    if (!c->d_hist[slots - 1]) RC(c->alloc(&c->d_hist[slots - 1], cw));
+    double2 *t = c->d_hist[slots - 1];
+    for (int j = slots - 1; j > 0; --j) c->d_hist[j] = c->d_hist[j - 1];
+    c->d_hist[0] = t;
+    CK(cudaMemcpyAsync(t, c->d_c0, sizeof(double2) * cw, cudaMemcpyDeviceToDevice, c->st));
+    c->nhist = slots;
+  }
+  if (np > 1) std::swap(c->d_c0, c->d_cp);
   CK(cudaStreamSynchronize(c->st));
   return 0;
 }
 int amdk_wfn_history_clear(amdk_ctx *c) {
   if (!c) return AMDK_ERR_BADARG;
-  c->have_hist = false;
+  c->nhist = 0;
   return 0;
 }
 

@@ -239,13 +239,14 @@ __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C
 // Density: one x-plane for a group of band pairs (density.f90:49-86);
 // rho_part[grp][kx][q][k'] += wa_t Re^2 + wb_t Im^2 in the permuted (ky, kz)
 // order of the vpsi kernel.  grid (n1, ngroups).  The group sum is kept in
-// shared memory in the data's precision (FP32 for float2), then added to the
-// FP64 partial grid.
+// shared memory in the data's precision (FP32 for float2), then stored to
+// (add = 0: the first batch of pairs) or added to (add = 1) the FP64 partial
+// grid.
 template <typename C, int N>
 __global__ void __launch_bounds__(PNT) k_pencil_density(PencilGeom pg, Plan<C> p, const C *__restrict__ rt, int T,
                                                         int per_group, const double *__restrict__ wa,
                                                         const double *__restrict__ wb, double *__restrict__ rho_part,
-                                                        int CTs) {
+                                                        int CTs, int add) {
   typedef decltype(C().x) Rl;
   constexpr int N1 = fft_n1(N), N2 = N / N1, NP = N + 1;
   extern __shared__ unsigned char smraw[];
@@ -290,7 +291,8 @@ __global__ void __launch_bounds__(PNT) k_pencil_density(PencilGeom pg, Plan<C> p
   double *out = rho_part + ((long)grp * pg.n1 + kx) * N * N;
   for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
     const int q = idx / N, k = idx % N;
-    out[idx] += (double)acc[q * NP + k];
+    const double v = (double)acc[q * NP + k];
+    out[idx] = add ? out[idx] + v : v;
   }
 }
 

@@ -1,0 +1,507 @@
+// Integer-slice GEMMs on the tcgen05 tensor cores (sm_100a) for the Gram and
+// rotation products of the mixed-precision path: the overlap S = C0^T C0 and
+// Lambda = C2^T C0 (OVLAP_D, wfn_initialize.f90:234-263; ortho_gs :481), and
+// the rotations C2 -= C0 Lambda (gradient.f90:31) and C0 U^{-1} (ortho_gs
+// DTRMM, wfn_initialize.f90:485).
+//
+// Method (the split-integer scheme of Ozaki et al., Numer. Algorithms 59, 95
+// (2012), with Ootomo-Ozaki-Yokota's int8 tensor-core variant, IJHPCA 2024):
+// every row r of an operand (a band) is scaled by a power of two sigma_r so
+// that |x| / sigma_r < 1/2, then cut into S signed 7-bit digits,
+//   x / sigma_r = sum_t d_t 2^{-7(t+1)} + O(2^{-7S}),  d_t in [-64, 64],
+// by repeated round-to-nearest (exact in FP64).  A product of two rows is
+//   sum_k x_k y_k = sigma_x sigma_y sum_{t,u} 2^{-7(t+u+2)} sum_k dx_t dy_u,
+// whose inner sums are exact int8 x int8 -> int32 tensor-core products; the
+// terms with t + u >= S are dropped (relative truncation ~2^{-7S}), and the
+// pairs with equal t + u share one int32 accumulator in tensor memory (S
+// accumulators of 128 x 128 = all 512 TMEM columns).  With S = 4 the products
+// carry 28 bits (FP32 has 24) and the accumulation is exact.
+//
+// Planes: int8 [S][128 rows][kpad], row r = band r (zero rows above the band
+// count), kpad = the real length 2*ngpw rounded up to 128 with zeros.  TMA
+// loads 64-byte (TN) or 128-byte (NN) swizzled tiles straight into the
+// canonical UMMA shared-memory layouts.
+//
+// TN (C = A B^T over the long real index, A and B K-major): one CTA per
+// chunk of 64-wide k tiles, 3-stage TMA -> MMA pipeline on mbarriers, one
+// thread issues the MMAs, four warps read the accumulators back and write an
+// FP64 partial; k_sgemm_reduce sums the partials and applies the scales.
+// NN (C[m][n] = sum_k A[m][k] B[k][n], A = the band planes read MN-major,
+// B a 128 x 128 matrix sliced per column after scaling its rows by the A
+// bands' sigma): persistent CTAs over 128-row tiles of the long index, the
+// epilogue writes (or subtracts from) FP64 output.
+//
+// Every wait is bounded (SG_SPIN polls): on expiry the kernel records a code
+// in *err, writes NaN where its result would go, waits (bounded) for its own
+// copies in flight, frees its tensor memory and returns.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace amdk {
+
+constexpr int SG_S = 4;          // digit planes per operand
+constexpr int SG_M = 128;        // rows per plane (bands, padded)
+constexpr int SG_TN_KT = 64;     // k bytes per TN stage (64-byte swizzle)
+constexpr int SG_TN_ST = 3;      // TN pipeline stages
+constexpr int SG_NN_ST = 2;      // NN pipeline stages
+constexpr int SG_TMEM_COLS = 512;
+constexpr long SG_SPIN = 1L << 22;
+
+// ------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t sg_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void sg_bar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void sg_bar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void sg_bar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void sg_bar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool sg_bar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for the phase of the given parity; false (and *err = code) on expiry
+__device__ __forceinline__ bool sg_bar_wait(uint32_t bar, uint32_t parity, int *err, int code) {
+  for (long it = 0; it < SG_SPIN; ++it) {
+    if (sg_bar_try(bar, parity)) return true;
+    if (it > 32) __nanosleep(64);
+  }
+  atomicExch(err, code);
+  return false;
+}
+__device__ __forceinline__ void sg_tma_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void sg_tmem_alloc(uint32_t slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(ncols) : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void sg_tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void sg_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void sg_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// D[tmem] (+)= A[smem] B[smem]^T, 128 x 128 x 32 int8 -> int32
+__device__ __forceinline__ void sg_mma_i8(uint32_t dtm, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtm),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+      : "memory");
+}
+// arrive on the mbarrier once every MMA issued so far by this thread is done
+__device__ __forceinline__ void sg_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+// 32 consecutive 32-bit columns of this thread's TMEM lane
+__device__ __forceinline__ void sg_tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Shared-memory matrix descriptor (tcgen05): start address, leading and
+// stride byte offsets (16-byte units), version 1, layout (2 = 128-byte
+// swizzle, 4 = 64-byte swizzle).
+__device__ __forceinline__ uint64_t sg_desc(uint32_t addr, uint32_t lbo, uint32_t sbo, uint32_t layout) {
+  return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) | ((uint64_t)layout << 61);
+}
+// Instruction descriptor, kind::i8: D s32 (bits 4-5 = 2), A and B signed
+// (bits 7-9, 10-12 = 1), A MN-major (bit 15) when a_mn, B K-major, N = 128
+// (bits 17-22 = N/8), M = 128 (bits 24-28 = M/16).
+__host__ __device__ constexpr uint32_t sg_idesc(bool a_mn) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+}
+__device__ __forceinline__ double sg_weight(int d) { return ldexp(1.0, -7 * (d + 2)); }
+
+// ---------------------------------------------------------------- slicing
+// Row r (a band: len reals at x + r*ldx) -> sigma_r and S digit planes.
+// grid SG_M (rows >= nrows are zero), block 512.
+template <int S>
+__global__ void __launch_bounds__(512) k_slice_rows(const double *__restrict__ x, long ldx, long len, int nrows,
+                                                    int8_t *__restrict__ planes, long kpad, double *__restrict__ scale) {
+  const int r = blockIdx.x, tid = threadIdx.x;
+  const long pstride = (long)SG_M * kpad;
+  int8_t *dst = planes + (long)r * kpad;
+  if (r >= nrows) {
+    for (long k = 8L * tid; k < kpad; k += 8L * blockDim.x)
+#pragma unroll
+      for (int t = 0; t < S; ++t) *reinterpret_cast<uint2 *>(dst + t * pstride + k) = make_uint2(0u, 0u);
+    if (tid == 0) scale[r] = 1.0;
+    return;
+  }
+  const double *xr = x + (long)r * ldx;
+  double m = 0.0;
+  for (long k = 2L * tid; k < len; k += 2L * blockDim.x) {
+    const double2 v = *reinterpret_cast<const double2 *>(xr + k);
+    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+  }
+  __shared__ double red[16];
+  __shared__ int s_e;
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((tid & 31) == 0) red[tid >> 5] = m;
+  __syncthreads();
+  if (tid < 32) {
+    double w = tid < (int)(blockDim.x >> 5) ? red[tid] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) w = fmax(w, __shfl_xor_sync(0xffffffffu, w, o));
+    if (tid == 0) {
+      int E = 0;
+      if (w > 0.0) frexp(w, &E);  // w = f 2^E, f in [1/2, 1): w / 2^(E+1) < 1/2
+      s_e = w > 0.0 ? E + 1 : 0;
+      scale[r] = ldexp(1.0, s_e);
+    }
+  }
+  __syncthreads();
+  const int e = s_e;
+  for (long k = 8L * tid; k < kpad; k += 8L * blockDim.x) {
+    double v[8];
+#pragma unroll
+    for (int i = 0; i < 8; i += 2) {
+      if (k + i < len) {
+        const double2 w = *reinterpret_cast<const double2 *>(xr + k + i);
+        v[i] = w.x;
+        v[i + 1] = w.y;
+      } else {
+        v[i] = v[i + 1] = 0.0;
+      }
+    }
+    uint32_t lo[S], hi[S];
+#pragma unroll
+    for (int t = 0; t < S; ++t) lo[t] = hi[t] = 0u;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      double y = ldexp(v[i], -e);
+#pragma unroll
+      for (int t = 0; t < S; ++t) {
+        y *= 128.0;
+        const double d = rint(y);
+        y -= d;
+        const uint32_t b = (uint32_t)(uint8_t)(int8_t)(int)d;
+        if (i < 4) lo[t] |= b << (8 * i);
+        else hi[t] |= b << (8 * (i - 4));
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < S; ++t) *reinterpret_cast<uint2 *>(dst + t * pstride + k) = make_uint2(lo[t], hi[t]);
+  }
+}
+
+// A small matrix B (nk x nn, column-major, ldb) for the NN product: column n
+// of diag(rowscale) B -> tau_n and S digit planes [t][n][k] (K-major rows n).
+// grid SG_M, block SG_M.
+template <int S>
+__global__ void __launch_bounds__(SG_M) k_slice_small(const double *__restrict__ B, int ldb, int nk, int nn,
+                                                      const double *__restrict__ rowscale, int8_t *__restrict__ planes,
+                                                      double *__restrict__ colscale) {
+  const int n = blockIdx.x, k = threadIdx.x;
+  const double v = (n < nn && k < nk) ? B[k + (long)ldb * n] * rowscale[k] : 0.0;
+  double m = fabs(v);
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double red[SG_M / 32];
+  if ((k & 31) == 0) red[k >> 5] = m;
+  __syncthreads();
+  double w = 0.0;
+#pragma unroll
+  for (int i = 0; i < SG_M / 32; ++i) w = fmax(w, red[i]);
+  int E = 0;
+  if (w > 0.0) frexp(w, &E);
+  const int e = w > 0.0 ? E + 1 : 0;
+  if (k == 0) colscale[n] = ldexp(1.0, e);
+  double y = ldexp(v, -e);
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    y *= 128.0;
+    const double d = rint(y);
+    y -= d;
+    planes[(long)t * SG_M * SG_M + n * SG_M + k] = (int8_t)(int)d;
+  }
+}
+
+// ------------------------------------------------------------------ TN GEMM
+template <int S> struct SgTn {
+  static constexpr int PLANE = SG_M * SG_TN_KT;  // 8 KB: 128 rows x 64 bytes
+  static constexpr int STAGE = 2 * S * PLANE;
+  static constexpr int SMEM = SG_TN_ST * STAGE + 1024 + 256;
+};
+// partial[chunk][n][m] = sum over the chunk's k of
+//   sum_{t+u<S} 2^{-7(t+u+2)} dA_t[m][k] dB_u[n][k]
+// (same != 0: B = A, loaded once).  grid = chunks, block 128.
+template <int S>
+__global__ void __launch_bounds__(128, 1) k_sgemm_tn(const __grid_constant__ CUtensorMap ta,
+                                                     const __grid_constant__ CUtensorMap tb, int same, int ktiles,
+                                                     int per_cta, double *__restrict__ partial, int *err) {
+  using G = SgTn<S>;
+  extern __shared__ unsigned char sg_raw[];
+  unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sg_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t *bars = reinterpret_cast<uint64_t *>(base + SG_TN_ST * G::STAGE);  // full[ST], empty[ST], done
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * SG_TN_ST + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int kt0 = blockIdx.x * per_cta;
+  const int nt = max(0, min(per_cta, ktiles - kt0));
+  const uint32_t full0 = sg_smem(bars), empty0 = sg_smem(bars + SG_TN_ST), done = sg_smem(bars + 2 * SG_TN_ST);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < SG_TN_ST; ++i) {
+      sg_bar_init(full0 + 8 * i, 1);
+      sg_bar_init(empty0 + 8 * i, 1);
+    }
+    sg_bar_init(done, 1);
+    sg_bar_fence_init();
+  }
+  if (warp == 0) sg_tmem_alloc(sg_smem(tslot), SG_TMEM_COLS);
+  sg_fence_before();
+  __syncthreads();
+  sg_fence_after();
+  const uint32_t tbase = *tslot;
+  const uint32_t bytes = (same ? 1u : 2u) * S * G::PLANE;
+  if (threadIdx.x == 0 && nt > 0) {
+    // producer: TMA of the S planes of A (and B) for each k tile
+    int issued = 0;
+    for (int i = 0; i < nt; ++i) {
+      const int s = i % SG_TN_ST;
+      if (i >= SG_TN_ST && !sg_bar_wait(empty0 + 8 * s, ((i / SG_TN_ST) - 1) & 1, err, 1)) break;
+      const uint32_t fb = full0 + 8 * s;
+      sg_bar_expect_tx(fb, bytes);
+      const uint32_t dA = sg_smem(base + s * G::STAGE), dB = dA + S * G::PLANE;
+      const int kx = (kt0 + i) * SG_TN_KT;
+#pragma unroll
+      for (int t = 0; t < S; ++t) sg_tma_2d(dA + t * G::PLANE, &ta, kx, t * SG_M, fb);
+      if (!same)
+#pragma unroll
+        for (int t = 0; t < S; ++t) sg_tma_2d(dB + t * G::PLANE, &tb, kx, t * SG_M, fb);
+      issued = i + 1;
+    }
+    // the copies in flight land before the block can leave
+    for (int i = max(0, issued - SG_TN_ST); i < issued; ++i) sg_bar_wait(full0 + 8 * (i % SG_TN_ST), (i / SG_TN_ST) & 1, err, 4);
+  } else if (threadIdx.x == 32 && nt > 0) {
+    // MMA issuer
+    constexpr uint32_t idesc = sg_idesc(false);
+    for (int i = 0; i < nt; ++i) {
+      const int s = i % SG_TN_ST;
+      if (!sg_bar_wait(full0 + 8 * s, (i / SG_TN_ST) & 1, err, 2)) break;
+      sg_fence_after();
+      const uint32_t aA = sg_smem(base + s * G::STAGE), aB = same ? aA : aA + S * G::PLANE;
+#pragma unroll
+      for (int t = 0; t < S; ++t)
+#pragma unroll
+        for (int u = 0; u < S - t; ++u)
+#pragma unroll
+          for (int kk = 0; kk < SG_TN_KT / 32; ++kk) {
+            const uint64_t ad = sg_desc(aA + t * G::PLANE + 32 * kk, 16, 512, 4);
+            const uint64_t bd = sg_desc(aB + u * G::PLANE + 32 * kk, 16, 512, 4);
+            sg_mma_i8(tbase + (uint32_t)((t + u) * SG_M), ad, bd, idesc, (i > 0 || t > 0 || kk > 0) ? 1u : 0u);
+          }
+      sg_commit(empty0 + 8 * s);
+    }
+    sg_commit(done);
+    sg_bar_wait(done, 0, err, 5);  // every MMA of this block has finished
+  }
+  __syncwarp();
+  // epilogue: lane m of warp w holds row m = 32 w + lane of every accumulator
+  const bool ok = __all_sync(0xffffffffu, nt > 0 && sg_bar_wait(done, 0, err, 3));
+  sg_fence_after();
+  const int m = 32 * warp + lane;
+  double *out = partial + (long)blockIdx.x * SG_M * SG_M;
+  for (int cb = 0; cb < SG_M / 32; ++cb) {
+    double v[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = 0.0;
+    if (ok) {
+#pragma unroll 1
+      for (int d = 0; d < S; ++d) {
+        uint32_t r[32];
+        sg_tmem_ld32(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * SG_M + 32 * cb), r);
+        const double w = sg_weight(d);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] += (double)(int)r[j] * w;
+      }
+    } else if (nt > 0) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = __longlong_as_double(0x7ff8000000000000LL);
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j) out[(cb * 32 + j) * SG_M + m] = v[j];
+  }
+  sg_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    sg_fence_after();
+    sg_tmem_dealloc(tbase, SG_TMEM_COLS);
+  }
+}
+
+// out[m + ldo n] = alpha sa[m] sb[n] sum_c partial[c][n][m], m < nm, n < nn.
+// grid nn, block SG_M.
+__global__ void k_sgemm_reduce(int nchunk, const double *__restrict__ partial, int nm, const double *__restrict__ sa,
+                               const double *__restrict__ sb, double alpha, double *__restrict__ out, int ldo) {
+  const int m = threadIdx.x, n = blockIdx.x;
+  if (m >= nm) return;
+  double s = 0.0;
+  for (int c = 0; c < nchunk; ++c) s += partial[(long)c * SG_M * SG_M + n * SG_M + m];
+  out[m + (long)ldo * n] = alpha * sa[m] * sb[n] * s;
+}
+
+// ------------------------------------------------------------------ NN GEMM
+template <int S> struct SgNn {
+  static constexpr int PLANE = SG_M * SG_M;  // 16 KB: 128 x 128 bytes
+  static constexpr int SMEM = S * PLANE + SG_NN_ST * S * PLANE + 1024 + 256;
+};
+// out[m + ldo n] (=, or -= when sub) colscale[n] sum_{t+u<S} 2^{-7(t+u+2)}
+//   sum_k dA_t[k][m] dB_u[n][k]   for m < mreal, n < nn,
+// A planes [t][k][m] (MN-major tiles of 128 m x 128 k), B planes [t][n][k].
+// Persistent: CTA b takes the 128-row tiles b, b + grid, ...  block 192:
+// warp 0 loads, warp 1 issues the MMAs (and owns the tensor memory), warps
+// 2-5 read the accumulators back (TMEM lanes 32 (w % 4) ...).
+template <int S>
+__global__ void __launch_bounds__(192, 1) k_sgemm_nn(const __grid_constant__ CUtensorMap ta,
+                                                     const __grid_constant__ CUtensorMap tb, int mtiles, long mreal,
+                                                     double *__restrict__ out, long ldo, int nn,
+                                                     const double *__restrict__ colscale, int sub, int *err) {
+  using G = SgNn<S>;
+  extern __shared__ unsigned char sg_raw[];
+  unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sg_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char *sB = base;
+  unsigned char *sA = base + S * G::PLANE;
+  // bfull, full[ST], empty[ST], tfull, tfree, fin
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sA + SG_NN_ST * S * G::PLANE);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 4 + 2 * SG_NN_ST);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t bfull = sg_smem(bars), full0 = sg_smem(bars + 1), empty0 = sg_smem(bars + 1 + SG_NN_ST);
+  const uint32_t tfull = sg_smem(bars + 1 + 2 * SG_NN_ST), tfree = sg_smem(bars + 2 + 2 * SG_NN_ST);
+  const uint32_t fin = sg_smem(bars + 3 + 2 * SG_NN_ST);
+  const int nq = blockIdx.x < mtiles ? (mtiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  if (threadIdx.x == 0) {
+    sg_bar_init(bfull, 1);
+    for (int i = 0; i < SG_NN_ST; ++i) {
+      sg_bar_init(full0 + 8 * i, 1);
+      sg_bar_init(empty0 + 8 * i, 1);
+    }
+    sg_bar_init(tfull, 1);
+    sg_bar_init(tfree, 4);
+    sg_bar_init(fin, 1);
+    sg_bar_fence_init();
+  }
+  if (warp == 1) sg_tmem_alloc(sg_smem(tslot), SG_TMEM_COLS);
+  sg_fence_before();
+  __syncthreads();
+  sg_fence_after();
+  const uint32_t tbase = *tslot;
+  if (threadIdx.x == 0 && nq > 0) {
+    sg_bar_expect_tx(bfull, S * G::PLANE);
+#pragma unroll
+    for (int t = 0; t < S; ++t) sg_tma_2d(sg_smem(sB + t * G::PLANE), &tb, 0, t * SG_M, bfull);
+    int issued = 0;
+    for (int q = 0; q < nq; ++q) {
+      const int s = q % SG_NN_ST;
+      if (q >= SG_NN_ST && !sg_bar_wait(empty0 + 8 * s, ((q / SG_NN_ST) - 1) & 1, err, 11)) break;
+      const uint32_t fb = full0 + 8 * s;
+      sg_bar_expect_tx(fb, S * G::PLANE);
+      const int m0 = (blockIdx.x + q * gridDim.x) * SG_M;
+#pragma unroll
+      for (int t = 0; t < S; ++t) sg_tma_2d(sg_smem(sA + (s * S + t) * G::PLANE), &ta, m0, t * SG_M, fb);
+      issued = q + 1;
+    }
+    sg_bar_wait(bfull, 0, err, 14);
+    for (int q = max(0, issued - SG_NN_ST); q < issued; ++q)
+      sg_bar_wait(full0 + 8 * (q % SG_NN_ST), (q / SG_NN_ST) & 1, err, 14);
+  } else if (threadIdx.x == 32 && nq > 0) {
+    constexpr uint32_t idesc = sg_idesc(true);
+    bool ok = sg_bar_wait(bfull, 0, err, 12);
+    for (int q = 0; q < nq && ok; ++q) {
+      const int s = q % SG_NN_ST;
+      if (!sg_bar_wait(full0 + 8 * s, (q / SG_NN_ST) & 1, err, 12)) break;
+      if (q > 0 && !sg_bar_wait(tfree, (q - 1) & 1, err, 13)) break;
+      sg_fence_after();
+      const uint32_t aA = sg_smem(sA + s * S * G::PLANE), aB = sg_smem(sB);
+#pragma unroll
+      for (int t = 0; t < S; ++t)
+#pragma unroll
+        for (int u = 0; u < S - t; ++u)
+#pragma unroll
+          for (int kk = 0; kk < SG_M / 32; ++kk) {
+            // A: 32 k rows of 128 bytes per MMA (four 8-row swizzle atoms)
+            const uint64_t ad = sg_desc(aA + t * G::PLANE + 4096 * kk, G::PLANE, 1024, 2);
+            const uint64_t bd = sg_desc(aB + u * G::PLANE + 32 * kk, 16, 1024, 2);
+            sg_mma_i8(tbase + (uint32_t)((t + u) * SG_M), ad, bd, idesc, (t > 0 || kk > 0) ? 1u : 0u);
+          }
+      sg_commit(empty0 + 8 * s);
+      sg_commit(tfull);
+    }
+    sg_commit(fin);
+    sg_bar_wait(fin, 0, err, 16);  // every MMA of this block has finished
+  } else if (warp >= 2) {
+    const int ew = warp & 3;
+    const int m = 32 * ew + lane;
+    for (int q = 0; q < nq; ++q) {
+      const bool ok = __all_sync(0xffffffffu, sg_bar_wait(tfull, q & 1, err, 15));
+      sg_fence_after();
+      const long gm = (long)(blockIdx.x + q * gridDim.x) * SG_M + m;
+      for (int cb = 0; cb < SG_M / 32; ++cb) {
+        double v[32];
+        if (ok) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) v[j] = 0.0;
+#pragma unroll 1
+          for (int d = 0; d < S; ++d) {
+            uint32_t r[32];
+            sg_tmem_ld32(tbase + ((uint32_t)(32 * ew) << 16) + (uint32_t)(d * SG_M + 32 * cb), r);
+            const double w = sg_weight(d);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) v[j] += (double)(int)r[j] * w;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) v[j] = __longlong_as_double(0x7ff8000000000000LL);
+        }
+        if (gm < mreal) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int n = 32 * cb + j;
+            if (n < nn) {
+              double *o = out + (long)n * ldo + gm;
+              const double val = v[j] * colscale[n];
+              *o = sub ? *o - val : val;
+            }
+          }
+        }
+      }
+      sg_fence_before();
+      __syncwarp();
+      if (lane == 0) sg_bar_arrive(tfree);
+      if (!ok) break;
+    }
+  }
+  sg_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    sg_fence_after();
+    sg_tmem_dealloc(tbase, SG_TMEM_COLS);
+  }
+}
+
+}  // namespace amdk

@@ -81,6 +81,7 @@ def load_library(path: str = LIBPATH):
     lib.amdk_set_positions.argtypes = [P, C.POINTER(C.c_double)]
     lib.amdk_set_precision.argtypes = [P, C.c_int]
     lib.amdk_wfn_extrapolate.argtypes = [P]
+    lib.amdk_wfn_set_predictor.argtypes = [P, C.c_int, C.c_void_p]
     lib.amdk_wfn_history_clear.argtypes = [P]
     lib.amdk_set_wfn.argtypes = [P, C.POINTER(C.c_double)]
     lib.amdk_get_wfn.argtypes = [P, C.POINTER(C.c_double)]
@@ -189,9 +190,18 @@ class Engine:
         self.precision = precision      # precision the engine was created with
         self.pair_precision = precision  # precision of the band-pair FFTs now
 
+    def set_predictor(self, npoints: int = 2, coef=None):
+        """Points (C0(t) included) and weights of the BOMD predictor; coef
+        None selects the always-stable predictor weights (aspc_coefficients)."""
+        w = None if coef is None else np.ascontiguousarray(coef, dtype=np.float64)
+        if w is not None and w.shape != (npoints,):
+            raise ValueError("coef must have npoints entries")
+        _check(self.lib.amdk_wfn_set_predictor(self.h, int(npoints), None if w is None else w.ctypes.data),
+               "amdk_wfn_set_predictor")
+
     def extrapolate(self):
-        """BOMD predictor: C0 <- 2 C0(t) - C0(t-dt) [C0(t-dt)^T C0(t)] once a
-        previous step is stored (stores C0(t)); orthonormalise afterwards."""
+        """BOMD predictor: C0 <- sum_j w_j C0(t-j dt) [C0(t-j dt)^T C0(t)] over
+        the stored steps (stores C0(t)); orthonormalise afterwards."""
         _check(self.lib.amdk_wfn_extrapolate(self.h), "amdk_wfn_extrapolate")
 
     def clear_history(self):

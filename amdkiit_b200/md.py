@@ -7,8 +7,10 @@ from the last CG iteration, half kick.  Units: bohr, Hartree, atomic time;
 constants from constants.f90:6-8.
 
 Option outside the reference (off by default): extrapolate=True predicts
-each step's starting wavefunction from the last two converged ones
-(C0 <- 2 C0(t) - C0(t-dt) [C0(t-dt)^T C0(t)], then ortho_gs) instead of
+each step's starting wavefunction from the last `predictor_points`
+converged ones (C0 <- sum_j w_j C0(t-j dt) [C0(t-j dt)^T C0(t)], then
+ortho_gs; weights of Kolafa's always-stable predictor, linear
+extrapolation 2 C0(t) - C0(t-dt)[...] for two points) instead of
 restarting from C0(t) as molecular_dynamics.f90:106-109 does; the converged
 state and the trajectory are the same to the SCF tolerance, the number of
 SCF iterations per step drops.
@@ -34,9 +36,11 @@ KBOLTZ = 0.316681534e-5
 
 class BOMD:
     def __init__(self, engine, temperature: float = 300.0, dt_fs: float = 0.5, seed: int = 2024,
-                 gcut: float = 1e-6, max_scf: int = 800, extrapolate: bool = False):
+                 gcut: float = 1e-6, max_scf: int = 800, extrapolate: bool = False,
+                 predictor_points: int = 2):
         self.e = engine
         self.extrapolate = extrapolate
+        self.predictor_points = predictor_points
         s = engine.system
         self.system = s
         self.dt = dt_fs / AU_TO_FS
@@ -87,6 +91,7 @@ class BOMD:
         """Forces at the initial geometry (molecular_dynamics.f90:56-60)."""
         self.e.set_positions(self.pos)
         if self.extrapolate:
+            self.e.set_predictor(self.predictor_points)
             self.e.clear_history()
         self.e.ortho()
         return self._scf()
@@ -118,3 +123,16 @@ class BOMD:
             if callback:
                 callback(i, n, self.energy, self.total_energy(), self.temperature())
         return time.perf_counter() - t0
+
+
+def aspc_coefficients(npoints: int):
+    """Weights of Kolafa's always-stable predictor with npoints = K + 2 points,
+    most recent first (J. Comput. Chem. 25, 335 (2004)):
+    B_j = (-1)^(j+1) j binom(2K+4, K+2-j) / binom(2K+2, K+1).  The engine
+    computes the same weights for amdk_wfn_set_predictor(coef=NULL)."""
+    from math import comb
+    if npoints <= 1:
+        return np.ones(1)
+    k = npoints - 2
+    return np.array([(-1) ** (j + 1) * j * comb(2 * k + 4, k + 2 - j) / comb(2 * k + 2, k + 1)
+                     for j in range(1, npoints + 1)])

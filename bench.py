@@ -43,7 +43,7 @@ WORKLOAD = "water32: 32 H2O, PBE, 70 Ry, 100^3 grid, 128 bands, GTH, Gamma"
 # DRAM bytes (read + write) per launch of the dominant kernel classes, from
 # one `ncu --set full` capture of each on this workload (one launch inside
 # `bench.py --steps 3 --warmup 3 --md-steps 0`); None where none was taken.
-TRAFFIC = {("z_vpsi", "mixed"): 145.60e6, ("z_vpsi", "fp64"): 347.54e6, ("z_density", "mixed"): 142.22e6}
+TRAFFIC = {("z_vpsi", "mixed"): 146.45e6, ("z_vpsi", "fp64"): 347.35e6, ("z_density", "mixed"): 142.22e6}
 
 
 def peaks():

@@ -166,11 +166,18 @@ int amdk_backward(amdk_ctx *ctx, double *dE_dR, double *dE_dpsi);
 
 /* Wavefunction predictor for BOMD (no reference counterpart: the reference
  * restarts each step from the previous C0, molecular_dynamics.f90:106-109).
- * With a previous step's C0 stored, C0 <- 2 C0(t) - C0(t-dt) M with
- * M = C0(t-dt)^T C0(t) (the overlap in the Gamma convention, aligning the
- * previous occupied subspace with the current one); C0(t) is then stored.
- * The caller orthonormalises afterwards (amdk_ortho), as after a geometry
- * update.  amdk_wfn_history_clear forgets the stored C0. */
+ * amdk_wfn_extrapolate predicts
+ *   C0 <- sum_j w_j C0(t-j dt) M_j,  M_j = C0(t-j dt)^T C0(t)
+ * (M_0 = 1; the overlap in the Gamma convention aligns step j's occupied
+ * subspace with the current one, a density-matrix extrapolation applied to
+ * C0(t)) and then stores C0(t).  The caller orthonormalises afterwards
+ * (amdk_ortho), as after a geometry update.  amdk_wfn_set_predictor sets
+ * the number of points (C0(t) included, 1..8; default 2) and their weights,
+ * most recent first; coef = NULL selects Kolafa's always-stable predictor
+ * weights for that many points ((2,-1) for 2: linear extrapolation).  Until
+ * enough steps are stored the always-stable weights of the points there are
+ * used.  amdk_wfn_history_clear forgets the stored steps. */
+int amdk_wfn_set_predictor(amdk_ctx *ctx, int npoints, const double *coef);
 int amdk_wfn_extrapolate(amdk_ctx *ctx);
 int amdk_wfn_history_clear(amdk_ctx *ctx);
 

@@ -105,3 +105,29 @@ def test_bomd_predictor_keeps_trajectory_and_saves_iterations():
     assert np.max(np.abs(runs[True].pos - runs[False].pos)) < 1e-6
     assert abs(runs[True].total_energy() - runs[False].total_energy()) < 1e-7
     assert np.mean(runs[True].scf_iterations[3:]) < np.mean(runs[False].scf_iterations[3:])
+
+
+def test_bomd_higher_order_predictor():
+    """Always-stable predictor weights over 4 points and explicit weights
+    reach the same trajectory as the reference driver to the SCF tolerance;
+    explicit (2, -1) weights are the default linear predictor bit for bit."""
+    s = configs.small_water()
+    runs = {}
+    for key, x, npts, coef in (("ref", False, 2, None), ("aspc4", True, 4, None), ("lin", True, 2, None),
+                               ("lin_w", True, 2, [2.0, -1.0]), ("poly3", True, 3, [3.0, -3.0, 1.0])):
+        e = _engine(s)
+        md = BOMD(e, temperature=300.0, dt_fs=0.5, seed=3, gcut=1e-7, extrapolate=x, predictor_points=npts)
+        md.start()
+        if coef is not None:
+            e.set_predictor(npts, coef)
+        for _ in range(6):
+            md.step()
+        runs[key] = (md, e.get_wfn())
+    ref = runs["ref"][0]
+    for key in ("aspc4", "lin", "poly3"):
+        md = runs[key][0]
+        assert np.max(np.abs(md.pos - ref.pos)) < 1e-6, key
+        assert abs(md.total_energy() - ref.total_energy()) < 1e-7, key
+        assert np.mean(md.scf_iterations[3:]) < np.mean(ref.scf_iterations[3:]), key
+    assert runs["lin"][0].scf_iterations == runs["lin_w"][0].scf_iterations
+    assert np.array_equal(runs["lin"][1], runs["lin_w"][1])
