@@ -148,13 +148,14 @@ struct amdk_ctx {
   bool use_graphs = true;
   bool tune = true;  // measure launch shapes at first use (AMDK_NO_TUNE=1: model only)
   bool overlap = true;  // C0-only work on the side stream (AMDK_NO_OVERLAP=1: one stream)
-  bool chol_regs = true;  // register Cholesky up to 128 bands (AMDK_CHOL_SHARED=1: blocked shared-memory kernel)
   // integer-slice tensor-core GEMMs of the mixed path (<= 128 bands;
   // AMDK_SLICE=1 turns them on, else DGEMM/DTRMM as the FP64 path)
   bool slice_gemm = false, sg_ready = false;
   int8_t *d_plA = nullptr, *d_plB = nullptr, *d_plS = nullptr;  // C0, C2, small-matrix digit planes
   double *d_sgA = nullptr, *d_sgB = nullptr, *d_sgS = nullptr;  // their row (column) scales
   double *d_sgpart = nullptr;
+  unsigned long long *d_sgmax = nullptr;  // per-band max |x| of the slicing pass
+  double *d_sgnsq = nullptr;               // per-band sums of squares (by segment) of the slicing pass
   int *d_sgerr = nullptr;
   long sg_kpad = 0;
   int sg_ktiles = 0, sg_per = 0, sg_chunks = 0, sg_mtiles = 0;
@@ -859,6 +860,8 @@ static int sg_setup(amdk_ctx *c) {
   RC(c->alloc(&c->d_sgB, SG_M));
   RC(c->alloc(&c->d_sgS, SG_M));
   RC(c->alloc(&c->d_sgpart, (size_t)c->sg_chunks * SG_M * SG_M));
+  RC(c->alloc(&c->d_sgmax, SG_M));
+  RC(c->alloc(&c->d_sgnsq, (size_t)SG_M * SG_SEG));
   c->d_sgerr = c->d_info + 1;
   RC(sg_encode(&c->tm_a_tn, c->d_plA, c->sg_kpad, SG_TN_KT, CU_TENSOR_MAP_SWIZZLE_64B));
   RC(sg_encode(&c->tm_b_tn, c->d_plB, c->sg_kpad, SG_TN_KT, CU_TENSOR_MAP_SWIZZLE_64B));
@@ -872,8 +875,12 @@ static int sg_setup(amdk_ctx *c) {
 // digit planes and row scales of the bands of x (C0 or C2)
 static void sg_slice(amdk_ctx *c, const double2 *x, int8_t *planes, double *scale) {
   const long K = 2L * c->hs.ngpw;
-  ++c->nlaunch;
-  k_slice_rows<SG_S><<<SG_M, 512, 0, c->st>>>((const double *)x, K, K, c->nstate, planes, c->sg_kpad, scale);
+  c->nlaunch += 2;
+  cudaMemsetAsync(c->d_sgmax, 0, sizeof(unsigned long long) * SG_M, c->st);
+  k_band_absmax<<<dim3(SG_SEG, c->nstate), 256, 0, c->st>>>((const double *)x, K, K, c->nstate, c->d_sgmax,
+                                                             c->d_sgnsq);
+  k_slice_rows<SG_S><<<dim3(SG_SEG, SG_M), 256, 0, c->st>>>((const double *)x, K, K, c->nstate, c->d_sgmax, planes,
+                                                            c->sg_kpad, scale);
 }
 // out (n x n) = alpha diag(sa) A B^T diag(sb), the product over the real index
 static void sg_tn(amdk_ctx *c, const CUtensorMap &ta, const CUtensorMap &tb, int same, const double *sa,
@@ -882,7 +889,8 @@ static void sg_tn(amdk_ctx *c, const CUtensorMap &ta, const CUtensorMap &tb, int
   c->nlaunch += 2;
   k_sgemm_tn<SG_S><<<c->sg_chunks, 128, SgTn<SG_S>::SMEM, c->st>>>(ta, tb, same, c->sg_ktiles, c->sg_per, c->d_sgpart,
                                                                      c->d_sgerr);
-  k_sgemm_reduce<<<n, SG_M, 0, c->st>>>(c->sg_chunks, c->d_sgpart, n, sa, sb, alpha, out, n);
+  k_sgemm_reduce<<<n, 4 * SG_M, 0, c->st>>>(c->sg_chunks, c->d_sgpart, n, sa, sb, same ? c->d_sgnsq : nullptr,
+                                            alpha, out, n);
 }
 // out (the real view, 2 ngpw x n) = (or -=, sub) C0 B for B n x n, with C0's
 // planes and scales in d_plA / d_sgA
@@ -891,7 +899,7 @@ static void sg_nn(amdk_ctx *c, const double *B, double2 *out, int sub) {
   const long K = 2L * c->hs.ngpw;
   c->nlaunch += 2;
   k_slice_small<SG_S><<<SG_M, SG_M, 0, c->st>>>(B, n, n, n, c->d_sgA, c->d_plS, c->d_sgS);
-  k_sgemm_nn<SG_S><<<std::min(c->sg_mtiles, c->nsm), 192, SgNn<SG_S>::SMEM, c->st>>>(
+  k_sgemm_nn<SG_S><<<std::min(c->sg_mtiles, c->nsm), SG_NN_THREADS, SgNn<SG_S>::SMEM, c->st>>>(
       c->tm_a_nn, c->tm_s_nn, c->sg_mtiles, K, (double *)out, K, n, c->d_sgS, sub, c->d_sgerr);
 }
 
@@ -982,13 +990,7 @@ static int do_ortho(amdk_ctx *c, bool check = true, bool swap = true) {
   const int np = (n + CHOL_B - 1) / CHOL_B * CHOL_B;
   const size_t sm = ((size_t)np * (np + 1) + (size_t)CHOL_B * np) * sizeof(double);
   ++c->nlaunch;
-  if (n <= 32 && c->chol_regs) {
-    k_chol_inv_r<32><<<1, CHR_NT, sizeof(double) * 32 * ChR<32>::LD, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
-  } else if (n <= 64 && c->chol_regs) {
-    k_chol_inv_r<64><<<1, CHR_NT, sizeof(double) * 64 * ChR<64>::LD, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
-  } else if (n <= 128 && c->chol_regs) {
-    k_chol_inv_r<128><<<1, CHR_NT, sizeof(double) * 128 * ChR<128>::LD, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
-  } else if (n <= CHOL_NMAX) {
+  if (n <= CHOL_NMAX) {
     k_chol_inv_s<<<1, CHOL_NT, sm, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
   } else {
     // DPOTRF + DTRTRI as the reference (wfn_initialize.f90:513,524), in place
@@ -1179,8 +1181,6 @@ static int build_device(amdk_ctx *c) {
     CK(cudaMemcpyToSymbol(c_twf, twf.data(), sizeof(float2) * CTW_LEN));
   }
   CK(cudaFuncSetAttribute(k_chol_inv_s, cudaFuncAttributeMaxDynamicSharedMemorySize, 216 * 1024));
-  CK(cudaFuncSetAttribute(k_chol_inv_r<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)(sizeof(double) * 128 * ChR<128>::LD)));
   // G vectors
   RC(c->up(&c->d_inyh, h.inyh));
   RC(c->up(&c->d_hg, h.hg));
@@ -1215,8 +1215,6 @@ static int build_device(amdk_ctx *c) {
     c->tune = !(nt && nt[0] == '1');
     const char *no = getenv("AMDK_NO_OVERLAP");
     c->overlap = !(no && no[0] == '1');
-    const char *cs = getenv("AMDK_CHOL_SHARED");
-    c->chol_regs = !(cs && cs[0] == '1');
   }
   if (h.nstate > CHOL_NMAX) {
     // large overlaps: cuSOLVER (its DTRTRI keeps a host workspace, so the

@@ -705,107 +705,6 @@ __global__ void __launch_bounds__(CHOL_NT) k_chol_inv_s(int n, const double *A, 
   if (tid == 0) *info = 0;
 }
 
-// Register-resident Cholesky + inverse for n <= 128, one block of CHR_NT
-// threads, the matrix padded to NP (32, 64 or 128) with the identity.
-// Thread (column j = tid % NP, class cls = tid / NP) holds the rows
-// i = CLS*m + cls of column j in registers (RPT = NP/CLS of them).
-// Factor, K = 0 .. NP-1 (right-looking, one barrier per step): the owners of
-// row K publish it to a double-buffered shared row; every thread reads the
-// pivot p = S_KK and updates its upper-triangle elements
-// S_ij -= S_Ki S_Kj / p (i, j > K); row K scaled by p^{-1/2} is U's row K,
-// kept in shared memory.  Inverse, K = NP-1 .. 0 (right-looking back
-// substitution on B = I): the owners of row K set X_Kj = B_Kj / U_KK and
-// publish it; every thread updates B_ij -= U_iK X_Kj for rows i < K.  Each
-// step's K is a template constant, so the register array is indexed
-// statically.  Same contract as k_chol_inv_s.
-constexpr int CHR_NT = 512;
-template <int NP> struct ChR {
-  static constexpr int CLS = CHR_NT / NP, RPT = NP / CLS, LD = NP + 1;
-};
-template <int NP, int K>
-__device__ __forceinline__ void chr_factor(double (&a)[ChR<NP>::RPT], double (*row)[NP], double *Us, int j, int cls,
-                                           int &bad) {
-  if constexpr (K < NP) {
-    constexpr int CLS = ChR<NP>::CLS, RPT = ChR<NP>::RPT, LD = ChR<NP>::LD, MK = K / CLS;
-    double *rb = row[K & 1];
-    const bool owner = cls == K % CLS && j >= K;
-    if (owner) rb[j] = a[MK];
-    __syncthreads();
-    const double p = rb[K];  // the same value in every thread
-    if (!(p > 0.0)) {
-      bad = K + 1;
-      return;
-    }
-    if (owner) Us[K + LD * j] = a[MK] * rsqrt(p);
-    if (j > K) {
-      const double rj = rb[j] / p;
-#pragma unroll
-      for (int m = (K + 1) / CLS; m < RPT; ++m) {
-        const int i = CLS * m + cls;
-        if (i > K && i <= j) a[m] -= rb[i] * rj;
-      }
-    }
-    chr_factor<NP, K + 1>(a, row, Us, j, cls, bad);
-  }
-}
-template <int NP, int K>
-__device__ __forceinline__ void chr_inverse(double (&b)[ChR<NP>::RPT], double (*row)[NP], const double *Us, int j,
-                                            int cls) {
-  if constexpr (K >= 0) {
-    constexpr int CLS = ChR<NP>::CLS, LD = ChR<NP>::LD, MK = K / CLS;
-    double *xb = row[K & 1];
-    if (cls == K % CLS && j >= K) {
-      b[MK] = b[MK] / Us[K + LD * K];
-      xb[j] = b[MK];
-    }
-    __syncthreads();
-    if (j >= K) {
-      const double xj = xb[j];
-#pragma unroll
-      for (int m = 0; m < (K + CLS - 1) / CLS; ++m) {
-        const int i = CLS * m + cls;
-        if (i < K) b[m] -= Us[i + LD * K] * xj;
-      }
-    }
-    chr_inverse<NP, K - 1>(b, row, Us, j, cls);
-  }
-}
-template <int NP>
-__global__ void __launch_bounds__(CHR_NT, 1) k_chol_inv_r(int n, const double *A, double *Ui, int *info) {
-  constexpr int CLS = ChR<NP>::CLS, RPT = ChR<NP>::RPT, LD = ChR<NP>::LD;
-  extern __shared__ double Us[];  // [NP][LD]: staging, then U (upper), then the output
-  __shared__ double row[2][NP];
-  const int tid = threadIdx.x, j = tid % NP, cls = tid / NP;
-  for (int idx = tid; idx < NP * NP; idx += CHR_NT) {
-    const int r = idx % NP, cidx = idx / NP;
-    Us[r + LD * cidx] = (r < n && cidx < n) ? A[r + (long)n * cidx] : (r == cidx ? 1.0 : 0.0);
-  }
-  __syncthreads();
-  double a[RPT];
-#pragma unroll
-  for (int m = 0; m < RPT; ++m) a[m] = Us[CLS * m + cls + LD * j];
-  __syncthreads();  // Us is overwritten by U's rows from here on
-  int bad = 0;
-  chr_factor<NP, 0>(a, row, Us, j, cls, bad);
-  if (bad) {
-    if (tid == 0) *info = bad;
-    return;
-  }
-#pragma unroll
-  for (int m = 0; m < RPT; ++m) a[m] = (CLS * m + cls == j) ? 1.0 : 0.0;
-  __syncthreads();  // U complete in shared memory
-  chr_inverse<NP, NP - 1>(a, row, Us, j, cls);
-  __syncthreads();  // every read of U done
-#pragma unroll
-  for (int m = 0; m < RPT; ++m) Us[CLS * m + cls + LD * j] = a[m];
-  __syncthreads();
-  for (int idx = tid; idx < n * n; idx += CHR_NT) {
-    const int r = idx % n, cidx = idx / n;
-    Ui[idx] = (r <= cidx) ? Us[r + LD * cidx] : 0.0;
-  }
-  if (tid == 0) *info = 0;
-}
-
 // e_sr (total_energy.f90:133-239) with minimum image: one thread per atom
 // sums its pair forces over every other atom (deterministic order) and the
 // pair energies with the atoms after it.  Pair terms are those of the

@@ -261,9 +261,34 @@ __global__ void __launch_bounds__(PNT) k_pencil_density(PencilGeom pg, Plan<C> p
   for (int idx = threadIdx.x; idx < N * NP; idx += blockDim.x) acc[idx] = (Rl)0;
   const int kx = blockIdx.x, grp = blockIdx.y;
   const int t0 = grp * per_group, t1 = min(T, t0 + per_group);
+  // the next pair's rays are loaded into registers while this pair is
+  // transformed (planes of up to PREF * blockDim rays; else loaded in turn)
+  constexpr int PREF = 4;
+  const bool pre = pg.nray <= PREF * (int)blockDim.x;
+  C nxt[PREF];
+  auto fetch = [&](int t) {
+    const C *pl = rt + ((long)t * pg.n1 + kx) * pg.nray;
+#pragma unroll
+    for (int i = 0; i < PREF; ++i) {
+      const int r = threadIdx.x + i * blockDim.x;
+      nxt[i] = r < pg.nray ? pl[r] : czero<C>();
+    }
+  };
+  if (pre && t0 < t1) fetch(t0);
   for (int t = t0; t < t1; ++t) {
-    const C *plane = rt + ((long)t * pg.n1 + kx) * pg.nray;
-    pencil_scatter<C, N>(P, plane, pg);
+    if (pre) {
+      for (int idx = threadIdx.x; idx < nz * NP; idx += blockDim.x) P[idx] = czero<C>();
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < PREF; ++i) {
+        const int r = threadIdx.x + i * blockDim.x;
+        if (r < pg.nray) P[pg.rpos[r]] = nxt[i];
+      }
+      __syncthreads();
+      if (t + 1 < t1) fetch(t + 1);
+    } else {
+      pencil_scatter<C, N>(P, rt + ((long)t * pg.n1 + kx) * pg.nray, pg);
+    }
     rows_nat_to_perm<C, N, 1>(P, nz, NP, tw);
     const Rl fa = (Rl)wa[t], fb = (Rl)wb[t];
     for (int q0 = 0; q0 < N; q0 += CTs) {

@@ -7,9 +7,10 @@
 // Method (the split-integer scheme of Ozaki et al., Numer. Algorithms 59, 95
 // (2012), with Ootomo-Ozaki-Yokota's int8 tensor-core variant, IJHPCA 2024):
 // every row r of an operand (a band) is scaled by a power of two sigma_r so
-// that |x| / sigma_r < 1/2, then cut into S signed 7-bit digits,
-//   x / sigma_r = sum_t d_t 2^{-7(t+1)} + O(2^{-7S}),  d_t in [-64, 64],
-// by repeated round-to-nearest (exact in FP64).  A product of two rows is
+// that |x| / sigma_r < 1/2, rounded to the fixed-point integer
+// v = rint(x / sigma_r 2^{7S}) (|v| <= 2^{7S-1}) and cut into S balanced
+// base-128 digits,
+//   x / sigma_r = sum_t d_t 2^{-7(t+1)} + O(2^{-7S}),  d_t in [-64, 64].  A product of two rows is
 //   sum_k x_k y_k = sigma_x sigma_y sum_{t,u} 2^{-7(t+u+2)} sum_k dx_t dy_u,
 // whose inner sums are exact int8 x int8 -> int32 tensor-core products; the
 // terms with t + u >= S are dropped (relative truncation ~2^{-7S}), and the
@@ -141,52 +142,92 @@ __host__ __device__ constexpr uint32_t sg_idesc(bool a_mn) {
 __device__ __forceinline__ double sg_weight(int d) { return ldexp(1.0, -7 * (d + 2)); }
 
 // ---------------------------------------------------------------- slicing
-// Row r (a band: len reals at x + r*ldx) -> sigma_r and S digit planes.
-// grid SG_M (rows >= nrows are zero), block 512.
-template <int S>
-__global__ void __launch_bounds__(512) k_slice_rows(const double *__restrict__ x, long ldx, long len, int nrows,
-                                                    int8_t *__restrict__ planes, long kpad, double *__restrict__ scale) {
-  const int r = blockIdx.x, tid = threadIdx.x;
-  const long pstride = (long)SG_M * kpad;
-  int8_t *dst = planes + (long)r * kpad;
-  if (r >= nrows) {
-    for (long k = 8L * tid; k < kpad; k += 8L * blockDim.x)
+// S balanced base-128 digits of y = x 2^{7S} / sigma (|y| < 2^{7S-1}), most
+// significant first: rint(y) = sum_t d_t 128^{S-1-t}, d_t in [-64, 63]
+// except d_0 in [-64, 64].
+template <int S> __device__ __forceinline__ void sg_digits(double y, int (&d)[S]) {
+  static_assert(S >= 1 && S <= 4, "the fixed-point value must fit 32 bits");
+  int v = __double2int_rn(y);
 #pragma unroll
-      for (int t = 0; t < S; ++t) *reinterpret_cast<uint2 *>(dst + t * pstride + k) = make_uint2(0u, 0u);
-    if (tid == 0) scale[r] = 1.0;
-    return;
+  for (int t = S - 1; t > 0; --t) {
+    const int q = ((v + 64) & 127) - 64;
+    d[t] = q;
+    v = (v - q) >> 7;
   }
+  d[0] = v;
+}
+// Per-row max |x| of the bands (len reals at x + r*ldx) and the row's sum of
+// squares by segment: grid (SG_SEG, nrows), block 256; bmax (as the bit
+// patterns of non-negative doubles, which order like the values) must be
+// cleared first; nsq[r * SG_SEG + segment].  The sums of squares give the
+// exact diagonal of a Gram matrix A A^T: there the dropped digit products
+// d_t d_u with t + u >= S include squares (t = u), which would bias it.
+constexpr int SG_SEG = 8;  // blocks per band in the slicing passes
+__global__ void __launch_bounds__(256) k_band_absmax(const double *__restrict__ x, long ldx, long len, int nrows,
+                                                     unsigned long long *__restrict__ bmax, double *__restrict__ nsq) {
+  const int r = blockIdx.y;
+  if (r >= nrows) return;
+  const long seg = (len / 2 + SG_SEG - 1) / SG_SEG * 2;  // even
+  const long k0 = blockIdx.x * seg, k1 = min(len, k0 + seg);
   const double *xr = x + (long)r * ldx;
-  double m = 0.0;
-  for (long k = 2L * tid; k < len; k += 2L * blockDim.x) {
+  double m = 0.0, q = 0.0;
+  for (long k = k0 + 2L * threadIdx.x; k < k1; k += 2L * blockDim.x) {
     const double2 v = *reinterpret_cast<const double2 *>(xr + k);
     m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+    q = fma(v.x, v.x, fma(v.y, v.y, q));
   }
-  __shared__ double red[16];
-  __shared__ int s_e;
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((tid & 31) == 0) red[tid >> 5] = m;
+  for (int o = 16; o > 0; o >>= 1) {
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    q += __shfl_xor_sync(0xffffffffu, q, o);
+  }
+  __shared__ double red[8], rq[8];
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = m;
+    rq[threadIdx.x >> 5] = q;
+  }
   __syncthreads();
-  if (tid < 32) {
-    double w = tid < (int)(blockDim.x >> 5) ? red[tid] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) w = fmax(w, __shfl_xor_sync(0xffffffffu, w, o));
-    if (tid == 0) {
-      int E = 0;
-      if (w > 0.0) frexp(w, &E);  // w = f 2^E, f in [1/2, 1): w / 2^(E+1) < 1/2
-      s_e = w > 0.0 ? E + 1 : 0;
-      scale[r] = ldexp(1.0, s_e);
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) {
+      m = fmax(m, red[i]);
+      q += rq[i];
     }
+    atomicMax(bmax + r, (unsigned long long)__double_as_longlong(m));
+    nsq[r * SG_SEG + blockIdx.x] = q;
   }
-  __syncthreads();
-  const int e = s_e;
-  for (long k = 8L * tid; k < kpad; k += 8L * blockDim.x) {
+}
+// Row r -> sigma_r = 2^e (max / 2^e < 1/2) and S digit planes; grid
+// (SG_SEG, SG_M) over kpad (rows >= nrows are zero), block 256.
+template <int S>
+__global__ void __launch_bounds__(256) k_slice_rows(const double *__restrict__ x, long ldx, long len, int nrows,
+                                                    const unsigned long long *__restrict__ bmax,
+                                                    int8_t *__restrict__ planes, long kpad, double *__restrict__ scale) {
+  const int r = blockIdx.y;
+  const long pstride = (long)SG_M * kpad;
+  const long seg = (kpad / 8 + SG_SEG - 1) / SG_SEG * 8;
+  const long k0 = blockIdx.x * seg, k1 = min(kpad, k0 + seg);
+  int8_t *dst = planes + (long)r * kpad;
+  if (r >= nrows) {
+    for (long k = k0 + 8L * threadIdx.x; k < k1; k += 8L * blockDim.x)
+#pragma unroll
+      for (int t = 0; t < S; ++t) *reinterpret_cast<uint2 *>(dst + t * pstride + k) = make_uint2(0u, 0u);
+    if (blockIdx.x == 0 && threadIdx.x == 0) scale[r] = 1.0;
+    return;
+  }
+  const double w = __longlong_as_double((long long)bmax[r]);
+  int E = 0;
+  if (w > 0.0) frexp(w, &E);  // w = f 2^E, f in [1/2, 1): w / 2^(E+1) < 1/2
+  const int e = w > 0.0 ? E + 1 : 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) scale[r] = ldexp(1.0, e);
+  const double sc = ldexp(1.0, 7 * S - e);  // x -> fixed point with 7S fraction bits
+  const double *xr = x + (long)r * ldx;
+  for (long k = k0 + 8L * threadIdx.x; k < k1; k += 8L * blockDim.x) {
     double v[8];
 #pragma unroll
     for (int i = 0; i < 8; i += 2) {
       if (k + i < len) {
-        const double2 w = *reinterpret_cast<const double2 *>(xr + k + i);
-        v[i] = w.x;
-        v[i + 1] = w.y;
+        const double2 q = *reinterpret_cast<const double2 *>(xr + k + i);
+        v[i] = q.x;
+        v[i + 1] = q.y;
       } else {
         v[i] = v[i + 1] = 0.0;
       }
@@ -196,13 +237,11 @@ __global__ void __launch_bounds__(512) k_slice_rows(const double *__restrict__ x
     for (int t = 0; t < S; ++t) lo[t] = hi[t] = 0u;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      double y = ldexp(v[i], -e);
+      int d[S];
+      sg_digits<S>(v[i] * sc, d);
 #pragma unroll
       for (int t = 0; t < S; ++t) {
-        y *= 128.0;
-        const double d = rint(y);
-        y -= d;
-        const uint32_t b = (uint32_t)(uint8_t)(int8_t)(int)d;
+        const uint32_t b = (uint32_t)(uint8_t)(int8_t)d[t];
         if (i < 4) lo[t] |= b << (8 * i);
         else hi[t] |= b << (8 * (i - 4));
       }
@@ -233,14 +272,10 @@ __global__ void __launch_bounds__(SG_M) k_slice_small(const double *__restrict__
   if (w > 0.0) frexp(w, &E);
   const int e = w > 0.0 ? E + 1 : 0;
   if (k == 0) colscale[n] = ldexp(1.0, e);
-  double y = ldexp(v, -e);
+  int d[S];
+  sg_digits<S>(v * ldexp(1.0, 7 * S - e), d);
 #pragma unroll
-  for (int t = 0; t < S; ++t) {
-    y *= 128.0;
-    const double d = rint(y);
-    y -= d;
-    planes[(long)t * SG_M * SG_M + n * SG_M + k] = (int8_t)(int)d;
-  }
+  for (int t = 0; t < S; ++t) planes[(long)t * SG_M * SG_M + n * SG_M + k] = (int8_t)d[t];
 }
 
 // ------------------------------------------------------------------ TN GEMM
@@ -355,15 +390,29 @@ __global__ void __launch_bounds__(128, 1) k_sgemm_tn(const __grid_constant__ CUt
   }
 }
 
-// out[m + ldo n] = alpha sa[m] sb[n] sum_c partial[c][n][m], m < nm, n < nn.
-// grid nn, block SG_M.
-__global__ void k_sgemm_reduce(int nchunk, const double *__restrict__ partial, int nm, const double *__restrict__ sa,
-                               const double *__restrict__ sb, double alpha, double *__restrict__ out, int ldo) {
-  const int m = threadIdx.x, n = blockIdx.x;
-  if (m >= nm) return;
+// out[m + ldo n] = alpha sa[m] sb[n] sum_c partial[c][n][m], m < nm, n < nn;
+// with nsq (a Gram matrix) the diagonal is alpha sum_seg nsq[m][seg] instead.
+// grid nn, block 4 SG_M: four interleaved partial sums per row, fixed order.
+__global__ void __launch_bounds__(4 * SG_M) k_sgemm_reduce(int nchunk, const double *__restrict__ partial, int nm,
+                                                           const double *__restrict__ sa, const double *__restrict__ sb,
+                                                           const double *__restrict__ nsq, double alpha,
+                                                           double *__restrict__ out, int ldo) {
+  const int m = threadIdx.x % SG_M, g = threadIdx.x / SG_M, n = blockIdx.x;
+  __shared__ double red[4][SG_M];
   double s = 0.0;
-  for (int c = 0; c < nchunk; ++c) s += partial[(long)c * SG_M * SG_M + n * SG_M + m];
-  out[m + (long)ldo * n] = alpha * sa[m] * sb[n] * s;
+#pragma unroll 8
+  for (int c = g; c < nchunk; c += 4) s += partial[(long)c * SG_M * SG_M + n * SG_M + m];
+  red[g][m] = s;
+  __syncthreads();
+  if (g == 0 && m < nm) {
+    double v = alpha * sa[m] * sb[n] * (((red[0][m] + red[1][m]) + red[2][m]) + red[3][m]);
+    if (nsq && m == n) {
+      double q = 0.0;
+      for (int i = 0; i < SG_SEG; ++i) q += nsq[m * SG_SEG + i];
+      v = alpha * q;
+    }
+    out[m + (long)ldo * n] = v;
+  }
 }
 
 // ------------------------------------------------------------------ NN GEMM
@@ -374,11 +423,14 @@ template <int S> struct SgNn {
 // out[m + ldo n] (=, or -= when sub) colscale[n] sum_{t+u<S} 2^{-7(t+u+2)}
 //   sum_k dA_t[k][m] dB_u[n][k]   for m < mreal, n < nn,
 // A planes [t][k][m] (MN-major tiles of 128 m x 128 k), B planes [t][n][k].
-// Persistent: CTA b takes the 128-row tiles b, b + grid, ...  block 192:
+// Persistent: CTA b takes the 128-row tiles b, b + grid, ...  block 320:
 // warp 0 loads, warp 1 issues the MMAs (and owns the tensor memory), warps
-// 2-5 read the accumulators back (TMEM lanes 32 (w % 4) ...).
+// 2-9 read the accumulators back (TMEM lanes 32 (w % 4) ..., columns
+// 64 ((w - 2) / 4) ...) and stream the FP64 result out, the old values of a
+// subtraction loaded before the accumulators are read.
+constexpr int SG_NN_THREADS = 320;
 template <int S>
-__global__ void __launch_bounds__(192, 1) k_sgemm_nn(const __grid_constant__ CUtensorMap ta,
+__global__ void __launch_bounds__(SG_NN_THREADS, 1) k_sgemm_nn(const __grid_constant__ CUtensorMap ta,
                                                      const __grid_constant__ CUtensorMap tb, int mtiles, long mreal,
                                                      double *__restrict__ out, long ldo, int nn,
                                                      const double *__restrict__ colscale, int sub, int *err) {
@@ -402,7 +454,7 @@ __global__ void __launch_bounds__(192, 1) k_sgemm_nn(const __grid_constant__ CUt
       sg_bar_init(empty0 + 8 * i, 1);
     }
     sg_bar_init(tfull, 1);
-    sg_bar_init(tfree, 4);
+    sg_bar_init(tfree, 8);
     sg_bar_init(fin, 1);
     sg_bar_fence_init();
   }
@@ -455,13 +507,18 @@ __global__ void __launch_bounds__(192, 1) k_sgemm_nn(const __grid_constant__ CUt
     sg_commit(fin);
     sg_bar_wait(fin, 0, err, 16);  // every MMA of this block has finished
   } else if (warp >= 2) {
-    const int ew = warp & 3;
+    const int ew = warp & 3, half = (warp - 2) >> 2;
     const int m = 32 * ew + lane;
     for (int q = 0; q < nq; ++q) {
       const bool ok = __all_sync(0xffffffffu, sg_bar_wait(tfull, q & 1, err, 15));
       sg_fence_after();
       const long gm = (long)(blockIdx.x + q * gridDim.x) * SG_M + m;
-      for (int cb = 0; cb < SG_M / 32; ++cb) {
+      for (int cb = 2 * half; cb < 2 * half + 2; ++cb) {
+        double old[32];
+        if (sub && gm < mreal) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) old[j] = (32 * cb + j < nn) ? out[(long)(32 * cb + j) * ldo + gm] : 0.0;
+        }
         double v[32];
         if (ok) {
 #pragma unroll
@@ -483,9 +540,8 @@ __global__ void __launch_bounds__(192, 1) k_sgemm_nn(const __grid_constant__ CUt
           for (int j = 0; j < 32; ++j) {
             const int n = 32 * cb + j;
             if (n < nn) {
-              double *o = out + (long)n * ldo + gm;
               const double val = v[j] * colscale[n];
-              *o = sub ? *o - val : val;
+              out[(long)n * ldo + gm] = sub ? old[j] - val : val;
             }
           }
         }

@@ -278,33 +278,14 @@ def test_graph_replay_with_profiling():
 
 
 @pytest.mark.parametrize("nmol", [1, 2, 5, 7, 8, 12, 16])
-@pytest.mark.parametrize("shared", [False, True])
-def test_ortho_matches_oracle_across_band_counts(nmol, shared, monkeypatch):
-    """ortho_gs for 4 to 64 bands: the register Cholesky (padded to 32, 64
-    or 128) and the blocked shared-memory kernel (16-column blocks)."""
+def test_ortho_matches_oracle_across_band_counts(nmol):
+    """ortho_gs for band counts that are and are not multiples of the
+    Cholesky kernel's 16-column blocks (4 to 64 bands)."""
     s = configs.cluster(nmol, 18.0, 900 + nmol, ecut=20.0)
-    if shared:
-        monkeypatch.setenv("AMDK_CHOL_SHARED", "1")
     o, e = pair(s)
     assert o.ortho() == 0
     e.ortho()
     assert rel(e.get_wfn(), o.c0()) < 1e-11
-
-
-def test_register_cholesky_matches_shared_kernel_128_bands(monkeypatch):
-    """water32's 128 bands: the register Cholesky and the blocked
-    shared-memory kernel give the same orthonormalised C0 to rounding."""
-    s = configs.water32()
-    monkeypatch.setenv("AMDK_CHOL_SHARED", "1")
-    ref = Engine(s, FP64)
-    monkeypatch.delenv("AMDK_CHOL_SHARED")
-    e = Engine(s, FP64)
-    g = ref.gvectors()
-    c = start_coefficients(g["hg"][: ref.ngpw], 2 * np.pi / s.alat, ref.nstate, 11)
-    for x in (ref, e):
-        x.set_wfn(c)
-        x.ortho()
-    assert rel(e.get_wfn(), ref.get_wfn()) < 1e-12
 
 
 def test_density_independent_of_measured_launch_shape(monkeypatch):
