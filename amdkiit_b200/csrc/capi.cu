@@ -149,8 +149,8 @@ struct amdk_ctx {
   bool tune = true;  // measure launch shapes at first use (AMDK_NO_TUNE=1: model only)
   bool overlap = true;  // C0-only work on the side stream (AMDK_NO_OVERLAP=1: one stream)
   // integer-slice tensor-core GEMMs of the mixed path (<= 128 bands;
-  // AMDK_SLICE=1 turns them on, else DGEMM/DTRMM as the FP64 path)
-  bool slice_gemm = false, sg_ready = false;
+  // AMDK_NO_SLICE=1: DGEMM/DTRMM as the FP64 path)
+  bool slice_gemm = true, sg_ready = false;
   int8_t *d_plA = nullptr, *d_plB = nullptr, *d_plS = nullptr;  // C0, C2, small-matrix digit planes
   double *d_sgA = nullptr, *d_sgB = nullptr, *d_sgS = nullptr;  // their row (column) scales
   double *d_sgpart = nullptr;
@@ -159,6 +159,7 @@ struct amdk_ctx {
   int *d_sgerr = nullptr;
   long sg_kpad = 0;
   int sg_ktiles = 0, sg_per = 0, sg_chunks = 0, sg_mtiles = 0;
+  void *sg_c0_buf = nullptr;  // the C0 buffer whose digit planes are in d_plA (written by the ortho)
   CUtensorMap tm_a_tn, tm_b_tn, tm_a_nn, tm_s_nn;
   bool warm[2] = {false, false};  // an eager iteration has run at this pair precision
   void *c0_first = nullptr;       // the buffer that held C0 at creation
@@ -843,8 +844,8 @@ static int sg_encode(CUtensorMap *m, void *base, long kdim, int box_x, CUtensorM
 }
 static int sg_setup(amdk_ctx *c) {
   const HostSetup &h = c->hs;
-  const char *ns = getenv("AMDK_SLICE");
-  c->slice_gemm = ns && ns[0] == '1';
+  const char *ns = getenv("AMDK_NO_SLICE");
+  c->slice_gemm = !(ns && ns[0] == '1');
   if (h.nstate > SG_M) return 0;
   const long K = 2L * h.ngpw;
   c->sg_kpad = (K + SG_M - 1) / SG_M * SG_M;
@@ -868,7 +869,9 @@ static int sg_setup(amdk_ctx *c) {
   RC(sg_encode(&c->tm_a_nn, c->d_plA, c->sg_kpad, SG_M, CU_TENSOR_MAP_SWIZZLE_128B));
   RC(sg_encode(&c->tm_s_nn, c->d_plS, SG_M, SG_M, CU_TENSOR_MAP_SWIZZLE_128B));
   CK(cudaFuncSetAttribute(k_sgemm_tn<SG_S>, cudaFuncAttributeMaxDynamicSharedMemorySize, SgTn<SG_S>::SMEM));
-  CK(cudaFuncSetAttribute(k_sgemm_nn<SG_S>, cudaFuncAttributeMaxDynamicSharedMemorySize, SgNn<SG_S>::SMEM));
+  CK(cudaFuncSetAttribute(k_sgemm_nn<SG_S, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, SgNn<SG_S>::SMEM));
+  CK(cudaFuncSetAttribute(k_sgemm_nn<SG_S, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, SgNn<SG_S>::SMEM));
+  CK(cudaFuncSetAttribute(k_sgemm_nn<SG_S, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, SgNn<SG_S>::SMEM));
   c->sg_ready = true;
   return 0;
 }
@@ -893,14 +896,27 @@ static void sg_tn(amdk_ctx *c, const CUtensorMap &ta, const CUtensorMap &tb, int
                                             alpha, out, n);
 }
 // out (the real view, 2 ngpw x n) = (or -=, sub) C0 B for B n x n, with C0's
-// planes and scales in d_plA / d_sgA
-static void sg_nn(amdk_ctx *c, const double *B, double2 *out, int sub) {
+// planes and scales in d_plA / d_sgA.  With digits (an orthonormalisation)
+// the result's own planes replace C0's in d_plA, scale 2 (|x| <= 1).
+static void sg_nn(amdk_ctx *c, const double *B, double2 *out, int sub, bool digits) {
   const int n = c->nstate;
   const long K = 2L * c->hs.ngpw;
   c->nlaunch += 2;
   k_slice_small<SG_S><<<SG_M, SG_M, 0, c->st>>>(B, n, n, n, c->d_sgA, c->d_plS, c->d_sgS);
-  k_sgemm_nn<SG_S><<<std::min(c->sg_mtiles, c->nsm), SG_NN_THREADS, SgNn<SG_S>::SMEM, c->st>>>(
-      c->tm_a_nn, c->tm_s_nn, c->sg_mtiles, K, (double *)out, K, n, c->d_sgS, sub, c->d_sgerr);
+  const dim3 grid(std::min(c->sg_mtiles, c->nsm));
+  if (sub)
+    k_sgemm_nn<SG_S, 1><<<grid, SG_NN_THREADS, SgNn<SG_S>::SMEM, c->st>>>(
+        c->tm_a_nn, c->tm_s_nn, c->sg_mtiles, K, (double *)out, K, n, c->d_sgS, nullptr, c->sg_kpad, c->d_sgerr);
+  else if (digits)
+    k_sgemm_nn<SG_S, 2><<<grid, SG_NN_THREADS, SgNn<SG_S>::SMEM, c->st>>>(
+        c->tm_a_nn, c->tm_s_nn, c->sg_mtiles, K, (double *)out, K, n, c->d_sgS, c->d_plA, c->sg_kpad, c->d_sgerr);
+  else
+    k_sgemm_nn<SG_S, 0><<<grid, SG_NN_THREADS, SgNn<SG_S>::SMEM, c->st>>>(
+        c->tm_a_nn, c->tm_s_nn, c->sg_mtiles, K, (double *)out, K, n, c->d_sgS, nullptr, c->sg_kpad, c->d_sgerr);
+  if (digits) {
+    ++c->nlaunch;
+    k_sg_fill<<<1, SG_M, 0, c->st>>>(c->d_sgA, n, 2.0);
+  }
 }
 
 static int do_gradient(amdk_ctx *c) {
@@ -910,7 +926,8 @@ static int do_gradient(amdk_ctx *c) {
   const bool sl = use_slice(c);
   if (sl) {
     sg_slice(c, c->d_c2, c->d_plB, c->d_sgB);
-    sg_slice(c, c->d_c0, c->d_plA, c->d_sgA);
+    // C0's planes are those the last orthonormalisation wrote, if C0 has not changed since
+    if (c->sg_c0_buf != (void *)c->d_c0) sg_slice(c, c->d_c0, c->d_plA, c->d_sgA);
     sg_tn(c, c->tm_b_tn, c->tm_a_tn, 0, c->d_sgB, c->d_sgA, 2.0, c->d_gam);
   } else {
     CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, (const double *)c->d_c2, K,
@@ -919,7 +936,7 @@ static int do_gradient(amdk_ctx *c) {
   ++c->nlaunch;
   k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c2, c->d_c0, c->d_gam, c->d_occ, 1, 0);
   if (sl)
-    sg_nn(c, c->d_gam, c->d_c2, 1);
+    sg_nn(c, c->d_gam, c->d_c2, 1, false);
   else
     CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &mone, (const double *)c->d_c0, K, c->d_gam, n, &one,
                    (double *)c->d_c2, K));
@@ -940,6 +957,7 @@ static int do_gradient(amdk_ctx *c) {
 // so that a captured graph of this step reads the current one
 static int do_pcg(amdk_ctx *c, int istep) {
   const HostSetup &h = c->hs;
+  c->sg_c0_buf = nullptr;  // C0 changes in place
   c->h_pin[S_NSCAL + 1] = (double)istep;
   CK(cudaMemcpyAsync(c->d_scal + S_ISTEP, c->h_pin + S_NSCAL + 1, sizeof(double), cudaMemcpyHostToDevice, c->st));
   int n = c->nstate, nocc = 0;
@@ -1012,13 +1030,15 @@ static int do_ortho(amdk_ctx *c, bool check = true, bool swap = true) {
   // C0 <- C0 U^{-1} (DTRMM, wfn_initialize.f90:485) out of place into the
   // spare buffer (ZCLEAN there), then the buffers swap roles
   if (sl)
-    sg_nn(c, c->d_uinv, c->d_cp, 0);
+    sg_nn(c, c->d_uinv, c->d_cp, 0, true);
   else
     CB(cublasDtrmm(c->cb, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, K, n, &one,
                    c->d_uinv, n, (const double *)c->d_c0, K, (double *)c->d_cp, K));
   ++c->nlaunch;
   k_zclean<<<nblk(n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_cp);
   if (swap) std::swap(c->d_c0, c->d_cp);
+  // the buffer whose digit planes d_plA holds (set again after a replayed graph)
+  c->sg_c0_buf = sl ? (void *)(swap ? c->d_c0 : c->d_cp) : nullptr;
   CK(cudaGetLastError());
   return 0;
 }
@@ -1704,6 +1724,7 @@ int amdk_set_wfn(amdk_ctx *c, const double *c0) {
   if (!c || !c0) return AMDK_ERR_BADARG;
   cudaSetDevice(c->device);
   CK(cudaMemcpy(c->d_c0, c0, sizeof(double2) * (size_t)c->hs.ngpw * c->nstate, cudaMemcpyHostToDevice));
+  c->sg_c0_buf = nullptr;
   return 0;
 }
 
@@ -1778,7 +1799,8 @@ int amdk_scf_iteration(amdk_ctx *c, int istep, double gcut, amdk_energies *e, do
     CK(cudaMemcpyAsync(c->h_pin + S_NSCAL, c->d_scal + S_GMAX, sizeof(double), cudaMemcpyDeviceToHost, c->st));
     return 0;
   };
-  if (graph) RC(run_segment(c, {0, q, parity, c->prof ? 1 : 0}, seg_a));
+  const int c0_digits = (use_slice(c) && c->sg_c0_buf == (void *)c->d_c0) ? 1 : 0;
+  if (graph) RC(run_segment(c, {0, q + 2 * c0_digits, parity, c->prof ? 1 : 0}, seg_a));
   else RC(seg_a());
   // GEMAX decides CHK_TFOR (forces or not) before PCG: the one host sync
   // inside the iteration
@@ -1801,6 +1823,7 @@ int amdk_scf_iteration(amdk_ctx *c, int istep, double gcut, amdk_energies *e, do
   };
   if (graph) RC(run_segment(c, {1, tfor ? 1 : 0, parity, c->prof ? 1 : 0}, seg_b));
   else RC(seg_b());
+  c->sg_c0_buf = use_slice(c) ? (void *)c->d_cp : nullptr;  // the ortho's output (digits written)
   std::swap(c->d_c0, c->d_cp);  // ortho's output buffer holds C0 now
   cudaEventRecord(c->ev1, c->st);
   CK(cudaEventSynchronize(c->ev1));
@@ -1884,6 +1907,7 @@ int amdk_wfn_extrapolate(amdk_ctx *c) {
     c->nhist = slots;
   }
   if (np > 1) std::swap(c->d_c0, c->d_cp);
+  c->sg_c0_buf = nullptr;
   CK(cudaStreamSynchronize(c->st));
   return 0;
 }

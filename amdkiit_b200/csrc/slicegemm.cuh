@@ -10,7 +10,8 @@
 // that |x| / sigma_r < 1/2, rounded to the fixed-point integer
 // v = rint(x / sigma_r 2^{7S}) (|v| <= 2^{7S-1}) and cut into S balanced
 // base-128 digits,
-//   x / sigma_r = sum_t d_t 2^{-7(t+1)} + O(2^{-7S}),  d_t in [-64, 64].  A product of two rows is
+//   x / sigma_r = sum_t d_t 2^{-7(t+1)} + O(2^{-7S}),  d_t in [-64, 64].
+// A product of two rows is
 //   sum_k x_k y_k = sigma_x sigma_y sum_{t,u} 2^{-7(t+u+2)} sum_k dx_t dy_u,
 // whose inner sums are exact int8 x int8 -> int32 tensor-core products; the
 // terms with t + u >= S are dropped (relative truncation ~2^{-7S}), and the
@@ -113,18 +114,22 @@ __device__ __forceinline__ void sg_mma_i8(uint32_t dtm, uint64_t adesc, uint64_t
 __device__ __forceinline__ void sg_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
-// 32 consecutive 32-bit columns of this thread's TMEM lane
-__device__ __forceinline__ void sg_tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+// 16 consecutive 32-bit columns of this thread's TMEM lane; the registers
+// are valid after sg_tmem_wait_ld (several loads may share one wait)
+__device__ __forceinline__ void sg_tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+      "[%16];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
-        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
+__device__ __forceinline__ void sg_tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+}
+__device__ __forceinline__ void sg_tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // Shared-memory matrix descriptor (tcgen05): start address, leading and
 // stride byte offsets (16-byte units), version 1, layout (2 = 128-byte
@@ -278,6 +283,11 @@ __global__ void __launch_bounds__(SG_M) k_slice_small(const double *__restrict__
   for (int t = 0; t < S; ++t) planes[(long)t * SG_M * SG_M + n * SG_M + k] = (int8_t)d[t];
 }
 
+__global__ void k_sg_fill(double *__restrict__ s, int n, double v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) s[i] = v;
+}
+
 // ------------------------------------------------------------------ TN GEMM
 template <int S> struct SgTn {
   static constexpr int PLANE = SG_M * SG_TN_KT;  // 8 KB: 128 rows x 64 bytes
@@ -362,25 +372,27 @@ __global__ void __launch_bounds__(128, 1) k_sgemm_tn(const __grid_constant__ CUt
   sg_fence_after();
   const int m = 32 * warp + lane;
   double *out = partial + (long)blockIdx.x * SG_M * SG_M;
-  for (int cb = 0; cb < SG_M / 32; ++cb) {
-    double v[32];
+  for (int cb = 0; cb < SG_M / 16; ++cb) {
+    double v[16];
 #pragma unroll
-    for (int j = 0; j < 32; ++j) v[j] = 0.0;
+    for (int j = 0; j < 16; ++j) v[j] = 0.0;
     if (ok) {
-#pragma unroll 1
+      uint32_t r[S][16];
+#pragma unroll
+      for (int d = 0; d < S; ++d) sg_tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * SG_M + 16 * cb), r[d]);
+      sg_tmem_wait_ld();
+#pragma unroll
       for (int d = 0; d < S; ++d) {
-        uint32_t r[32];
-        sg_tmem_ld32(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * SG_M + 32 * cb), r);
         const double w = sg_weight(d);
 #pragma unroll
-        for (int j = 0; j < 32; ++j) v[j] += (double)(int)r[j] * w;
+        for (int j = 0; j < 16; ++j) v[j] += (double)(int)r[d][j] * w;
       }
     } else if (nt > 0) {
 #pragma unroll
-      for (int j = 0; j < 32; ++j) v[j] = __longlong_as_double(0x7ff8000000000000LL);
+      for (int j = 0; j < 16; ++j) v[j] = __longlong_as_double(0x7ff8000000000000LL);
     }
 #pragma unroll
-    for (int j = 0; j < 32; ++j) out[(cb * 32 + j) * SG_M + m] = v[j];
+    for (int j = 0; j < 16; ++j) out[(cb * 16 + j) * SG_M + m] = v[j];
   }
   sg_fence_before();
   __syncthreads();
@@ -420,20 +432,27 @@ template <int S> struct SgNn {
   static constexpr int PLANE = SG_M * SG_M;  // 16 KB: 128 x 128 bytes
   static constexpr int SMEM = S * PLANE + SG_NN_ST * S * PLANE + 1024 + 256;
 };
-// out[m + ldo n] (=, or -= when sub) colscale[n] sum_{t+u<S} 2^{-7(t+u+2)}
+// out[m + ldo n] (=, or -= for MODE 1) colscale[n] sum_{t+u<S} 2^{-7(t+u+2)}
 //   sum_k dA_t[k][m] dB_u[n][k]   for m < mreal, n < nn,
 // A planes [t][k][m] (MN-major tiles of 128 m x 128 k), B planes [t][n][k].
-// Persistent: CTA b takes the 128-row tiles b, b + grid, ...  block 320:
+// Persistent: CTA b takes the 128-row tiles b, b + grid, ...  block 576:
 // warp 0 loads, warp 1 issues the MMAs (and owns the tensor memory), warps
-// 2-9 read the accumulators back (TMEM lanes 32 (w % 4) ..., columns
-// 64 ((w - 2) / 4) ...) and stream the FP64 result out, the old values of a
-// subtraction loaded before the accumulators are read.
-constexpr int SG_NN_THREADS = 320;
-template <int S>
+// 2-17 read the accumulators back (TMEM lanes 32 (w % 4) ..., columns
+// 32 ((w - 2) / 4) ...), 8 columns at a time with one TMEM wait for the S
+// accumulators, which are combined exactly in 64-bit integers
+// (sum_d acc_d 128^{S-1-d}, below 2^45) and converted once; the old values of
+// a subtraction are loaded before the accumulators are read.  MODE 0 stores,
+// 1 subtracts, 2 stores and also cuts the result into the S digit planes
+// dig[t][n][m] with the fixed scale sigma = 2 (an orthonormalisation: its
+// output bands satisfy |x| <= 1), ready as the next product's operand,
+// setting its real index 1 (Im c(G=0)) to zero as ZCLEAN does.
+constexpr int SG_NN_THREADS = 576;
+template <int S, int MODE>
 __global__ void __launch_bounds__(SG_NN_THREADS, 1) k_sgemm_nn(const __grid_constant__ CUtensorMap ta,
                                                      const __grid_constant__ CUtensorMap tb, int mtiles, long mreal,
                                                      double *__restrict__ out, long ldo, int nn,
-                                                     const double *__restrict__ colscale, int sub, int *err) {
+                                                     const double *__restrict__ colscale,
+                                                     int8_t *__restrict__ dig, long kpad, int *err) {
   using G = SgNn<S>;
   extern __shared__ unsigned char sg_raw[];
   unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sg_raw) + 1023) & ~uintptr_t(1023));
@@ -447,6 +466,8 @@ __global__ void __launch_bounds__(SG_NN_THREADS, 1) k_sgemm_nn(const __grid_cons
   const uint32_t tfull = sg_smem(bars + 1 + 2 * SG_NN_ST), tfree = sg_smem(bars + 2 + 2 * SG_NN_ST);
   const uint32_t fin = sg_smem(bars + 3 + 2 * SG_NN_ST);
   const int nq = blockIdx.x < mtiles ? (mtiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  __shared__ double cs[SG_M];  // colscale 2^{-7(S+1)}
+  for (int i = threadIdx.x; i < SG_M; i += blockDim.x) cs[i] = i < nn ? ldexp(colscale[i], -7 * (S + 1)) : 0.0;
   if (threadIdx.x == 0) {
     sg_bar_init(bfull, 1);
     for (int i = 0; i < SG_NN_ST; ++i) {
@@ -454,7 +475,7 @@ __global__ void __launch_bounds__(SG_NN_THREADS, 1) k_sgemm_nn(const __grid_cons
       sg_bar_init(empty0 + 8 * i, 1);
     }
     sg_bar_init(tfull, 1);
-    sg_bar_init(tfree, 8);
+    sg_bar_init(tfree, (SG_NN_THREADS - 64) / 32);
     sg_bar_init(fin, 1);
     sg_bar_fence_init();
   }
@@ -507,42 +528,53 @@ __global__ void __launch_bounds__(SG_NN_THREADS, 1) k_sgemm_nn(const __grid_cons
     sg_commit(fin);
     sg_bar_wait(fin, 0, err, 16);  // every MMA of this block has finished
   } else if (warp >= 2) {
-    const int ew = warp & 3, half = (warp - 2) >> 2;
+    const int ew = warp & 3, cg = (warp - 2) >> 2;
     const int m = 32 * ew + lane;
     for (int q = 0; q < nq; ++q) {
       const bool ok = __all_sync(0xffffffffu, sg_bar_wait(tfull, q & 1, err, 15));
       sg_fence_after();
       const long gm = (long)(blockIdx.x + q * gridDim.x) * SG_M + m;
-      for (int cb = 2 * half; cb < 2 * half + 2; ++cb) {
-        double old[32];
-        if (sub && gm < mreal) {
-#pragma unroll
-          for (int j = 0; j < 32; ++j) old[j] = (32 * cb + j < nn) ? out[(long)(32 * cb + j) * ldo + gm] : 0.0;
-        }
-        double v[32];
-        if (ok) {
-#pragma unroll
-          for (int j = 0; j < 32; ++j) v[j] = 0.0;
+      const bool row_ok = gm < mreal;
 #pragma unroll 1
-          for (int d = 0; d < S; ++d) {
-            uint32_t r[32];
-            sg_tmem_ld32(tbase + ((uint32_t)(32 * ew) << 16) + (uint32_t)(d * SG_M + 32 * cb), r);
-            const double w = sg_weight(d);
+      for (int cb = 4 * cg; cb < 4 * cg + 4; ++cb) {
+        double old[8];
+        if (MODE == 1 && row_ok) {
 #pragma unroll
-            for (int j = 0; j < 32; ++j) v[j] += (double)(int)r[j] * w;
+          for (int j = 0; j < 8; ++j) old[j] = (8 * cb + j < nn) ? out[(long)(8 * cb + j) * ldo + gm] : 0.0;
+        }
+        double v[8];
+        if (ok) {
+          uint32_t r[S][8];
+#pragma unroll
+          for (int d = 0; d < S; ++d) sg_tmem_ld8(tbase + ((uint32_t)(32 * ew) << 16) + (uint32_t)(d * SG_M + 8 * cb), r[d]);
+          sg_tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            long long t = (int)r[0][j];
+#pragma unroll
+            for (int d = 1; d < S; ++d) t = t * 128 + (int)r[d][j];
+            v[j] = (double)t * cs[8 * cb + j];
           }
         } else {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) v[j] = __longlong_as_double(0x7ff8000000000000LL);
+          for (int j = 0; j < 8; ++j) v[j] = __longlong_as_double(0x7ff8000000000000LL);
         }
-        if (gm < mreal) {
+        if (row_ok) {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int n = 32 * cb + j;
-            if (n < nn) {
-              const double val = v[j] * colscale[n];
-              out[(long)n * ldo + gm] = sub ? old[j] - val : val;
+          for (int j = 0; j < 8; ++j) {
+            const int n = 8 * cb + j;
+            double val = v[j];
+            if (MODE == 1) val = old[j] - val;
+            if (MODE == 2) {
+              val = (gm == 1) ? 0.0 : val;
+              int dd[S];
+              sg_digits<S>(val * (double)(1 << (7 * S - 1)), dd);
+              if (n < nn) {
+#pragma unroll
+                for (int t = 0; t < S; ++t) dig[((long)t * SG_M + n) * kpad + gm] = (int8_t)dd[t];
+              }
             }
+            if (n < nn) out[(long)n * ldo + gm] = val;
           }
         }
       }

@@ -22,11 +22,11 @@ def rel(a, b):
 
 
 def engines(system, monkeypatch, prec=MIXED):
-    monkeypatch.delenv("AMDK_SLICE", raising=False)
+    """(DGEMM engine, slice-GEMM engine, the default) on the same start."""
+    monkeypatch.setenv("AMDK_NO_SLICE", "1")
     ref = Engine(system, prec)
-    monkeypatch.setenv("AMDK_SLICE", "1")
+    monkeypatch.delenv("AMDK_NO_SLICE")
     e = Engine(system, prec)
-    monkeypatch.delenv("AMDK_SLICE")
     g = ref.gvectors()
     c = start_coefficients(g["hg"][: ref.ngpw], 2 * np.pi / system.alat, ref.nstate, 5)
     for x in (ref, e):
