@@ -890,7 +890,7 @@ static void sg_tn(amdk_ctx *c, const CUtensorMap &ta, const CUtensorMap &tb, int
                   const double *sb, double alpha, double *out) {
   const int n = c->nstate;
   c->nlaunch += 2;
-  k_sgemm_tn<SG_S><<<c->sg_chunks, 128, SgTn<SG_S>::SMEM, c->st>>>(ta, tb, same, c->sg_ktiles, c->sg_per, c->d_sgpart,
+  k_sgemm_tn<SG_S><<<c->sg_chunks, SG_TN_THREADS, SgTn<SG_S>::SMEM, c->st>>>(ta, tb, same, c->sg_ktiles, c->sg_per, c->d_sgpart,
                                                                      c->d_sgerr);
   k_sgemm_reduce<<<n, 4 * SG_M, 0, c->st>>>(c->sg_chunks, c->d_sgpart, n, sa, sb, same ? c->d_sgnsq : nullptr,
                                             alpha, out, n);

@@ -335,8 +335,13 @@ __global__ void k_rho_reduce_p(int n, int n1f, int n2f, int ngroups, const doubl
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
     const int kx = kx0 + j, k = k0 + threadIdx.x;
     double s = 0.0;
-    if (kx < n && k < n)
-      for (int g = 0; g < ngroups; ++g) s += part[g * gstride + ((long)kx * n + q) * n + k];
+    if (kx < n && k < n) {
+      const double *pp = part + ((long)kx * n + q) * n + k;
+      // the loads are independent: unrolled, several are in flight while the
+      // sum keeps its group order
+#pragma unroll 8
+      for (int g = 0; g < ngroups; ++g) s += pp[g * gstride];
+    }
     tile[j][threadIdx.x] = s;
   }
   __syncthreads();

@@ -144,7 +144,6 @@ __device__ __forceinline__ uint64_t sg_desc(uint32_t addr, uint32_t lbo, uint32_
 __host__ __device__ constexpr uint32_t sg_idesc(bool a_mn) {
   return (2u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
 }
-__device__ __forceinline__ double sg_weight(int d) { return ldexp(1.0, -7 * (d + 2)); }
 
 // ---------------------------------------------------------------- slicing
 // S balanced base-128 digits of y = x 2^{7S} / sigma (|y| < 2^{7S-1}), most
@@ -296,22 +295,29 @@ template <int S> struct SgTn {
 };
 // partial[chunk][n][m] = sum over the chunk's k of
 //   sum_{t+u<S} 2^{-7(t+u+2)} dA_t[m][k] dB_u[n][k]
-// (same != 0: B = A, loaded once).  grid = chunks, block 128.
+// (same != 0: B = A, loaded once).  grid = chunks, block SG_TN_THREADS:
+// thread 0 loads, thread 32 issues the MMAs, all eight warps read the
+// accumulators back (TMEM lanes 32 (w % 4) ..., columns 64 (w / 4) ...) and
+// combine them exactly in 64-bit integers.
+constexpr int SG_TN_THREADS = 256;
 template <int S>
-__global__ void __launch_bounds__(128, 1) k_sgemm_tn(const __grid_constant__ CUtensorMap ta,
+__global__ void __launch_bounds__(SG_TN_THREADS, 1) k_sgemm_tn(const __grid_constant__ CUtensorMap ta,
                                                      const __grid_constant__ CUtensorMap tb, int same, int ktiles,
                                                      int per_cta, double *__restrict__ partial, int *err) {
   using G = SgTn<S>;
   extern __shared__ unsigned char sg_raw[];
   unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sg_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t *bars = reinterpret_cast<uint64_t *>(base + SG_TN_ST * G::STAGE);  // full[ST], empty[ST], done
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * SG_TN_ST + 1);
+  // a Gram product (same) stages A alone, so twice as many stages fit
+  const int nst = same ? 2 * SG_TN_ST : SG_TN_ST;
+  const int sbytes = (same ? 1 : 2) * S * G::PLANE;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(base + SG_TN_ST * G::STAGE);  // full[2 ST], empty[2 ST], done
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 4 * SG_TN_ST + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int kt0 = blockIdx.x * per_cta;
   const int nt = max(0, min(per_cta, ktiles - kt0));
-  const uint32_t full0 = sg_smem(bars), empty0 = sg_smem(bars + SG_TN_ST), done = sg_smem(bars + 2 * SG_TN_ST);
+  const uint32_t full0 = sg_smem(bars), empty0 = sg_smem(bars + 2 * SG_TN_ST), done = sg_smem(bars + 4 * SG_TN_ST);
   if (threadIdx.x == 0) {
-    for (int i = 0; i < SG_TN_ST; ++i) {
+    for (int i = 0; i < 2 * SG_TN_ST; ++i) {
       sg_bar_init(full0 + 8 * i, 1);
       sg_bar_init(empty0 + 8 * i, 1);
     }
@@ -323,16 +329,16 @@ __global__ void __launch_bounds__(128, 1) k_sgemm_tn(const __grid_constant__ CUt
   __syncthreads();
   sg_fence_after();
   const uint32_t tbase = *tslot;
-  const uint32_t bytes = (same ? 1u : 2u) * S * G::PLANE;
+  const uint32_t bytes = (uint32_t)sbytes;
   if (threadIdx.x == 0 && nt > 0) {
     // producer: TMA of the S planes of A (and B) for each k tile
     int issued = 0;
     for (int i = 0; i < nt; ++i) {
-      const int s = i % SG_TN_ST;
-      if (i >= SG_TN_ST && !sg_bar_wait(empty0 + 8 * s, ((i / SG_TN_ST) - 1) & 1, err, 1)) break;
+      const int s = i % nst;
+      if (i >= nst && !sg_bar_wait(empty0 + 8 * s, ((i / nst) - 1) & 1, err, 1)) break;
       const uint32_t fb = full0 + 8 * s;
       sg_bar_expect_tx(fb, bytes);
-      const uint32_t dA = sg_smem(base + s * G::STAGE), dB = dA + S * G::PLANE;
+      const uint32_t dA = sg_smem(base + s * sbytes), dB = dA + S * G::PLANE;
       const int kx = (kt0 + i) * SG_TN_KT;
 #pragma unroll
       for (int t = 0; t < S; ++t) sg_tma_2d(dA + t * G::PLANE, &ta, kx, t * SG_M, fb);
@@ -342,15 +348,15 @@ __global__ void __launch_bounds__(128, 1) k_sgemm_tn(const __grid_constant__ CUt
       issued = i + 1;
     }
     // the copies in flight land before the block can leave
-    for (int i = max(0, issued - SG_TN_ST); i < issued; ++i) sg_bar_wait(full0 + 8 * (i % SG_TN_ST), (i / SG_TN_ST) & 1, err, 4);
+    for (int i = max(0, issued - nst); i < issued; ++i) sg_bar_wait(full0 + 8 * (i % nst), (i / nst) & 1, err, 4);
   } else if (threadIdx.x == 32 && nt > 0) {
     // MMA issuer
     constexpr uint32_t idesc = sg_idesc(false);
     for (int i = 0; i < nt; ++i) {
-      const int s = i % SG_TN_ST;
-      if (!sg_bar_wait(full0 + 8 * s, (i / SG_TN_ST) & 1, err, 2)) break;
+      const int s = i % nst;
+      if (!sg_bar_wait(full0 + 8 * s, (i / nst) & 1, err, 2)) break;
       sg_fence_after();
-      const uint32_t aA = sg_smem(base + s * G::STAGE), aB = same ? aA : aA + S * G::PLANE;
+      const uint32_t aA = sg_smem(base + s * sbytes), aB = same ? aA : aA + S * G::PLANE;
 #pragma unroll
       for (int t = 0; t < S; ++t)
 #pragma unroll
@@ -367,25 +373,28 @@ __global__ void __launch_bounds__(128, 1) k_sgemm_tn(const __grid_constant__ CUt
     sg_bar_wait(done, 0, err, 5);  // every MMA of this block has finished
   }
   __syncwarp();
-  // epilogue: lane m of warp w holds row m = 32 w + lane of every accumulator
+  // epilogue: lane m of warp w holds row m = 32 (w % 4) + lane of every accumulator
   const bool ok = __all_sync(0xffffffffu, nt > 0 && sg_bar_wait(done, 0, err, 3));
   sg_fence_after();
-  const int m = 32 * warp + lane;
+  const int ew = warp & 3, half = warp >> 2;
+  const int m = 32 * ew + lane;
+  const double w0 = ldexp(1.0, -7 * (S + 1));
   double *out = partial + (long)blockIdx.x * SG_M * SG_M;
-  for (int cb = 0; cb < SG_M / 16; ++cb) {
+  for (int cb = 4 * half; cb < 4 * half + 4; ++cb) {
     double v[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) v[j] = 0.0;
     if (ok) {
       uint32_t r[S][16];
 #pragma unroll
-      for (int d = 0; d < S; ++d) sg_tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * SG_M + 16 * cb), r[d]);
+      for (int d = 0; d < S; ++d) sg_tmem_ld16(tbase + ((uint32_t)(32 * ew) << 16) + (uint32_t)(d * SG_M + 16 * cb), r[d]);
       sg_tmem_wait_ld();
 #pragma unroll
-      for (int d = 0; d < S; ++d) {
-        const double w = sg_weight(d);
+      for (int j = 0; j < 16; ++j) {
+        long long t = (int)r[0][j];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] += (double)(int)r[d][j] * w;
+        for (int d = 1; d < S; ++d) t = t * 128 + (int)r[d][j];
+        v[j] = (double)t * w0;
       }
     } else if (nt > 0) {
 #pragma unroll
