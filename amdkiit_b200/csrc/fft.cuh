@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(256) k_x_bwd_field(const double2 *__restrict__
   load_tw<C, N>(tw, p);
   const long line0 = (long)blockIdx.x * LX;
   const long nlines = (long)T * R;
-  for (int idx = threadIdx.x; idx < LX * n1; idx += blockDim.x) {
+  auto gather = [&](int idx) {
     const int l = idx / n1, k = idx % n1;
     const long line = line0 + l;
     C v = czero<C>();
@@ -460,7 +460,24 @@ __global__ void __launch_bounds__(256) k_x_bwd_field(const double2 *__restrict__
         v = mk((decltype(v.x))a.x, (decltype(v.x))a.y);
       }
     }
-    sa[k * es + l] = v;
+    return v;
+  };
+  if constexpr (N > 0) {
+    // all of a thread's gathers in flight at once (256 threads per block)
+    constexpr int CNT = (LX * N + 255) / 256;
+    C v[CNT];
+#pragma unroll
+    for (int i = 0; i < CNT; ++i) {
+      const int idx = threadIdx.x + 256 * i;
+      v[i] = idx < LX * N ? gather(idx) : czero<C>();
+    }
+#pragma unroll
+    for (int i = 0; i < CNT; ++i) {
+      const int idx = threadIdx.x + 256 * i;
+      if (idx < LX * N) sa[(idx % N) * es + idx / N] = v[i];
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < LX * n1; idx += blockDim.x) sa[(idx % n1) * es + idx / n1] = gather(idx);
   }
   __syncthreads();
   C *res = fft_tile<C, N, LX, LX + 1>(sa, sb, p, tw, +1);
@@ -513,7 +530,7 @@ __global__ void __launch_bounds__(256) k_y(int sphere, int dir, Geom g, Plan<C> 
   const int *ri = g.rayidx[sphere] + (long)zi * n2;
   C *R = rb + (long)t * rstride;
   C *S = sbuf + (long)t * sstride + (long)zi * n2 * n1;
-  for (int idx = threadIdx.x; idx < TX * n2; idx += blockDim.x) {
+  auto fetch = [&](int idx) {
     const int ky = idx / TX, tx = idx % TX, kx = kx0 + tx;
     C v = czero<C>();
     if (kx < n1) {
@@ -524,7 +541,24 @@ __global__ void __launch_bounds__(256) k_y(int sphere, int dir, Geom g, Plan<C> 
         v = S[(long)ky * n1 + kx];
       }
     }
-    sa[ky * TX + tx] = v;
+    return v;
+  };
+  if constexpr (N > 0) {
+    // all of a thread's loads in flight at once (256 threads per block)
+    constexpr int CNT = (TX * N + 255) / 256;
+    C v[CNT];
+#pragma unroll
+    for (int i = 0; i < CNT; ++i) {
+      const int idx = threadIdx.x + 256 * i;
+      v[i] = idx < TX * N ? fetch(idx) : czero<C>();
+    }
+#pragma unroll
+    for (int i = 0; i < CNT; ++i) {
+      const int idx = threadIdx.x + 256 * i;
+      if (idx < TX * N) sa[idx] = v[i];
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < TX * n2; idx += blockDim.x) sa[idx] = fetch(idx);
   }
   __syncthreads();
   C *res = fft_tile<C, N, TX, TX>(sa, sb, p, tw, dir);
@@ -574,11 +608,35 @@ __global__ void __launch_bounds__(256) k_z(int sphere, int T, Geom g, Plan<C> p,
   for (int t = tb; t < te; ++t) {
     C *S = sbuf + (long)t * sstride;
     if (MODE == Z_TO_GRID || MODE == Z_VPSI || MODE == Z_DENSITY) {
-      for (int idx = threadIdx.x; idx < TX * n3; idx += blockDim.x) sa[idx] = czero<C>();
-      __syncthreads();
-      for (int idx = threadIdx.x; idx < TX * nz; idx += blockDim.x) {
-        const int zi = idx / TX, tx = idx % TX, kx = kx0 + tx;
-        if (kx < n1) sa[zl[zi] * TX + tx] = S[(long)zi * plane + (long)ky * n1 + kx];
+      if constexpr (N > 0) {
+        // the slab loads are issued before the clearing barrier (256 threads per block)
+        constexpr int CNT = (TX * N + 255) / 256;
+        C v[CNT];
+        int dst[CNT];
+#pragma unroll
+        for (int i = 0; i < CNT; ++i) {
+          const int idx = threadIdx.x + 256 * i;
+          dst[i] = -1;
+          if (idx < TX * nz) {
+            const int zi = idx / TX, tx = idx % TX, kx = kx0 + tx;
+            if (kx < n1) {
+              v[i] = S[(long)zi * plane + (long)ky * n1 + kx];
+              dst[i] = zl[zi] * TX + tx;
+            }
+          }
+        }
+        for (int idx = threadIdx.x; idx < TX * n3; idx += blockDim.x) sa[idx] = czero<C>();
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < CNT; ++i)
+          if (dst[i] >= 0) sa[dst[i]] = v[i];
+      } else {
+        for (int idx = threadIdx.x; idx < TX * n3; idx += blockDim.x) sa[idx] = czero<C>();
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < TX * nz; idx += blockDim.x) {
+          const int zi = idx / TX, tx = idx % TX, kx = kx0 + tx;
+          if (kx < n1) sa[zl[zi] * TX + tx] = S[(long)zi * plane + (long)ky * n1 + kx];
+        }
       }
       __syncthreads();
       C *res = fft_tile<C, N, TX, TX>(sa, sb, p, tw, +1);
@@ -617,7 +675,7 @@ __global__ void __launch_bounds__(256) k_z(int sphere, int T, Geom g, Plan<C> p,
         __syncthreads();
       }
     } else {  // FROM_GRID
-      for (int idx = threadIdx.x; idx < TX * n3; idx += blockDim.x) {
+      auto fetch = [&](int idx) {
         const int kz = idx / TX, tx = idx % TX, kx = kx0 + tx;
         C v = czero<C>();
         if (kx < n1) {
@@ -625,7 +683,23 @@ __global__ void __launch_bounds__(256) k_z(int sphere, int T, Geom g, Plan<C> p,
           if (MODE == Z_FROM_GRID_REAL) v.x = (R)rgrid[o];
           else { double2 c = cgrid[o]; v.x = (R)c.x; v.y = (R)c.y; }
         }
-        sa[idx] = v;
+        return v;
+      };
+      if constexpr (N > 0) {
+        constexpr int CNT = (TX * N + 255) / 256;
+        C v[CNT];
+#pragma unroll
+        for (int i = 0; i < CNT; ++i) {
+          const int idx = threadIdx.x + 256 * i;
+          v[i] = idx < TX * N ? fetch(idx) : czero<C>();
+        }
+#pragma unroll
+        for (int i = 0; i < CNT; ++i) {
+          const int idx = threadIdx.x + 256 * i;
+          if (idx < TX * N) sa[idx] = v[i];
+        }
+      } else {
+        for (int idx = threadIdx.x; idx < TX * n3; idx += blockDim.x) sa[idx] = fetch(idx);
       }
       __syncthreads();
       C *res = fft_tile<C, N, TX, TX>(sa, sb, p, tw, -1);
