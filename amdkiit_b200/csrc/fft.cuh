@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(256) k_x_bwd_field(const double2 *__restrict__
                                                      int sphere, int T, Geom g, Plan<C> p, C *__restrict__ rb) {
   extern __shared__ unsigned char smraw[];
   C *sa = reinterpret_cast<C *>(smraw);
-  const int n1 = g.n1, R = g.nray[sphere];
+  const int n1 = g.n1, R = sphere ? g.nray[1] : g.nray[0];
   const int es = LX + 1;
   C *sb = sa + n1 * es;
   C *tw = sb + n1 * es;
@@ -493,7 +493,7 @@ template <typename C, int N = 0>
 __global__ void __launch_bounds__(256) k_x_fwd(int sphere, int T, Geom g, Plan<C> p, C *__restrict__ rb) {
   extern __shared__ unsigned char smraw[];
   C *sa = reinterpret_cast<C *>(smraw);
-  const int n1 = g.n1, R = g.nray[sphere];
+  const int n1 = g.n1, R = sphere ? g.nray[1] : g.nray[0];
   const int es = LX + 1;
   C *sb = sa + n1 * es;
   C *tw = sb + n1 * es;
@@ -522,12 +522,12 @@ __global__ void __launch_bounds__(256) k_y(int sphere, int dir, Geom g, Plan<C> 
                                            long rstride, long sstride) {
   extern __shared__ unsigned char smraw[];
   C *sa = reinterpret_cast<C *>(smraw);
-  const int n1 = g.n1, n2 = g.n2, nz = g.nz[sphere];
+  const int n1 = g.n1, n2 = g.n2, nz = sphere ? g.nz[1] : g.nz[0];
   C *sb = sa + n2 * TX;
   C *tw = sb + n2 * TX;
   load_tw<C, N>(tw, p);
   const int kx0 = blockIdx.x * TX, zi = blockIdx.y, t = blockIdx.z;
-  const int *ri = g.rayidx[sphere] + (long)zi * n2;
+  const int *ri = (sphere ? g.rayidx[1] : g.rayidx[0]) + (long)zi * n2;
   C *R = rb + (long)t * rstride;
   C *S = sbuf + (long)t * sstride + (long)zi * n2 * n1;
   auto fetch = [&](int idx) {
@@ -593,12 +593,12 @@ __global__ void __launch_bounds__(256) k_z(int sphere, int T, Geom g, Plan<C> p,
   typedef decltype(C().x) R;
   extern __shared__ unsigned char smraw[];
   C *sa = reinterpret_cast<C *>(smraw);
-  const int n1 = g.n1, n2 = g.n2, n3 = g.n3, nz = g.nz[sphere];
+  const int n1 = g.n1, n2 = g.n2, n3 = g.n3, nz = sphere ? g.nz[1] : g.nz[0];
   C *sb = sa + n3 * TX;
   C *tw = sb + n3 * TX;
   load_tw<C, N>(tw, p);
   const int kx0 = blockIdx.x * TX, ky = blockIdx.y;
-  const int *zl = g.zlist[sphere];
+  const int *zl = sphere ? g.zlist[1] : g.zlist[0];
   const long plane = (long)n2 * n1;
   double acc[16];  // TX*n3 <= 16*blockDim (checked at setup)
   if (MODE == Z_DENSITY)

@@ -593,10 +593,14 @@ __device__ __forceinline__ void warp_chol_inv16(double *D, int ld, int base, int
     const double inv = rsqrt(d);
     if (l == j) col[j] = d * inv;
     else if (l > j) col[j] *= inv;
+    // constant bounds: the loop unrolls and col[] stays in registers (a bound
+    // that depends on j left it in local memory, doubling the kernel's time)
 #pragma unroll
-    for (int a = j + 1; a < CHOL_B; ++a) {
-      const double uja = __shfl_sync(0xffffffffu, col[j], a);
-      if (l >= a) col[a] -= uja * col[j];
+    for (int a = 0; a < CHOL_B; ++a) {
+      if (a > j) {
+        const double uja = __shfl_sync(0xffffffffu, col[j], a);
+        if (l >= a) col[a] -= uja * col[j];
+      }
     }
   }
   if (own) {
@@ -610,7 +614,8 @@ __device__ __forceinline__ void warp_chol_inv16(double *D, int ld, int base, int
   for (int i = CHOL_B - 1; i >= 0; --i) {
     double t = 0.0;
 #pragma unroll
-    for (int k = i + 1; k < CHOL_B; ++k) t += D[i + ld * k] * x[k];
+    for (int k = 0; k < CHOL_B; ++k)
+      if (k > i) t += D[i + ld * k] * x[k];
     const double di = 1.0 / D[i + ld * i];
     x[i] = (i == l) ? di : ((i < l) ? -t * di : 0.0);
   }
