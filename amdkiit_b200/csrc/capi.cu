@@ -963,12 +963,12 @@ static int do_pcg(amdk_ctx *c, int istep) {
   int n = c->nstate, nocc = 0;
   for (int i = 0; i < n; i++)
     if (h.occ[i] > 1e-5) nocc++;
-  long tot = (long)h.ngpw * n;
   ++c->nlaunch;
-  k_precon<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngpw, n, nocc, c->d_vpp, c->d_occ, c->d_c2, c->d_cp, c->d_part);
+  k_precon<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngpw, n, nocc, c->d_vpp, c->d_occ, c->d_c2, c->d_part);
   RC(finish_sums(c, 1, S_GG));
   ++c->nlaunch;
-  k_pcg_update<<<RED_BLOCKS * 4, NTHR, 0, c->st>>>(tot, c->d_scal, c->d_cp, c->d_hnm1, c->d_c0);
+  k_pcg_update_c2<<<RED_BLOCKS * 4, NTHR, 0, c->st>>>(h.ngpw, n, c->d_scal, c->d_vpp, c->d_occ, c->d_c2, c->d_hnm1,
+                                                     c->d_c0);
   ++c->nlaunch;
   k_copy_scalar<<<1, 1, 0, c->st>>>(c->d_scal + S_GG, c->d_scal + S_GGPREV);
   CK(cudaGetLastError());

@@ -281,18 +281,23 @@ __device__ void xc_pz(double rho, double &e, double &v) {
   v = 4.0 / 3.0 * ex + (eps - rs / 3.0 * deps);
 }
 __device__ void xc_pbe(double rho, double sigma, double &e, double &v, double &vs) {
+  // PBE exchange and correlation (PW92 correlation, unpolarised); the
+  // reciprocals of rho and k_F are formed once and r_s = (9 pi/4)^(1/3) / k_F
   const double pi = 4.0 * atan(1.0), fp = 16.0 * atan(1.0);
   const double kappa = 0.804, mu = 0.2195149727645171, beta = 0.06672455060314922;
   const double gamma = (1.0 - log(2.0)) / (pi * pi);
+  const double ir = 1.0 / rho;
   double kf = cbrt(3.0 * pi * pi * rho);
+  const double ikf = 1.0 / kf;
   double exu = -3.0 / fp * kf * rho;
-  double s2 = sigma / (4.0 * kf * kf * rho * rho);
-  double den = 1.0 + mu * s2 / kappa;
-  double Fx = 1.0 + kappa - kappa / den, dF = mu / (den * den);
+  const double q4 = 0.25 * ikf * ikf * ir * ir;  // 1 / (4 kf^2 rho^2)
+  double s2 = sigma * q4;
+  const double iden = 1.0 / (1.0 + mu * s2 / kappa);
+  double Fx = 1.0 + kappa - kappa * iden, dF = mu * iden * iden;
   double ex = exu * Fx;
-  double vx = 4.0 / 3.0 * exu / rho * Fx + exu * dF * (-8.0 / 3.0 * s2 / rho);
-  double vsx = exu * dF / (4.0 * kf * kf * rho * rho);
-  double rs = cbrt(3.0 / (fp * rho));
+  double vx = 4.0 / 3.0 * exu * ir * Fx + exu * dF * (-8.0 / 3.0 * s2 * ir);
+  double vsx = exu * dF * q4;
+  double rs = 1.9191582926775128 * ikf;  // (9 pi / 4)^(1/3) / k_F
   const double A = 0.0310907, a1 = 0.21370, b1 = 7.5957, b2 = 3.5876, b3 = 1.6382, b4 = 0.49294;
   double sq = sqrt(rs);
   double q = 2.0 * A * (b1 * sq + b2 * rs + b3 * rs * sq + b4 * rs * rs);
@@ -300,19 +305,20 @@ __device__ void xc_pbe(double rho, double sigma, double &e, double &v, double &v
   double L = log(1.0 + 1.0 / q), dL = -dq / (q * q + q);
   double ec = -2.0 * A * (1.0 + a1 * rs) * L;
   double dec = -2.0 * A * a1 * L - 2.0 * A * (1.0 + a1 * rs) * dL;
-  double t2 = pi * sigma / (16.0 * kf * rho * rho);
-  double bg = beta / gamma, E = exp(-ec / gamma), AA = bg / (E - 1.0);
-  double At2 = AA * t2, num = 1.0 + At2, dd = 1.0 + At2 + At2 * At2;
-  double Q = t2 * num / dd;
+  double t2 = pi * sigma * 0.25 * q4 * kf;  // pi sigma / (16 kf rho^2)
+  double bg = beta / gamma, E = exp(-ec / gamma), iE1 = 1.0 / (E - 1.0), AA = bg * iE1;
+  double At2 = AA * t2, num = 1.0 + At2, idd = 1.0 / (1.0 + At2 + At2 * At2);
+  double Q = t2 * num * idd;
+  const double ibq = 1.0 / (1.0 + bg * Q);
   double H = gamma * log(1.0 + bg * Q);
-  double dHdQ = beta / (1.0 + bg * Q);
-  double dQdt2 = (num + t2 * AA) / dd - t2 * num * (AA + 2.0 * AA * AA * t2) / (dd * dd);
-  double dQdA = (t2 * t2) / dd - t2 * num * (t2 + 2.0 * AA * t2 * t2) / (dd * dd);
-  double dAdec = bg * E / (gamma * (E - 1.0) * (E - 1.0));
-  double decdrho = dec * (-rs / (3.0 * rho));
-  double dt2drho = -7.0 / 3.0 * t2 / rho;
+  double dHdQ = beta * ibq;
+  double dQdt2 = (num + t2 * AA) * idd - t2 * num * (AA + 2.0 * AA * AA * t2) * idd * idd;
+  double dQdA = (t2 * t2) * idd - t2 * num * (t2 + 2.0 * AA * t2 * t2) * idd * idd;
+  double dAdec = bg * E * iE1 * iE1 / gamma;
+  double decdrho = dec * (-rs * ir / 3.0);
+  double dt2drho = -7.0 / 3.0 * t2 * ir;
   double vc = ec + H + rho * (decdrho + dHdQ * dQdA * dAdec * decdrho + dHdQ * dQdt2 * dt2drho);
-  double vsc = rho * dHdQ * dQdt2 * pi / (16.0 * kf * rho * rho);
+  double vsc = rho * dHdQ * dQdt2 * pi * 0.25 * q4 * kf;
   e = ex + rho * (ec + H);
   v = vx + vc;
   vs = vsx + vsc;
@@ -520,9 +526,9 @@ __global__ void k_finish_max(const double *part, int nb, double *out) {
   if (threadIdx.x == 0) *out = sqrt(fmax(r, 0.0));  // partials hold |c2|^2
 }
 
-// PRECON + GGNORM (cg.f90:239-245, 419-449): cp = fi K c2; partial DOTP sums
+// PRECON + GGNORM (cg.f90:239-245, 419-449): partial DOTP sums of fi K c2
 __global__ void k_precon(int ngpw, int nstate, int nocc, const double *vpp, const double *occ, const double2 *c2,
-                         double2 *cp, double *part) {
+                         double *part) {
   __shared__ double sh[32];
   double s = 0;
   BandWalk w((long)ngpw * nstate, ngpw);
@@ -538,29 +544,44 @@ __global__ void k_precon(int ngpw, int nstate, int nocc, const double *vpp, cons
     const double f = fi * vpp[g];
     const double2 c = c2[w.k];
     const double2 v = make_double2(f * c.x, f * c.y);
-    cp[w.k] = v;
     if (b < nocc) s += (g == 0) ? v.x * v.x : 2.0 * (v.x * v.x + v.y * v.y);
   }
   double r = block_sum(s, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = r;
 }
-// PCG direction and step (cg.f90:247-281); scal[0] = ggnorm (new),
-// scal[1] = previous ggnorm, scal[8] = the CG step number;
-// gamma = forget * new/prev
-__global__ void k_pcg_update(long tot, const double *scal, double2 *cp, double2 *hnm1, double2 *c0) {
+// PCG direction and step (cg.f90:247-281) from C2 itself: the preconditioned
+// gradient K(G) C2 / f_i whose norm k_precon sums is formed again here
+// instead of being stored and read back (the same operations, so the same
+// values).  scal[0] = ggnorm (new), scal[1] = previous ggnorm, scal[8] = the
+// CG step number; gamma = forget * new/prev.
+__global__ void k_pcg_update_c2(int ngpw, int nstate, const double *scal, const double *vpp, const double *occ,
+                                const double2 *__restrict__ c2, double2 *__restrict__ hnm1, double2 *__restrict__ c0) {
   const int istep = (int)scal[8];
   double forget = istep <= 10 ? 0.60 : (istep <= 20 ? 0.91 : 0.95);
   double gamma = (istep == 1) ? 0.0 : forget * (scal[0] / scal[1]);
   const double dt = 5.0 * 5.0 / 400.0;
-  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < tot; k += (long)gridDim.x * blockDim.x) {
-    double2 d = cp[k];
-    if (istep > 1) {
-      d.x += gamma * hnm1[k].x;
-      d.y += gamma * hnm1[k].y;
+  BandWalk w((long)ngpw * nstate, ngpw);
+  int bf = -1;
+  double fi = 1.0;
+#pragma unroll 4
+  for (; w.k < w.k1; w.next(ngpw)) {
+    if (w.b != bf) {
+      bf = w.b;
+      fi = occ[w.b] > 0.01 ? 1.0 / occ[w.b] : 1.0;
     }
-    hnm1[k] = d;
-    c0[k].x += dt * d.x;
-    c0[k].y += dt * d.y;
+    const double f = fi * vpp[w.g];
+    const double2 c = c2[w.k];
+    double2 d = make_double2(f * c.x, f * c.y);
+    if (istep > 1) {
+      const double2 h = hnm1[w.k];
+      d.x += gamma * h.x;
+      d.y += gamma * h.y;
+    }
+    hnm1[w.k] = d;
+    double2 x = c0[w.k];
+    x.x += dt * d.x;
+    x.y += dt * d.y;
+    c0[w.k] = x;
   }
 }
 __global__ void k_copy_scalar(const double *src, double *dst) { *dst = *src; }
@@ -583,14 +604,16 @@ constexpr int CHOL_B = 16;
 __device__ __forceinline__ void warp_chol_inv16(double *D, int ld, int base, int *bad) {
   const int l = threadIdx.x & 31;
   const bool own = l < CHOL_B;
-  double col[CHOL_B];
+  double col[CHOL_B], invd[CHOL_B];  // invd[j] = 1 / U_jj, the same in every lane
+  int badj = 0;
 #pragma unroll
   for (int r = 0; r < CHOL_B; ++r) col[r] = own ? D[r + ld * l] : 0.0;
 #pragma unroll
   for (int j = 0; j < CHOL_B; ++j) {
     const double d = __shfl_sync(0xffffffffu, col[j], j);
-    if (!(d > 0.0) && l == 0 && *bad == 0) *bad = base + j + 1;
+    if (!(d > 0.0) && badj == 0) badj = base + j + 1;
     const double inv = rsqrt(d);
+    invd[j] = inv;
     if (l == j) col[j] = d * inv;
     else if (l > j) col[j] *= inv;
     // constant bounds: the loop unrolls and col[] stays in registers (a bound
@@ -603,6 +626,7 @@ __device__ __forceinline__ void warp_chol_inv16(double *D, int ld, int base, int
       }
     }
   }
+  if (l == 0 && badj && *bad == 0) *bad = badj;
   if (own) {
 #pragma unroll
     for (int r = 0; r < CHOL_B; ++r)
@@ -616,7 +640,7 @@ __device__ __forceinline__ void warp_chol_inv16(double *D, int ld, int base, int
 #pragma unroll
     for (int k = 0; k < CHOL_B; ++k)
       if (k > i) t += D[i + ld * k] * x[k];
-    const double di = 1.0 / D[i + ld * i];
+    const double di = invd[i];
     x[i] = (i == l) ? di : ((i < l) ? -t * di : 0.0);
   }
   __syncwarp();
@@ -648,8 +672,11 @@ __global__ void __launch_bounds__(CHOL_NT) k_chol_inv_s(int n, const double *A, 
     for (int p = 0; c0 + 32 * p < np; ++p) {
       const int c = c0 + hc + 32 * p;
       double t = 0.0;
-      if (c < np)
-        for (int s = 0; s <= hr; ++s) t += M[(k0 + s) + ld * (k0 + hr)] * M[(k0 + s) + ld * c];
+      if (c < np) {
+#pragma unroll
+        for (int s = 0; s < CHOL_B; ++s)  // constant bounds: the loads issue together
+          if (s <= hr) t += M[(k0 + s) + ld * (k0 + hr)] * M[(k0 + s) + ld * c];
+      }
       __syncwarp();
       if (c < np) M[(k0 + hr) + ld * c] = t;
       __syncwarp();
@@ -661,10 +688,13 @@ __global__ void __launch_bounds__(CHOL_NT) k_chol_inv_s(int n, const double *A, 
 #pragma unroll
       for (int s = 0; s < CHOL_B; ++s) uc[s] = M[(k0 + s) + ld * c];
       for (int r = c0 + lane; r <= c; r += 32) {
-        double t = 0.0;
+        double t0 = 0.0, t1 = 0.0;  // two chains of eight
 #pragma unroll
-        for (int s = 0; s < CHOL_B; ++s) t += M[(k0 + s) + ld * r] * uc[s];
-        M[r + ld * c] -= t;
+        for (int s = 0; s < CHOL_B; s += 2) {
+          t0 = fma(M[(k0 + s) + ld * r], uc[s], t0);
+          t1 = fma(M[(k0 + s + 1) + ld * r], uc[s + 1], t1);
+        }
+        M[r + ld * c] -= t0 + t1;
       }
     }
     __syncthreads();
@@ -679,8 +709,11 @@ __global__ void __launch_bounds__(CHOL_NT) k_chol_inv_s(int n, const double *A, 
     for (int p = 0; c0 + 32 * p < np; ++p) {
       const int c = c0 + hc + 32 * p;
       double t = 0.0;
-      if (c < np)
-        for (int s = hr; s < CHOL_B; ++s) t += M[(k0 + hr) + ld * (k0 + s)] * M[(k0 + s) + ld * c];
+      if (c < np) {
+#pragma unroll
+        for (int s = 0; s < CHOL_B; ++s)
+          if (s >= hr) t += M[(k0 + hr) + ld * (k0 + s)] * M[(k0 + s) + ld * c];
+      }
       __syncwarp();
       if (c < np) M[(k0 + hr) + ld * c] = t;
       __syncwarp();
@@ -696,9 +729,13 @@ __global__ void __launch_bounds__(CHOL_NT) k_chol_inv_s(int n, const double *A, 
 #pragma unroll
       for (int s = 0; s < CHOL_B; ++s) xc[s] = (s <= smax) ? M[(k0 + s) + ld * c] : 0.0;
       for (int i = lane; i < k0; i += 32) {
-        double t = 0.0;
+        double t0 = 0.0, t1 = 0.0;
 #pragma unroll
-        for (int s = 0; s < CHOL_B; ++s) t += Ut[s * np + i] * xc[s];
+        for (int s = 0; s < CHOL_B; s += 2) {
+          t0 = fma(Ut[s * np + i], xc[s], t0);
+          t1 = fma(Ut[(s + 1) * np + i], xc[s + 1], t1);
+        }
+        const double t = t0 + t1;
         M[i + ld * c] = (c < c0) ? -t : M[i + ld * c] - t;
       }
     }
