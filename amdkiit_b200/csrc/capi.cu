@@ -846,7 +846,9 @@ static int sg_setup(amdk_ctx *c) {
   const HostSetup &h = c->hs;
   const char *ns = getenv("AMDK_NO_SLICE");
   c->slice_gemm = !(ns && ns[0] == '1');
-  if (h.nstate > SG_M) return 0;
+  // below 64 bands the products are small and the slicing launches cost more
+  // than they save (water1: 4 bands, 3250 vs 3800 SCF iter/s)
+  if (h.nstate > SG_M || h.nstate < 64) return 0;
   const long K = 2L * h.ngpw;
   c->sg_kpad = (K + SG_M - 1) / SG_M * SG_M;
   c->sg_ktiles = (int)(c->sg_kpad / SG_TN_KT);
@@ -964,11 +966,11 @@ static int do_pcg(amdk_ctx *c, int istep) {
   for (int i = 0; i < n; i++)
     if (h.occ[i] > 1e-5) nocc++;
   ++c->nlaunch;
-  k_precon<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngpw, n, nocc, c->d_vpp, c->d_occ, c->d_c2, c->d_part);
+  k_precon<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngpw, n, nocc, c->d_vpp, c->d_occ, c->d_c2, c->d_cp, c->d_part);
   RC(finish_sums(c, 1, S_GG));
   ++c->nlaunch;
-  k_pcg_update_c2<<<RED_BLOCKS * 4, NTHR, 0, c->st>>>(h.ngpw, n, c->d_scal, c->d_vpp, c->d_occ, c->d_c2, c->d_hnm1,
-                                                     c->d_c0);
+  const long tot = (long)h.ngpw * n;
+  k_pcg_update<<<RED_BLOCKS * 4, NTHR, 0, c->st>>>(tot, c->d_scal, c->d_cp, c->d_hnm1, c->d_c0);
   ++c->nlaunch;
   k_copy_scalar<<<1, 1, 0, c->st>>>(c->d_scal + S_GG, c->d_scal + S_GGPREV);
   CK(cudaGetLastError());

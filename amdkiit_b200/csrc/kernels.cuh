@@ -526,9 +526,9 @@ __global__ void k_finish_max(const double *part, int nb, double *out) {
   if (threadIdx.x == 0) *out = sqrt(fmax(r, 0.0));  // partials hold |c2|^2
 }
 
-// PRECON + GGNORM (cg.f90:239-245, 419-449): partial DOTP sums of fi K c2
+// PRECON + GGNORM (cg.f90:239-245, 419-449): cp = fi K c2; partial DOTP sums
 __global__ void k_precon(int ngpw, int nstate, int nocc, const double *vpp, const double *occ, const double2 *c2,
-                         double *part) {
+                         double2 *cp, double *part) {
   __shared__ double sh[32];
   double s = 0;
   BandWalk w((long)ngpw * nstate, ngpw);
@@ -544,44 +544,29 @@ __global__ void k_precon(int ngpw, int nstate, int nocc, const double *vpp, cons
     const double f = fi * vpp[g];
     const double2 c = c2[w.k];
     const double2 v = make_double2(f * c.x, f * c.y);
+    cp[w.k] = v;
     if (b < nocc) s += (g == 0) ? v.x * v.x : 2.0 * (v.x * v.x + v.y * v.y);
   }
   double r = block_sum(s, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = r;
 }
-// PCG direction and step (cg.f90:247-281) from C2 itself: the preconditioned
-// gradient K(G) C2 / f_i whose norm k_precon sums is formed again here
-// instead of being stored and read back (the same operations, so the same
-// values).  scal[0] = ggnorm (new), scal[1] = previous ggnorm, scal[8] = the
-// CG step number; gamma = forget * new/prev.
-__global__ void k_pcg_update_c2(int ngpw, int nstate, const double *scal, const double *vpp, const double *occ,
-                                const double2 *__restrict__ c2, double2 *__restrict__ hnm1, double2 *__restrict__ c0) {
+// PCG direction and step (cg.f90:247-281); scal[0] = ggnorm (new),
+// scal[1] = previous ggnorm, scal[8] = the CG step number;
+// gamma = forget * new/prev
+__global__ void k_pcg_update(long tot, const double *scal, double2 *cp, double2 *hnm1, double2 *c0) {
   const int istep = (int)scal[8];
   double forget = istep <= 10 ? 0.60 : (istep <= 20 ? 0.91 : 0.95);
   double gamma = (istep == 1) ? 0.0 : forget * (scal[0] / scal[1]);
   const double dt = 5.0 * 5.0 / 400.0;
-  BandWalk w((long)ngpw * nstate, ngpw);
-  int bf = -1;
-  double fi = 1.0;
-#pragma unroll 4
-  for (; w.k < w.k1; w.next(ngpw)) {
-    if (w.b != bf) {
-      bf = w.b;
-      fi = occ[w.b] > 0.01 ? 1.0 / occ[w.b] : 1.0;
-    }
-    const double f = fi * vpp[w.g];
-    const double2 c = c2[w.k];
-    double2 d = make_double2(f * c.x, f * c.y);
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < tot; k += (long)gridDim.x * blockDim.x) {
+    double2 d = cp[k];
     if (istep > 1) {
-      const double2 h = hnm1[w.k];
-      d.x += gamma * h.x;
-      d.y += gamma * h.y;
+      d.x += gamma * hnm1[k].x;
+      d.y += gamma * hnm1[k].y;
     }
-    hnm1[w.k] = d;
-    double2 x = c0[w.k];
-    x.x += dt * d.x;
-    x.y += dt * d.y;
-    c0[w.k] = x;
+    hnm1[k] = d;
+    c0[k].x += dt * d.x;
+    c0[k].y += dt * d.y;
   }
 }
 __global__ void k_copy_scalar(const double *src, double *dst) { *dst = *src; }

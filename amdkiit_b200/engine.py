@@ -170,6 +170,13 @@ def host_gvectors(system: System) -> dict:
                 nhrays=info.nhrays, nr=tuple(info.nr))
 
 
+# mixed-precision CG hands over to FP64 at this GEMAX (or after MIXED_STALL
+# iterations without a new minimum): below it the FP32 pair transforms and the
+# 28-bit Gram products limit the gradient
+MIXED_GCUT = 1e-6
+MIXED_STALL = 40
+
+
 class Engine:
     """One system resident on one GPU."""
 
@@ -358,23 +365,33 @@ class Engine:
     def wfn_opt(self, max_step: int = 800, gcut: float = 1e-7, callback=None, refine: bool = True):
         """do_opt.f90:51-138: CG iterations until GEMAX < gcut.
 
-        On a mixed-precision engine with refine=True the iterations that
-        follow the first GEMAX < gcut run with FP64 band-pair transforms until
-        GEMAX < gcut holds there too, so the returned energy, gradient and
-        forces are those of the FP64 path at a converged wavefunction (the CG
-        history carries on; only the FFT precision changes)."""
+        On a mixed-precision engine with refine=True the iterations run with
+        FP64 band-pair transforms (and FP64 Gram products) from the first one
+        with GEMAX < max(gcut, MIXED_GCUT), or once GEMAX has not reached a
+        new minimum for MIXED_STALL iterations, until GEMAX < gcut holds
+        there: the returned energy, gradient and forces are those of the FP64
+        path at a converged wavefunction (the CG history carries on; only the
+        precision changes).  The mixed path's gradient carries FP32-level
+        errors, so a tighter gcut than MIXED_GCUT is reached in FP64."""
         e, g = None, None
         refining = False
+        best, since = float("inf"), 0
+        switch = max(gcut, MIXED_GCUT)
         try:
             for i in range(1, max_step + 1):
                 e, g, conv = self.scf_iteration(i, gcut)
                 if callback:
                     callback(i, e, g)
-                if conv:
-                    if refine and self.pair_precision == MIXED and not refining:
+                if refine and self.pair_precision == MIXED and not refining:
+                    if g < best:
+                        best, since = g, 0
+                    else:
+                        since += 1
+                    if g < switch or since >= MIXED_STALL:
                         refining = True
                         self.set_precision(FP64)
                         continue
+                if conv:
                     return i, e, g
             return max_step, e, g
         finally:

@@ -303,6 +303,7 @@ def config_report(args, local):
         for pname, prec in (("fp64", FP64), ("mixed", MIXED)):
             e = Engine(s, precision=prec, device=local)
             row["grid"] = list(e.nr)
+            row["nstate"] = e.nstate
             c0 = start(e, s)
             e.set_wfn(c0)
             e.ortho()

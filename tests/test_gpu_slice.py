@@ -34,8 +34,8 @@ def engines(system, monkeypatch, prec=MIXED):
     return ref, e
 
 
-SYSTEMS = {"water1": lambda: configs.small_water(xc=XC_PBE),
-           "cluster5": lambda: configs.cluster(5, 18.0, 905, ecut=20.0),
+# the slice products are used from 64 bands (16 molecules) to 128 (water32)
+SYSTEMS = {"cluster16": lambda: configs.cluster(16, 18.0, 916, ecut=20.0),
            "water32": configs.water32}
 
 
@@ -47,7 +47,7 @@ def test_slice_ortho_matches_dgemm(name, monkeypatch):
     assert rel(e.get_wfn(), ref.get_wfn()) < 1e-5
 
 
-@pytest.mark.parametrize("name", ["water1", "water32"])
+@pytest.mark.parametrize("name", ["cluster16", "water32"])
 def test_slice_cg_iteration_matches_dgemm(name, monkeypatch):
     """From a random start (ill-conditioned overlap, large gradient)."""
     ref, e = engines(SYSTEMS[name](), monkeypatch)
@@ -91,7 +91,7 @@ def test_slice_fp64_engine_keeps_dgemm(monkeypatch):
 
 
 def test_slice_mixed_converged_energy_matches_fp64(monkeypatch):
-    s = configs.small_water(xc=XC_PBE)
+    s = configs.cluster(16, 18.0, 916, ecut=20.0)
     ref, e = engines(s, monkeypatch)
     e64 = Engine(s, FP64)
     e64.set_wfn(ref.get_wfn())
