@@ -894,7 +894,7 @@ static void sg_tn(amdk_ctx *c, const CUtensorMap &ta, const CUtensorMap &tb, int
   c->nlaunch += 2;
   k_sgemm_tn<SG_S><<<c->sg_chunks, SG_TN_THREADS, SgTn<SG_S>::SMEM, c->st>>>(ta, tb, same, c->sg_ktiles, c->sg_per, c->d_sgpart,
                                                                      c->d_sgerr);
-  k_sgemm_reduce<<<n, 4 * SG_M, 0, c->st>>>(c->sg_chunks, c->d_sgpart, n, sa, sb, same ? c->d_sgnsq : nullptr,
+  k_sgemm_reduce<<<n, SG_RG * SG_M, 0, c->st>>>(c->sg_chunks, c->d_sgpart, n, sa, sb, same ? c->d_sgnsq : nullptr,
                                             alpha, out, n);
 }
 // out (the real view, 2 ngpw x n) = (or -=, sub) C0 B for B n x n, with C0's

@@ -413,20 +413,25 @@ __global__ void __launch_bounds__(SG_TN_THREADS, 1) k_sgemm_tn(const __grid_cons
 
 // out[m + ldo n] = alpha sa[m] sb[n] sum_c partial[c][n][m], m < nm, n < nn;
 // with nsq (a Gram matrix) the diagonal is alpha sum_seg nsq[m][seg] instead.
-// grid nn, block 4 SG_M: four interleaved partial sums per row, fixed order.
-__global__ void __launch_bounds__(4 * SG_M) k_sgemm_reduce(int nchunk, const double *__restrict__ partial, int nm,
-                                                           const double *__restrict__ sa, const double *__restrict__ sb,
-                                                           const double *__restrict__ nsq, double alpha,
-                                                           double *__restrict__ out, int ldo) {
+// grid nn, block SG_RG SG_M: SG_RG interleaved partial sums per row, fixed order.
+constexpr int SG_RG = 8;
+__global__ void __launch_bounds__(SG_RG * SG_M) k_sgemm_reduce(int nchunk, const double *__restrict__ partial, int nm,
+                                                               const double *__restrict__ sa,
+                                                               const double *__restrict__ sb,
+                                                               const double *__restrict__ nsq, double alpha,
+                                                               double *__restrict__ out, int ldo) {
   const int m = threadIdx.x % SG_M, g = threadIdx.x / SG_M, n = blockIdx.x;
-  __shared__ double red[4][SG_M];
+  __shared__ double red[SG_RG][SG_M];
   double s = 0.0;
 #pragma unroll 8
-  for (int c = g; c < nchunk; c += 4) s += partial[(long)c * SG_M * SG_M + n * SG_M + m];
+  for (int c = g; c < nchunk; c += SG_RG) s += partial[(long)c * SG_M * SG_M + n * SG_M + m];
   red[g][m] = s;
   __syncthreads();
   if (g == 0 && m < nm) {
-    double v = alpha * sa[m] * sb[n] * (((red[0][m] + red[1][m]) + red[2][m]) + red[3][m]);
+    double t = 0.0;
+#pragma unroll
+    for (int i = 0; i < SG_RG; ++i) t += red[i][m];
+    double v = alpha * sa[m] * sb[n] * t;
     if (nsq && m == n) {
       double q = 0.0;
       for (int i = 0; i < SG_SEG; ++i) q += nsq[m * SG_SEG + i];
