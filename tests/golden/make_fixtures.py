@@ -49,6 +49,28 @@ def parse_out(path):
     return e, g, (int(iters[-1]) if iters else None)
 
 
+def parse_md_start_forces(path):
+    """The ionic forces of the converged start of an MD run: the first
+    ATOM / COORDINATES / FORCES table after END OF FORCES INITIALIZATION
+    (molecular_dynamics.f90:92-95 prints it, 4 significant figures)."""
+    txt = open(path).read()
+    txt = txt[txt.index("END OF FORCES INITIALIZATION"):]
+    num = r"(-?[0-9.]+(?:E[-+]?\d+)?)"
+    rows = re.findall(r"^\s+(\d+)\s+([A-Z][a-z]?)" + (r"\s+" + num) * 6 + r"\s*$", txt, re.M)
+    out, seen = [], set()
+    for r in rows:
+        i = int(r[0])
+        if i in seen:
+            break
+        seen.add(i)
+        out.append([float(v) for v in r[2:]])
+    a = np.array(out)
+    return a[:, :3], a[:, 3:]
+
+
+MD_FORCES = {"water32_mt": "tests/32_water/md"}
+
+
 def save_system(path, s):
     d = dict(a_cell=s.a_cell, alat=s.alat, symmetry=s.symmetry, ecut=s.ecut, xc=s.xc, nsp=len(s.species))
     for i, (sp, pos) in enumerate(zip(s.species, s.positions)):
@@ -70,6 +92,12 @@ def main(root):
         save_system(os.path.join(HERE, name + ".npz"), s)
         e, g, it = parse_out(os.path.join(d, "amdkiit.out"))
         golden[name] = dict(energies=e, gvectors=g, iterations=it, source=rel + "/amdkiit.out")
+        if name in MD_FORCES:
+            # the MD run starts from the same input geometry; its first force
+            # table is the converged force at that geometry
+            md = MD_FORCES[name] + "/amdkiit.out"
+            pos, frc = parse_md_start_forces(os.path.join(root, md))
+            golden[name]["md_start"] = dict(positions=pos.tolist(), forces=frc.tolist(), source=md)
         print(name, e.get("etotal"), g)
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(golden, f, indent=1, sort_keys=True)

@@ -4,6 +4,8 @@ The reference prints its converged energy breakdown (eprint.f90:1-14); the
 oracle, started from this build's seeded guess instead of the atomic guess,
 must reach the same total energy within 1e-6 Ha/atom (components within
 2e-5 Ha: they converge more slowly than the variational total)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -48,3 +50,36 @@ def test_reference_gsphere_sizes(name):
     assert g["ngpw"] == ref["ngpw"] and g["ngrho"] == ref["ngrho"]
     assert g["ngrays"] == ref["ngrays"] and g["nhrays"] == ref["nhrays"]
     assert g["nr"][1] == ref["ny"] and g["nr"][2] == ref["nz"]
+
+
+def _md_start(name):
+    ref = golden()[name]["md_start"]
+    return np.array(ref["positions"]), np.array(ref["forces"])
+
+
+def test_md_start_geometry_is_the_fixture():
+    """The 32-water MD run (tests/32_water/md) starts from the wf_opt input
+    geometry, so its first force table pins the forces of that fixture; the
+    atoms are listed species by species in the fixture's order."""
+    s = load_fixture("water32_mt")
+    pos, frc = _md_start("water32_mt")
+    assert pos.shape == frc.shape == (s.nat, 3)
+    assert np.max(np.abs(np.concatenate(s.positions) - pos)) < 1e-5
+
+
+def species_forces(force, system):
+    """(nsp, na_max, 3) force array -> (nat, 3) in species order."""
+    return np.concatenate([force[i, :n] for i, n in enumerate(system.na)])
+
+
+@pytest.mark.slow
+@pytest.mark.skipif(os.environ.get("AMDK_SLOW") != "1", reason="~30 min CPU run; set AMDK_SLOW=1")
+def test_reference_water32_energy_and_forces():
+    """tests/32_water: E_tot -548.0385056774 (wf_opt) within 1e-6 Ha/atom and
+    the converged start forces of the MD run within 1e-4 Ha/bohr (the printed
+    forces carry 4 significant figures, at most 5e-6 Ha/bohr of rounding)."""
+    s, o = _converge("water32_mt", gcut=1e-6, max_step=400)
+    ref = golden()["water32_mt"]["energies"]
+    assert abs(o.d("etotal") - ref["etotal"]) < E_TOL_PER_ATOM * s.nat
+    _, frc = _md_start("water32_mt")
+    assert np.max(np.abs(species_forces(o.force(), s) - frc)) < 1e-4
