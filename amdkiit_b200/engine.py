@@ -152,6 +152,22 @@ def _check(rc, what=""):
         raise AmdkError(f"{what} failed ({rc}): {msg}")
 
 
+def subspace_eigenvalues(c0: np.ndarray, hc: np.ndarray) -> np.ndarray:
+    """Eigenvalues (Ha, ascending) of H in the span of the bands c0, given
+    hc = H|c0> band by band.  Both are (nstate, ngpw) on the G half sphere
+    with G = 0 first, so <a|b> = 2 Re sum_G a*(G) b(G) - a(0) b(0) (real
+    bands at the Gamma point).  The reference prints no eigenvalues; this
+    forms the nstate x nstate subspace Hamiltonian and overlap and solves
+    H x = e S x (S = 1 for orthonormal bands)."""
+    import scipy.linalg
+
+    def gram(a, b):
+        return 2.0 * np.real(np.conj(a) @ b.T) - np.outer(a[:, 0].real, b[:, 0].real)
+
+    h = gram(c0, hc)
+    return scipy.linalg.eigh(0.5 * (h + h.T), gram(c0, c0), eigvals_only=True)
+
+
 def host_gvectors(system: System) -> dict:
     """The G half-sphere and ray maps from the library's host setup (no GPU)."""
     lib = load_library()
@@ -299,6 +315,19 @@ class Engine:
 
     def apply_h(self):
         _check(self.lib.amdk_apply_h(self.h), "amdk_apply_h")
+
+    def eigenvalues(self) -> np.ndarray:
+        """Eigenvalues (Ha) of the Hamiltonian in the occupied subspace at the
+        current wavefunction.  Density, potential, projections and H|psi> run
+        on the GPU; C2 = -f_i H|psi_i> with f_i = 2 (the pair unpack of
+        wfn_initialize.f90:342-361 scales by f_i/2 and the pair transform
+        doubles V psi), so H|psi_i> = -C2_i / 2.  The nstate x nstate
+        matrix is formed and diagonalised on the host.  Overwrites C2."""
+        self.density()
+        self.potential()
+        self.energy()
+        self.apply_h()
+        return subspace_eigenvalues(self.get_wfn(), -0.5 * self.get("c2"))
 
     def gradient(self) -> float:
         g = C.c_double()

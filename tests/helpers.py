@@ -61,3 +61,19 @@ class OracleEngine:
     def get(self, name):
         assert name == "force"
         return self.o.force()
+
+
+def oracle_eigenvalues(o) -> np.ndarray:
+    """Subspace eigenvalues (Ha) at the oracle's current C0: the stages of one
+    iteration up to H|psi> (C2 = -f_i H|psi_i>, f_i = 2), then the same
+    nstate x nstate diagonalisation the engine uses."""
+    from amdkiit_b200.engine import subspace_eigenvalues
+    for r in ("eval_density", "rhor2g", "eval_pot", "cal_vpot_ex", "pp_energy", "vpsi", "fnonloc"):
+        o.call(r)
+    return subspace_eigenvalues(o.c0(), -0.5 * o.c2())
+
+
+def golden_oracle(name: str) -> dict:
+    """Converged oracle outputs at full size (tests/golden/make_oracle_fixtures.py)."""
+    with open(os.path.join(GOLDEN, f"oracle_{name}.json")) as f:
+        return json.load(f)
