@@ -237,12 +237,16 @@ def run_arm(prec, args, local, dist, world):
 
     # BOMD: velocity-Verlet steps (0.5 fs, 300 K, GRAD_CUTOFF 1e-6), each a
     # full wavefunction optimisation from the previous wavefunction
-    md_line, e_conv, f_conv = None, None, None
+    md_line, e_conv, f_conv, eig_conv = None, None, None, None
     if args.md_steps > 0:
         from amdkiit_b200.md import BOMD
         md = BOMD(e, temperature=300.0, dt_fs=0.5, seed=2024, gcut=1e-6)
         md.start()
         e_conv, f_conv = md.energy, np.array(md.force)
+        try:  # subspace eigenvalues at the converged start (this arm's precision)
+            eig_conv = e.eigenvalues()
+        except Exception as exc:  # reported, never fatal to the bench line
+            eig_conv = str(exc)
         e0 = md.total_energy()
         barrier()
         md_wall = tmax(md.run(args.md_steps))
@@ -269,7 +273,7 @@ def run_arm(prec, args, local, dist, world):
            "launches": launches, "kern": kern, "clocks": clocks, "energy": en["etotal"], "gemax": gm,
            "e2e": {"value": world * ke / e2e_s, "unit": UNIT, "h2d_bytes_per_step": wfn_bytes,
                    "d2h_bytes_per_step": wfn_bytes + 9 * 8 + 8},
-           "md": md_line, "e_conv": e_conv, "f_conv": f_conv, "dtype": "f64" if prec == FP64 else "f32+f64"}
+           "md": md_line, "e_conv": e_conv, "f_conv": f_conv, "eig_conv": eig_conv, "dtype": "f64" if prec == FP64 else "f32+f64"}
     e.close()
     return out
 
@@ -489,6 +493,12 @@ def main():
                         "dE_Ha_per_atom": de, "dF_max_Ha_per_bohr": df,
                         "within_tolerance": bool(de <= 1e-6 and df <= 1e-4),
                         "compared_at": "converged MD start geometry (GRAD_CUTOFF 1e-6)"})
+            ea, eb = mx["eig_conv"], f64["eig_conv"]
+            if isinstance(ea, np.ndarray) and isinstance(eb, np.ndarray):
+                cmp["dEig_max_Ha"] = float(np.max(np.abs(ea - eb)))
+            else:
+                cmp["dEig_max_Ha"] = None
+                cmp["eigenvalue_error"] = ea if isinstance(ea, str) else eb
         line["mixed_vs_fp64"] = cmp
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nth = os.cpu_count() or 1
