@@ -13,7 +13,7 @@ from amdkiit_b200 import configs
 from amdkiit_b200.engine import FP64, Engine
 from amdkiit_b200.inputs import XC_PBE
 from oracle.oracle import Oracle
-from tests.helpers import golden, load_fixture, start_coefficients
+from tests.helpers import golden, golden_oracle, load_fixture, oracle_eigenvalues, start_coefficients
 
 pytestmark = pytest.mark.gpu
 
@@ -169,6 +169,44 @@ def test_reference_energy_on_gpu():
     ref = golden()["water1_mt"]["energies"]
     assert abs(en["etotal"] - ref["etotal"]) < 1e-6 * s.nat
     assert abs(en["esr"] - ref["esr"]) < 1e-9 and abs(en["eself"] - ref["eself"]) < 1e-9
+
+
+def test_reference_water32_on_gpu():
+    """The 32-water reference runs (tests/32_water: MT psp, Teter93, 80 Ry,
+    108^3, 128 bands, GRAD_CUTOFF 1e-6) through the GPU path: E_tot of
+    wf_opt within 1e-6 Ha/atom, and the ionic forces at convergence within
+    1e-4 Ha/bohr of the first force table of the MD run, which starts from
+    the same geometry (4 printed significant figures)."""
+    s = load_fixture("water32_mt")
+    e = Engine(s, FP64)
+    g = e.gvectors()
+    tp = 2 * np.pi / s.alat
+    e.set_wfn(start_coefficients(g["hg"][: e.ngpw], tp, e.nstate))
+    e.ortho()
+    n, en, gm = e.wfn_opt(600, 1e-6)
+    assert gm < 1e-6
+    ref = golden()["water32_mt"]
+    assert abs(en["etotal"] - ref["energies"]["etotal"]) < 1e-6 * s.nat
+    f = e.ionic_forces()
+    f = np.concatenate([f[i, :k] for i, k in enumerate(s.na)])
+    assert np.max(np.abs(f - np.array(ref["md_start"]["forces"]))) < 1e-4
+    # subspace eigenvalues against the oracle converged from the same start
+    # (tests/golden/make_oracle_fixtures.py): within 1e-5 Ha
+    orc = golden_oracle("water32_mt")
+    assert np.max(np.abs(e.eigenvalues() - np.array(orc["eigenvalues"]))) < 1e-5
+    e.close()
+
+
+@pytest.mark.parametrize("name", ["small_water_pbe", "si_fcc_mt"])
+def test_eigenvalues_match_oracle(name):
+    """Subspace eigenvalues from the GPU's H|psi> and from the oracle's at the
+    same orthonormalised start agree to 1e-10 Ha."""
+    s = SYSTEMS[name]()
+    o, e = pair(s)
+    assert o.ortho() == 0
+    e.ortho()
+    d = np.max(np.abs(e.eigenvalues() - oracle_eigenvalues(o)))
+    assert d < 1e-10
 
 
 def test_set_precision_switches_pair_transforms():
