@@ -68,7 +68,19 @@ def parse_md_start_forces(path):
     return a[:, :3], a[:, 3:]
 
 
-MD_FORCES = {"water32_mt": "tests/32_water/md"}
+MD_FORCES = {"water32_mt": "tests/32_water/md", "water1_mt": "tests/1_water/md"}
+GEO_GRADIENTS = {"water1_mt": "tests/1_water/geo_opt/atom_force.dat"}
+
+
+def parse_first_gradient(path):
+    """The first block of a geometry optimisation's atom_force.dat: atom
+    count, ENERGY= E step, then one line per atom with dE/dR (Ha/bohr, 16
+    digits), at the run's input geometry."""
+    lines = open(path).read().split("\n")
+    nat = int(lines[0].split()[0])
+    energy = float(lines[1].split()[1])
+    grad = [[float(v) for v in ln.split()[1:4]] for ln in lines[2:2 + nat]]
+    return energy, grad
 
 
 def save_system(path, s):
@@ -98,6 +110,11 @@ def main(root):
             md = MD_FORCES[name] + "/amdkiit.out"
             pos, frc = parse_md_start_forces(os.path.join(root, md))
             golden[name]["md_start"] = dict(positions=pos.tolist(), forces=frc.tolist(), source=md)
+        if name in GEO_GRADIENTS:
+            # the geometry optimisation starts from the same input; its first
+            # gradient is taken at the converged start geometry
+            en, grad = parse_first_gradient(os.path.join(root, GEO_GRADIENTS[name]))
+            golden[name]["geo_start"] = dict(energy=en, gradient=grad, source=GEO_GRADIENTS[name])
         print(name, e.get("etotal"), g)
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(golden, f, indent=1, sort_keys=True)

@@ -38,6 +38,14 @@ def test_reference_energy(name):
         assert abs(e[k] - ref[k]) < 1e-9, k
     for k in ("eke", "estat", "eloc", "enl", "exc"):
         assert abs(e[k] - ref[k]) < COMP_TOL, k
+    start = golden()[name].get("geo_start")
+    if start:
+        # tests/1_water/geo_opt/atom_force.dat: dE/dR at the same converged
+        # start, 16 digits; the forces are ~7e-5 Ha/bohr, so 1e-5 is a tight
+        # pin (measured 1.1e-6, the two runs' convergence)
+        f = species_forces(o.force(), s)
+        assert np.max(np.abs(f + np.array(start["gradient"]))) < 1e-5
+        assert np.max(np.abs(f - _md_start(name)[1])) < 1e-5
 
 
 @pytest.mark.parametrize("name", ["si_fcc_mt", "water1_mt", "water32_mt"])
