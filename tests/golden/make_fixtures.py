@@ -68,6 +68,17 @@ def parse_md_start_forces(path):
     return a[:, :3], a[:, 3:]
 
 
+# cases whose committed run left only the per-iteration energy file (no
+# amdkiit.out): the last line of SP_ENERGY.dat is the converged total energy
+ENERGY_ONLY = {"h2_upf": ("tests/H2_upf", "SP_ENERGY.dat")}
+
+
+def parse_sp_energy(path):
+    """Last line of SP_ENERGY.dat: iteration, E_tot (6 decimals), time."""
+    last = [ln for ln in open(path).read().split("\n") if ln.strip()][-1]
+    return float(last.split()[1])
+
+
 MD_FORCES = {"water32_mt": "tests/32_water/md", "water1_mt": "tests/1_water/md"}
 GEO_GRADIENTS = {"water1_mt": "tests/1_water/geo_opt/atom_force.dat"}
 
@@ -116,6 +127,12 @@ def main(root):
             en, grad = parse_first_gradient(os.path.join(root, GEO_GRADIENTS[name]))
             golden[name]["geo_start"] = dict(energy=en, gradient=grad, source=GEO_GRADIENTS[name])
         print(name, e.get("etotal"), g)
+    for name, (rel, efile) in ENERGY_ONLY.items():
+        s = load_reference_input(os.path.join(root, rel))
+        save_system(os.path.join(HERE, name + ".npz"), s)
+        golden[name] = dict(energies={"etotal": parse_sp_energy(os.path.join(root, rel, efile))},
+                            energy_decimals=6, source=rel + "/" + efile)
+        print(name, golden[name]["energies"]["etotal"])
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(golden, f, indent=1, sort_keys=True)
 

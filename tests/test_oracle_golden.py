@@ -114,3 +114,14 @@ def test_oracle_water32_fixture_matches_reference():
     ev = np.array(orc["eigenvalues"])
     nel = sum(sp.zv * n for sp, n in zip(s.species, s.na))
     assert ev.shape == (round(nel / 2),) and np.all(np.diff(ev) >= 0)
+
+
+def test_reference_upf_energy():
+    """tests/H2_upf: the UPF path with an ONCV hydrogen (three projectors, the
+    h_ij sum of upf_fnl/upf_fnonloc), Teter93, 80 Ry (the reader's default),
+    90^3.  The reference printed E_tot to 6 decimals (-1.024460); the oracle
+    must agree within that rounding plus 1e-6 Ha/atom."""
+    s, o = _converge("h2_upf", gcut=1e-7, max_step=800)
+    ref = golden()["h2_upf"]
+    tol = 0.5 * 10.0 ** -ref["energy_decimals"] + E_TOL_PER_ATOM * s.nat
+    assert abs(o.d("etotal") - ref["energies"]["etotal"]) < tol
