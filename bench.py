@@ -416,6 +416,28 @@ def cufft_compare(args, local):
     return 0
 
 
+def compare_arms(f64: dict, mx: dict) -> dict:
+    """The FP64 arm's numbers beside the mixed arm's line, and, when both ran
+    MD, the mixed-vs-FP64 differences at the converged MD start: energy per
+    atom, max force component, max subspace eigenvalue."""
+    cmp = {"fp64_value": f64["value"], "fp64_ms_per_step": f64["ms_per_step"], "fp64_e2e": f64["e2e"]["value"],
+           "fp64_md": f64["md"], "scf_speedup": mx["value"] / f64["value"], "fp64_clocks": f64["clocks"]}
+    if f64["md"] and mx["md"]:
+        de = abs(mx["e_conv"] - f64["e_conv"]) / f64["nat"]
+        df = float(np.max(np.abs(mx["f_conv"] - f64["f_conv"])))
+        cmp.update({"md_speedup": mx["md"]["steps_per_s"] / f64["md"]["steps_per_s"],
+                    "dE_Ha_per_atom": de, "dF_max_Ha_per_bohr": df,
+                    "within_tolerance": bool(de <= 1e-6 and df <= 1e-4),
+                    "compared_at": "converged MD start geometry (GRAD_CUTOFF 1e-6)"})
+        ea, eb = mx.get("eig_conv"), f64.get("eig_conv")
+        if isinstance(ea, np.ndarray) and isinstance(eb, np.ndarray):
+            cmp["dEig_max_Ha"] = float(np.max(np.abs(ea - eb)))
+        else:
+            cmp["dEig_max_Ha"] = None
+            cmp["eigenvalue_error"] = ea if isinstance(ea, str) else eb
+    return cmp
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -483,23 +505,7 @@ def main():
         "wall_ms_per_step": head["wall_ms_per_step"],
     }
     if "fp64" in arms and "mixed" in arms:
-        f64, mx = arms["fp64"], arms["mixed"]
-        cmp = {"fp64_value": f64["value"], "fp64_ms_per_step": f64["ms_per_step"], "fp64_e2e": f64["e2e"]["value"],
-               "fp64_md": f64["md"], "scf_speedup": mx["value"] / f64["value"], "fp64_clocks": f64["clocks"]}
-        if f64["md"] and mx["md"]:
-            de = abs(mx["e_conv"] - f64["e_conv"]) / f64["nat"]
-            df = float(np.max(np.abs(mx["f_conv"] - f64["f_conv"])))
-            cmp.update({"md_speedup": mx["md"]["steps_per_s"] / f64["md"]["steps_per_s"],
-                        "dE_Ha_per_atom": de, "dF_max_Ha_per_bohr": df,
-                        "within_tolerance": bool(de <= 1e-6 and df <= 1e-4),
-                        "compared_at": "converged MD start geometry (GRAD_CUTOFF 1e-6)"})
-            ea, eb = mx["eig_conv"], f64["eig_conv"]
-            if isinstance(ea, np.ndarray) and isinstance(eb, np.ndarray):
-                cmp["dEig_max_Ha"] = float(np.max(np.abs(ea - eb)))
-            else:
-                cmp["dEig_max_Ha"] = None
-                cmp["eigenvalue_error"] = ea if isinstance(ea, str) else eb
-        line["mixed_vs_fp64"] = cmp
+        line["mixed_vs_fp64"] = compare_arms(arms["fp64"], arms["mixed"])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nth = os.cpu_count() or 1
         v, dt, done = cpu_reference_iterations(1, 0, nth)

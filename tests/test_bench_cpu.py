@@ -5,6 +5,7 @@ import json
 import os
 import socket
 
+import numpy as np
 import pytest
 import torch.distributed as dist
 import torch.multiprocessing as mp
@@ -63,3 +64,27 @@ def test_reference_arm_json(monkeypatch, capsys):
 def test_reference_arm_other_ranks_print_nothing(capsys):
     assert bench.run_reference(_Args, 1) == 0
     assert capsys.readouterr().out == ""
+
+
+def _arm(value, e, f, eig, md=True):
+    return {"value": value, "ms_per_step": 1000.0 / value, "e2e": {"value": value / 2}, "clocks": {},
+            "md": {"steps_per_s": value / 100} if md else None, "nat": 3,
+            "e_conv": e, "f_conv": np.array(f), "eig_conv": eig}
+
+
+def test_compare_arms_differences():
+    f64 = _arm(400.0, -17.0, [[0.1, 0.0, 0.0]], np.array([-0.9, -0.3]))
+    mx = _arm(600.0, -17.0 + 3e-7, [[0.1 + 2e-6, 0.0, 0.0]], np.array([-0.9, -0.3 + 4e-8]))
+    c = bench.compare_arms(f64, mx)
+    assert abs(c["scf_speedup"] - 1.5) < 1e-12 and abs(c["md_speedup"] - 1.5) < 1e-12
+    assert abs(c["dE_Ha_per_atom"] - 1e-7) < 1e-12 and abs(c["dF_max_Ha_per_bohr"] - 2e-6) < 1e-12
+    assert abs(c["dEig_max_Ha"] - 4e-8) < 1e-12 and c["within_tolerance"]
+
+
+def test_compare_arms_reports_eigenvalue_failure_and_no_md():
+    f64 = _arm(400.0, -17.0, [[0.0, 0.0, 0.0]], np.array([-0.5]))
+    mx = _arm(600.0, -17.0, [[0.0, 0.0, 0.0]], "amdk_apply_h failed (-5): ...")
+    c = bench.compare_arms(f64, mx)
+    assert c["dEig_max_Ha"] is None and c["eigenvalue_error"].startswith("amdk_apply_h")
+    c = bench.compare_arms(_arm(400.0, 0, [[0, 0, 0]], None, md=False), _arm(600.0, 0, [[0, 0, 0]], None, md=False))
+    assert "dE_Ha_per_atom" not in c and abs(c["scf_speedup"] - 1.5) < 1e-12
