@@ -158,7 +158,8 @@ def test_fft_sphere_roundtrip_and_numpy():
 
 def test_reference_energy_on_gpu():
     """The 1-water reference run (tests/1_water/wf_opt: MT psp, Teter93,
-    80 Ry, 108^3) through the GPU path: E_tot within 1e-6 Ha/atom."""
+    80 Ry, 108^3) through the GPU path: E_tot within 1e-6 Ha/atom, forces
+    within 1e-5 Ha/bohr of the reference's start gradient."""
     s = load_fixture("water1_mt")
     e = Engine(s, FP64)
     g = e.gvectors()
@@ -169,6 +170,12 @@ def test_reference_energy_on_gpu():
     ref = golden()["water1_mt"]["energies"]
     assert abs(en["etotal"] - ref["etotal"]) < 1e-6 * s.nat
     assert abs(en["esr"] - ref["esr"]) < 1e-9 and abs(en["eself"] - ref["eself"]) < 1e-9
+    # forces against the reference's geometry-optimisation start gradient
+    # (tests/1_water/geo_opt/atom_force.dat, same input geometry)
+    f = e.ionic_forces()
+    f = np.concatenate([f[i, :k] for i, k in enumerate(s.na)])
+    grad = np.array(golden()["water1_mt"]["geo_start"]["gradient"])
+    assert np.max(np.abs(f + grad)) < 1e-5
 
 
 def test_reference_water32_on_gpu():
@@ -193,6 +200,25 @@ def test_reference_water32_on_gpu():
     # subspace eigenvalues against the oracle converged from the same start
     # (tests/golden/make_oracle_fixtures.py): within 1e-5 Ha
     orc = golden_oracle("water32_mt")
+    assert np.max(np.abs(e.eigenvalues() - np.array(orc["eigenvalues"]))) < 1e-5
+    e.close()
+
+
+def test_reference_water2_on_gpu():
+    """The 2-water reference run (tests/2_water/wf_opt, 8 bands, default
+    GRAD_CUTOFF 1e-7) through the GPU path: E_tot within 1e-6 Ha/atom, and
+    the subspace eigenvalues within 1e-5 Ha of the oracle converged from the
+    same start (tests/golden/make_oracle_fixtures.py)."""
+    s = load_fixture("water2_mt")
+    e = Engine(s, FP64)
+    g = e.gvectors()
+    tp = 2 * np.pi / s.alat
+    e.set_wfn(start_coefficients(g["hg"][: e.ngpw], tp, e.nstate))
+    e.ortho()
+    n, en, gm = e.wfn_opt(600, 1e-7)
+    assert gm < 1e-7
+    assert abs(en["etotal"] - golden()["water2_mt"]["energies"]["etotal"]) < 1e-6 * s.nat
+    orc = golden_oracle("water2_mt")
     assert np.max(np.abs(e.eigenvalues() - np.array(orc["eigenvalues"]))) < 1e-5
     e.close()
 
