@@ -80,7 +80,8 @@ def parse_sp_energy(path):
 
 
 MD_FORCES = {"water32_mt": "tests/32_water/md", "water1_mt": "tests/1_water/md"}
-GEO_GRADIENTS = {"water1_mt": "tests/1_water/geo_opt/atom_force.dat"}
+GEO_GRADIENTS = {"water1_mt": "tests/1_water/geo_opt/atom_force.dat",
+                 "water2_mt": "tests/2_water/geo_opt/atom_force.dat"}
 
 
 def parse_first_gradient(path):

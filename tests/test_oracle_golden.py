@@ -114,6 +114,10 @@ def test_oracle_fixture_matches_reference(name):
     if "md_start" in ref:
         _, frc = _md_start(name)
         assert np.max(np.abs(np.array(orc["forces"]) - frc)) < 1e-4
+    if "geo_start" in ref:
+        # a geometry optimisation from the same input: its first gradient,
+        # 16 digits (2-water: forces up to 3e-4, measured 4.2e-6)
+        assert np.max(np.abs(np.array(orc["forces"]) + np.array(ref["geo_start"]["gradient"]))) < 1e-5
     ev = np.array(orc["eigenvalues"])
     nel = sum(sp.zv * n for sp, n in zip(s.species, s.na))
     assert ev.shape == (round(nel / 2),) and np.all(np.diff(ev) >= 0)
