@@ -79,6 +79,10 @@ def parse_sp_energy(path):
     return float(last.split()[1])
 
 
+# open-shell runs (the LSD branch is outside the path): only the system and
+# the G-sphere / ray counts of the rank table are kept, not the energies
+GSPHERE_ONLY = {"o2_singlet": "tests/O2/singlet_sp_cube"}
+
 MD_FORCES = {"water32_mt": "tests/32_water/md", "water1_mt": "tests/1_water/md"}
 GEO_GRADIENTS = {"water1_mt": "tests/1_water/geo_opt/atom_force.dat",
                  "water2_mt": "tests/2_water/geo_opt/atom_force.dat"}
@@ -128,6 +132,12 @@ def main(root):
             en, grad = parse_first_gradient(os.path.join(root, GEO_GRADIENTS[name]))
             golden[name]["geo_start"] = dict(energy=en, gradient=grad, source=GEO_GRADIENTS[name])
         print(name, e.get("etotal"), g)
+    for name, rel in GSPHERE_ONLY.items():
+        s = load_reference_input(os.path.join(root, rel))
+        save_system(os.path.join(HERE, name + ".npz"), s)
+        _, g, _ = parse_out(os.path.join(root, rel, "amdkiit.out"))
+        golden[name] = dict(gvectors=g, source=rel + "/amdkiit.out")
+        print(name, g)
     for name, (rel, efile) in ENERGY_ONLY.items():
         s = load_reference_input(os.path.join(root, rel))
         save_system(os.path.join(HERE, name + ".npz"), s)

@@ -16,6 +16,7 @@ SYSTEMS = {
     "water1": configs.water1,
     "si64": configs.si64,
     "water32": configs.water32,
+    "o2_angstrom_cell": lambda: load_fixture("o2_singlet"),
 }
 
 

@@ -48,7 +48,7 @@ def test_reference_energy(name):
         assert np.max(np.abs(f - _md_start(name)[1])) < 1e-5
 
 
-@pytest.mark.parametrize("name", ["si_fcc_mt", "water1_mt", "water32_mt"])
+@pytest.mark.parametrize("name", ["si_fcc_mt", "water1_mt", "water32_mt", "o2_singlet"])
 def test_reference_gsphere_sizes(name):
     """G-vector counts and ray counts summed over the reference's rank table."""
     s = load_fixture(name)
