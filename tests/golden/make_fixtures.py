@@ -85,7 +85,8 @@ GSPHERE_ONLY = {"o2_singlet": "tests/O2/singlet_sp_cube"}
 
 MD_FORCES = {"water32_mt": "tests/32_water/md", "water1_mt": "tests/1_water/md"}
 GEO_GRADIENTS = {"water1_mt": "tests/1_water/geo_opt/atom_force.dat",
-                 "water2_mt": "tests/2_water/geo_opt/atom_force.dat"}
+                 "water2_mt": "tests/2_water/geo_opt/atom_force.dat",
+                 "si_fcc_mt": "tests/bulk_si/geo_opt/atom_force.dat"}
 
 
 def parse_first_gradient(path):

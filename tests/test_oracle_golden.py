@@ -40,12 +40,13 @@ def test_reference_energy(name):
         assert abs(e[k] - ref[k]) < COMP_TOL, k
     start = golden()[name].get("geo_start")
     if start:
-        # tests/1_water/geo_opt/atom_force.dat: dE/dR at the same converged
-        # start, 16 digits; the forces are ~7e-5 Ha/bohr, so 1e-5 is a tight
-        # pin (measured 1.1e-6, the two runs' convergence)
+        # <case>/geo_opt/atom_force.dat: dE/dR at the same converged start,
+        # 16 digits (1-water: forces ~7e-5 Ha/bohr, measured 1.1e-6; Si FCC:
+        # 1.6e-3 Ha/bohr, s and p projectors)
         f = species_forces(o.force(), s)
         assert np.max(np.abs(f + np.array(start["gradient"]))) < 1e-5
-        assert np.max(np.abs(f - _md_start(name)[1])) < 1e-5
+        if "md_start" in golden()[name]:
+            assert np.max(np.abs(f - _md_start(name)[1])) < 1e-5
 
 
 @pytest.mark.parametrize("name", ["si_fcc_mt", "water1_mt", "water32_mt", "o2_singlet"])
