@@ -17,6 +17,7 @@ SYSTEMS = {
     "si64": configs.si64,
     "water32": configs.water32,
     "o2_angstrom_cell": lambda: load_fixture("o2_singlet"),
+    "h2_upf_90": lambda: load_fixture("h2_upf"),
 }
 
 

@@ -92,6 +92,11 @@ def test_reference_water32_energy_and_forces():
     assert abs(o.d("etotal") - ref["etotal"]) < E_TOL_PER_ATOM * s.nat
     _, frc = _md_start("water32_mt")
     assert np.max(np.abs(species_forces(o.force(), s) - frc)) < 1e-4
+    # the committed fixture is what this run gives
+    from tests.helpers import golden_oracle, oracle_eigenvalues
+    fix = golden_oracle("water32_mt")
+    assert abs(o.d("etotal") - fix["energies"]["etotal"]) < 1e-9
+    assert np.max(np.abs(oracle_eigenvalues(o) - np.array(fix["eigenvalues"]))) < 1e-9
 
 
 @pytest.mark.parametrize("name", ["water2_mt", "water32_mt"])
