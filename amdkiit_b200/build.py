@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libamdk.so")
 SOURCES = ["capi.cu", "setup.cpp"]
-HEADERS = ["amdk_internal.h", "fft.cuh", "kernels.cuh", "pencil.cuh", os.path.join("..", "..", "include", "amdk.h")]
+HEADERS = ["amdk_internal.h", "fft.cuh", "kernels.cuh", "pencil.cuh", "slicegemm.cuh", os.path.join("..", "..", "include", "amdk.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -10,7 +10,6 @@
 #include <cstring>
 #include <functional>
 #include <map>
-#include <mutex>
 #include <queue>
 #include <type_traits>
 #include <string>
@@ -336,7 +335,16 @@ static void *rays(amdk_ctx *c, int sphere) { return sphere ? c->d_rbf : c->d_rb;
 static long rstride(amdk_ctx *c, int sphere) { return (long)c->geom.nray[sphere] * c->geom.n1; }
 static long sstride(amdk_ctx *c, int sphere) { return (long)c->geom.nz[sphere] * c->geom.n2 * c->geom.n1; }
 
-template <typename C> static void y_pass(amdk_ctx *c, int sphere, int dir, int T) {
+// Ray and slab buffers of a slab-path transform; null members select the
+// context's own (the allocation-free entry passes its fixed scratch instead).
+struct XBufs {
+  void *rays = nullptr;
+  void *slab = nullptr;
+};
+static void *rays_of(amdk_ctx *c, int sphere, const XBufs &b) { return b.rays ? b.rays : rays(c, sphere); }
+static void *slab_of(amdk_ctx *c, const XBufs &b) { return b.slab ? b.slab : c->d_sb; }
+
+template <typename C> static void y_pass(amdk_ctx *c, int sphere, int dir, int T, const XBufs &b = XBufs{}) {
   const Geom &g = c->geom;
   dim3 grid((g.n1 + TX - 1) / TX, g.nz[sphere], T);
   prof_begin(c, KT_Y, (double)T * (rstride(c, sphere) + sstride(c, sphere)) * sizeof(C));
@@ -344,13 +352,14 @@ template <typename C> static void y_pass(amdk_ctx *c, int sphere, int dir, int T
   with_n(g.n2, [&](auto NC) {
     constexpr int N = decltype(NC)::value;
     smem_opt_in<k_y<C, N>>();
-    k_y<C, N><<<grid, NTHR, yz_smem<C>(g.n2), c->st>>>(sphere, dir, g, plan<C>(c, 1), (C *)rays(c, sphere), (C *)c->d_sb,
-                                                      rstride(c, sphere), sstride(c, sphere));
+    k_y<C, N><<<grid, NTHR, yz_smem<C>(g.n2), c->st>>>(sphere, dir, g, plan<C>(c, 1), (C *)rays_of(c, sphere, b),
+                                                      (C *)slab_of(c, b), rstride(c, sphere), sstride(c, sphere));
   });
   prof_end(c);
 }
 template <typename C, int MODE>
-static void z_pass(amdk_ctx *c, int sphere, int T, double2 *cg, const double *rg, int pair0 = 0) {
+static void z_pass(amdk_ctx *c, int sphere, int T, double2 *cg, const double *rg, int pair0 = 0,
+                   const XBufs &b = XBufs{}) {
   const Geom &g = c->geom;
   dim3 grid((g.n1 + TX - 1) / TX, g.n2, MODE == Z_DENSITY ? 1 : T);
   long gs = (long)g.n1 * g.n2 * g.n3;
@@ -363,13 +372,13 @@ static void z_pass(amdk_ctx *c, int sphere, int T, double2 *cg, const double *rg
   with_n(g.n3, [&](auto NC) {
     constexpr int N = decltype(NC)::value;
     smem_opt_in<k_z<C, MODE, N>>();
-    k_z<C, MODE, N><<<grid, NTHR, yz_smem<C>(g.n3), c->st>>>(sphere, T, g, plan<C>(c, 2), (C *)c->d_sb,
+    k_z<C, MODE, N><<<grid, NTHR, yz_smem<C>(g.n3), c->st>>>(sphere, T, g, plan<C>(c, 2), (C *)slab_of(c, b),
                                                              sstride(c, sphere), cg, rg, gs, c->d_vpot, c->d_rho,
                                                              c->d_wa + pair0, c->d_wb + pair0);
   });
   prof_end(c);
 }
-template <typename C> static void x_fwd(amdk_ctx *c, int sphere, int T) {
+template <typename C> static void x_fwd(amdk_ctx *c, int sphere, int T, const XBufs &b = XBufs{}) {
   const Geom &g = c->geom;
   long lines = (long)T * g.nray[sphere];
   prof_begin(c, KT_X, 2.0 * lines * g.n1 * sizeof(C));
@@ -377,7 +386,8 @@ template <typename C> static void x_fwd(amdk_ctx *c, int sphere, int T) {
   with_n(g.n1, [&](auto NC) {
     constexpr int N = decltype(NC)::value;
     smem_opt_in<k_x_fwd<C, N>>();
-    k_x_fwd<C, N><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(sphere, T, g, plan<C>(c, 0), (C *)rays(c, sphere));
+    k_x_fwd<C, N><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(sphere, T, g, plan<C>(c, 0),
+                                                                     (C *)rays_of(c, sphere, b));
   });
   prof_end(c);
 }
@@ -385,7 +395,8 @@ template <typename C> static void x_fwd(amdk_ctx *c, int sphere, int T) {
 // T fields on the density sphere (fp at +G, fm at -G) -> real or complex
 // grids (FP64 in and out; C is the precision of the transform itself)
 template <typename C = double2>
-static int field_to_grid(amdk_ctx *c, int T, const double2 *fp, const double2 *fm, double2 *cgrid) {
+static int field_to_grid(amdk_ctx *c, int T, const double2 *fp, const double2 *fm, double2 *cgrid,
+                         const XBufs &b = XBufs{}) {
   const Geom &g = c->geom;
   long lines = (long)T * g.nray[1];
   ++c->nlaunch;
@@ -393,19 +404,19 @@ static int field_to_grid(amdk_ctx *c, int T, const double2 *fp, const double2 *f
     constexpr int N = decltype(NC)::value;
     smem_opt_in<k_x_bwd_field<C, N>>();
     k_x_bwd_field<C, N><<<nblk(lines, LX), NTHR, x_smem<C>(g.n1), c->st>>>(fp, fm, g.ngrho, 1, T, g, plan<C>(c, 0),
-                                                                         (C *)c->d_rbf);
+                                                                         (C *)rays_of(c, 1, b));
   });
-  y_pass<C>(c, 1, +1, T);
-  z_pass<C, Z_TO_GRID>(c, 1, T, cgrid, nullptr);
+  y_pass<C>(c, 1, +1, T, b);
+  z_pass<C, Z_TO_GRID>(c, 1, T, cgrid, nullptr, 0, b);
   return 0;
 }
 // T complex grids (or one real grid) -> forward transform left in the ray buffer
 template <typename C = double2>
-static int grid_to_rays(amdk_ctx *c, int T, const double2 *cgrid, const double *rgrid) {
-  if (rgrid) z_pass<C, Z_FROM_GRID_REAL>(c, 1, 1, nullptr, rgrid);
-  else z_pass<C, Z_FROM_GRID_CPLX>(c, 1, T, (double2 *)cgrid, nullptr);
-  y_pass<C>(c, 1, -1, T);
-  x_fwd<C>(c, 1, T);
+static int grid_to_rays(amdk_ctx *c, int T, const double2 *cgrid, const double *rgrid, const XBufs &b = XBufs{}) {
+  if (rgrid) z_pass<C, Z_FROM_GRID_REAL>(c, 1, 1, nullptr, rgrid, 0, b);
+  else z_pass<C, Z_FROM_GRID_CPLX>(c, 1, T, (double2 *)cgrid, nullptr, 0, b);
+  y_pass<C>(c, 1, -1, T, b);
+  x_fwd<C>(c, 1, T, b);
   return 0;
 }
 
@@ -2034,33 +2045,31 @@ int amdk_profile_get(amdk_ctx *c, int kind, long *launches, double *total_ms, do
 // the -G field of one FP64 transform) lives in this file-scope array, which
 // every GPU that loads the library holds until the process exits.  Host code
 // must not pass the array's name to a kernel: on the host that name is only a
-// stand-in, so the device address is looked up once per device with
-// cudaGetSymbolAddress and cached.
+// stand-in, so each call looks the device address up with
+// cudaGetSymbolAddress on the current device (a cached address would go stale
+// if the caller reset the device and a new context took its place).
 // ---------------------------------------------------------------------------
 constexpr size_t kNoAllocScratchBytes = (size_t)24 << 20;  // 24 MiB
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
-static std::mutex g_noalloc_mu;
-constexpr int kNoAllocMaxDevices = 128;
-static void *g_noalloc_addr[kNoAllocMaxDevices] = {};
 
-// Device address of the scratch array on `device` (which must be current).
-static int noalloc_scratch(int device, unsigned char **out) {
-  if (device < 0 || device >= kNoAllocMaxDevices) {
-    set_error("amdk_fft_sphere_noalloc: device ordinal out of range");
-    return AMDK_ERR_BADARG;
+// Device address of the scratch array on the current device.
+static int noalloc_scratch(unsigned char **out) {
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    set_error(std::string("amdk_fft_sphere_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+    return AMDK_ERR_CUDA;
   }
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[device]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      set_error(std::string("amdk_fft_sphere_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
-      return AMDK_ERR_CUDA;
-    }
-    g_noalloc_addr[device] = p;
-  }
-  *out = (unsigned char *)g_noalloc_addr[device];
+  *out = (unsigned char *)p;
   return 0;
+}
+
+// Scratch bytes one transform of this context's density sphere needs.
+static size_t noalloc_bytes(amdk_ctx *c, size_t *rbytes, size_t *sbytes) {
+  auto round256 = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  *rbytes = round256((size_t)rstride(c, 1) * sizeof(double2));
+  *sbytes = round256((size_t)sstride(c, 1) * sizeof(double2));
+  return *rbytes + *sbytes + round256((size_t)c->hs.ngrho * sizeof(double2));
 }
 
 int amdk_fft_sphere_noalloc(amdk_ctx *c, int sign, double *coef, double *grid) {
@@ -2070,48 +2079,34 @@ int amdk_fft_sphere_noalloc(amdk_ctx *c, int sign, double *coef, double *grid) {
   }
   CK(cudaSetDevice(c->device));
   const HostSetup &h = c->hs;
-  const Geom &g = c->geom;
-  auto round256 = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  const size_t rbytes = round256((size_t)rstride(c, 1) * sizeof(double2));
-  const size_t sbytes = round256((size_t)sstride(c, 1) * sizeof(double2));
-  const size_t fbytes = round256((size_t)h.ngrho * sizeof(double2));
-  if (rbytes + sbytes + fbytes > kNoAllocScratchBytes) {
-    set_error("amdk_fft_sphere_noalloc: this grid needs " + std::to_string(rbytes + sbytes + fbytes) +
+  size_t rbytes = 0, sbytes = 0;
+  const size_t need = noalloc_bytes(c, &rbytes, &sbytes);
+  if (need > kNoAllocScratchBytes) {
+    set_error("amdk_fft_sphere_noalloc: this grid needs " + std::to_string(need) +
               " bytes of scratch; the fixed maximum is " + std::to_string(kNoAllocScratchBytes) +
               " bytes (use amdk_fft_sphere)");
     return AMDK_ERR_UNSUPPORTED;
   }
   unsigned char *base = nullptr;
-  RC(noalloc_scratch(c->device, &base));
-  double2 *R = (double2 *)base;
-  double2 *S = (double2 *)(base + rbytes);
+  RC(noalloc_scratch(&base));
+  // the inputs may have been written on any stream of the caller's (an
+  // OpenACC async queue, a torch stream, the legacy default stream): wait
+  // for all work on the device before reading them
+  CK(cudaDeviceSynchronize());
+  const XBufs b{base, base + rbytes};
   double2 *FM = (double2 *)(base + rbytes + sbytes);
-  const long npt = (long)g.n1 * g.n2 * g.n3;
-  const long lines = (long)g.nray[1];
-  const dim3 gy((g.n1 + TX - 1) / TX, g.nz[1], 1), gz((g.n1 + TX - 1) / TX, g.n2, 1);
+  const long npt = (long)h.nr[0] * h.nr[1] * h.nr[2];
   if (sign == -1) {
     // coef (+G half) -> complex grid; the -G values are conj(coef)
     ++c->nlaunch;
     k_conj_field<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, (const double2 *)coef, FM);
-    ++c->nlaunch;
-    k_x_bwd_field<double2><<<nblk(lines, LX), NTHR, x_smem<double2>(g.n1), c->st>>>(
-        (const double2 *)coef, FM, g.ngrho, 1, 1, g, c->pd[0], R);
-    ++c->nlaunch;
-    k_y<double2><<<gy, NTHR, yz_smem<double2>(g.n2), c->st>>>(1, +1, g, c->pd[1], R, S, rstride(c, 1), sstride(c, 1));
-    ++c->nlaunch;
-    k_z<double2, Z_TO_GRID><<<gz, NTHR, yz_smem<double2>(g.n3), c->st>>>(
-        1, 1, g, c->pd[2], S, sstride(c, 1), (double2 *)grid, nullptr, npt, nullptr, nullptr, nullptr, nullptr);
+    RC(field_to_grid<double2>(c, 1, (const double2 *)coef, FM, (double2 *)grid, b));
   } else {
     // complex grid -> coef = F(+G)/N
+    RC(grid_to_rays<double2>(c, 1, (const double2 *)grid, nullptr, b));
     ++c->nlaunch;
-    k_z<double2, Z_FROM_GRID_CPLX><<<gz, NTHR, yz_smem<double2>(g.n3), c->st>>>(
-        1, 1, g, c->pd[2], S, sstride(c, 1), (double2 *)grid, nullptr, npt, nullptr, nullptr, nullptr, nullptr);
-    ++c->nlaunch;
-    k_y<double2><<<gy, NTHR, yz_smem<double2>(g.n2), c->st>>>(1, -1, g, c->pd[1], R, S, rstride(c, 1), sstride(c, 1));
-    ++c->nlaunch;
-    k_x_fwd<double2><<<nblk(lines, LX), NTHR, x_smem<double2>(g.n1), c->st>>>(1, 1, g, c->pd[0], R);
-    ++c->nlaunch;
-    k_gather_p<double2><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_posp, R, 1.0 / (double)npt, (double2 *)coef);
+    k_gather_p<double2><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_posp, (double2 *)b.rays, 1.0 / (double)npt,
+                                                           (double2 *)coef);
   }
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->st));

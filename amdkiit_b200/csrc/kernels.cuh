@@ -172,7 +172,7 @@ __global__ void k_projectors(int ngpw, int nproj, const int *inyh, int nh1, int 
   }
   P[(long)j * ngpw + g] = v;
 }
-// hess (cg.f90:141-199): K(G) = 1/max(1/2 |G|^2 + V_loc(0) + sum n_s w twnl^2, 0.5)
+// hess (cg.f90:3-61): K(G) = 1/max(1/2 |G|^2 + V_loc(0) + sum n_s w twnl^2, 0.5)
 __global__ void k_hess(int ngpw, const double *hg, double tpiba2, const double2 *evps, const double *twnl, int nsp,
                        int nghmax, const int *na, const int *ngh, const double *wsg, double *vpp) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -526,7 +526,7 @@ __global__ void k_finish_max(const double *part, int nb, double *out) {
   if (threadIdx.x == 0) *out = sqrt(fmax(r, 0.0));  // partials hold |c2|^2
 }
 
-// PRECON + GGNORM (cg.f90:239-245, 419-449): cp = fi K c2; partial DOTP sums
+// PRECON + GGNORM (cg.f90:102-107, 281-311): cp = fi K c2; partial DOTP sums
 __global__ void k_precon(int ngpw, int nstate, int nocc, const double *vpp, const double *occ, const double2 *c2,
                          double2 *cp, double *part) {
   __shared__ double sh[32];
@@ -550,7 +550,7 @@ __global__ void k_precon(int ngpw, int nstate, int nocc, const double *vpp, cons
   double r = block_sum(s, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = r;
 }
-// PCG direction and step (cg.f90:247-281); scal[0] = ggnorm (new),
+// PCG direction and step (cg.f90:109-143); scal[0] = ggnorm (new),
 // scal[1] = previous ggnorm, scal[8] = the CG step number;
 // gamma = forget * new/prev
 __global__ void k_pcg_update(long tot, const double *scal, double2 *cp, double2 *hnm1, double2 *c0) {

@@ -186,11 +186,15 @@ def host_gvectors(system: System) -> dict:
                 nhrays=info.nhrays, nr=tuple(info.nr))
 
 
-# mixed-precision CG hands over to FP64 at this GEMAX (or after MIXED_STALL
-# iterations without a new minimum): below it the FP32 pair transforms and the
-# 28-bit Gram products limit the gradient
+# mixed-precision CG hands over to FP64 at this GEMAX: below it the FP32 pair
+# transforms and the 28-bit Gram products limit the gradient.  It also hands
+# over after MIXED_STALL iterations without a new GEMAX minimum, but only once
+# GEMAX has come within MIXED_STALL_ZONE x MIXED_GCUT: higher up a plateau is
+# the CG's own (the reference's fixed-step PCG plateaus for hundreds of
+# iterations on bulk Si in FP64 too), not the FP32 noise floor
 MIXED_GCUT = 1e-6
 MIXED_STALL = 40
+MIXED_STALL_ZONE = 10.0
 
 
 class Engine:
@@ -396,9 +400,9 @@ class Engine:
 
         On a mixed-precision engine with refine=True the iterations run with
         FP64 band-pair transforms (and FP64 Gram products) from the first one
-        with GEMAX < max(gcut, MIXED_GCUT), or once GEMAX has not reached a
-        new minimum for MIXED_STALL iterations, until GEMAX < gcut holds
-        there: the returned energy, gradient and forces are those of the FP64
+        with GEMAX < max(gcut, MIXED_GCUT), or once GEMAX, within
+        MIXED_STALL_ZONE of that threshold, has not reached a new minimum for
+        MIXED_STALL iterations, until GEMAX < gcut holds there: the returned energy, gradient and forces are those of the FP64
         path at a converged wavefunction (the CG history carries on; only the
         precision changes).  The mixed path's gradient carries FP32-level
         errors, so a tighter gcut than MIXED_GCUT is reached in FP64."""
@@ -416,7 +420,7 @@ class Engine:
                         best, since = g, 0
                     else:
                         since += 1
-                    if g < switch or since >= MIXED_STALL:
+                    if g < switch or (best < MIXED_STALL_ZONE * switch and since >= MIXED_STALL):
                         refining = True
                         self.set_precision(FP64)
                         continue

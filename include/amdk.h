@@ -146,7 +146,7 @@ int amdk_energy(amdk_ctx *ctx, amdk_energies *out);
 int amdk_apply_h(amdk_ctx *ctx);
 /* gradient.f90:5-61 forces (Lambda, C2 -= C0 Lambda, ZCLEAN) + eval_GMAX */
 int amdk_gradient(amdk_ctx *ctx, double *gemax);
-/* cg.f90:201-283 PCG (hess, precon, direction, C0 += 0.0625 d) */
+/* cg.f90:63-145 PCG (hess, precon, direction, C0 += 0.0625 d) */
 int amdk_pcg(amdk_ctx *ctx, int istep);
 /* One CG iteration of do_opt.f90:80-128 (density ... ortho_gs), ionic
  * forces included once GEMAX < 3*gcut as in CHK_TFOR (gradient.f90:113-136). */
@@ -211,11 +211,14 @@ int amdk_launch_count(amdk_ctx *ctx, long *n);
  * (nr3*nr2*nr1 complex) are DEVICE pointers owned by the caller; the call
  * allocates nothing.  Its scratch is one fixed 24 MiB device array inside the
  * library (held by every GPU that loads it), which limits it to grids whose
- * density-sphere transform fits (about 90^3); larger grids return
- * AMDK_ERR_UNSUPPORTED.  The first call on a device looks up the array's
- * device address, so make that first call before any stream capture.  All
- * calls share the array: calls that overlap on the GPU (several contexts or
- * threads at once) race.  Returns after the transform has finished. */
+ * density-sphere transform fits (about 90^3: the 90^3 H2 cell needs 22.3 MB);
+ * larger grids return AMDK_ERR_UNSUPPORTED.  Each call looks up the array's
+ * device address on the current device, so make the first call before any
+ * stream capture.  The call starts with a device-wide synchronisation, so
+ * inputs written on any stream of the caller's are complete before it reads
+ * them, and returns after the transform has finished.  All calls share the
+ * array: calls that overlap on the GPU (several contexts or threads at once)
+ * race. */
 int amdk_fft_sphere_noalloc(amdk_ctx *ctx, int sign, double *coef, double *grid);
 
 /* Elapsed device time of the last amdk_scf_iteration, milliseconds. */

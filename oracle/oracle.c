@@ -1741,7 +1741,7 @@ void orc_nlfor(orc_sys *s) {
 }
 
 /* ------------------------------------------------------------------ */
-/* cg.f90:141-199 hess, :201-283 PCG, :419-449 PRECON                   */
+/* cg.f90:3-61 hess, :63-145 PCG, :281-311 PRECON                       */
 /* ------------------------------------------------------------------ */
 static double dotp(const zc *a, const zc *b, int n) { /* wfn_initialize.f90:382-426 with g0_stat */
   const double *A = (const double *)a, *B = (const double *)b;

@@ -1,8 +1,8 @@
 """Host logic of Engine.wfn_opt that needs no GPU: when a mixed-precision
 engine hands the CG iterations over to FP64 (GEMAX below max(gcut, 1e-6), or
-no new GEMAX minimum for MIXED_STALL iterations) and that it then iterates
-in FP64 to gcut.  The engine's GPU calls are replaced by a scripted GEMAX
-sequence."""
+no new GEMAX minimum for MIXED_STALL iterations once GEMAX is within
+MIXED_STALL_ZONE of that threshold) and that it then iterates in FP64 to
+gcut.  The engine's GPU calls are replaced by a scripted GEMAX sequence."""
 from amdkiit_b200 import engine as eng
 from amdkiit_b200.engine import FP64, MIXED, Engine
 
@@ -58,3 +58,13 @@ def test_no_refinement_requested():
     e = scripted([1e-3, 5e-8], [])
     n, en, g = e.wfn_opt(100, 1e-7, refine=False)
     assert [p for p, _ in e.trace] == [MIXED, MIXED] and n == 2
+
+
+def test_plateau_far_above_the_threshold_stays_mixed():
+    """A plateau at 1e-4 (the CG's own, as on bulk Si in FP64) does not hand
+    over: only GEMAX below the threshold does."""
+    plateau = [1e-3] + [2e-4] * (3 * eng.MIXED_STALL) + [5e-7]
+    e = scripted(plateau, [9e-8])
+    n, en, g = e.wfn_opt(400, 1e-7)
+    precs = [p for p, _ in e.trace]
+    assert precs.count(MIXED) == len(plateau) and precs[-1] == FP64
