@@ -56,6 +56,7 @@ class BOMD:
         self.force = None
         self.energy = None
         self.scf_iterations = []
+        self.step_wall = []   # host wall clock of each step of run(), s
 
     def _init_velocities(self, temperature, seed):
         rng = np.random.default_rng(seed)
@@ -119,7 +120,9 @@ class BOMD:
     def run(self, nsteps: int, callback=None):
         t0 = time.perf_counter()
         for i in range(nsteps):
+            t = time.perf_counter()
             n = self.step()
+            self.step_wall.append(time.perf_counter() - t)
             if callback:
                 callback(i, n, self.energy, self.total_energy(), self.temperature())
         return time.perf_counter() - t0

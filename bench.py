@@ -25,7 +25,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -56,54 +55,66 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks, power and throttle reasons sampled every `period_s` on a
+    background thread through NVML (nvidia-smi's own source of these
+    figures), from start() to stop(): a bench arm brackets its timed
+    iterations, the end-to-end iterations and the MD steps with it."""
 
-    def __init__(self, gpu_index: int):
+    # NVML clocks-event reason bits (nvml.h nvmlClocksEventReason*)
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
+
+    def __init__(self, gpu_index: int, period_s: float = 0.02):
         self.idx = gpu_index
-        self.proc = None
-        self.lines = []
+        self.period = period_s
+        self.samples = []
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self.t = None
+        self.err = None
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        idx = self.idx
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        parts = [x for x in vis.split(",") if x.strip()]
+        if parts and all(x.strip().isdigit() for x in parts) and self.idx < len(parts):
+            idx = int(parts[self.idx])
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(idx)
 
     def start(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except Exception:
-            self.proc = None
+            nv, h = self._handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        except Exception as exc:  # reported in the line, never fatal
+            self.err = f"NVML unavailable: {exc}"
+            return
 
-    def _read(self):
-        for ln in self.proc.stdout:
-            self.lines.append(ln.strip())
+        def loop():
+            while not self._stop.is_set():
+                try:
+                    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                    self.samples.append((float(sm), int(rs), pw))
+                except Exception as exc:
+                    self.err = str(exc)
+                    return
+                self._stop.wait(self.period)
+        self.t = threading.Thread(target=loop, daemon=True)
+        self.t.start()
 
     def stop(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if self.t is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.err or "no samples"], "samples": 0}
+        self._stop.set()
+        self.t.join(timeout=5)
+        sm = [x[0] for x in self.samples]
+        reasons = sorted(n for n, bit in self.REASONS.items() if any(x[1] & bit for x in self.samples))
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(sm), "period_ms": 1000.0 * self.period,
+                "power_w_max": max((x[2] for x in self.samples), default=None),
+                "window": "whole arm: timed, end-to-end and MD iterations"}
 
 
 def setup_engine(precision: int, device: int):
@@ -150,14 +161,16 @@ def cpu_reference_iterations(steps: int, warmup: int, nthreads: int, budget_s: f
 # seconds per core count, so it runs at most REF_WARMUP + REF_BUDGET_S worth
 # of iterations whatever --steps asks for.
 REF_WARMUP = 1
-REF_BUDGET_S = 60.0
+REF_STEPS = 20
+REF_BUDGET_S = 30.0
 
 
 def run_reference(args, rank):
     if rank != 0:
         return 0
     nth = os.cpu_count() or 1
-    v, dt, done = cpu_reference_iterations(args.steps, min(args.warmup, REF_WARMUP), nth, REF_BUDGET_S)
+    v, dt, done = cpu_reference_iterations(min(args.steps, REF_STEPS), min(args.warmup, REF_WARMUP), nth,
+                                           REF_BUDGET_S)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": done,
         "warmup": min(args.warmup, REF_WARMUP), "ms_per_step": 1000.0 * dt / done, "higher_is_better": True,
@@ -204,7 +217,7 @@ def run_arm(prec, args, local, dist, world):
 
     clk = ClockSampler(local)
     barrier()
-    clk.start()
+    clk.start()   # stopped after the MD steps: the whole arm under load
     e.profile(True)
     n0 = e.launch_count()
     dev_ms = 0.0
@@ -214,7 +227,6 @@ def run_arm(prec, args, local, dist, world):
         dev_ms += e.last_iteration_ms()
     wall = time.perf_counter() - t0
     launches = e.launch_count() - n0
-    clocks = clk.stop()
     barrier()
     kern = {name: e.profile_get(k) for k, name in e.KERNELS.items()}
     e.profile(False)
@@ -248,12 +260,17 @@ def run_arm(prec, args, local, dist, world):
         except Exception as exc:  # reported, never fatal to the bench line
             eig_conv = str(exc)
         e0 = md.total_energy()
+        etot = [e0]
         barrier()
-        md_wall = tmax(md.run(args.md_steps))
+        md_wall = tmax(md.run(args.md_steps, callback=lambda i, n, ep, et, T: etot.append(et)))
         its = md.scf_iterations[1:]
         md_line = {"steps_per_s": world * args.md_steps / md_wall, "unit": "MD step/s", "steps": args.md_steps,
+                   "step_s_median": float(np.median(md.step_wall)), "step_s_mean": float(np.mean(md.step_wall)),
                    "scf_iterations_per_step": float(np.mean(its)), "dt_fs": 0.5, "temperature_K": 300.0,
-                   "grad_cutoff": 1e-6, "energy_drift_Ha": md.total_energy() - e0, "timing": "host wall clock"}
+                   "grad_cutoff": 1e-6, "energy_drift_Ha": md.total_energy() - e0,
+                   "energy_fluctuation_Ha": float(np.max(np.abs(np.array(etot) - e0))),
+                   "timing": "host wall clock per step (each step ends on a host synchronisation); "
+                             "steps_per_s = steps / total"}
         # the same steps with the wavefunction predictor (an option outside
         # the reference's driver): reported beside, not as the MD number
         mdx = BOMD(e, temperature=300.0, dt_fs=0.5, seed=2024, gcut=1e-6, extrapolate=True,
@@ -265,10 +282,12 @@ def run_arm(prec, args, local, dist, world):
         nx = max(args.md_steps, 3)
         x_wall = tmax(mdx.run(nx))
         md_line["extrapolated"] = {"steps_per_s": world * nx / x_wall, "steps": nx,
+                                   "step_s_median": float(np.median(mdx.step_wall)),
                                    "scf_iterations_per_step": float(np.mean(mdx.scf_iterations[PREDICTOR_POINTS:])),
                                    "predictor": f"always-stable predictor, {PREDICTOR_POINTS} points: "
                                                 "C0(t+dt) = sum_j w_j C0(t-j dt) [C0(t-j dt)^T C0(t)], then ortho"}
-    out = {"prec": prec, "nat": s.nat, "value": world * args.steps / (dev_ms / 1000.0),
+    clocks = clk.stop()
+    out = {"prec": prec, "nat": s.nat, "na": list(s.na), "value": world * args.steps / (dev_ms / 1000.0),
            "ms_per_step": dev_ms / args.steps, "wall_ms_per_step": 1000.0 * wall / args.steps,
            "launches": launches, "kern": kern, "clocks": clocks, "energy": en["etotal"], "gemax": gm,
            "e2e": {"value": world * ke / e2e_s, "unit": UNIT, "h2d_bytes_per_step": wfn_bytes,
@@ -314,7 +333,7 @@ def config_report(args, local):
             row[pname + "_scf_iter_per_s"] = timed(e, steps)
             e.set_wfn(c0)
             e.ortho()
-            n, en, gm = e.wfn_opt(1500, 1e-6)
+            n, en, gm = e.wfn_opt(4000, 1e-6)
             res[pname] = (en["etotal"], e.get("force") if n > 1 else e.ionic_forces(), n)
             e.close()
         row["scf_speedup"] = row["mixed_scf_iter_per_s"] / row["fp64_scf_iter_per_s"]
@@ -416,10 +435,26 @@ def cufft_compare(args, local):
     return 0
 
 
-def compare_arms(f64: dict, mx: dict) -> dict:
+def oracle_fixture():
+    """The oracle's converged water32 energy and forces (a committed JSON
+    fixture; the oracle itself does not run here), or None."""
+    p = os.path.join(ROOT, "tests", "golden", "oracle_water32.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f)
+
+
+def species_forces(force, na):
+    """(nsp, na_max, 3) force array -> (nat, 3) in species order."""
+    return np.concatenate([np.asarray(force)[i, :k] for i, k in enumerate(na)])
+
+
+def compare_arms(f64: dict, mx: dict, fixture: dict | None = None) -> dict:
     """The FP64 arm's numbers beside the mixed arm's line, and, when both ran
     MD, the mixed-vs-FP64 differences at the converged MD start: energy per
-    atom, max force component, max subspace eigenvalue."""
+    atom, max force component, max subspace eigenvalue; with the oracle's
+    converged fixture of the same system, each arm's differences from it."""
     cmp = {"fp64_value": f64["value"], "fp64_ms_per_step": f64["ms_per_step"], "fp64_e2e": f64["e2e"]["value"],
            "fp64_md": f64["md"], "scf_speedup": mx["value"] / f64["value"], "fp64_clocks": f64["clocks"]}
     if f64["md"] and mx["md"]:
@@ -429,6 +464,15 @@ def compare_arms(f64: dict, mx: dict) -> dict:
                     "dE_Ha_per_atom": de, "dF_max_Ha_per_bohr": df,
                     "within_tolerance": bool(de <= 1e-6 and df <= 1e-4),
                     "compared_at": "converged MD start geometry (GRAD_CUTOFF 1e-6)"})
+        fx = fixture
+        if fx is not None:
+            f_ref = np.array(fx["forces"])
+            cmp["vs_oracle"] = {
+                arm: {"dE_Ha_per_atom": abs(d["e_conv"] - fx["energies"]["etotal"]) / d["nat"],
+                      "dF_max_Ha_per_bohr": float(np.max(np.abs(species_forces(d["f_conv"], d["na"]) - f_ref)))}
+                for arm, d in (("fp64", f64), ("mixed", mx))}
+            cmp["vs_oracle"]["fixture"] = ("tests/golden/oracle_water32.json: the CPU restatement converged to GEMAX "
+                                           f"< {fx['gcut']:g} from the seeded start ({fx['iterations']} iterations)")
         ea, eb = mx.get("eig_conv"), f64.get("eig_conv")
         if isinstance(ea, np.ndarray) and isinstance(eb, np.ndarray):
             cmp["dEig_max_Ha"] = float(np.max(np.abs(ea - eb)))
@@ -447,7 +491,8 @@ def main():
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
                     help="both: mixed precision is the headline value, FP64 is measured beside it")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--md-steps", type=int, default=3)
+    ap.add_argument("--md-steps", type=int, default=20,
+                    help="velocity-Verlet steps per arm (200: the 32-water drift run)")
     ap.add_argument("--configs", action="store_true",
                     help="report configurations 0, 1, 2 and 4 instead of the headline line")
     ap.add_argument("--cufft", action="store_true",
@@ -505,13 +550,14 @@ def main():
         "wall_ms_per_step": head["wall_ms_per_step"],
     }
     if "fp64" in arms and "mixed" in arms:
-        line["mixed_vs_fp64"] = compare_arms(arms["fp64"], arms["mixed"])
+        line["mixed_vs_fp64"] = compare_arms(arms["fp64"], arms["mixed"], oracle_fixture())
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nth = os.cpu_count() or 1
-        v, dt, done = cpu_reference_iterations(1, 0, nth)
+        v, dt, done = cpu_reference_iterations(REF_STEPS, REF_WARMUP, nth, REF_BUDGET_S)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nth, "kind": "port",
-                                "sample": "1 CG iteration of water32 (first iteration after ortho), CPU restatement, "
-                                          "OpenMP on all host threads"}
+                                "sample": f"{done} CG iterations of water32 (after {REF_WARMUP} warm-up, bounded at "
+                                          f"{REF_BUDGET_S:.0f} s of timed work; the reference arm's window), CPU "
+                                          "restatement of the reference's FP64 path, OpenMP on all host threads"}
     if dist:
         dist.barrier()
         dist.destroy_process_group()

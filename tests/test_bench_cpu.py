@@ -68,7 +68,7 @@ def test_reference_arm_other_ranks_print_nothing(capsys):
 
 def _arm(value, e, f, eig, md=True):
     return {"value": value, "ms_per_step": 1000.0 / value, "e2e": {"value": value / 2}, "clocks": {},
-            "md": {"steps_per_s": value / 100} if md else None, "nat": 3,
+            "md": {"steps_per_s": value / 100} if md else None, "nat": 3, "na": [1],
             "e_conv": e, "f_conv": np.array(f), "eig_conv": eig}
 
 
@@ -88,3 +88,21 @@ def test_compare_arms_reports_eigenvalue_failure_and_no_md():
     assert c["dEig_max_Ha"] is None and c["eigenvalue_error"].startswith("amdk_apply_h")
     c = bench.compare_arms(_arm(400.0, 0, [[0, 0, 0]], None, md=False), _arm(600.0, 0, [[0, 0, 0]], None, md=False))
     assert "dE_Ha_per_atom" not in c and abs(c["scf_speedup"] - 1.5) < 1e-12
+
+
+def test_compare_arms_against_the_oracle_fixture():
+    f64 = _arm(400.0, -17.0, [[[0.1, 0.0, 0.0]]], None)
+    mx = _arm(600.0, -17.0 + 3e-7, [[[0.1 + 2e-6, 0.0, 0.0]]], None)
+    fx = {"energies": {"etotal": -17.0 - 6e-7}, "forces": [[0.1 - 1e-6, 0.0, 0.0]], "gcut": 1e-6, "iterations": 9}
+    v = bench.compare_arms(f64, mx, fx)["vs_oracle"]
+    assert abs(v["fp64"]["dE_Ha_per_atom"] - 2e-7) < 1e-12 and abs(v["mixed"]["dE_Ha_per_atom"] - 3e-7) < 1e-12
+    assert abs(v["fp64"]["dF_max_Ha_per_bohr"] - 1e-6) < 1e-12 and abs(v["mixed"]["dF_max_Ha_per_bohr"] - 3e-6) < 1e-12
+
+
+def test_clock_sampler_without_nvml(monkeypatch):
+    """No NVML (no GPU here): the sampler reports why, never raises."""
+    cs = bench.ClockSampler(0)
+    monkeypatch.setattr(cs, "_handle", lambda: (_ for _ in ()).throw(RuntimeError("no driver")))
+    cs.start()
+    out = cs.stop()
+    assert out["samples"] == 0 and out["sm_mhz"] is None and "no driver" in out["reasons"][0]

@@ -15,6 +15,9 @@
 - water32 ionic forces: central finite differences (delta = 1e-3 bohr) of the
   GPU total energy on 6 seeded atom components against the backward entry
   (dE/dR), within 1e-4 Ha/bohr, for an FP64 and a mixed engine.
+- si64 (64 Si, GTH with s and p projectors, 30 Ry, 72^3, 128 bands): the
+  backward entry against central finite differences on 2 seeded atom
+  components, within 1e-4 Ha/bohr.
 - Si FCC (the reference's bulk_si run, s and p projectors): the GPU ionic
   forces at convergence against the reference's geometry-optimisation start
   gradient (tests/bulk_si/geo_opt/atom_force.dat), within 1e-5 Ha/bohr."""
@@ -24,7 +27,7 @@ import pytest
 from amdkiit_b200 import configs
 from amdkiit_b200.engine import FP64, MIXED, Engine
 from oracle.oracle import Oracle
-from tests.helpers import golden, golden_oracle, load_fixture, oracle_eigenvalues, start_coefficients
+from tests.helpers import golden, golden_oracle, load_fixture, start_coefficients
 
 pytestmark = pytest.mark.gpu
 
@@ -144,7 +147,7 @@ def _energy_at(e, atco, c0, gcut):
     e.set_positions(atco)
     e.set_wfn(c0)
     e.ortho()
-    n, en, gm = e.wfn_opt(3000, gcut)
+    n, en, gm = e.wfn_opt(4000, gcut)
     assert gm < gcut
     return en["etotal"]
 
@@ -179,6 +182,32 @@ def test_water32_backward_matches_finite_differences():
         print((isp, ia, k), fd, grad[isp, ia, k], grad_mx[isp, ia, k])
         assert abs(fd - grad[isp, ia, k]) < F_TOL, (isp, ia, k, fd, grad[isp, ia, k])
         assert abs(fd - grad_mx[isp, ia, k]) < F_TOL, (isp, ia, k, fd, grad_mx[isp, ia, k])
+    e.close()
+
+
+def test_si64_backward_matches_finite_differences():
+    """p-projector forces (NLFOR with l = 1, the dbeta projections of all
+    three directions) through the backward entry against central
+    differences of the converged GPU energy; the reference's fixed-step PCG
+    needs ~1600 iterations from the seeded start on this cell."""
+    s = configs.si64()
+    e = Engine(s, FP64)
+    e.set_wfn(seeded(e, s))
+    e.ortho()
+    n, en, gm = e.wfn_opt(4000, 1e-7)
+    assert gm < 1e-7, (n, gm)
+    grad = e.backward()
+    c0 = e.get_wfn()
+    x0 = s.atco()
+    rng = np.random.default_rng(64)
+    d = 1e-3
+    for _ in range(2):
+        ia, k = int(rng.integers(s.na[0])), int(rng.integers(3))
+        xp = x0.copy(); xp[0, ia, k] += d
+        xm = x0.copy(); xm[0, ia, k] -= d
+        fd = (_energy_at(e, xp, c0, 1e-8) - _energy_at(e, xm, c0, 1e-8)) / (2 * d)
+        print((0, ia, k), fd, grad[0, ia, k])
+        assert abs(fd - grad[0, ia, k]) < F_TOL, (ia, k, fd, grad[0, ia, k])
     e.close()
 
 
