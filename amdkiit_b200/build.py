@@ -21,14 +21,27 @@ def _nvcc() -> str:
     return cand
 
 
-def needs_build() -> bool:
-    if not os.path.exists(LIB):
-        return True
-    t = os.path.getmtime(LIB)
+STAMP = LIB + ".sources"
+
+
+def _sources_digest() -> str:
+    """SHA-256 over the sources and headers the library is built from."""
+    import hashlib
+    h = hashlib.sha256()
     for f in SOURCES + HEADERS:
-        if os.path.getmtime(os.path.join(CSRC, f)) > t:
-            return True
-    return False
+        with open(os.path.join(CSRC, f), "rb") as fh:
+            h.update(f.encode() + b"\0" + fh.read())
+    return h.hexdigest()
+
+
+def needs_build() -> bool:
+    """True unless libamdk.so exists and was built from the current sources
+    (a digest of their contents, not their modification times, which a
+    copy of the tree does not keep)."""
+    if not os.path.exists(LIB) or not os.path.exists(STAMP):
+        return True
+    with open(STAMP) as f:
+        return f.read().strip() != _sources_digest()
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
@@ -53,6 +66,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)
     os.replace(tmp, LIB)
+    with open(STAMP, "w") as f:
+        f.write(_sources_digest() + "\n")
     return LIB
 
 

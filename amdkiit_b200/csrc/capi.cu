@@ -10,6 +10,7 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <mutex>
 #include <queue>
 #include <type_traits>
 #include <string>
@@ -131,6 +132,7 @@ struct amdk_ctx {
   double *d_gam = nullptr, *d_uinv = nullptr;
   int *d_info = nullptr;
   double *d_part = nullptr, *d_scal = nullptr, *d_force = nullptr, *d_esr = nullptr, *d_fsr = nullptr;
+  unsigned *d_ticket = nullptr;  // tickets of the self-finishing reductions (TK_*)
   // pencil path (cubic grids with a specialised length): tables and buffers
   bool pencil_vpsi = false, pencil_density = false;
   double *h_pin = nullptr;  // pinned: scalar slots [S_NSCAL], GEMAX, CG step
@@ -138,6 +140,7 @@ struct amdk_ctx {
   // GEMAX read), keyed by segment, precision/forces flag, which buffer holds
   // C0, and profiling
   struct SegGraph {
+    cudaGraph_t graph = nullptr;  // kept: an ensemble launches it as a child graph
     cudaGraphExec_t exec = nullptr;
     std::vector<ProfRec> recs;
     size_t nevents = 0;
@@ -157,8 +160,15 @@ struct amdk_ctx {
   double *d_sgnsq = nullptr;               // per-band sums of squares (by segment) of the slicing pass
   int *d_sgerr = nullptr;
   long sg_kpad = 0;
+  long sg_plim = SG_SPIN;  // poll limit of the slice kernels' pipeline waits (options.reserved[0])
   int sg_ktiles = 0, sg_per = 0, sg_chunks = 0, sg_mtiles = 0;
   void *sg_c0_buf = nullptr;  // the C0 buffer whose digit planes are in d_plA (written by the ortho)
+  // projector planes (mixed path, nproj <= 128; 3 nproj <= 128 for the dbeta rows):
+  // P and Q = -i G_k P sliced once per geometry, for fnl and D_FNL on the tensor cores
+  bool sg_proj = false, sg_dproj = false;
+  int8_t *d_plP = nullptr, *d_plQ = nullptr;
+  double *d_sgP = nullptr, *d_sgQ = nullptr;
+  CUtensorMap tm_p_tn, tm_q_tn;
   CUtensorMap tm_a_tn, tm_b_tn, tm_a_nn, tm_s_nn;
   bool warm[2] = {false, false};  // an eager iteration has run at this pair precision
   void *c0_first = nullptr;       // the buffer that held C0 at creation
@@ -173,11 +183,14 @@ struct amdk_ctx {
   int *h_info = nullptr;    // pinned: Cholesky status
   int pencil_groups = 1;  // upper bound on the density pair groups
   int ct_vpsi = 0, ct_dens = 0;  // column tiles of the pencil kernels (current precision)
+  int ns_dens = 1;               // register slots of the density kernel's sums (tiles x task rounds)
+  int nsd_p[2] = {1, 1};
   bool pv_p[2] = {false, false}, pd_p[2] = {false, false};  // per pair precision: FP64, mixed
   int ctv_p[2] = {0, 0}, ctd_p[2] = {0, 0};
   int pn1 = 0, pn2 = 0;          // two-level split n = pn1 * pn2
   int nsm = 148;
   std::map<int, int> pencil_grp_cache;
+  int vpsi_tuned[2] = {0, 0};  // batch size the V(r)psi column tile was measured for, per precision
   PencilGeom pg{};
   int *d_rpos = nullptr, *d_gmapt = nullptr, *d_zinv = nullptr, *d_postp = nullptr, *d_postm = nullptr;
   double *d_rhopart = nullptr;
@@ -252,8 +265,6 @@ static void prof_harvest(amdk_ctx *c) {
   c->evused = 0;
 }
 
-// scalar slots in d_scal
-enum { S_GG = 0, S_GGPREV, S_EH, S_ELOC, S_EXC, S_EKIN, S_ENL, S_GMAX, S_ISTEP, S_NSCAL = 16 };
 
 static int nblk(long n, int t = NTHR) { return (int)std::min<long>((n + t - 1) / t, 1L << 30); }
 
@@ -308,8 +319,9 @@ template <auto K> static void smem_opt_in() {
   (void)done;
 }
 
-template <typename C> static size_t x_smem(int n1) { return 2 * (size_t)n1 * (LX + 1) * sizeof(C) + n1 * sizeof(C); }
-template <typename C> static size_t yz_smem(int n) { return 2 * (size_t)n * TX * sizeof(C) + n * sizeof(C); }
+// shared memory of the slab-path kernels: two tiles and the twiddle tables (2n)
+template <typename C> static size_t x_smem(int n1) { return 2 * (size_t)n1 * (LX + 1) * sizeof(C) + 2 * n1 * sizeof(C); }
+template <typename C> static size_t yz_smem(int n) { return 2 * (size_t)n * TX * sizeof(C) + 2 * n * sizeof(C); }
 
 template <typename C> static void set_smem_attrs() {
   int mx = 227 * 1024;
@@ -422,12 +434,10 @@ static int grid_to_rays(amdk_ctx *c, int T, const double2 *cgrid, const double *
 
 // ------------------------------------------------------------------ pencil path
 // shared memory of a pencil block: slab plane, column tile of ct columns,
-// twiddles and the kz -> slab index table (+ the accumulator for the density)
+// the twiddle tables (2n) and the kz -> slab index table
 template <typename C> static size_t pencil_smem(int n, int nz, int ct) {
-  return ((size_t)(nz + ct) * (n + 1) + n) * sizeof(C) + n * sizeof(int);
+  return ((size_t)(nz + ct) * (n + 1) + 2 * n) * sizeof(C) + n * sizeof(int);
 }
-// density accumulator: FP32 for float2 data (the mixed path ends on FP64), FP64 otherwise
-template <typename C> static size_t pencil_acc_smem(int n) { return (size_t)n * (n + 1) * (sizeof(C) == 8 ? 4 : 8); }
 // widest column tile with the block within `budget` bytes (0: none fits)
 template <typename C> static int pencil_tile(int n, int nz, size_t extra, size_t budget) {
   const size_t base = pencil_smem<C>(n, nz, 0) + extra;
@@ -437,7 +447,30 @@ template <typename C> static int pencil_tile(int n, int nz, size_t extra, size_t
   const int tiles = (n + widest - 1) / widest;  // equal tiles
   return (n + tiles - 1) / tiles;
 }
-template <typename C> static size_t xt_smem(int n1) { return ((size_t)XL * (n1 + 1) + n1) * sizeof(C); }
+// Column tiles of the density pencil kernel: the fewest equal tiles (1, 2 or
+// 4) whose block fits the shared memory of two blocks per SM (else of one),
+// whose group sums fit 1, 2 or 4 register slots (tiles x rounds of PNT
+// tasks) and whose final staging of the sums (n x (n+1) reals) fits over the
+// plane and the tile.  ct = 0 when none does.
+static void density_tiles(int n, int nz, size_t csize, size_t lim, int *ct, int *ns) {
+  *ct = 0;
+  *ns = 1;
+  const int n1f = fft_n1(n);
+  for (size_t budget : {lim / 2, lim})
+    for (int tiles : {1, 2, 4}) {
+      const int w = (n + tiles - 1) / tiles;
+      const size_t smem = ((size_t)(nz + w) * (n + 1) + 2 * n) * csize + n * sizeof(int);
+      const int reps = (w * n1f + PNT - 1) / PNT;
+      const int slots = tiles * reps;
+      const bool stage_ok = (size_t)n * (n + 1) * (csize / 2) <= (size_t)(nz + w) * (n + 1) * csize;
+      if (smem <= budget && stage_ok && (slots == 1 || slots == 2 || slots == 4) && (n + w - 1) / w == tiles) {
+        *ct = w;
+        *ns = slots;
+        return;
+      }
+    }
+}
+template <typename C> static size_t xt_smem(int n1) { return ((size_t)XL * (n1 + 1) + 2 * n1) * sizeof(C); }
 // Pair groups of the density pencil kernel: each (x-plane, group) block sums
 // its group's pairs into its own partial grid.  Pick the group count whose
 // block list, scheduled greedily on the SMs, ends first; each group also
@@ -499,35 +532,168 @@ template <typename C> static void xt_fwd(amdk_ctx *c, int T) {
   });
   prof_end(c);
 }
+// ------------------------------------------------------------------ tuning
+// Launch shapes measured at first use (AMDK_NO_TUNE=1: the model's choice
+// instead) are kept per context and, when AMDK_TUNE_CACHE names a file, in
+// that JSON object of "key": value pairs (keys name the kernel, precision,
+// grid, slab planes and batch), so that later contexts and processes reuse
+// them without measuring.
+static std::mutex g_tune_mu;
+static std::map<std::string, int> g_tune;
+static bool g_tune_loaded = false;
+static const char *tune_path() {
+  const char *p = getenv("AMDK_TUNE_CACHE");
+  return (p && *p) ? p : nullptr;
+}
+static void tune_load_locked() {
+  if (g_tune_loaded) return;
+  g_tune_loaded = true;
+  const char *path = tune_path();
+  if (!path) return;
+  FILE *f = std::fopen(path, "r");
+  if (!f) return;
+  std::string txt;
+  char buf[4096];
+  size_t nr;
+  while ((nr = std::fread(buf, 1, sizeof(buf), f)) > 0) txt.append(buf, nr);
+  std::fclose(f);
+  size_t i = 0;
+  while ((i = txt.find('"', i)) != std::string::npos) {
+    const size_t j = txt.find('"', i + 1);
+    if (j == std::string::npos) break;
+    const size_t k = txt.find(':', j);
+    if (k == std::string::npos) break;
+    g_tune[txt.substr(i + 1, j - i - 1)] = (int)std::strtol(txt.c_str() + k + 1, nullptr, 10);
+    i = txt.find_first_of(",}", k);
+    if (i == std::string::npos) break;
+  }
+}
+static bool tune_get(const std::string &key, int *v) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  tune_load_locked();
+  auto it = g_tune.find(key);
+  if (it == g_tune.end()) return false;
+  *v = it->second;
+  return true;
+}
+static void tune_put(const std::string &key, int v) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  tune_load_locked();
+  g_tune[key] = v;
+  const char *path = tune_path();
+  if (!path) return;
+  const std::string tmp = std::string(path) + ".tmp";
+  FILE *f = std::fopen(tmp.c_str(), "w");
+  if (!f) return;
+  std::fprintf(f, "{\n");
+  size_t n = 0;
+  for (auto &kv : g_tune) std::fprintf(f, "  \"%s\": %d%s\n", kv.first.c_str(), kv.second, ++n < g_tune.size() ? "," : "");
+  std::fprintf(f, "}\n");
+  std::fclose(f);
+  std::rename(tmp.c_str(), path);
+}
+// key of a tuned pencil launch shape
+static std::string pencil_key(const amdk_ctx *c, const char *what, int T) {
+  const Geom &g = c->geom;
+  return std::string(what) + "/" + (c->precision == AMDK_MIXED ? "mixed" : "fp64") + "/" + std::to_string(g.n1) + "x" +
+         std::to_string(g.n2) + "x" + std::to_string(g.n3) + "/nz" + std::to_string(c->pg.nz) + "/T" + std::to_string(T);
+}
+
+template <typename C, int N> static void launch_pencil_vpsi(amdk_ctx *c, int T, int ct, C *rb) {
+  typedef decltype(C().x) Rl;
+  smem_opt_in<k_pencil_vpsi<C, N>>();
+  ++c->nlaunch;
+  k_pencil_vpsi<C, N><<<dim3(c->geom.n1, T), PNT, pencil_smem<C>(N, c->pg.nz, ct), c->st>>>(
+      c->pg, plan<C>(c, 1), rb, (const Rl *)c->d_vt, ct);
+}
+// Column-tile width of the V(r)psi pencil kernel for T pairs: measured once
+// per shape (every width ceil(N/t), t = 1..6, whose block fits, launched on a
+// scratch copy of the ray buffer, which the kernel transforms in place),
+// from the tuning cache, or the model's choice (capture, AMDK_NO_TUNE=1).
+template <typename C, int N> static int vpsi_tile(amdk_ctx *c, int T) {
+  const std::string key = pencil_key(c, "pencil_vpsi_tile", T);
+  const int q = (c->precision == AMDK_MIXED) ? 1 : 0;
+  int best = c->ctv_p[q];
+  if (c->vpsi_tuned[q] == T) return best;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(c->st, &cap);
+  if (cap != cudaStreamCaptureStatusNone || !c->tune) return best;
+  int cached = 0;
+  if (tune_get(key, &cached) && cached >= 8 && pencil_smem<C>(N, c->pg.nz, cached) <= 227 * 1024) {
+    best = cached;
+  } else {
+    const size_t bytes = (size_t)T * rstride(c, 0) * sizeof(C);
+    C *scratch = nullptr;
+    if (cudaMalloc(&scratch, bytes) == cudaSuccess) {
+      cudaMemcpyAsync(scratch, c->d_rb, bytes, cudaMemcpyDeviceToDevice, c->st);
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      const long nl = c->nlaunch;
+      float best_ms = 1e30f;
+      int prev = 0;
+      for (int t = 1; t <= 6; ++t) {
+        const int w = (N + t - 1) / t;
+        if (w == prev || w < 8 || pencil_smem<C>(N, c->pg.nz, w) > 227 * 1024) continue;
+        prev = w;
+        launch_pencil_vpsi<C, N>(c, T, w, scratch);  // warm
+        cudaEventRecord(e0, c->st);
+        launch_pencil_vpsi<C, N>(c, T, w, scratch);
+        launch_pencil_vpsi<C, N>(c, T, w, scratch);
+        cudaEventRecord(e1, c->st);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = w;
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      cudaStreamSynchronize(c->st);
+      cudaFree(scratch);
+      c->nlaunch = nl;  // tuning launches are not part of the work
+      tune_put(key, best);
+    }
+    cudaGetLastError();
+  }
+  c->ctv_p[q] = best;
+  c->ct_vpsi = best;
+  c->vpsi_tuned[q] = T;
+  return best;
+}
 template <typename C> static void pencil_vpsi(amdk_ctx *c, int T) {
   const Geom &g = c->geom;
   typedef decltype(C().x) Rl;
   const double npt = (double)g.n1 * g.n2 * g.n3;
-  prof_begin(c, KT_ZVPSI, 2.0 * T * rstride(c, 0) * sizeof(C) + npt * sizeof(Rl));
   with_n(g.n2, [&](auto NC) {
     constexpr int N = decltype(NC)::value;
     if constexpr (N > 0) {
-      smem_opt_in<k_pencil_vpsi<C, N>>();
-      ++c->nlaunch;
-      const size_t sm = pencil_smem<C>(N, c->pg.nz, c->ct_vpsi);
-      k_pencil_vpsi<C, N><<<dim3(g.n1, T), PNT, sm, c->st>>>(c->pg, plan<C>(c, 1), (C *)c->d_rb, (const Rl *)c->d_vt,
-                                                             c->ct_vpsi);
+      const int ct = vpsi_tile<C, N>(c, T);
+      prof_begin(c, KT_ZVPSI, 2.0 * T * rstride(c, 0) * sizeof(C) + npt * sizeof(Rl));
+      launch_pencil_vpsi<C, N>(c, T, ct, (C *)c->d_rb);
+      prof_end(c);
     }
   });
-  prof_end(c);
 }
-template <typename C> static void launch_pencil_density(amdk_ctx *c, int p0, int T, int grp, int add) {
+template <typename C, int N, int NS> static void launch_pencil_density_ns(amdk_ctx *c, int p0, int T, int grp, int add) {
   const Geom &g = c->geom;
-  const size_t sm = pencil_acc_smem<C>(g.n2) + pencil_smem<C>(g.n2, c->pg.nz, c->ct_dens);
+  const size_t sm = pencil_smem<C>(N, c->pg.nz, c->ct_dens);
   const int per = (T + grp - 1) / grp;
-  with_n(g.n2, [&](auto NC) {
-    constexpr int N = decltype(NC)::value;
-    if constexpr (N > 0) {
-      smem_opt_in<k_pencil_density<C, N>>();
-      ++c->nlaunch;
-      k_pencil_density<C, N><<<dim3(g.n1, grp), PNT, sm, c->st>>>(c->pg, plan<C>(c, 1), (const C *)c->d_rb, T, per,
+  smem_opt_in<k_pencil_density<C, N, NS>>();
+  ++c->nlaunch;
+  k_pencil_density<C, N, NS><<<dim3(g.n1, grp), PNT, sm, c->st>>>(c->pg, plan<C>(c, 1), (const C *)c->d_rb, T, per,
                                                                   c->d_wa + p0, c->d_wb + p0, c->d_rhopart, c->ct_dens,
                                                                   add);
+}
+template <typename C> static void launch_pencil_density(amdk_ctx *c, int p0, int T, int grp, int add) {
+  with_n(c->geom.n2, [&](auto NC) {
+    constexpr int N = decltype(NC)::value;
+    if constexpr (N > 0) {
+      if (c->ns_dens == 1) launch_pencil_density_ns<C, N, 1>(c, p0, T, grp, add);
+      else if (c->ns_dens == 2) launch_pencil_density_ns<C, N, 2>(c, p0, T, grp, add);
+      else launch_pencil_density_ns<C, N, 4>(c, p0, T, grp, add);
     }
   });
 }
@@ -538,7 +704,7 @@ template <typename C> static void launch_pencil_density(amdk_ctx *c, int p0, int
 // choice is used instead.
 template <typename C> static int density_groups(amdk_ctx *c, int T) {
   const Geom &g = c->geom;
-  const size_t sm = pencil_acc_smem<C>(g.n2) + pencil_smem<C>(g.n2, c->pg.nz, c->ct_dens);
+  const size_t sm = pencil_smem<C>(g.n2, c->pg.nz, c->ct_dens);
   const int key = 2 * T + (c->precision == AMDK_MIXED ? 1 : 0);
   auto it = c->pencil_grp_cache.find(key);
   if (it != c->pencil_grp_cache.end()) return it->second;
@@ -546,7 +712,13 @@ template <typename C> static int density_groups(amdk_ctx *c, int T) {
                                    c->pencil_groups);
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(c->st, &cap);
-  if (cap == cudaStreamCaptureStatusNone && c->tune) {
+  const std::string tkey = pencil_key(c, "pencil_density_groups", T) + "/ct" + std::to_string(c->ct_dens) + "/ns" +
+                           std::to_string(c->ns_dens);
+  int cached = 0;
+  if (cap == cudaStreamCaptureStatusNone && c->tune && tune_get(tkey, &cached) && cached >= 1 &&
+      cached <= std::min(c->pencil_groups, T)) {
+    best = cached;
+  } else if (cap == cudaStreamCaptureStatusNone && c->tune) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -571,6 +743,7 @@ template <typename C> static int density_groups(amdk_ctx *c, int T) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->nlaunch = nl;  // tuning launches are not part of the work
+    tune_put(tkey, best);
   }
   c->pencil_grp_cache.emplace(key, best);
   return best;
@@ -586,11 +759,6 @@ template <typename C> static void pencil_density(amdk_ctx *c, int p0, int T) {
 }
 
 // ------------------------------------------------------------------ routines
-static int finish_sums(amdk_ctx *c, int nk, int slot) {
-  ++c->nlaunch;
-  k_finish_sum<<<nk, NTHR, 0, c->st>>>(c->d_part, RED_BLOCKS, c->d_scal + slot, nk);
-  return 0;
-}
 
 template <typename C> static int density_pairs_t(amdk_ctx *c) {
   const HostSetup &h = c->hs;
@@ -663,8 +831,7 @@ template <typename C> static int potential_t(amdk_ctx *c) {
   // eval_pot in G space and E_H, E_loc sums
   ++c->nlaunch;
   k_vloc_g<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngrho, c->d_hg, h.tpiba2, c->d_rhog, c->d_erhos, c->d_evps, c->d_vg,
-                                           c->d_part);
-  RC(finish_sums(c, 2, S_EH));
+                                           c->d_part, c->d_scal + S_EH, c->d_ticket + TK_VLOC);
   int gga = (h.xc == AMDK_XC_PBE);
   double2 *g0 = c->d_cgrid, *g1 = c->d_cgrid + npt;
   if (gga) {
@@ -673,8 +840,13 @@ template <typename C> static int potential_t(amdk_ctx *c) {
     RC(field_to_grid<C>(c, 2, c->d_fp, c->d_fm, c->d_cgrid));
   }
   ++c->nlaunch;
-  k_xc<<<RED_BLOCKS, NTHR, 0, c->st>>>(npt, h.xc, c->d_rho, g0, g1, c->d_part);
-  RC(finish_sums(c, 1, S_EXC));
+  // the functional in the transforms' precision (FP32 on the mixed path)
+  if (sizeof(C) == sizeof(float2))
+    k_xc<float><<<RED_BLOCKS, NTHR, 0, c->st>>>(npt, h.xc, c->d_rho, g0, g1, c->d_part, c->d_scal + S_EXC,
+                                               c->d_ticket + TK_XC);
+  else
+    k_xc<double><<<RED_BLOCKS, NTHR, 0, c->st>>>(npt, h.xc, c->d_rho, g0, g1, c->d_part, c->d_scal + S_EXC,
+                                                c->d_ticket + TK_XC);
   RC(grid_to_rays<C>(c, gga ? 2 : 1, c->d_cgrid, nullptr));
   double scale = 1.0 / (double)npt;
   ++c->nlaunch;
@@ -703,20 +875,43 @@ static int do_potential(amdk_ctx *c) {
   return potential_t<double2>(c);
 }
 
+// The unpack of pairs [p0, p0+T) (kinetic term, occupation scaling) fused
+// with fnonloc for the first UNPACK_NPJ projectors; further projectors are
+// added in chunks (k_fnonloc_add).  pp/pm: +G/-G positions in the ray buffer.
+template <typename C> static void unpack_h(amdk_ctx *c, int p0, int T, const int *pp, const int *pm) {
+  typedef decltype(C().x) Rl;
+  const HostSetup &h = c->hs;
+  const Geom &g = c->geom;
+  const double scale = 1.0 / ((double)g.n1 * g.n2 * g.n3);
+  const int npj0 = std::min(c->nproj, UNPACK_NPJ);
+  const int nb = std::min(2 * T, c->nstate - 2 * p0);
+  ++c->nlaunch;
+  constexpr int PAIRS = unpack_pairs<C>();
+  const dim3 gu(nblk(h.ngpw, 128), (T + PAIRS - 1) / PAIRS);
+  k_unpack_fnonloc<C><<<gu, 128, (size_t)2 * PAIRS * npj0 * sizeof(Rl), c->st>>>(
+      h.ngpw, c->nstate, 2 * p0, T, npj0, pp, pm, (const C *)c->d_rb, rstride(c, 0), scale, c->d_hg, h.tpiba2,
+      c->d_occ, c->d_P, c->d_D, c->nproj, c->d_c0, c->d_c2);
+  for (int j0 = npj0; j0 < c->nproj; j0 += UNPACK_NPJ) {
+    const int npj = std::min(UNPACK_NPJ, c->nproj - j0);
+    smem_opt_in<k_fnonloc_add<UNPACK_NPJ>>();
+    ++c->nlaunch;
+    const dim3 ga(nblk(h.ngpw, 128), (nb + FNL_BANDS - 1) / FNL_BANDS);
+    k_fnonloc_add<UNPACK_NPJ><<<ga, 128, (size_t)FNL_BANDS * npj * sizeof(double), c->st>>>(
+        h.ngpw, 2 * p0, nb, j0, npj, c->d_P, c->d_D, c->nproj, c->d_c2);
+  }
+}
+
+// vpsi + fnonloc: C2 = -f H C0 (C2 is written, not accumulated)
 template <typename C> static int apply_h_t(amdk_ctx *c) {
   const HostSetup &h = c->hs;
   const Geom &g = c->geom;
-  double scale = 1.0 / ((double)g.n1 * g.n2 * g.n3);
   if (c->pencil_vpsi) {
     for (int p0 = 0; p0 < c->npairs; p0 += c->batch) {
       int T = std::min(c->batch, c->npairs - p0);
       xt_bwd_pair<C>(c, p0, T);
       pencil_vpsi<C>(c, T);
       xt_fwd<C>(c, T);
-      dim3 gu(nblk(h.ngpw), T);
-      ++c->nlaunch;
-      k_unpack_vpsi<C><<<gu, NTHR, 0, c->st>>>(h.ngpw, c->nstate, 2 * p0, T, c->d_postp, c->d_postm, (C *)c->d_rb,
-                                               rstride(c, 0), scale, c->d_hg, h.tpiba2, c->d_occ, c->d_c0, c->d_c2);
+      unpack_h<C>(c, p0, T, c->d_postp, c->d_postm);
     }
     CK(cudaGetLastError());
     return 0;
@@ -735,96 +930,13 @@ template <typename C> static int apply_h_t(amdk_ctx *c) {
     z_pass<C, Z_VPSI>(c, 0, T, nullptr, nullptr);
     y_pass<C>(c, 0, -1, T);
     x_fwd<C>(c, 0, T);
-    dim3 gu(nblk(h.ngpw), T);
-    ++c->nlaunch;
-    k_unpack_vpsi<C><<<gu, NTHR, 0, c->st>>>(h.ngpw, c->nstate, 2 * p0, T, c->d_posp, c->d_posm, (C *)c->d_rb,
-                                             rstride(c, 0), scale, c->d_hg, h.tpiba2, c->d_occ, c->d_c0, c->d_c2);
+    unpack_h<C>(c, p0, T, c->d_posp, c->d_posm);
   }
   CK(cudaGetLastError());
   return 0;
 }
 
 // fnl (pseudopotential.f90:164-226): nl = 2 P^T C0; hn = H nl
-static int do_fnl(amdk_ctx *c) {
-  const HostSetup &h = c->hs;
-  if (c->nproj == 0) return 0;
-  const double two = 2.0, one = 1.0, zero = 0.0;
-  int n = c->nstate, K = 2 * h.ngpw;
-  CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, c->nproj, n, K, &two, (const double *)c->d_P, K,
-                 (const double *)c->d_c0, K, &zero, c->d_nl, c->nproj));
-  CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, c->nproj, n, c->nproj, &one, c->d_H, c->nproj, c->d_nl, c->nproj, &zero,
-                 c->d_hn, c->nproj));
-  return 0;
-}
-
-// energies from the device scalar slots (copied to the host)
-static int fill_energies(amdk_ctx *c, const double *sc, amdk_energies *e) {
-  const HostSetup &h = c->hs;
-  e->eh = sc[S_EH];
-  e->eloc = 2.0 * sc[S_ELOC] * h.omega;
-  e->eself = c->eself;
-  e->esr = c->esr;
-  e->estat = (sc[S_EH] * h.omega) + c->esr - c->eself;
-  e->eke = sc[S_EKIN] * h.tpiba2;
-  e->exc = h.omega / (double)(h.nr[0] * h.nr[1] * h.nr[2]) * sc[S_EXC];
-  e->enl = sc[S_ENL];
-  e->etotal = e->enl + e->eloc + e->eke + e->exc + e->estat;
-  if (!std::isfinite(e->etotal)) {
-    set_error("non-finite total energy");
-    return AMDK_ERR_NONFINITE;
-  }
-  return 0;
-}
-
-// pp_energy + e_total.  With e the energies are read back now (one stream
-// synchronisation); without, the scalar slots are copied to the pinned host
-// buffer in stream order for fill_energies after the caller's own sync.
-// the C0-only part of pp_energy/e_total: projections, E_nl, E_kin
-static int energy_c0_terms(amdk_ctx *c) {
-  const HostSetup &h = c->hs;
-  RC(do_fnl(c));
-  if (c->nproj) {
-    ++c->nlaunch;
-    k_nl_energy_d<<<RED_BLOCKS, NTHR, 0, c->st>>>(c->nproj, c->nstate, c->d_nl, c->d_hn, c->d_occ, c->d_D, c->d_part);
-    RC(finish_sums(c, 1, S_ENL));
-  } else {
-    CK(cudaMemsetAsync(c->d_scal + S_ENL, 0, sizeof(double), c->st));
-  }
-  ++c->nlaunch;
-  k_ekin<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngpw, c->nstate, c->d_c0, c->d_hg, c->d_occ, c->d_part);
-  RC(finish_sums(c, 1, S_EKIN));
-  return 0;
-}
-static int do_energy(amdk_ctx *c, amdk_energies *e) {
-  RC(energy_c0_terms(c));
-  CK(cudaMemcpyAsync(c->h_pin, c->d_scal, sizeof(double) * S_NSCAL, cudaMemcpyDeviceToHost, c->st));
-  if (e) {
-    CK(cudaStreamSynchronize(c->st));
-    RC(fill_energies(c, c->h_pin, e));
-  }
-  return 0;
-}
-
-static int do_fnonloc(amdk_ctx *c) {
-  const HostSetup &h = c->hs;
-  if (c->nproj == 0) return 0;
-  const double one = 1.0;
-  int K = 2 * h.ngpw;
-  CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, K, c->nstate, c->nproj, &one, (const double *)c->d_P, K, c->d_D,
-                 c->nproj, &one, (double *)c->d_c2, K));
-  ++c->nlaunch;
-  k_fnonloc_g0<<<nblk(c->nstate), NTHR, 0, c->st>>>(c->nproj, c->nstate, h.ngpw, c->d_P, c->d_D, c->d_c2);
-  CK(cudaGetLastError());
-  return 0;
-}
-
-static int do_apply_h(amdk_ctx *c) {
-  if (c->precision == AMDK_MIXED) RC(apply_h_t<float2>(c));
-  else RC(apply_h_t<double2>(c));
-  return do_fnonloc(c);
-}
-
-// forces (gradient.f90:5-34) and eval_GMAX
 // ------------------------------------------------- integer-slice GEMMs
 // Mixed path with at most 128 bands: Lambda, S, C2 -= C0 Lambda and C0 U^{-1}
 // on the int8 tensor cores (slicegemm.cuh) instead of DGEMM/DTRMM.
@@ -888,26 +1000,49 @@ static int sg_setup(amdk_ctx *c) {
   c->sg_ready = true;
   return 0;
 }
-// digit planes and row scales of the bands of x (C0 or C2)
-static void sg_slice(amdk_ctx *c, const double2 *x, int8_t *planes, double *scale) {
+// digit planes and row scales of the first nrows rows of x (C0, C2 or a
+// projector matrix; rows up to 128 are planes of zeros)
+static void sg_slice(amdk_ctx *c, const double2 *x, int8_t *planes, double *scale, int nrows = -1) {
   const long K = 2L * c->hs.ngpw;
+  if (nrows < 0) nrows = c->nstate;
   c->nlaunch += 2;
   cudaMemsetAsync(c->d_sgmax, 0, sizeof(unsigned long long) * SG_M, c->st);
-  k_band_absmax<<<dim3(SG_SEG, c->nstate), 256, 0, c->st>>>((const double *)x, K, K, c->nstate, c->d_sgmax,
-                                                             c->d_sgnsq);
-  k_slice_rows<SG_S><<<dim3(SG_SEG, SG_M), 256, 0, c->st>>>((const double *)x, K, K, c->nstate, c->d_sgmax, planes,
+  k_band_absmax<<<dim3(SG_SEG, nrows), 256, 0, c->st>>>((const double *)x, K, K, nrows, c->d_sgmax, c->d_sgnsq);
+  k_slice_rows<SG_S><<<dim3(SG_SEG, SG_M), 256, 0, c->st>>>((const double *)x, K, K, nrows, c->d_sgmax, planes,
                                                             c->sg_kpad, scale);
 }
-// out (n x n) = alpha diag(sa) A B^T diag(sb), the product over the real index
+// out (nm x n, leading dimension ldo) = alpha diag(sa) A B^T diag(sb), the
+// product over the real index; n = nstate columns (B = C0 or C2 planes)
 static void sg_tn(amdk_ctx *c, const CUtensorMap &ta, const CUtensorMap &tb, int same, const double *sa,
-                  const double *sb, double alpha, double *out) {
+                  const double *sb, double alpha, double *out, int nm = -1, int ldo = -1) {
   const int n = c->nstate;
+  if (nm < 0) nm = n;
+  if (ldo < 0) ldo = n;
   c->nlaunch += 2;
   k_sgemm_tn<SG_S><<<c->sg_chunks, SG_TN_THREADS, SgTn<SG_S>::SMEM, c->st>>>(ta, tb, same, c->sg_ktiles, c->sg_per, c->d_sgpart,
-                                                                     c->d_sgerr);
-  k_sgemm_reduce<<<n, SG_RG * SG_M, 0, c->st>>>(c->sg_chunks, c->d_sgpart, n, sa, sb, same ? c->d_sgnsq : nullptr,
-                                            alpha, out, n);
+                                                                     c->d_sgerr, c->sg_plim);
+  k_sgemm_reduce<<<n, SG_RG * SG_M, 0, c->st>>>(c->sg_chunks, c->d_sgpart, nm, sa, sb, same ? c->d_sgnsq : nullptr,
+                                            alpha, out, ldo);
 }
+// projector planes: set up once the projector count is known (mixed-capable
+// contexts with slice products)
+static int sg_proj_setup(amdk_ctx *c) {
+  if (!c->sg_ready || c->nproj == 0 || c->nproj > SG_M) return 0;
+  const size_t pl = (size_t)SG_S * SG_M * c->sg_kpad;
+  RC(c->alloc(&c->d_plP, pl));
+  RC(c->alloc(&c->d_sgP, SG_M));
+  RC(sg_encode(&c->tm_p_tn, c->d_plP, c->sg_kpad, SG_TN_KT, CU_TENSOR_MAP_SWIZZLE_64B));
+  c->sg_proj = true;
+  if (3 * c->nproj <= SG_M) {
+    RC(c->alloc(&c->d_plQ, pl));
+    RC(c->alloc(&c->d_sgQ, SG_M));
+    RC(sg_encode(&c->tm_q_tn, c->d_plQ, c->sg_kpad, SG_TN_KT, CU_TENSOR_MAP_SWIZZLE_64B));
+    c->sg_dproj = true;
+  }
+  return 0;
+}
+// C0's digit planes are those of the current C0 (written by the last ortho)
+static bool c0_planes_current(const amdk_ctx *c) { return c->sg_c0_buf == (const void *)c->d_c0; }
 // out (the real view, 2 ngpw x n) = (or -=, sub) C0 B for B n x n, with C0's
 // planes and scales in d_plA / d_sgA.  With digits (an orthonormalisation)
 // the result's own planes replace C0's in d_plA, scale 2 (|x| <= 1).
@@ -919,17 +1054,104 @@ static void sg_nn(amdk_ctx *c, const double *B, double2 *out, int sub, bool digi
   const dim3 grid(std::min(c->sg_mtiles, c->nsm));
   if (sub)
     k_sgemm_nn<SG_S, 1><<<grid, SG_NN_THREADS, SgNn<SG_S>::SMEM, c->st>>>(
-        c->tm_a_nn, c->tm_s_nn, c->sg_mtiles, K, (double *)out, K, n, c->d_sgS, nullptr, c->sg_kpad, c->d_sgerr);
+        c->tm_a_nn, c->tm_s_nn, c->sg_mtiles, K, (double *)out, K, n, c->d_sgS, nullptr, c->sg_kpad, c->d_sgerr, c->sg_plim);
   else if (digits)
     k_sgemm_nn<SG_S, 2><<<grid, SG_NN_THREADS, SgNn<SG_S>::SMEM, c->st>>>(
-        c->tm_a_nn, c->tm_s_nn, c->sg_mtiles, K, (double *)out, K, n, c->d_sgS, c->d_plA, c->sg_kpad, c->d_sgerr);
+        c->tm_a_nn, c->tm_s_nn, c->sg_mtiles, K, (double *)out, K, n, c->d_sgS, c->d_plA, c->sg_kpad, c->d_sgerr, c->sg_plim);
   else
     k_sgemm_nn<SG_S, 0><<<grid, SG_NN_THREADS, SgNn<SG_S>::SMEM, c->st>>>(
-        c->tm_a_nn, c->tm_s_nn, c->sg_mtiles, K, (double *)out, K, n, c->d_sgS, nullptr, c->sg_kpad, c->d_sgerr);
+        c->tm_a_nn, c->tm_s_nn, c->sg_mtiles, K, (double *)out, K, n, c->d_sgS, nullptr, c->sg_kpad, c->d_sgerr, c->sg_plim);
   if (digits) {
     ++c->nlaunch;
     k_sg_fill<<<1, SG_M, 0, c->st>>>(c->d_sgA, n, 2.0);
   }
+}
+
+// On the mixed path with the projector planes and C0's current planes: the
+// int8 tensor-core slice product (nl = 2 P^T C0, FP32-level accuracy);
+// otherwise DGEMM.
+static int do_fnl(amdk_ctx *c) {
+  const HostSetup &h = c->hs;
+  if (c->nproj == 0) return 0;
+  if (use_slice(c) && c->sg_proj && c0_planes_current(c)) {
+    sg_tn(c, c->tm_p_tn, c->tm_a_tn, 0, c->d_sgP, c->d_sgA, 2.0, c->d_nl, c->nproj, c->nproj);
+    return 0;
+  }
+  const double two = 2.0, zero = 0.0;
+  int n = c->nstate, K = 2 * h.ngpw;
+  CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, c->nproj, n, K, &two, (const double *)c->d_P, K,
+                 (const double *)c->d_c0, K, &zero, c->d_nl, c->nproj));
+  return 0;
+}
+
+// energies from the device scalar slots (copied to the host)
+static int fill_energies(amdk_ctx *c, const double *sc, amdk_energies *e) {
+  const HostSetup &h = c->hs;
+  e->eh = sc[S_EH];
+  e->eloc = 2.0 * sc[S_ELOC] * h.omega;
+  e->eself = c->eself;
+  e->esr = c->esr;
+  e->estat = (sc[S_EH] * h.omega) + c->esr - c->eself;
+  e->eke = sc[S_EKIN] * h.tpiba2;
+  e->exc = h.omega / (double)(h.nr[0] * h.nr[1] * h.nr[2]) * sc[S_EXC];
+  e->enl = sc[S_ENL];
+  e->etotal = e->enl + e->eloc + e->eke + e->exc + e->estat;
+  if (!std::isfinite(e->etotal)) {
+    set_error("non-finite total energy");
+    return AMDK_ERR_NONFINITE;
+  }
+  return 0;
+}
+
+// pp_energy + e_total.  With e the energies are read back now (one stream
+// synchronisation); without, the scalar slots are copied to the pinned host
+// buffer in stream order for fill_energies after the caller's own sync.
+// the C0-only part of pp_energy/e_total: projections, E_nl, E_kin
+static int energy_c0_terms(amdk_ctx *c) {
+  const HostSetup &h = c->hs;
+  RC(do_fnl(c));
+  if (c->nproj) {
+    ++c->nlaunch;
+    k_nl_energy_d<<<nblk((long)c->nproj * c->nstate), NTHR, 0, c->st>>>(c->nproj, c->nstate, c->d_H, c->d_nl, c->d_hn,
+                                                                          c->d_occ, c->d_D, c->d_part,
+                                                  c->d_scal + S_ENL, c->d_ticket + TK_ENL);
+  } else {
+    CK(cudaMemsetAsync(c->d_scal + S_ENL, 0, sizeof(double), c->st));
+  }
+  ++c->nlaunch;
+  k_ekin<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngpw, c->nstate, c->d_c0, c->d_hg, c->d_occ, c->d_part,
+                                         c->d_scal + S_EKIN, c->d_ticket + TK_EKIN);
+  return 0;
+}
+static int do_energy(amdk_ctx *c, amdk_energies *e) {
+  RC(energy_c0_terms(c));
+  CK(cudaMemcpyAsync(c->h_pin, c->d_scal, sizeof(double) * S_NSCAL, cudaMemcpyDeviceToHost, c->st));
+  if (e) {
+    CK(cudaStreamSynchronize(c->st));
+    RC(fill_energies(c, c->h_pin, e));
+  }
+  return 0;
+}
+
+static int do_apply_h(amdk_ctx *c) {
+  if (c->precision == AMDK_MIXED) return apply_h_t<float2>(c);
+  return apply_h_t<double2>(c);
+}
+
+// forces (gradient.f90:5-34) and eval_GMAX
+// occupied bands (occupation above 1e-5, as eval_GMAX and PCG count them)
+static int n_occupied(const amdk_ctx *c) {
+  int nocc = 0;
+  for (int i = 0; i < c->nstate; i++)
+    if (c->hs.occ[i] > 1e-5) nocc++;
+  return nocc;
+}
+// GEMAX and the preconditioned-gradient norm of PCG from the current C2, in
+// one pass: S_GMAX and S_GG
+static void gmax_precon(amdk_ctx *c) {
+  ++c->nlaunch;
+  k_gmax_precon<<<RED_BLOCKS, NTHR, 0, c->st>>>(c->hs.ngpw, n_occupied(c), c->d_vpp, c->d_occ, c->d_c2, c->d_part,
+                                                c->d_scal + S_GMAX, c->d_ticket + TK_GRAD);
 }
 
 static int do_gradient(amdk_ctx *c) {
@@ -955,33 +1177,24 @@ static int do_gradient(amdk_ctx *c) {
                    (double *)c->d_c2, K));
   ++c->nlaunch;
   k_zclean<<<nblk(n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c2);
-  int nocc = 0;
-  for (int i = 0; i < n; i++)
-    if (h.occ[i] > 1e-5) nocc++;
-  ++c->nlaunch;
-  k_gmax<<<RED_BLOCKS, NTHR, 0, c->st>>>((long)nocc * h.ngpw, c->d_c2, c->d_part);
-  ++c->nlaunch;
-  k_finish_max<<<1, NTHR, 0, c->st>>>(c->d_part, RED_BLOCKS, c->d_scal + S_GMAX);
+  gmax_precon(c);
   CK(cudaGetLastError());
   return 0;
 }
 
 // PCG; the step number goes through pinned host memory and the S_ISTEP slot
-// so that a captured graph of this step reads the current one
-static int do_pcg(amdk_ctx *c, int istep) {
+// so that a captured graph of this step reads the current one.  The
+// gradient norm S_GG is the one do_gradient left for the current C2
+// (recompute: form it here, for a caller that changed C2 since).
+static int do_pcg(amdk_ctx *c, int istep, bool recompute = false) {
   const HostSetup &h = c->hs;
   c->sg_c0_buf = nullptr;  // C0 changes in place
   c->h_pin[S_NSCAL + 1] = (double)istep;
   CK(cudaMemcpyAsync(c->d_scal + S_ISTEP, c->h_pin + S_NSCAL + 1, sizeof(double), cudaMemcpyHostToDevice, c->st));
-  int n = c->nstate, nocc = 0;
-  for (int i = 0; i < n; i++)
-    if (h.occ[i] > 1e-5) nocc++;
+  if (recompute) gmax_precon(c);
   ++c->nlaunch;
-  k_precon<<<RED_BLOCKS, NTHR, 0, c->st>>>(h.ngpw, n, nocc, c->d_vpp, c->d_occ, c->d_c2, c->d_cp, c->d_part);
-  RC(finish_sums(c, 1, S_GG));
-  ++c->nlaunch;
-  const long tot = (long)h.ngpw * n;
-  k_pcg_update<<<RED_BLOCKS * 4, NTHR, 0, c->st>>>(tot, c->d_scal, c->d_cp, c->d_hnm1, c->d_c0);
+  k_pcg_update<<<RED_BLOCKS * 4, NTHR, 0, c->st>>>(h.ngpw, c->nstate, c->d_scal, c->d_vpp, c->d_occ, c->d_c2, c->d_hnm1,
+                                                   c->d_c0);
   ++c->nlaunch;
   k_copy_scalar<<<1, 1, 0, c->st>>>(c->d_scal + S_GG, c->d_scal + S_GGPREV);
   CK(cudaGetLastError());
@@ -992,14 +1205,18 @@ static int do_pcg(amdk_ctx *c, int istep) {
 // copied to the pinned host buffer in stream order (checked by the caller
 // after its own sync with check_ortho).
 static int check_ortho(amdk_ctx *c) {
+  // an expired wait comes first: its NaN results reach the overlap, whose
+  // Cholesky then fails too; the recorded code is cleared once reported
+  if (c->h_info[1]) {
+    set_error("tensor-core slice GEMM: a pipeline wait expired (code " + std::to_string(c->h_info[1]) + ")");
+    c->h_info[1] = 0;
+    CK(cudaMemset(c->d_info + 1, 0, sizeof(int)));
+    return AMDK_ERR_TIMEOUT;
+  }
   const int info = c->h_info[0];
   if (info) {
     set_error("overlap matrix not positive definite at leading minor " + std::to_string(info));
     return AMDK_ERR_NOT_SPD;
-  }
-  if (c->h_info[1]) {
-    set_error("tensor-core slice GEMM: a pipeline wait expired (code " + std::to_string(c->h_info[1]) + ")");
-    return AMDK_ERR_TIMEOUT;
   }
   return 0;
 }
@@ -1083,6 +1300,11 @@ static int do_positions(amdk_ctx *c, const double *atco) {
     ++c->nlaunch;
     k_projectors<<<dim3(nblk(h.ngpw), c->nproj), NTHR, 0, c->st>>>(h.ngpw, c->nproj, c->d_inyh, nh1, nh2, nh3, aa, pa,
                                                                    c->d_twnl, c->d_P);
+    // the G_k-weighted projectors of D_FNL (nuclear_grad.f90:314-372)
+    ++c->nlaunch;
+    k_dproj<<<dim3(nblk(h.ngpw), c->nproj, 3), NTHR, 0, c->st>>>(h.ngpw, c->nproj, c->d_gvec, c->d_P, c->d_Q);
+    if (c->sg_proj) sg_slice(c, c->d_P, c->d_plP, c->d_sgP, c->nproj);
+    if (c->sg_dproj) sg_slice(c, c->d_Q, c->d_plQ, c->d_sgQ, 3 * c->nproj);
   }
   ++c->nlaunch;
   k_hess<<<nblk(h.ngpw), NTHR, 0, c->st>>>(h.ngpw, c->d_hg, h.tpiba2, c->d_evps, c->d_twnl, h.nsp, h.nghmax, c->d_na,
@@ -1109,12 +1331,16 @@ static int do_ionic_forces(amdk_ctx *c) {
   k_potfor<<<dim3(pnb, h.nat), NTHR, 0, c->st>>>(h.ngrho, c->d_inyh, nh1, nh2, nh3, aa, c->d_hg, c->d_gvec, h.tpiba2,
                                                  c->d_rhog, c->d_erhos, c->d_vps, c->d_rhos, omtp, c->d_part);
   if (c->nproj) {
-    ++c->nlaunch;
-    k_dproj<<<dim3(nblk(h.ngpw), c->nproj, 3), NTHR, 0, c->st>>>(h.ngpw, c->nproj, c->d_gvec, c->d_P, c->d_Q);
+    // dfnl = 2 tpiba Q^T C0: the int8 slice product on the mixed path (C0's
+    // planes current), DGEMM otherwise
     const double tfac = 2.0 * h.tpiba, zero = 0.0;
-    int K = 2 * h.ngpw;
-    CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, 3 * c->nproj, c->nstate, K, &tfac, (const double *)c->d_Q, K,
-                   (const double *)c->d_c0, K, &zero, c->d_dfnl, 3 * c->nproj));
+    if (use_slice(c) && c->sg_dproj && c0_planes_current(c)) {
+      sg_tn(c, c->tm_q_tn, c->tm_a_tn, 0, c->d_sgQ, c->d_sgA, tfac, c->d_dfnl, 3 * c->nproj, 3 * c->nproj);
+    } else {
+      int K = 2 * h.ngpw;
+      CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, 3 * c->nproj, c->nstate, K, &tfac, (const double *)c->d_Q, K,
+                     (const double *)c->d_c0, K, &zero, c->d_dfnl, 3 * c->nproj));
+    }
   }
   ++c->nlaunch;
   k_force_total<<<h.nat, NTHR, 0, c->st>>>(h.nat, c->nproj, c->nstate, c->d_pisa, c->d_hn, c->d_dfnl, c->d_occ, c->d_part,
@@ -1132,6 +1358,7 @@ static void set_pair_precision(amdk_ctx *c, int prec) {
   c->pencil_density = c->pd_p[q];
   c->ct_vpsi = c->ctv_p[q];
   c->ct_dens = c->ctd_p[q];
+  c->ns_dens = c->nsd_p[q];
 }
 
 static int build_device(amdk_ctx *c) {
@@ -1299,6 +1526,8 @@ static int build_device(amdk_ctx *c) {
   CK(cudaMemset(c->d_info, 0, 2 * sizeof(int)));
   RC(c->alloc(&c->d_part, (size_t)RED_BLOCKS * 4 + 3L * 64 * h.nat + 64));
   RC(c->alloc(&c->d_scal, S_NSCAL));
+  RC(c->alloc(&c->d_ticket, TK_N));
+  CK(cudaMemset(c->d_ticket, 0, TK_N * sizeof(unsigned)));
   CK(cudaMallocHost(&c->h_pin, sizeof(double) * (S_NSCAL + 8)));
   CK(cudaMallocHost(&c->h_info, sizeof(int) * 4));
   c->h_info[0] = c->h_info[1] = 0;
@@ -1320,17 +1549,16 @@ static int build_device(amdk_ctx *c) {
       c->pn1 = fft_n1(n1);
       c->pn2 = n1 / c->pn1;
       // V(r)psi: two blocks per SM when the tile can stay at least half the
-      // plane wide, else one; the density block carries its accumulator
+      // plane wide, else one
       int ct2 = pencil_tile<double2>(n1, nz0, 0, lim / 2), ct1 = pencil_tile<double2>(n1, nz0, 0, lim);
       c->ctv_p[0] = (2 * ct2 >= n1) ? ct2 : ct1;
-      c->ctd_p[0] = pencil_tile<double2>(n1, nz0, pencil_acc_smem<double2>(n1), lim);
       ct2 = pencil_tile<float2>(n1, nz0, 0, lim / 2);
       ct1 = pencil_tile<float2>(n1, nz0, 0, lim);
       c->ctv_p[1] = (2 * ct2 >= n1) ? ct2 : ct1;
-      // density: two blocks per SM when that leaves at most four column tiles
-      ct2 = pencil_tile<float2>(n1, nz0, pencil_acc_smem<float2>(n1), lim / 2);
-      ct1 = pencil_tile<float2>(n1, nz0, pencil_acc_smem<float2>(n1), lim);
-      c->ctd_p[1] = (4 * ct2 >= n1) ? ct2 : ct1;
+      // density: equal column tiles (1, 2 or 4) whose sums fit 1, 2 or 4
+      // register slots; two blocks per SM when possible
+      density_tiles(n1, nz0, sizeof(double2), lim, &c->ctd_p[0], &c->nsd_p[0]);
+      density_tiles(n1, nz0, sizeof(float2), lim, &c->ctd_p[1], &c->nsd_p[1]);
     }
     for (int q = 0; q < 2; ++q) {
       c->pv_p[q] = ok && !off && c->ctv_p[q] >= 8;
@@ -1481,6 +1709,7 @@ static int build_device(amdk_ctx *c) {
         }
       }
     RC(c->up(&c->d_H, H));
+    RC(sg_proj_setup(c));
   }
   double es = 0.0;
   for (int is = 0; is < h.nsp; is++) es = es + (double)h.na[is] * h.zv[is] * h.zv[is] / RAGGIO;
@@ -1510,22 +1739,19 @@ struct OnSideStream {
 };
 
 // Segment A of the CG iteration with the C0-only work (projections, E_nl,
-// E_kin, the clearing of C2) on the side stream; the context stream runs the
-// density, rho(G), the potential, then (after the join) V(r)psi, fnonloc
-// and the gradient.  The x pass of H|psi> is the density's: the density
+// E_kin) on the side stream; the context stream runs the density, rho(G),
+// the potential, then (after the join) V(r)psi with fnonloc and the
+// gradient.  The x pass of H|psi> is the density's: the density
 // kernel only reads the transposed ray buffer, and the field transforms have
 // their own, so V(r)psi starts from it as it is.  Same results as the
 // sequential order; used on the pencil path with all pairs in one batch.
 template <typename C> static int seg_a_overlap(amdk_ctx *c) {
-  const HostSetup &h = c->hs;
-  const Geom &g = c->geom;
   const int T = c->npairs;
   CK(cudaEventRecord(c->ev_fork, c->st));
   CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
   {
     OnSideStream side(c);
     RC(energy_c0_terms(c));
-    CK(cudaMemsetAsync(c->d_c2, 0, sizeof(double2) * (size_t)h.ngpw * c->nstate, c->st));
     CK(cudaEventRecord(c->ev_side_done, c->st));
   }
   RC(density_pairs_t<C>(c));
@@ -1535,55 +1761,160 @@ template <typename C> static int seg_a_overlap(amdk_ctx *c) {
   CK(cudaMemcpyAsync(c->h_pin, c->d_scal, sizeof(double) * S_NSCAL, cudaMemcpyDeviceToHost, c->st));
   pencil_vpsi<C>(c, T);
   xt_fwd<C>(c, T);
-  dim3 gu(nblk(h.ngpw), T);
-  ++c->nlaunch;
-  k_unpack_vpsi<C><<<gu, NTHR, 0, c->st>>>(h.ngpw, c->nstate, 0, T, c->d_postp, c->d_postm, (C *)c->d_rb, rstride(c, 0),
-                                           1.0 / ((double)g.n1 * g.n2 * g.n3), c->d_hg, h.tpiba2, c->d_occ, c->d_c0,
-                                           c->d_c2);
-  RC(do_fnonloc(c));
+  unpack_h<C>(c, 0, T, c->d_postp, c->d_postm);
   RC(do_gradient(c));
   CK(cudaMemcpyAsync(c->h_pin + S_NSCAL, c->d_scal + S_GMAX, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   return 0;
 }
 
-// Run one segment of the CG iteration: captured into a CUDA graph the first
-// time its key is seen, replayed afterwards.  body() only enqueues work on
-// the context stream (no host synchronisation, no host-side state change the
-// replay would miss).  A capture that fails turns graphs off and runs eagerly.
-template <typename F> static int run_segment(amdk_ctx *c, const std::array<int, 4> &key, F &&body) {
+// One segment of the CG iteration as a CUDA graph: captured the first time
+// its key is seen, then kept.  body() only enqueues work on the context
+// stream (no host synchronisation, no host-side state change a replay would
+// miss).  A capture that fails turns graphs off for the context (nullptr: the
+// caller runs body() eagerly).
+template <typename F> static amdk_ctx::SegGraph *ensure_segment(amdk_ctx *c, const std::array<int, 4> &key, F &&body) {
   auto it = c->graphs.find(key);
-  if (it == c->graphs.end()) {
-    const size_t rec0 = c->recs.size(), ev0 = c->evused;
-    const long nl0 = c->nlaunch;
-    if (cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-      cudaGetLastError();
-      c->use_graphs = false;
-      return body();
-    }
-    const int rc = body();
-    cudaGraph_t g = nullptr;
-    const cudaError_t ce = cudaStreamEndCapture(c->st, &g);
-    amdk_ctx::SegGraph sg;
-    const bool ok = rc == 0 && ce == cudaSuccess && g && cudaGraphInstantiate(&sg.exec, g, 0) == cudaSuccess;
-    if (g) cudaGraphDestroy(g);
-    sg.recs.assign(c->recs.begin() + rec0, c->recs.end());
-    sg.nevents = c->evused - ev0;
-    sg.nlaunch = c->nlaunch - nl0;
-    c->recs.resize(rec0);
-    c->evused = ev0;
-    c->nlaunch = nl0;
-    if (!ok) {
-      cudaGetLastError();
-      if (sg.exec) cudaGraphExecDestroy(sg.exec);
-      c->use_graphs = false;
-      return rc ? rc : body();
-    }
-    it = c->graphs.emplace(key, std::move(sg)).first;
+  if (it != c->graphs.end()) return &it->second;
+  const size_t rec0 = c->recs.size(), ev0 = c->evused;
+  const long nl0 = c->nlaunch;
+  if (cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    c->use_graphs = false;
+    return nullptr;
   }
-  CK(cudaGraphLaunch(it->second.exec, c->st));
-  c->recs.insert(c->recs.end(), it->second.recs.begin(), it->second.recs.end());
-  c->evused += it->second.nevents;
-  c->nlaunch += it->second.nlaunch;
+  const int rc = body();
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(c->st, &g);
+  amdk_ctx::SegGraph sg;
+  const bool ok = rc == 0 && ce == cudaSuccess && g && cudaGraphInstantiate(&sg.exec, g, 0) == cudaSuccess;
+  sg.graph = g;
+  sg.recs.assign(c->recs.begin() + rec0, c->recs.end());
+  sg.nevents = c->evused - ev0;
+  sg.nlaunch = c->nlaunch - nl0;
+  c->recs.resize(rec0);
+  c->evused = ev0;
+  c->nlaunch = nl0;
+  if (!ok) {
+    cudaGetLastError();
+    if (sg.exec) cudaGraphExecDestroy(sg.exec);
+    if (g) cudaGraphDestroy(g);
+    c->use_graphs = false;
+    return nullptr;
+  }
+  return &c->graphs.emplace(key, std::move(sg)).first->second;
+}
+// the bookkeeping of a segment launched (alone or inside an ensemble graph)
+static void account_segment(amdk_ctx *c, const amdk_ctx::SegGraph &sg) {
+  c->recs.insert(c->recs.end(), sg.recs.begin(), sg.recs.end());
+  c->evused += sg.nevents;
+  c->nlaunch += sg.nlaunch;
+}
+template <typename F> static int run_segment(amdk_ctx *c, const std::array<int, 4> &key, F &&body) {
+  amdk_ctx::SegGraph *sg = ensure_segment(c, key, body);
+  if (!sg) return body();
+  CK(cudaGraphLaunch(sg->exec, c->st));
+  account_segment(c, *sg);
+  return 0;
+}
+
+// The pieces of one CG iteration (do_opt.f90:80-128), shared by
+// amdk_scf_iteration and amdk_ensemble_iteration: segment A (density ...
+// H|psi>, gradient, GEMAX copied to pinned memory), the host's CHK_TFOR
+// decision on GEMAX, segment B (forces, PCG, ortho) and the bookkeeping after.
+static bool iter_overlap(const amdk_ctx *c) {
+  return c->overlap && c->pencil_vpsi && c->pencil_density && c->batch == c->npairs;
+}
+static int seg_a_body(amdk_ctx *c) {
+  const int q = (c->precision == AMDK_MIXED) ? 1 : 0;
+  if (iter_overlap(c)) return q ? seg_a_overlap<float2>(c) : seg_a_overlap<double2>(c);
+  RC(do_density(c));
+  RC(do_potential(c));
+  RC(do_energy(c, nullptr));  // energies read after the end-of-iteration sync
+  RC(do_apply_h(c));
+  RC(do_gradient(c));
+  CK(cudaMemcpyAsync(c->h_pin + S_NSCAL, c->d_scal + S_GMAX, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  return 0;
+}
+static std::array<int, 4> seg_a_key(const amdk_ctx *c) {
+  const int q = (c->precision == AMDK_MIXED) ? 1 : 0;
+  const int parity = (c->d_c0 == c->c0_first) ? 0 : 1;
+  const int c0_digits = (use_slice(c) && c->sg_c0_buf == (void *)c->d_c0) ? 1 : 0;
+  return {0, q + 2 * c0_digits, parity, c->prof ? 1 : 0};
+}
+// after segment A has finished: GEMAX, CHK_TFOR (gradient.f90:113-136)
+static int chk_tfor(amdk_ctx *c, int istep, double gcut, double *gm) {
+  *gm = c->h_pin[S_NSCAL];
+  if (!std::isfinite(*gm)) {
+    set_error("non-finite wavefunction gradient");
+    return AMDK_ERR_NONFINITE;
+  }
+  if (istep == 1) c->tfor = false;
+  else if (*gm < 3 * gcut) c->tfor = true;
+  c->h_pin[S_NSCAL + 1] = (double)istep;  // read by the PCG step through a captured copy
+  return 0;
+}
+static int seg_b_body(amdk_ctx *c, int istep) {
+  if (c->tfor) RC(do_ionic_forces(c));
+  RC(do_pcg(c, istep));
+  RC(do_ortho(c, false, false));
+  return 0;
+}
+static std::array<int, 4> seg_b_key(const amdk_ctx *c) {
+  const int parity = (c->d_c0 == c->c0_first) ? 0 : 1;
+  return {1, c->tfor ? 1 : 0, parity, c->prof ? 1 : 0};
+}
+// after segment B has finished: the ortho's output buffer holds C0, status
+// and energies
+static int iter_end(amdk_ctx *c, double gm, double gcut, amdk_energies *e, double *gemax, int *converged) {
+  c->sg_c0_buf = use_slice(c) ? (void *)c->d_cp : nullptr;  // the ortho's output (digits written)
+  std::swap(c->d_c0, c->d_cp);
+  prof_harvest(c);
+  c->warm[(c->precision == AMDK_MIXED) ? 1 : 0] = true;
+  RC(check_ortho(c));
+  amdk_energies en;
+  RC(fill_energies(c, c->h_pin, &en));
+  if (e) *e = en;
+  if (gemax) *gemax = gm;
+  if (converged) *converged = gm < gcut;
+  return 0;
+}
+
+// Several contexts (independent systems on one GPU) advanced together: each
+// segment of every member's CG iteration is one CUDA graph launch, the
+// members' segment graphs being child graphs of one parent (cached by the
+// members' segment keys), which run concurrently.
+struct amdk_ensemble {
+  std::vector<amdk_ctx *> m;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0;
+  std::map<std::vector<std::array<int, 4>>, cudaGraphExec_t> parents;
+};
+// the parent graph of the members' segment graphs for these keys
+static int ensemble_parent(amdk_ensemble *E, const std::vector<std::array<int, 4>> &keys,
+                           const std::vector<amdk_ctx::SegGraph *> &sgs, cudaGraphExec_t *out) {
+  auto it = E->parents.find(keys);
+  if (it != E->parents.end()) {
+    *out = it->second;
+    return 0;
+  }
+  cudaGraph_t parent = nullptr;
+  CK(cudaGraphCreate(&parent, 0));
+  for (amdk_ctx::SegGraph *sg : sgs) {
+    cudaGraphNode_t node;
+    const cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, sg->graph);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(parent);
+      CK(e);
+    }
+  }
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t e = cudaGraphInstantiate(&exec, parent, 0);
+  cudaGraphDestroy(parent);
+  CK(e);
+  E->parents.emplace(keys, exec);
+  *out = exec;
   return 0;
 }
 
@@ -1602,6 +1933,7 @@ int amdk_create(const amdk_system *sys, const amdk_options *opt, amdk_ctx **out)
     c->device = opt->device;
     c->precision = opt->precision;
     c->batch = opt->pair_batch;
+    if (opt->reserved[0] != 0) c->sg_plim = std::max(opt->reserved[0], 0);
   }
   int rc = host_setup(sys, c->hs);
   if (rc) {
@@ -1645,8 +1977,10 @@ int amdk_destroy(amdk_ctx *c) {
   cudaSetDevice(c->device);
   if (c->st) cudaStreamSynchronize(c->st);
   for (void *p : c->allocs) cudaFree(p);
-  for (auto &kv : c->graphs)
+  for (auto &kv : c->graphs) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  }
   if (c->h_pin) cudaFreeHost(c->h_pin);
   if (c->cs) cusolverDnDestroy(c->cs);
   if (c->h_trtri_ws) std::free(c->h_trtri_ws);
@@ -1772,7 +2106,6 @@ int amdk_energy(amdk_ctx *c, amdk_energies *e) {
 int amdk_apply_h(amdk_ctx *c) {
   if (!c) return AMDK_ERR_BADARG;
   cudaSetDevice(c->device);
-  CK(cudaMemsetAsync(c->d_c2, 0, sizeof(double2) * (size_t)c->hs.ngpw * c->nstate, c->st));
   return do_apply_h(c);
 }
 int amdk_gradient(amdk_ctx *c, double *gemax) {
@@ -1788,7 +2121,7 @@ int amdk_gradient(amdk_ctx *c, double *gemax) {
 int amdk_pcg(amdk_ctx *c, int istep) {
   if (!c || istep < 1) return AMDK_ERR_BADARG;
   cudaSetDevice(c->device);
-  return do_pcg(c, istep);
+  return do_pcg(c, istep, true);
 }
 
 int amdk_scf_iteration(amdk_ctx *c, int istep, double gcut, amdk_energies *e, double *gemax, int *converged) {
@@ -1798,68 +2131,142 @@ int amdk_scf_iteration(amdk_ctx *c, int istep, double gcut, amdk_energies *e, do
   // graphs from the second iteration on, once this precision has run eagerly
   // (first-call setup of kernels and cuBLAS stays out of the capture)
   const bool graph = c->use_graphs && istep > 1 && c->warm[q];
-  const int parity = (c->d_c0 == c->c0_first) ? 0 : 1;
   cudaEventRecord(c->ev0, c->st);
-  const bool overlap = c->overlap && c->pencil_vpsi && c->pencil_density && c->batch == c->npairs;
-  auto seg_a = [&]() -> int {
-    if (overlap) return q ? seg_a_overlap<float2>(c) : seg_a_overlap<double2>(c);
-    RC(do_density(c));
-    RC(do_potential(c));
-    RC(do_energy(c, nullptr));  // energies read after the end-of-iteration sync
-    CK(cudaMemsetAsync(c->d_c2, 0, sizeof(double2) * (size_t)c->hs.ngpw * c->nstate, c->st));
-    RC(do_apply_h(c));
-    RC(do_gradient(c));
-    CK(cudaMemcpyAsync(c->h_pin + S_NSCAL, c->d_scal + S_GMAX, sizeof(double), cudaMemcpyDeviceToHost, c->st));
-    return 0;
-  };
-  const int c0_digits = (use_slice(c) && c->sg_c0_buf == (void *)c->d_c0) ? 1 : 0;
-  if (graph) RC(run_segment(c, {0, q + 2 * c0_digits, parity, c->prof ? 1 : 0}, seg_a));
+  auto seg_a = [&]() -> int { return seg_a_body(c); };
+  if (graph) RC(run_segment(c, seg_a_key(c), seg_a));
   else RC(seg_a());
   // GEMAX decides CHK_TFOR (forces or not) before PCG: the one host sync
   // inside the iteration
   CK(cudaStreamSynchronize(c->st));
-  const double gm = c->h_pin[S_NSCAL];
-  if (!std::isfinite(gm)) {
-    set_error("non-finite wavefunction gradient");
-    return AMDK_ERR_NONFINITE;
-  }
-  // CHK_TFOR (gradient.f90:113-136)
-  if (istep == 1) c->tfor = false;
-  else if (gm < 3 * gcut) c->tfor = true;
-  const bool tfor = c->tfor;
-  c->h_pin[S_NSCAL + 1] = (double)istep;
-  auto seg_b = [&]() -> int {
-    if (tfor) RC(do_ionic_forces(c));
-    RC(do_pcg(c, istep));
-    RC(do_ortho(c, false, false));
-    return 0;
-  };
-  if (graph) RC(run_segment(c, {1, tfor ? 1 : 0, parity, c->prof ? 1 : 0}, seg_b));
+  double gm = 0;
+  RC(chk_tfor(c, istep, gcut, &gm));
+  auto seg_b = [&]() -> int { return seg_b_body(c, istep); };
+  if (graph) RC(run_segment(c, seg_b_key(c), seg_b));
   else RC(seg_b());
-  c->sg_c0_buf = use_slice(c) ? (void *)c->d_cp : nullptr;  // the ortho's output (digits written)
-  std::swap(c->d_c0, c->d_cp);  // ortho's output buffer holds C0 now
   cudaEventRecord(c->ev1, c->st);
   CK(cudaEventSynchronize(c->ev1));
   float ms = 0;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
   c->last_ms = ms;
-  prof_harvest(c);
-  c->warm[q] = true;
-  RC(check_ortho(c));
-  amdk_energies en;
-  RC(fill_energies(c, c->h_pin, &en));
-  if (e) *e = en;
-  if (gemax) *gemax = gm;
-  if (converged) *converged = gm < gcut;
+  return iter_end(c, gm, gcut, e, gemax, converged);
+}
+
+int amdk_ensemble_create(amdk_ctx **ctx, int n, amdk_ensemble **out) {
+  if (!ctx || n < 1 || !out) return AMDK_ERR_BADARG;
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (!ctx[i] || ctx[i]->device != ctx[0]->device) {
+      set_error("amdk_ensemble_create: null context or members on different devices");
+      return AMDK_ERR_BADARG;
+    }
+    for (int j = 0; j < i; ++j)
+      if (ctx[j] == ctx[i]) {
+        set_error("amdk_ensemble_create: a context appears twice");
+        return AMDK_ERR_BADARG;
+      }
+  }
+  amdk_ensemble *E = new amdk_ensemble();
+  E->m.assign(ctx, ctx + n);
+  E->device = ctx[0]->device;
+  cudaSetDevice(E->device);
+  if (cudaStreamCreateWithFlags(&E->st, cudaStreamNonBlocking) != cudaSuccess || cudaEventCreate(&E->ev0) != cudaSuccess ||
+      cudaEventCreate(&E->ev1) != cudaSuccess) {
+    set_error("amdk_ensemble_create: stream or event creation failed");
+    amdk_ensemble_destroy(E);
+    return AMDK_ERR_CUDA;
+  }
+  *out = E;
+  return 0;
+}
+
+int amdk_ensemble_destroy(amdk_ensemble *E) {
+  if (!E) return 0;
+  cudaSetDevice(E->device);
+  if (E->st) cudaStreamSynchronize(E->st);
+  for (auto &kv : E->parents) cudaGraphExecDestroy(kv.second);
+  if (E->ev0) cudaEventDestroy(E->ev0);
+  if (E->ev1) cudaEventDestroy(E->ev1);
+  if (E->st) cudaStreamDestroy(E->st);
+  delete E;
+  return 0;
+}
+
+int amdk_ensemble_iteration(amdk_ensemble *E, const int *istep, double gcut, amdk_energies *e, double *gemax,
+                            int *converged) {
+  if (!E || !istep) return AMDK_ERR_BADARG;
+  const int n = (int)E->m.size();
+  cudaSetDevice(E->device);
+  for (int i = 0; i < n; ++i)
+    if (istep[i] < 1) {
+      set_error("amdk_ensemble_iteration: CG step below 1");
+      return AMDK_ERR_BADARG;
+    }
+  // members that cannot replay graphs yet (first iteration, first at this
+  // precision, graphs off, profiling on) iterate on their own
+  bool together = true;
+  for (amdk_ctx *c : E->m) {
+    const int q = (c->precision == AMDK_MIXED) ? 1 : 0;
+    together = together && c->use_graphs && c->warm[q] && !c->prof;
+  }
+  for (int i = 0; i < n; ++i) together = together && istep[i] > 1;
+  if (!together) {
+    for (int i = 0; i < n; ++i)
+      RC(amdk_scf_iteration(E->m[i], istep[i], gcut, e ? e + i : nullptr, gemax ? gemax + i : nullptr,
+                            converged ? converged + i : nullptr));
+    return 0;
+  }
+  std::vector<std::array<int, 4>> keys(n);
+  std::vector<amdk_ctx::SegGraph *> sgs(n);
+  auto run_all = [&](bool b, const std::vector<int> &steps) -> int {
+    for (int i = 0; i < n; ++i) {
+      amdk_ctx *c = E->m[i];
+      keys[i] = b ? seg_b_key(c) : seg_a_key(c);
+      const int st = steps[i];
+      sgs[i] = b ? ensure_segment(c, keys[i], [&]() -> int { return seg_b_body(c, st); })
+                 : ensure_segment(c, keys[i], [&]() -> int { return seg_a_body(c); });
+      if (!sgs[i]) {
+        set_error("amdk_ensemble_iteration: a member's segment could not be captured");
+        return AMDK_ERR_CUDA;
+      }
+    }
+    cudaGraphExec_t exec = nullptr;
+    RC(ensemble_parent(E, keys, sgs, &exec));
+    CK(cudaGraphLaunch(exec, E->st));
+    for (int i = 0; i < n; ++i) account_segment(E->m[i], *sgs[i]);
+    return 0;
+  };
+  const std::vector<int> steps(istep, istep + n);
+  CK(cudaEventRecord(E->ev0, E->st));
+  RC(run_all(false, steps));
+  CK(cudaStreamSynchronize(E->st));
+  std::vector<double> gm(n);
+  for (int i = 0; i < n; ++i) RC(chk_tfor(E->m[i], istep[i], gcut, &gm[i]));
+  RC(run_all(true, steps));
+  CK(cudaEventRecord(E->ev1, E->st));
+  CK(cudaEventSynchronize(E->ev1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, E->ev0, E->ev1);
+  E->last_ms = ms;
+  for (int i = 0; i < n; ++i) {
+    E->m[i]->last_ms = ms;
+    RC(iter_end(E->m[i], gm[i], gcut, e ? e + i : nullptr, gemax ? gemax + i : nullptr, converged ? converged + i : nullptr));
+  }
+  return 0;
+}
+
+int amdk_ensemble_last_ms(amdk_ensemble *E, double *ms) {
+  if (!E || !ms) return AMDK_ERR_BADARG;
+  *ms = E->last_ms;
   return 0;
 }
 
 int amdk_ionic_forces(amdk_ctx *c, double *force) {
   if (!c || !force) return AMDK_ERR_BADARG;
   cudaSetDevice(c->device);
-  // forces of the current C0: density (for POTFOR) and projections (NLFOR)
+  // forces of the current C0: density (for POTFOR) and projections with
+  // H nl (NLFOR)
   RC(do_density(c));
-  RC(do_fnl(c));
+  RC(energy_c0_terms(c));
   RC(do_ionic_forces(c));
   CK(cudaMemcpyAsync(force, c->d_force, sizeof(double) * 3 * c->hs.na_max * c->hs.nsp, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -1946,7 +2353,6 @@ int amdk_backward(amdk_ctx *c, double *dE_dR, double *dE_dpsi) {
     for (size_t k = 0; k < nf; k++) dE_dR[k] = -f[k];
   }
   if (dE_dpsi) {
-    CK(cudaMemsetAsync(c->d_c2, 0, sizeof(double2) * (size_t)h.ngpw * c->nstate, c->st));
     RC(do_apply_h(c));
     const size_t nc = 2 * (size_t)h.ngpw * c->nstate;
     CK(cudaMemcpyAsync(dE_dpsi, c->d_c2, sizeof(double) * nc, cudaMemcpyDeviceToHost, c->st));
@@ -1977,6 +2383,7 @@ int amdk_get_array(amdk_ctx *c, const char *name, void *dst, size_t bytes) {
   else if (k == "eigrxrhos") { src = c->d_erhos; n = h.ngrho * sizeof(double2); }
   else if (k == "vpp") { src = c->d_vpp; n = h.ngpw * sizeof(double); }
   else if (k == "force") { src = c->d_force; n = 3 * h.na_max * h.nsp * sizeof(double); }
+  else if (k == "overlap") { src = c->d_gam; n = (size_t)c->nstate * c->nstate * sizeof(double); }
   else {
     set_error("amdk_get_array: unknown array " + k);
     return AMDK_ERR_BADARG;

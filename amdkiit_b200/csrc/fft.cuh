@@ -184,12 +184,6 @@ __device__ C *smem_fft(C *a, C *b, int L, int es, const Plan<C> &p, int sg) {
   return a;
 }
 
-// copy the twiddles of the compile-time path into shared memory
-template <typename C, int N> __device__ __forceinline__ void load_tw(C *tw, const Plan<C> &p) {
-  if constexpr (N > 0) {
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = p.w[i];
-  }
-}
 
 // ---------------------------------------------------------------- register FFT
 // Small DFTs held in registers (R <= 16 with factors 2, 3, 4, 5) and the
@@ -256,78 +250,33 @@ template <typename C, int R, int SG> struct Dft {
   }
 };
 
-// v[k] *= W_N^(SG j k), k = 1..R-1, from the shared table tw[e] = exp(-2 pi i e/N)
-template <typename C, int N, int R, int SG>
-__device__ __forceinline__ void twiddle_n(C (&v)[R], int j, const C *tw) {
-  int e = 0;
+// Twiddles of the two-level transform of a specialised length N = N1*N2,
+// built per block in shared memory (2N entries) from the plan's
+// w[e] = exp(-2 pi i e/N): tw[j2*N1 + k1] = W_N^(j2 k1) (table 0, the
+// twiddles of a natural-order-in transform's first phase) and
+// tw[N + k1*N2 + k2] = W_N^(k1 k2) (table 1, those of a permuted-order-in
+// transform's first phase).  A thread reads its row with constant offsets,
+// so no exponent arithmetic is left in the butterflies.
+template <typename C, int N> __device__ __forceinline__ void load_tw(C *tw, const Plan<C> &p) {
+  if constexpr (N > 0) {
+    constexpr int N1 = fft_n1(N), N2 = N / N1;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      tw[i] = p.w[(i / N1) * (i % N1) % N];
+      tw[N + i] = p.w[(i / N2) * (i % N2) % N];
+    }
+  }
+}
+// v[k] *= W_N^(SG j k), k = 1..R-1, from row j of twiddle table TAB (table 0
+// for R = N1, j = j2; table 1 for R = N2, j = k1)
+template <typename C, int N, int R, int SG, int TAB>
+__device__ __forceinline__ void twiddle_tab(C (&v)[R], int j, const C *tw) {
+  const C *row = tw + TAB * N + j * R;
 #pragma unroll
   for (int k = 1; k < R; ++k) {
-    e += j;
-    if (e >= N) e -= N;
-    C w = tw[e];
+    C w = row[k];
     if (SG > 0) w.y = -w.y;
     v[k] = cmul(v[k], w);
   }
-}
-
-// Length-N transforms of nrow rows (row r at P + r*stride), in place.
-// nat_to_perm: natural order in, X[k1 + N1*k2] left at position k1*N2 + k2.
-// perm_to_nat: that permuted order in, natural order out.  Each phase's
-// sub-transform reads and writes the same positions, so a phase needs no
-// barrier inside; the two phases are separated by one.
-template <typename C, int N, int SG>
-__device__ __forceinline__ void rows_nat_to_perm(C *P, int nrow, int stride, const C *tw) {
-  constexpr int N1 = fft_n1(N), N2 = N / N1;
-  for (int idx = threadIdx.x; idx < nrow * N2; idx += blockDim.x) {
-    const int r = idx % nrow, j2 = idx / nrow;
-    C *row = P + r * stride;
-    C v[N1];
-#pragma unroll
-    for (int j1 = 0; j1 < N1; ++j1) v[j1] = row[j2 + N2 * j1];
-    Dft<C, N1, SG>::run(v);
-    twiddle_n<C, N, N1, SG>(v, j2, tw);
-#pragma unroll
-    for (int k1 = 0; k1 < N1; ++k1) row[k1 * N2 + j2] = v[k1];
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < nrow * N1; idx += blockDim.x) {
-    const int r = idx % nrow, k1 = idx / nrow;
-    C *row = P + r * stride + k1 * N2;
-    C u[N2];
-#pragma unroll
-    for (int j2 = 0; j2 < N2; ++j2) u[j2] = row[j2];
-    Dft<C, N2, SG>::run(u);
-#pragma unroll
-    for (int k2 = 0; k2 < N2; ++k2) row[k2] = u[k2];
-  }
-  __syncthreads();
-}
-template <typename C, int N, int SG>
-__device__ __forceinline__ void rows_perm_to_nat(C *P, int nrow, int stride, const C *tw) {
-  constexpr int N1 = fft_n1(N), N2 = N / N1;
-  for (int idx = threadIdx.x; idx < nrow * N1; idx += blockDim.x) {
-    const int r = idx % nrow, k1 = idx / nrow;
-    C *row = P + r * stride + k1 * N2;
-    C u[N2];
-#pragma unroll
-    for (int k2 = 0; k2 < N2; ++k2) u[k2] = row[k2];
-    Dft<C, N2, SG>::run(u);
-    twiddle_n<C, N, N2, SG>(u, k1, tw);
-#pragma unroll
-    for (int n2 = 0; n2 < N2; ++n2) row[n2] = u[n2];
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < nrow * N2; idx += blockDim.x) {
-    const int r = idx % nrow, n2 = idx / nrow;
-    C *row = P + r * stride;
-    C w[N1];
-#pragma unroll
-    for (int k1 = 0; k1 < N1; ++k1) w[k1] = row[k1 * N2 + n2];
-    Dft<C, N1, SG>::run(w);
-#pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) row[n2 + N2 * n1] = w[n1];
-  }
-  __syncthreads();
 }
 
 // Two-level register FFT of a tile of L lines (element k of line l at
@@ -344,7 +293,7 @@ __device__ __forceinline__ void tile_reg_fft(C *a, C *b, const C *tw) {
 #pragma unroll
     for (int j1 = 0; j1 < N1; ++j1) v[j1] = a[(j2 + N2 * j1) * ES + l];
     Dft<C, N1, SG>::run(v);
-    twiddle_n<C, N, N1, SG>(v, j2, tw);
+    twiddle_tab<C, N, N1, SG, 0>(v, j2, tw);
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) a[(k1 * N2 + j2) * ES + l] = v[k1];
   }

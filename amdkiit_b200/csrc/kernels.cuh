@@ -51,6 +51,47 @@ __global__ void k_finish_sum(const double *part, int nb, double *out, int nk) {
   if (threadIdx.x == 0 && k < nk) out[k] = r;
 }
 
+// Reductions finished by the kernel that produces them: each block reduces
+// its threads' v[k] (a sum, or a max for the bits of MAXMASK), writes its
+// partials part[k*gridDim + block], and the last block to arrive (an atomic
+// ticket taken after a fence) reduces the partials in block order into out[k]
+// and re-arms the ticket.  Deterministic for a fixed launch shape; one launch
+// instead of a partials kernel and a finishing kernel.  Every thread of every
+// block must call it; a ticket serves one kernel at a time.
+template <int NK, unsigned MAXMASK = 0u>
+__device__ void reduce_and_finish(const double (&v)[NK], double *part, double *out, unsigned *ticket) {
+  __shared__ double sh[32];
+  __shared__ unsigned last;
+  double r[NK];
+#pragma unroll
+  for (int k = 0; k < NK; ++k) r[k] = ((MAXMASK >> k) & 1u) ? block_max(v[k], sh) : block_sum(v[k], sh);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NK; ++k) part[(long)k * gridDim.x + blockIdx.x] = r[k];
+    __threadfence();
+    last = (atomicAdd(ticket, 1u) == gridDim.x - 1) ? 1u : 0u;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < NK; ++k) {
+    const bool mx = (MAXMASK >> k) & 1u;
+    double a = mx ? -1.0 : 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+      const double x = __ldcg(part + (long)k * gridDim.x + i);
+      a = mx ? fmax(a, x) : a + x;
+    }
+    const double t = mx ? block_max(a, sh) : block_sum(a, sh);
+    if (threadIdx.x == 0) out[k] = t;
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
+}
+// slots of the device scalar array: CG norms, energy sums, GEMAX, CG step
+enum { S_GGPREV = 1, S_EH = 2, S_ELOC, S_EXC, S_EKIN, S_ENL, S_ISTEP = 8, S_GMAX = 9, S_GG = 10, S_NSCAL = 16 };
+// tickets of the self-finishing reductions (one per kernel)
+enum { TK_VLOC = 0, TK_XC, TK_ENL, TK_EKIN, TK_GRAD, TK_N = 8 };
+
 // ---------------------------------------------------------------- tables
 // spline_inter (spline_inter.f90:1-36) evaluated at one point; the hunt is
 // spline_hunt's linear search done by bisection (same interval).  Points
@@ -202,8 +243,7 @@ __global__ void k_gather_p(int ng, const int *pos_p, const C *rb, double scale, 
 // partial sums: part[0*nb+b] = Re sum 4pi/G^2 |rho+rho_ion|^2,
 // part[1*nb+b] = Re sum eigrxvps conj(rho) (G=0 weighted 1/2).
 __global__ void k_vloc_g(int ngrho, const double *hg, double tpiba2, const double2 *rhog, const double2 *erhos,
-                         const double2 *evps, double2 *vg, double *part) {
-  __shared__ double sh[32];
+                         const double2 *evps, double2 *vg, double *part, double *out, unsigned *ticket) {
   const double fp = 16.0 * atan(1.0);
   double eh = 0, el = 0;
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngrho; g += gridDim.x * blockDim.x) {
@@ -219,12 +259,8 @@ __global__ void k_vloc_g(int ngrho, const double *hg, double tpiba2, const doubl
       el += e.x * rg.x + e.y * rg.y;
     }
   }
-  double a = block_sum(eh, sh);
-  double b = block_sum(el, sh);
-  if (threadIdx.x == 0) {
-    part[blockIdx.x] = a;
-    part[gridDim.x + blockIdx.x] = b;
-  }
+  const double v[2] = {eh, el};
+  reduce_and_finish<2>(v, part, out, ticket);  // out[0] = E_H sum, out[1] = E_loc sum
 }
 
 // GRAD_CAL fields (xc.f90:471-487): t=0: rho + i d_x rho, t=1: d_y rho + i d_z rho
@@ -248,87 +284,92 @@ __global__ void k_conj_field(int ng, const double2 *fp, double2 *fm) {
 }
 
 // ---------------------------------------------------------------- XC
-__device__ void xc_teter93(double rho, double &e, double &v) {
-  const double a0 = 0.4581652932831429, a1 = 2.217058676663745, a2 = 0.7405551735357053, a3 = 0.01968227878617998;
-  const double b1 = 1.0, b2 = 4.504130959426697, b3 = 1.110667363742916, b4 = 0.02359291751427506;
-  const double fp = 16.0 * atan(1.0);
-  double rs = cbrt(3.0 / (fp * rho));
-  double num = a0 + rs * (a1 + rs * (a2 + rs * a3));
-  double den = rs * (b1 + rs * (b2 + rs * (b3 + rs * b4)));
-  double dnum = a1 + rs * (2.0 * a2 + rs * 3.0 * a3);
-  double dden = b1 + rs * (2.0 * b2 + rs * (3.0 * b3 + rs * 4.0 * b4));
-  double eps = -num / den;
-  double deps = -(dnum * den - num * dden) / (den * den);
+// The functionals in the arithmetic type R: double on the FP64 path, float on
+// the mixed path (whose last iterations run this in FP64 again).
+template <typename R> __device__ void xc_teter93(R rho, R &e, R &v) {
+  const R a0 = (R)0.4581652932831429, a1 = (R)2.217058676663745, a2 = (R)0.7405551735357053,
+          a3 = (R)0.01968227878617998;
+  const R b1 = (R)1.0, b2 = (R)4.504130959426697, b3 = (R)1.110667363742916, b4 = (R)0.02359291751427506;
+  const R fp = (R)12.566370614359172954;  // 4 pi
+  R rs = cbrt((R)3 / (fp * rho));
+  R num = a0 + rs * (a1 + rs * (a2 + rs * a3));
+  R den = rs * (b1 + rs * (b2 + rs * (b3 + rs * b4)));
+  R dnum = a1 + rs * ((R)2 * a2 + rs * (R)3 * a3);
+  R dden = b1 + rs * ((R)2 * b2 + rs * ((R)3 * b3 + rs * (R)4 * b4));
+  R eps = -num / den;
+  R deps = -(dnum * den - num * dden) / (den * den);
   e = rho * eps;
-  v = eps - rs / 3.0 * deps;
+  v = eps - rs / (R)3 * deps;
 }
-__device__ void xc_pz(double rho, double &e, double &v) {
-  const double pi = 4.0 * atan(1.0), fp = 16.0 * atan(1.0);
-  double ex = -0.75 * cbrt(3.0 / pi) * cbrt(rho);
-  double rs = cbrt(3.0 / (fp * rho)), eps, deps;
-  if (rs >= 1.0) {
-    const double gg = -0.1423, b1 = 1.0529, b2 = 0.3334;
-    double sq = sqrt(rs), den = 1.0 + b1 * sq + b2 * rs;
+template <typename R> __device__ void xc_pz(R rho, R &e, R &v) {
+  const R pi = (R)3.14159265358979323846, fp = (R)12.566370614359172954;
+  R ex = (R)-0.75 * cbrt((R)3 / pi) * cbrt(rho);
+  R rs = cbrt((R)3 / (fp * rho)), eps, deps;
+  if (rs >= (R)1) {
+    const R gg = (R)-0.1423, b1 = (R)1.0529, b2 = (R)0.3334;
+    R sq = sqrt(rs), den = (R)1 + b1 * sq + b2 * rs;
     eps = gg / den;
-    deps = -gg * (0.5 * b1 / sq + b2) / (den * den);
+    deps = -gg * ((R)0.5 * b1 / sq + b2) / (den * den);
   } else {
-    const double A = 0.0311, B = -0.048, Cc = 0.0020, D = -0.0116;
-    double lr = log(rs);
+    const R A = (R)0.0311, B = (R)-0.048, Cc = (R)0.0020, D = (R)-0.0116;
+    R lr = log(rs);
     eps = A * lr + B + Cc * rs * lr + D * rs;
     deps = A / rs + Cc * lr + Cc + D;
   }
   e = rho * ex + rho * eps;
-  v = 4.0 / 3.0 * ex + (eps - rs / 3.0 * deps);
+  v = (R)4 / (R)3 * ex + (eps - rs / (R)3 * deps);
 }
-__device__ void xc_pbe(double rho, double sigma, double &e, double &v, double &vs) {
+template <typename R> __device__ void xc_pbe(R rho, R sigma, R &e, R &v, R &vs) {
   // PBE exchange and correlation (PW92 correlation, unpolarised); the
   // reciprocals of rho and k_F are formed once and r_s = (9 pi/4)^(1/3) / k_F
-  const double pi = 4.0 * atan(1.0), fp = 16.0 * atan(1.0);
-  const double kappa = 0.804, mu = 0.2195149727645171, beta = 0.06672455060314922;
-  const double gamma = (1.0 - log(2.0)) / (pi * pi);
-  const double ir = 1.0 / rho;
-  double kf = cbrt(3.0 * pi * pi * rho);
-  const double ikf = 1.0 / kf;
-  double exu = -3.0 / fp * kf * rho;
-  const double q4 = 0.25 * ikf * ikf * ir * ir;  // 1 / (4 kf^2 rho^2)
-  double s2 = sigma * q4;
-  const double iden = 1.0 / (1.0 + mu * s2 / kappa);
-  double Fx = 1.0 + kappa - kappa * iden, dF = mu * iden * iden;
-  double ex = exu * Fx;
-  double vx = 4.0 / 3.0 * exu * ir * Fx + exu * dF * (-8.0 / 3.0 * s2 * ir);
-  double vsx = exu * dF * q4;
-  double rs = 1.9191582926775128 * ikf;  // (9 pi / 4)^(1/3) / k_F
-  const double A = 0.0310907, a1 = 0.21370, b1 = 7.5957, b2 = 3.5876, b3 = 1.6382, b4 = 0.49294;
-  double sq = sqrt(rs);
-  double q = 2.0 * A * (b1 * sq + b2 * rs + b3 * rs * sq + b4 * rs * rs);
-  double dq = 2.0 * A * (0.5 * b1 / sq + b2 + 1.5 * b3 * sq + 2.0 * b4 * rs);
-  double L = log(1.0 + 1.0 / q), dL = -dq / (q * q + q);
-  double ec = -2.0 * A * (1.0 + a1 * rs) * L;
-  double dec = -2.0 * A * a1 * L - 2.0 * A * (1.0 + a1 * rs) * dL;
-  double t2 = pi * sigma * 0.25 * q4 * kf;  // pi sigma / (16 kf rho^2)
-  double bg = beta / gamma, E = exp(-ec / gamma), iE1 = 1.0 / (E - 1.0), AA = bg * iE1;
-  double At2 = AA * t2, num = 1.0 + At2, idd = 1.0 / (1.0 + At2 + At2 * At2);
-  double Q = t2 * num * idd;
-  const double ibq = 1.0 / (1.0 + bg * Q);
-  double H = gamma * log(1.0 + bg * Q);
-  double dHdQ = beta * ibq;
-  double dQdt2 = (num + t2 * AA) * idd - t2 * num * (AA + 2.0 * AA * AA * t2) * idd * idd;
-  double dQdA = (t2 * t2) * idd - t2 * num * (t2 + 2.0 * AA * t2 * t2) * idd * idd;
-  double dAdec = bg * E * iE1 * iE1 / gamma;
-  double decdrho = dec * (-rs * ir / 3.0);
-  double dt2drho = -7.0 / 3.0 * t2 * ir;
-  double vc = ec + H + rho * (decdrho + dHdQ * dQdA * dAdec * decdrho + dHdQ * dQdt2 * dt2drho);
-  double vsc = rho * dHdQ * dQdt2 * pi * 0.25 * q4 * kf;
+  const R pi = (R)3.14159265358979323846, fp = (R)12.566370614359172954;
+  const R kappa = (R)0.804, mu = (R)0.2195149727645171, beta = (R)0.06672455060314922;
+  const R gamma = ((R)1 - log((R)2)) / (pi * pi);
+  const R ir = (R)1 / rho;
+  R kf = cbrt((R)3 * pi * pi * rho);
+  const R ikf = (R)1 / kf;
+  R exu = (R)-3 / fp * kf * rho;
+  const R q4 = (R)0.25 * ikf * ikf * ir * ir;  // 1 / (4 kf^2 rho^2)
+  R s2 = sigma * q4;
+  const R iden = (R)1 / ((R)1 + mu * s2 / kappa);
+  R Fx = (R)1 + kappa - kappa * iden, dF = mu * iden * iden;
+  R ex = exu * Fx;
+  R vx = (R)4 / (R)3 * exu * ir * Fx + exu * dF * ((R)-8 / (R)3 * s2 * ir);
+  R vsx = exu * dF * q4;
+  R rs = (R)1.9191582926775128 * ikf;  // (9 pi / 4)^(1/3) / k_F
+  const R A = (R)0.0310907, a1 = (R)0.21370, b1 = (R)7.5957, b2 = (R)3.5876, b3 = (R)1.6382, b4 = (R)0.49294;
+  R sq = sqrt(rs);
+  R q = (R)2 * A * (b1 * sq + b2 * rs + b3 * rs * sq + b4 * rs * rs);
+  R dq = (R)2 * A * ((R)0.5 * b1 / sq + b2 + (R)1.5 * b3 * sq + (R)2 * b4 * rs);
+  R L = log((R)1 + (R)1 / q), dL = -dq / (q * q + q);
+  R ec = (R)-2 * A * ((R)1 + a1 * rs) * L;
+  R dec = (R)-2 * A * a1 * L - (R)2 * A * ((R)1 + a1 * rs) * dL;
+  R t2 = pi * sigma * (R)0.25 * q4 * kf;  // pi sigma / (16 kf rho^2)
+  R bg = beta / gamma, E = exp(-ec / gamma), iE1 = (R)1 / (E - (R)1), AA = bg * iE1;
+  R At2 = AA * t2, num = (R)1 + At2, idd = (R)1 / ((R)1 + At2 + At2 * At2);
+  R Q = t2 * num * idd;
+  const R ibq = (R)1 / ((R)1 + bg * Q);
+  R H = gamma * log((R)1 + bg * Q);
+  R dHdQ = beta * ibq;
+  R dQdt2 = (num + t2 * AA) * idd - t2 * num * (AA + (R)2 * AA * AA * t2) * idd * idd;
+  R dQdA = (t2 * t2) * idd - t2 * num * (t2 + (R)2 * AA * t2 * t2) * idd * idd;
+  R dAdec = bg * E * iE1 * iE1 / gamma;
+  R decdrho = dec * (-rs * ir / (R)3);
+  R dt2drho = (R)-7 / (R)3 * t2 * ir;
+  R vc = ec + H + rho * (decdrho + dHdQ * dQdA * dAdec * decdrho + dHdQ * dQdt2 * dt2drho);
+  R vsc = rho * dHdQ * dQdt2 * pi * (R)0.25 * q4 * kf;
   e = ex + rho * (ec + H);
   v = vx + vc;
   vs = vsx + vsc;
 }
 
 // cal_vpot_ex pointwise part (xc.f90:66-131): smoothing below 4e-8, etxc
-// partial sums, and the two complex fields for the G-space assembly:
-// g0 <- v1 + i v2 d_x rho, g1 <- v2 d_y rho + i v2 d_z rho  (xc.f90:262-279)
-__global__ void k_xc(long npt, int xc, const double *rho, double2 *g0, double2 *g1, double *part) {
-  __shared__ double sh[32];
+// sums, and the two complex fields for the G-space assembly:
+// g0 <- v1 + i v2 d_x rho, g1 <- v2 d_y rho + i v2 d_z rho  (xc.f90:262-279).
+// The functional runs in R; the E_xc sums and the fields are FP64.
+template <typename R>
+__global__ void k_xc(long npt, int xc, const double *rho, double2 *g0, double2 *g1, double *part, double *out,
+                     unsigned *ticket) {
   const double gc = 1.0e-8;
   double sm = 0;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < npt; i += (long)gridDim.x * blockDim.x) {
@@ -339,11 +380,11 @@ __global__ void k_xc(long npt, int xc, const double *rho, double2 *g0, double2 *
       dx = a.y; dy = b.x; dz = b.y;
       sigma = dx * dx + (dy * dy + dz * dz);
     }
-    double e = 0, v = 0, vs = 0;
+    R e = 0, v = 0, vs = 0;
     if (r > 1e-30) {
-      if (xc == 0) xc_teter93(r, e, v);
-      else if (xc == 1) xc_pz(r, e, v);
-      else xc_pbe(r, sigma, e, v, vs);
+      if (xc == 0) xc_teter93<R>((R)r, e, v);
+      else if (xc == 1) xc_pz<R>((R)r, e, v);
+      else xc_pbe<R>((R)r, (R)sigma, e, v, vs);
     }
     double rt = r > 0.0 ? r : 0.0, v1 = 0, v2 = 0;
     if (rt > 0.1 * gc) {
@@ -354,15 +395,15 @@ __global__ void k_xc(long npt, int xc, const double *rho, double2 *g0, double2 *
         smoo = 1.0 / (1.0 + texp);
         dsmoo = 3.0 / gc * texp * smoo * smoo;
       }
-      sm += smoo * e;
-      v1 = dsmoo * e + smoo * v;
-      v2 = smoo * (2.0 * vs);
+      sm += smoo * (double)e;
+      v1 = dsmoo * (double)e + smoo * (double)v;
+      v2 = smoo * (2.0 * (double)vs);
     }
     g0[i] = make_double2(v1, v2 * dx);
     if (xc == 2) g1[i] = make_double2(v2 * dy, v2 * dz);
   }
-  double s = block_sum(sm, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = s;
+  const double vv[1] = {sm};
+  reduce_and_finish<1>(vv, part, out, ticket);
 }
 
 // G-space assembly of the XC potential (xc.f90:257-297): from the forward
@@ -393,30 +434,118 @@ __global__ void k_xc_combine(int ngrho, int gga, const int *pos_p, const int *po
 }
 
 // ---------------------------------------------------------------- vpsi unpack
-// (wfn_initialize.f90:342-361): FP = F(G)+F(-G), FM = F(G)-F(-G);
-// C2_a = -f_a/2 (tpiba2 hg c_a + (Re FP, Im FM)), C2_b = -f_b/2 (... + (Im FP, -Re FM))
+// vpsi unpack (wfn_initialize.f90:342-361) fused with fnonloc / upf_fnonloc
+// (wfn_initialize.f90:560-695) for the projectors j < npj:
+//   C2_a = -f_a/2 (tpiba2 hg c_a + (Re FP, Im FM)) + sum_j P_j(G) D(j, a)
+//   C2_b = -f_b/2 (tpiba2 hg c_b + (Im FP, -Re FM)) + sum_j P_j(G) D(j, b)
+// with FP = F(G)+F(-G), FM = F(G)-F(-G) of the pair's forward transform in the
+// ray buffer.  grid (ngpw/128, ceil(T/PAIRS)): a thread takes one G and the
+// PAIRS pairs of its block's chunk (8 on FP32 data, 4 in FP64, whose sums
+// take twice the registers); it first sums the projector
+// terms of the chunk's bands (P_j(G) read once per chunk, coalesced over G and
+// L2-resident; the chunk's rows of D in shared memory), then unpacks, so C2
+// is written once.  P holds P_j(0)/2 at G = 0 (the convention of fnl's real
+// dot products); the full value is used here.  The projector sums run in the
+// transform's precision (FP32 with packed FMAs on the mixed path).
+constexpr int UNPACK_NPJ = 32;
+template <typename C> __host__ __device__ constexpr int unpack_pairs() { return sizeof(C) == sizeof(float2) ? 8 : 4; }
 template <typename C>
-__global__ void k_unpack_vpsi(int ngpw, int nstate, int band0, int T, const int *pos_p, const int *pos_m, const C *rb,
-                              long rstride, double scale, const double *hg, double tpiba2, const double *occ,
-                              const double2 *c0, double2 *c2) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  int t = blockIdx.y;
-  if (g >= ngpw || t >= T) return;
-  const C *R = rb + (long)t * rstride;
-  C pp = R[pos_p[g]], pm = R[pos_m[g]];
-  double fpx = ((double)pp.x + (double)pm.x) * scale, fpy = ((double)pp.y + (double)pm.y) * scale;
-  double fmx = ((double)pp.x - (double)pm.x) * scale, fmy = ((double)pp.y - (double)pm.y) * scale;
-  double kin = tpiba2 * hg[g];
-  int ba = band0 + 2 * t, bb = ba + 1;
-  double fi = occ[ba] * 0.5;
-  if (fi == 0.0) fi = 1.0;
-  double2 ca = c0[(long)ba * ngpw + g];
-  c2[(long)ba * ngpw + g] = make_double2(-fi * (kin * ca.x + fpx), -fi * (kin * ca.y + fmy));
-  if (bb < nstate) {
-    double fb = occ[bb] * 0.5;
-    if (fb == 0.0) fb = 1.0;
-    double2 cb = c0[(long)bb * ngpw + g];
-    c2[(long)bb * ngpw + g] = make_double2(-fb * (kin * cb.x + fpy), -fb * (kin * cb.y - fmx));
+__global__ void __launch_bounds__(128) k_unpack_fnonloc(int ngpw, int nstate, int band0, int T, int npj,
+                                                        const int *__restrict__ pos_p, const int *__restrict__ pos_m,
+                                                        const C *__restrict__ rb, long rstride, double scale,
+                                                        const double *__restrict__ hg, double tpiba2,
+                                                        const double *__restrict__ occ, const double2 *__restrict__ P,
+                                                        const double *__restrict__ D, int nproj,
+                                                        const double2 *__restrict__ c0, double2 *__restrict__ c2) {
+  typedef decltype(C().x) Rl;
+  constexpr int PAIRS = unpack_pairs<C>(), NB = 2 * PAIRS;
+  extern __shared__ unsigned char smraw[];
+  Rl *Ds = reinterpret_cast<Rl *>(smraw);  // [j][band - b0]
+  const int t0 = blockIdx.y * PAIRS, t1 = min(T, t0 + PAIRS);
+  const int b0 = band0 + 2 * t0;
+  const int nb = min(2 * (t1 - t0), nstate - b0);
+  for (int i = threadIdx.x; i < NB * npj; i += blockDim.x) {
+    const int j = i / NB, b = i - j * NB;
+    Ds[i] = b < nb ? (Rl)D[j + (long)nproj * (b0 + b)] : (Rl)0;
+  }
+  __syncthreads();
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngpw) return;
+  C acc[NB];
+#pragma unroll
+  for (int b = 0; b < NB; ++b) acc[b] = czero<C>();
+  const double gw = (g == 0) ? 2.0 : 1.0;
+#pragma unroll 4
+  for (int j = 0; j < npj; ++j) {
+    const double2 v = P[(long)j * ngpw + g];
+    const C pj = mk((Rl)(gw * v.x), (Rl)(gw * v.y));
+    const Rl *dj = Ds + j * NB;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) acc[b] = cfmas(pj, dj[b], acc[b]);
+  }
+  const int pp = pos_p[g], pm = pos_m[g];
+  const double kin = tpiba2 * hg[g];
+#pragma unroll
+  for (int tt = 0; tt < PAIRS; ++tt) {
+    const int t = t0 + tt;
+    if (t >= t1) break;
+    const C *R = rb + (long)t * rstride;
+    const C vp = R[pp], vm = R[pm];
+    const double fpx = ((double)vp.x + (double)vm.x) * scale, fpy = ((double)vp.y + (double)vm.y) * scale;
+    const double fmx = ((double)vp.x - (double)vm.x) * scale, fmy = ((double)vp.y - (double)vm.y) * scale;
+    const int ba = band0 + 2 * t, bb = ba + 1;
+    double fi = occ[ba] * 0.5;
+    if (fi == 0.0) fi = 1.0;
+    const double2 ca = c0[(long)ba * ngpw + g];
+    const C na = acc[2 * tt];
+    c2[(long)ba * ngpw + g] =
+        make_double2(-fi * (kin * ca.x + fpx) + (double)na.x, -fi * (kin * ca.y + fmy) + (double)na.y);
+    if (bb < nstate) {
+      const C nbv = acc[2 * tt + 1];
+      double fb = occ[bb] * 0.5;
+      if (fb == 0.0) fb = 1.0;
+      const double2 cb = c0[(long)bb * ngpw + g];
+      c2[(long)bb * ngpw + g] =
+          make_double2(-fb * (kin * cb.x + fpy) + (double)nbv.x, -fb * (kin * cb.y - fmx) + (double)nbv.y);
+    }
+  }
+}
+// fnonloc for projectors j0 .. j0+npj-1 beyond the first UNPACK_NPJ, FP64:
+// C2(b, G) += sum_j P_j(G) D(j, b) for bands band0 .. band0+nball-1; grid
+// (ngpw/128, ceil(nball/FNL_BANDS)), FNL_BANDS bands per block
+constexpr int FNL_BANDS = 16;
+template <int NPJ>
+__global__ void __launch_bounds__(128) k_fnonloc_add(int ngpw, int band0, int nball, int j0, int npj,
+                                                     const double2 *__restrict__ P, const double *__restrict__ D,
+                                                     int nproj, double2 *__restrict__ c2) {
+  extern __shared__ double Dsd[];  // [b][j]
+  band0 += blockIdx.y * FNL_BANDS;
+  const int nb = min(FNL_BANDS, nball - (int)blockIdx.y * FNL_BANDS);
+  for (int i = threadIdx.x; i < nb * npj; i += blockDim.x) {
+    const int b = i / npj, j = i - b * npj;
+    Dsd[i] = D[j0 + j + (long)nproj * (band0 + b)];
+  }
+  __syncthreads();
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngpw) return;
+  double2 pj[NPJ];
+#pragma unroll
+  for (int j = 0; j < NPJ; ++j) {
+    pj[j] = make_double2(0.0, 0.0);
+    if (j < npj) {
+      double2 v = P[(long)(j0 + j) * ngpw + g];
+      if (g == 0) v = make_double2(2.0 * v.x, 2.0 * v.y);
+      pj[j] = v;
+    }
+  }
+  for (int b = 0; b < nb; ++b) {
+    const double *d = Dsd + b * npj;
+    double2 a = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int j = 0; j < NPJ; ++j)
+      if (j < npj) a = cfmas(pj[j], d[j], a);
+    double2 &o = c2[(long)(band0 + b) * ngpw + g];
+    o = make_double2(o.x + a.x, o.y + a.y);
   }
 }
 
@@ -447,8 +576,8 @@ struct BandWalk {
   }
 };
 
-__global__ void k_ekin(int ngpw, int nstate, const double2 *c0, const double *hg, const double *occ, double *part) {
-  __shared__ double sh[32];
+__global__ void k_ekin(int ngpw, int nstate, const double2 *c0, const double *hg, const double *occ, double *part,
+                       double *out, unsigned *ticket) {
   double s = 0;
   BandWalk w((long)ngpw * nstate, ngpw);
 #pragma unroll 4
@@ -456,8 +585,8 @@ __global__ void k_ekin(int ngpw, int nstate, const double2 *c0, const double *hg
     const double2 c = c0[w.k];
     s += occ[w.b] * hg[w.g] * (c.x * c.x + c.y * c.y);
   }
-  double r = block_sum(s, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = r;
+  const double v[1] = {s};
+  reduce_and_finish<1>(v, part, out, ticket);
 }
 // c = 2 a - c (wavefunction predictor)
 // c = w a + c (the current step's term of the wavefunction predictor)
@@ -502,36 +631,15 @@ __global__ void k_zclean(int n, int ngpw, double2 *c) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) c[(long)i * ngpw].y = 0.0;
 }
-// eval_GMAX (gradient.f90:36-61): max |C2| over occupied bands
-// max |c2|^2 per block (the square root is taken once, in k_finish_max)
-__global__ void k_gmax(long tot, const double2 *c2, double *part) {
-  __shared__ double sh[32];
-  double m = -1.0;
-  const long stride = (long)gridDim.x * blockDim.x;
-  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  for (; k + 3 * stride < tot; k += 4 * stride) {
-    const double2 a = c2[k], b = c2[k + stride], c = c2[k + 2 * stride], d = c2[k + 3 * stride];
-    m = fmax(fmax(m, fmax(a.x * a.x + a.y * a.y, b.x * b.x + b.y * b.y)),
-             fmax(c.x * c.x + c.y * c.y, d.x * d.x + d.y * d.y));
-  }
-  for (; k < tot; k += stride) m = fmax(m, c2[k].x * c2[k].x + c2[k].y * c2[k].y);
-  double r = block_max(m, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = r;
-}
-__global__ void k_finish_max(const double *part, int nb, double *out) {
-  __shared__ double sh[32];
-  double m = -1.0;
-  for (int i = threadIdx.x; i < nb; i += blockDim.x) m = fmax(m, part[i]);
-  double r = block_max(m, sh);
-  if (threadIdx.x == 0) *out = sqrt(fmax(r, 0.0));  // partials hold |c2|^2
-}
-
-// PRECON + GGNORM (cg.f90:102-107, 281-311): cp = fi K c2; partial DOTP sums
-__global__ void k_precon(int ngpw, int nstate, int nocc, const double *vpp, const double *occ, const double2 *c2,
-                         double2 *cp, double *part) {
-  __shared__ double sh[32];
-  double s = 0;
-  BandWalk w((long)ngpw * nstate, ngpw);
+// eval_GMAX (gradient.f90:36-61) and the preconditioned-gradient norm of
+// PRECON + GGNORM (cg.f90:102-107, 281-311) in one pass over the occupied
+// bands of C2: out[0] = GEMAX = max |C2|, out[1] = sum_i DOTP(cp_i, cp_i)
+// with cp = f_i^-1 K(G) C2 (f_i^-1 = 1 for f_i <= 0.01); cp itself is not
+// stored, the PCG update forms it again from C2.
+__global__ void k_gmax_precon(int ngpw, int nocc, const double *vpp, const double *occ, const double2 *c2,
+                              double *part, double *out, unsigned *ticket) {
+  double m = 0.0, s = 0.0;
+  BandWalk w((long)ngpw * nocc, ngpw);
   int bf = -1;
   double fi = 1.0;
 #pragma unroll 4
@@ -541,48 +649,66 @@ __global__ void k_precon(int ngpw, int nstate, int nocc, const double *vpp, cons
       bf = b;
       fi = occ[b] > 0.01 ? 1.0 / occ[b] : 1.0;
     }
-    const double f = fi * vpp[g];
     const double2 c = c2[w.k];
+    const double a2 = c.x * c.x + c.y * c.y;
+    m = fmax(m, a2);
+    const double f = fi * vpp[g];
     const double2 v = make_double2(f * c.x, f * c.y);
-    cp[w.k] = v;
-    if (b < nocc) s += (g == 0) ? v.x * v.x : 2.0 * (v.x * v.x + v.y * v.y);
+    s += (g == 0) ? v.x * v.x : 2.0 * (v.x * v.x + v.y * v.y);
   }
-  double r = block_sum(s, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = r;
+  const double vals[2] = {sqrt(m), s};  // sqrt is monotonic: the max of the roots is the root of the max
+  reduce_and_finish<2, 1u>(vals, part, out, ticket);
 }
-// PCG direction and step (cg.f90:109-143); scal[0] = ggnorm (new),
-// scal[1] = previous ggnorm, scal[8] = the CG step number;
-// gamma = forget * new/prev
-__global__ void k_pcg_update(long tot, const double *scal, double2 *cp, double2 *hnm1, double2 *c0) {
-  const int istep = (int)scal[8];
-  double forget = istep <= 10 ? 0.60 : (istep <= 20 ? 0.91 : 0.95);
-  double gamma = (istep == 1) ? 0.0 : forget * (scal[0] / scal[1]);
+// PCG direction and step (cg.f90:109-143) with cp = f_i^-1 K(G) C2 (PRECON,
+// cg.f90:281-311); gamma = forget * ggnorm(new) / ggnorm(previous)
+__global__ void k_pcg_update(int ngpw, int nstate, const double *scal, const double *vpp, const double *occ,
+                             const double2 *__restrict__ c2, double2 *__restrict__ hnm1, double2 *__restrict__ c0) {
+  const int istep = (int)scal[S_ISTEP];
+  const double forget = istep <= 10 ? 0.60 : (istep <= 20 ? 0.91 : 0.95);
+  const double gamma = (istep == 1) ? 0.0 : forget * (scal[S_GG] / scal[S_GGPREV]);
   const double dt = 5.0 * 5.0 / 400.0;
-  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < tot; k += (long)gridDim.x * blockDim.x) {
-    double2 d = cp[k];
-    if (istep > 1) {
-      d.x += gamma * hnm1[k].x;
-      d.y += gamma * hnm1[k].y;
+  BandWalk w((long)ngpw * nstate, ngpw);
+  int bf = -1;
+  double fi = 1.0;
+#pragma unroll 4
+  for (; w.k < w.k1; w.next(ngpw)) {
+    if (w.b != bf) {
+      bf = w.b;
+      fi = occ[bf] > 0.01 ? 1.0 / occ[bf] : 1.0;
     }
-    hnm1[k] = d;
-    c0[k].x += dt * d.x;
-    c0[k].y += dt * d.y;
+    const double f = fi * vpp[w.g];
+    const double2 c = c2[w.k];
+    double2 d = make_double2(f * c.x, f * c.y);
+    if (istep > 1) {
+      const double2 h = hnm1[w.k];
+      d.x += gamma * h.x;
+      d.y += gamma * h.y;
+    }
+    hnm1[w.k] = d;
+    double2 x = c0[w.k];
+    x.x += dt * d.x;
+    x.y += dt * d.y;
+    c0[w.k] = x;
   }
 }
 __global__ void k_copy_scalar(const double *src, double *dst) { *dst = *src; }
 
 // Shared-memory blocked Cholesky + inverse for n <= CHOL_NMAX, one block of
-// CHOL_NT threads.  The matrix is padded to np = 16*ceil(n/16) with the
-// identity and held in shared memory with leading dimension np+1.  Per
-// 16-column block k (right-looking): one warp factors the diagonal block in
-// registers (lane l holds column l, rows of other lanes arrive by shuffles)
-// and inverts it in place (X_kk = U_kk^{-1}, back substitution per column);
-// all threads then form the panel U_k,c = X_kk^T S_k,c and update the
-// trailing upper triangle S_c,d -= U_k,c^T U_k,d.  The inverse is completed
-// by block back substitution, j = last ... 0: X_j,c = X_jj R_j,c (c > j),
-// then R_i,c -= U_i,j X_j,c (i < j, c >= j; the block c = j becomes
-// -U_i,j X_jj), with R = I to start.  A non-positive pivot sets *info to its
-// 1-based index; Ui gets U^{-1} (upper, zero below).
+// CHOL_NT threads (DPOTRF + DTRTRI of UINV, wfn_initialize.f90:504-530).
+// The matrix is padded to np = 16*ceil(n/16) with the identity and held in
+// shared memory with leading dimension np+1.  Per 16-column block k
+// (right-looking), with U_kk and X_kk = U_kk^{-1} already in the diagonal
+// block:
+//   phase 2 (all warps): the panel U_k,c = X_kk^T S_k,c (c beyond block k)
+//     and T = U_0:k,k X_kk (the rows above block k, stored aside);
+//   phase 3: warp 0 applies this step's update to the next diagonal block
+//     and factors and inverts it in registers (lookahead), while the other
+//     warps update the trailing upper triangle S_c,d -= U_k,c^T U_k,d and
+//     form the inverse's block column X_0:k,k = -X_0:k,0:k T.
+// X overwrites U block column by block column once T has consumed it, so the
+// inverse needs no separate back substitution: two barriers per block.  A
+// non-positive pivot sets *info to its 1-based index; Ui gets U^{-1} (upper,
+// zero below).
 constexpr int CHOL_NMAX = 144;
 constexpr int CHOL_NT = 512;
 constexpr int CHOL_B = 16;
@@ -640,7 +766,7 @@ __global__ void __launch_bounds__(CHOL_NT) k_chol_inv_s(int n, const double *A, 
   extern __shared__ double M[];
   __shared__ int bad;
   const int np = (n + CHOL_B - 1) / CHOL_B * CHOL_B, ld = np + 1, nb = np / CHOL_B;
-  double *Ut = M + (size_t)np * ld;  // [CHOL_B][np]: a column block of U, rows above it
+  double *Tb = M + (size_t)np * ld;  // [np][CHOL_B]: T(i, s) at Tb[i*CHOL_B + s]
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
   const int hr = lane & 15, hc = 2 * w + (lane >> 4);  // half-warp: row hr of column hc (+32p)
   if (tid == 0) bad = 0;
@@ -648,12 +774,12 @@ __global__ void __launch_bounds__(CHOL_NT) k_chol_inv_s(int n, const double *A, 
     for (int a = lane; a < np; a += 32)
       M[a + ld * b] = (a < n && b < n) ? A[a + (long)n * b] : (a == b ? 1.0 : 0.0);
   __syncthreads();
+  if (w == 0) warp_chol_inv16(M, ld, 0, &bad);
+  __syncthreads();
   for (int kb = 0; kb < nb; ++kb) {
-    const int k0 = CHOL_B * kb, c0 = k0 + CHOL_B;
-    if (w == 0) warp_chol_inv16(M + k0 + ld * k0, ld, k0, &bad);
-    __syncthreads();
     if (bad) break;
-    // panel: U(k0+r, c) = sum_{s<=r} X(s,r) S(k0+s, c); column c lives in one half-warp
+    const int k0 = CHOL_B * kb, c0 = k0 + CHOL_B;
+    // phase 2a: panel, U(k0+r, c) = sum_{s<=r} X(s,r) S(k0+s, c); column c lives in one half-warp
     for (int p = 0; c0 + 32 * p < np; ++p) {
       const int c = c0 + hc + 32 * p;
       double t = 0.0;
@@ -666,20 +792,79 @@ __global__ void __launch_bounds__(CHOL_NT) k_chol_inv_s(int n, const double *A, 
       if (c < np) M[(k0 + hr) + ld * c] = t;
       __syncwarp();
     }
+    // phase 2b: T(i, s) = sum_{s' <= s} U(i, k0+s') X(s', s), rows i < k0
+    for (int idx = tid; idx < k0 * CHOL_B; idx += blockDim.x) {
+      const int i = idx / CHOL_B, s = idx - i * CHOL_B;
+      double t0 = 0.0, t1 = 0.0;
+#pragma unroll
+      for (int q = 0; q < CHOL_B; q += 2) {
+        if (q <= s) t0 = fma(M[i + ld * (k0 + q)], M[(k0 + q) + ld * (k0 + s)], t0);
+        if (q + 1 <= s) t1 = fma(M[i + ld * (k0 + q + 1)], M[(k0 + q + 1) + ld * (k0 + s)], t1);
+      }
+      Tb[i * CHOL_B + s] = t0 + t1;
+    }
     __syncthreads();
-    // trailing update: warp per column c, lanes over rows r <= c
-    for (int c = c0 + w; c < np; c += nw) {
-      double uc[CHOL_B];
+    if (w == 0) {
+      // lookahead: this step's update of the next diagonal block, then its
+      // factor and inverse
+      if (c0 < np) {
+        for (int e = lane; e < CHOL_B * CHOL_B; e += 32) {
+          const int r = c0 + (e & 15), c = c0 + (e >> 4);
+          if (r <= c) {
+            double t0 = 0.0, t1 = 0.0;
 #pragma unroll
-      for (int s = 0; s < CHOL_B; ++s) uc[s] = M[(k0 + s) + ld * c];
-      for (int r = c0 + lane; r <= c; r += 32) {
-        double t0 = 0.0, t1 = 0.0;  // two chains of eight
-#pragma unroll
-        for (int s = 0; s < CHOL_B; s += 2) {
-          t0 = fma(M[(k0 + s) + ld * r], uc[s], t0);
-          t1 = fma(M[(k0 + s + 1) + ld * r], uc[s + 1], t1);
+            for (int s = 0; s < CHOL_B; s += 2) {
+              t0 = fma(M[(k0 + s) + ld * r], M[(k0 + s) + ld * c], t0);
+              t1 = fma(M[(k0 + s + 1) + ld * r], M[(k0 + s + 1) + ld * c], t1);
+            }
+            M[r + ld * c] -= t0 + t1;
+          }
         }
-        M[r + ld * c] -= t0 + t1;
+        __syncwarp();
+        warp_chol_inv16(M + c0 + ld * c0, ld, c0, &bad);
+      }
+    } else {
+      // warps 1..nw-1: the inverse's block column k, one lane per (row i < k0,
+      // four columns s0..s0+3: four independent sums); the lanes of a warp
+      // step through m together (from the warp's smallest row, masked below
+      // their own), so T(m, .) is a broadcast and X(i, m) a contiguous row
+      for (int base = tid - 32 - lane; base < 4 * k0; base += blockDim.x - 32) {
+        const int idx = base + lane;
+        const bool act = idx < 4 * k0;
+        const int grp = act ? idx / k0 : 0, i = act ? idx - grp * k0 : k0, s0 = 4 * grp;
+        const int m0 = __reduce_min_sync(0xffffffffu, i);
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        for (int m = m0; m < k0; ++m) {
+          const double x = (m >= i) ? M[i + ld * m] : 0.0;
+          const double2 ta = *reinterpret_cast<const double2 *>(Tb + m * CHOL_B + s0);
+          const double2 tb = *reinterpret_cast<const double2 *>(Tb + m * CHOL_B + s0 + 2);
+          a0 = fma(x, ta.x, a0);
+          a1 = fma(x, ta.y, a1);
+          a2 = fma(x, tb.x, a2);
+          a3 = fma(x, tb.y, a3);
+        }
+        if (act) {
+          M[i + ld * (k0 + s0)] = -a0;
+          M[i + ld * (k0 + s0 + 1)] = -a1;
+          M[i + ld * (k0 + s0 + 2)] = -a2;
+          M[i + ld * (k0 + s0 + 3)] = -a3;
+        }
+      }
+      const int ntask = max(0, np - c0 - CHOL_B);
+      for (int task = w - 1; task < ntask; task += nw - 1) {
+        const int c = c0 + CHOL_B + task;
+        double uc[CHOL_B];
+#pragma unroll
+        for (int s = 0; s < CHOL_B; ++s) uc[s] = M[(k0 + s) + ld * c];
+        for (int r = c0 + lane; r <= c; r += 32) {
+          double t0 = 0.0, t1 = 0.0;  // two chains of eight
+#pragma unroll
+          for (int s = 0; s < CHOL_B; s += 2) {
+            t0 = fma(M[(k0 + s) + ld * r], uc[s], t0);
+            t1 = fma(M[(k0 + s + 1) + ld * r], uc[s + 1], t1);
+          }
+          M[r + ld * c] -= t0 + t1;
+        }
       }
     }
     __syncthreads();
@@ -688,45 +873,6 @@ __global__ void __launch_bounds__(CHOL_NT) k_chol_inv_s(int n, const double *A, 
     if (tid == 0) *info = bad;
     return;
   }
-  for (int jb = nb - 1; jb >= 0; --jb) {
-    const int k0 = CHOL_B * jb, c0 = k0 + CHOL_B;
-    // X_j,c = X_jj R_j,c, c >= c0
-    for (int p = 0; c0 + 32 * p < np; ++p) {
-      const int c = c0 + hc + 32 * p;
-      double t = 0.0;
-      if (c < np) {
-#pragma unroll
-        for (int s = 0; s < CHOL_B; ++s)
-          if (s >= hr) t += M[(k0 + hr) + ld * (k0 + s)] * M[(k0 + s) + ld * c];
-      }
-      __syncwarp();
-      if (c < np) M[(k0 + hr) + ld * c] = t;
-      __syncwarp();
-    }
-    if (k0 == 0) break;
-    // copy U_i,j (rows i < k0) aside, then R_i,c -= U_i,j X_j,c for c >= k0
-    for (int s = w; s < CHOL_B; s += nw)
-      for (int i = lane; i < k0; i += 32) Ut[s * np + i] = M[i + ld * (k0 + s)];
-    __syncthreads();
-    for (int c = k0 + w; c < np; c += nw) {
-      const int smax = (c < c0) ? c - k0 : CHOL_B - 1;  // X_jj is upper triangular
-      double xc[CHOL_B];
-#pragma unroll
-      for (int s = 0; s < CHOL_B; ++s) xc[s] = (s <= smax) ? M[(k0 + s) + ld * c] : 0.0;
-      for (int i = lane; i < k0; i += 32) {
-        double t0 = 0.0, t1 = 0.0;
-#pragma unroll
-        for (int s = 0; s < CHOL_B; s += 2) {
-          t0 = fma(Ut[s * np + i], xc[s], t0);
-          t1 = fma(Ut[(s + 1) * np + i], xc[s + 1], t1);
-        }
-        const double t = t0 + t1;
-        M[i + ld * c] = (c < c0) ? -t : M[i + ld * c] - t;
-      }
-    }
-    __syncthreads();
-  }
-  __syncthreads();  // the last block row (jb = 0) left the loop right after its writes
   for (int b = w; b < n; b += nw)
     for (int a = lane; a < n; a += 32) Ui[a + (long)n * b] = (a <= b) ? M[a + ld * b] : 0.0;
   if (tid == 0) *info = 0;
@@ -789,34 +935,27 @@ __global__ void k_esr_par(int nat, const int *isa_is, const int *isa_ia, int na_
   if (threadIdx.x == 0) out[0] = e;
 }
 
-// fnonloc G=0 row (P holds the halved G=0 entry): C2_b(0) += sum_j P_j(0) D(j,b)
-__global__ void k_fnonloc_g0(int nproj, int nstate, int ngpw, const double2 *P, const double *D, double2 *c2) {
-  int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nstate) return;
-  double x = 0, y = 0;
-  for (int j = 0; j < nproj; ++j) {
-    double d = D[j + (long)nproj * b];
-    x += P[(long)j * ngpw].x * d;
-    y += P[(long)j * ngpw].y * d;
-  }
-  c2[(long)b * ngpw].x += x;
-  c2[(long)b * ngpw].y += y;
-}
 // D = -f' (H nl), f' = occ (1 when < 1e-5)   (FNONLOC T = -FFI*WSG, UPF DDIA)
 // and E_nl partial: sum_b occ_b sum_j nl(j,b) (H nl)(j,b)
-__global__ void k_nl_energy_d(int nproj, int nstate, const double *nl, const double *hn, const double *occ, double *D,
-                              double *part) {
-  __shared__ double sh[32];
+// with (H nl)(j, b) = sum_j' H(j, j') nl(j', b) formed here (H couples the
+// projectors of one atom: wsg on the diagonal, or hlsg between projectors of
+// equal l and m) and stored for the forces
+__global__ void k_nl_energy_d(int nproj, int nstate, const double *H, const double *nl, double *hn, const double *occ,
+                              double *D, double *part, double *out, unsigned *ticket) {
   double s = 0;
   long tot = (long)nproj * nstate;
   for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < tot; k += (long)gridDim.x * blockDim.x) {
-    int b = (int)(k / nproj);
+    const int b = (int)(k / nproj), j = (int)(k - (long)b * nproj);
+    const double *nb = nl + (long)nproj * b;
+    double h = 0.0;
+    for (int jp = 0; jp < nproj; ++jp) h += H[j + (long)nproj * jp] * nb[jp];
+    hn[k] = h;
     double f = occ[b] < 1e-5 ? 1.0 : occ[b];
-    D[k] = -f * hn[k];
-    s += occ[b] * nl[k] * hn[k];
+    D[k] = -f * h;
+    s += occ[b] * nl[k] * h;
   }
-  double r = block_sum(s, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = r;
+  const double v[1] = {s};
+  reduce_and_finish<1>(v, part, out, ticket);
 }
 
 // ---------------------------------------------------------------- forces

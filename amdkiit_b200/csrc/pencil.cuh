@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(512) k_xt_bwd_pair(const double2 *__restrict__
       }
     }
     Dft<C, N1, 1>::run(v);
-    twiddle_n<C, N, N1, 1>(v, j2, tw);
+    twiddle_tab<C, N, N1, 1, 0>(v, j2, tw);
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) S[l * NP + k1 * N2 + j2] = v[k1];
   }
@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(512) k_xt_fwd(int T, PencilGeom pg, Plan<C> p,
       for (int j1 = 0; j1 < N1; ++j1) v[j1] = czero<C>();
     }
     Dft<C, N1, -1>::run(v);
-    twiddle_n<C, N, N1, -1>(v, j2, tw);
+    twiddle_tab<C, N, N1, -1, 0>(v, j2, tw);
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) S[l * NP + k1 * N2 + j2] = v[k1];
   }
@@ -142,6 +142,83 @@ __global__ void __launch_bounds__(512) k_xt_fwd(int T, PencilGeom pg, Plan<C> p,
   }
 }
 
+// x = q d + r for task indices: q = (x m) >> 20 with m = 2^20/d + 1 is exact
+// while x d < 2^20 (here x < 16 d and d <= 256), three integer instructions
+// instead of a division by a run-time value
+struct DivMod {
+  unsigned d, m;
+  __device__ __forceinline__ explicit DivMod(int dd) : d((unsigned)dd), m((1u << 20) / (unsigned)dd + 1u) {}
+  __device__ __forceinline__ void operator()(int x, int &q, int &r) const {
+    const unsigned qq = ((unsigned)x * m) >> 20;
+    q = (int)qq;
+    r = x - (int)(qq * d);
+  }
+};
+
+// Length-N transforms of the nz rows of the slab plane P (row stride N+1), in
+// place.  nat_to_perm: natural order in, X[k1 + N1*k2] left at position
+// k1*N2 + k2.  perm_to_nat: that permuted order in, natural order out.  Each
+// phase's sub-transform reads and writes the same positions, so a phase needs
+// no barrier inside; the two phases are separated by one.
+template <typename C, int N, int SG>
+__device__ __forceinline__ void rows_nat_to_perm(C *P, int nrow, const DivMod &dr, const C *tw) {
+  constexpr int N1 = fft_n1(N), N2 = N / N1, NP = N + 1;
+  for (int idx = threadIdx.x; idx < nrow * N2; idx += blockDim.x) {
+    int j2, r;
+    dr(idx, j2, r);
+    C *row = P + r * NP;
+    C v[N1];
+#pragma unroll
+    for (int j1 = 0; j1 < N1; ++j1) v[j1] = row[j2 + N2 * j1];
+    Dft<C, N1, SG>::run(v);
+    twiddle_tab<C, N, N1, SG, 0>(v, j2, tw);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) row[k1 * N2 + j2] = v[k1];
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < nrow * N1; idx += blockDim.x) {
+    int k1, r;
+    dr(idx, k1, r);
+    C *row = P + r * NP + k1 * N2;
+    C u[N2];
+#pragma unroll
+    for (int j2 = 0; j2 < N2; ++j2) u[j2] = row[j2];
+    Dft<C, N2, SG>::run(u);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) row[k2] = u[k2];
+  }
+  __syncthreads();
+}
+template <typename C, int N, int SG>
+__device__ __forceinline__ void rows_perm_to_nat(C *P, int nrow, const DivMod &dr, const C *tw) {
+  constexpr int N1 = fft_n1(N), N2 = N / N1, NP = N + 1;
+  for (int idx = threadIdx.x; idx < nrow * N1; idx += blockDim.x) {
+    int k1, r;
+    dr(idx, k1, r);
+    C *row = P + r * NP + k1 * N2;
+    C u[N2];
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) u[k2] = row[k2];
+    Dft<C, N2, SG>::run(u);
+    twiddle_tab<C, N, N2, SG, 1>(u, k1, tw);
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) row[n2] = u[n2];
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < nrow * N2; idx += blockDim.x) {
+    int n2, r;
+    dr(idx, n2, r);
+    C *row = P + r * NP;
+    C w[N1];
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) w[k1] = row[k1 * N2 + n2];
+    Dft<C, N1, SG>::run(w);
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) row[n2 + N2 * n1] = w[n1];
+  }
+  __syncthreads();
+}
+
 // scatter the rays of one x-plane into P (zero elsewhere)
 template <typename C, int N>
 __device__ __forceinline__ void pencil_scatter(C *P, const C *__restrict__ rt_plane, const PencilGeom &pg) {
@@ -155,10 +232,12 @@ __device__ __forceinline__ void pencil_scatter(C *P, const C *__restrict__ rt_pl
 // thread (column, j2) takes the slab planes at kz = j2 + N2*j1 (zero where
 // the slab has no plane) and leaves W_N^(j2 k1) DFT_N1 in S[col][k1*N2 + j2].
 template <typename C, int N>
-__device__ __forceinline__ void zcols_phase_a(const C *P, C *S, const int *zinv, int q0, int ct, const C *tw) {
+__device__ __forceinline__ void zcols_phase_a(const C *P, C *S, const int *zinv, int q0, int ct, const DivMod &dq,
+                                              const C *tw) {
   constexpr int N1 = fft_n1(N), N2 = N / N1, NP = N + 1;
   for (int idx = threadIdx.x; idx < ct * N2; idx += blockDim.x) {
-    const int qq = idx % ct, j2 = idx / ct;
+    int j2, qq;
+    dq(idx, j2, qq);
     C v[N1];
 #pragma unroll
     for (int j1 = 0; j1 < N1; ++j1) {
@@ -166,17 +245,33 @@ __device__ __forceinline__ void zcols_phase_a(const C *P, C *S, const int *zinv,
       v[j1] = (zi >= 0) ? P[zi * NP + q0 + qq] : czero<C>();
     }
     Dft<C, N1, 1>::run(v);
-    twiddle_n<C, N, N1, 1>(v, j2, tw);
+    twiddle_tab<C, N, N1, 1, 0>(v, j2, tw);
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) S[qq * NP + k1 * N2 + j2] = v[k1];
   }
 }
+
+// shared memory of a pencil block: P[nz][N+1], S[CTs][N+1], the twiddle
+// tables (2N) and the kz -> slab index table zinv[N]
+template <typename C, int N> struct PencilSmem {
+  C *P, *S, *tw;
+  int *zinv;
+  __device__ __forceinline__ PencilSmem(unsigned char *raw, int nz, int CTs) {
+    constexpr int NP = N + 1;
+    P = reinterpret_cast<C *>(raw);
+    S = P + nz * NP;
+    tw = S + CTs * NP;
+    zinv = reinterpret_cast<int *>(tw + 2 * N);
+  }
+};
 
 // One x-plane of one band pair through y, z, V(r), z, y (vpsi,
 // wfn_initialize.f90:311-340).  grid (n1, T).  P[zi][q] holds the slab
 // plane (row stride N+1); after the backward y transform column q carries
 // ky = q/N2 + N1*(q%N2).  vp[kx][q][k'] is V at that ky and at
 // kz = k'/N2 + N1*(k'%N2), the order in which the z transform leaves psi.
+// The column tiles are CTs wide (the last may be narrower); the V values of a
+// thread's first task of a tile are loaded before the tile's first phase.
 template <typename C, int N>
 __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C *__restrict__ rt,
                                                      const decltype(C().x) *__restrict__ vp, int CTs) {
@@ -184,27 +279,47 @@ __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C
   constexpr int N1 = fft_n1(N), N2 = N / N1, NP = N + 1;
   extern __shared__ unsigned char smraw[];
   const int nz = pg.nz;
-  C *P = reinterpret_cast<C *>(smraw);
-  C *S = P + nz * NP;
-  C *tw = S + CTs * NP;
-  int *zinv = reinterpret_cast<int *>(tw + N);
+  PencilSmem<C, N> sm(smraw, nz, CTs);
+  C *P = sm.P, *S = sm.S, *tw = sm.tw;
+  const int *zinv = sm.zinv;
   load_tw<C, N>(tw, p);
-  for (int i = threadIdx.x; i < N; i += blockDim.x) zinv[i] = pg.zinv[i];
+  for (int i = threadIdx.x; i < N; i += blockDim.x) sm.zinv[i] = pg.zinv[i];
   const int kx = blockIdx.x, t = blockIdx.y;
   C *plane = rt + ((long)t * pg.n1 + kx) * pg.nray;
   pencil_scatter<C, N>(P, plane, pg);
-  rows_nat_to_perm<C, N, 1>(P, nz, NP, tw);
+  const DivMod dz(nz);
+  rows_nat_to_perm<C, N, 1>(P, nz, dz, tw);
   const Rl *V = vp + (long)kx * N * N;
   for (int q0 = 0; q0 < N; q0 += CTs) {
     const int ct = min(CTs, N - q0);
-    zcols_phase_a<C, N>(P, S, zinv, q0, ct, tw);
+    const DivMod dq(ct);
+    // V of this thread's first middle task, in flight during phase A
+    int k1_0 = 0, qq_0 = 0;
+    dq(threadIdx.x, k1_0, qq_0);
+    const bool has0 = threadIdx.x < ct * N1;
+    Rl v0[N2];
+    {
+      const Rl *vv = V + (long)(q0 + qq_0) * N + k1_0 * N2;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) v0[k2] = has0 ? vv[k2] : (Rl)0;
+    }
+    zcols_phase_a<C, N>(P, S, zinv, q0, ct, dq, tw);
     __syncthreads();
     // DFT_N2 -> psi(kz = k1 + N1*k2), times V, then the first phase of the
     // forward z transform, in registers
     for (int idx = threadIdx.x; idx < ct * N1; idx += blockDim.x) {
-      const int qq = idx % ct, k1 = idx / ct;
+      int k1, qq;
+      dq(idx, k1, qq);
       C *row = S + qq * NP + k1 * N2;
-      const Rl *vv = V + (long)(q0 + qq) * N + k1 * N2;
+      Rl vv[N2];
+      if (idx == threadIdx.x) {
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) vv[k2] = v0[k2];
+      } else {
+        const Rl *vg = V + (long)(q0 + qq) * N + k1 * N2;
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) vv[k2] = vg[k2];
+      }
       C u[N2];
 #pragma unroll
       for (int j2 = 0; j2 < N2; ++j2) u[j2] = row[j2];
@@ -212,14 +327,15 @@ __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C
 #pragma unroll
       for (int k2 = 0; k2 < N2; ++k2) u[k2] = cscale(u[k2], vv[k2]);
       Dft<C, N2, -1>::run(u);
-      twiddle_n<C, N, N2, -1>(u, k1, tw);
+      twiddle_tab<C, N, N2, -1, 1>(u, k1, tw);
 #pragma unroll
       for (int n2 = 0; n2 < N2; ++n2) row[n2] = u[n2];
     }
     __syncthreads();
     // second phase: x(kz = n2 + N2*n1), stored back for the slab planes only
     for (int idx = threadIdx.x; idx < ct * N2; idx += blockDim.x) {
-      const int qq = idx % ct, n2 = idx / ct;
+      int n2, qq;
+      dq(idx, n2, qq);
       C w[N1];
 #pragma unroll
       for (int k1 = 0; k1 < N1; ++k1) w[k1] = S[qq * NP + k1 * N2 + n2];
@@ -232,18 +348,21 @@ __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C
     }
     __syncthreads();
   }
-  rows_perm_to_nat<C, N, -1>(P, nz, NP, tw);
+  rows_perm_to_nat<C, N, -1>(P, nz, dz, tw);
   for (int r = threadIdx.x; r < pg.nray; r += blockDim.x) plane[r] = P[pg.rpos[r]];
 }
 
 // Density: one x-plane for a group of band pairs (density.f90:49-86);
 // rho_part[grp][kx][q][k'] += wa_t Re^2 + wb_t Im^2 in the permuted (ky, kz)
-// order of the vpsi kernel.  grid (n1, ngroups).  The group sum is kept in
-// shared memory in the data's precision (FP32 for float2), then stored to
-// (add = 0: the first batch of pairs) or added to (add = 1) the FP64 partial
-// grid.
-template <typename C, int N>
-__global__ void __launch_bounds__(PNT) k_pencil_density(PencilGeom pg, Plan<C> p, const C *__restrict__ rt, int T,
+// order of the vpsi kernel.  grid (n1, ngroups).  A thread takes the same
+// (column, k1) tasks for every pair, so its group sums stay in registers
+// (NS slots of N2 values: column tiles x task rounds, NS = ntiles * reps with
+// reps = ceil(CTs N1 / PNT)), in the data's precision (FP32 for float2: the
+// mixed path ends on FP64).  At the end the sums go through shared memory
+// (over P and S) and are stored to (add = 0: the first batch of pairs) or
+// added to (add = 1) the FP64 partial grid.
+template <typename C, int N, int NS>
+__global__ void __launch_bounds__(PNT, sizeof(C) == 8 ? 2 : 1) k_pencil_density(PencilGeom pg, Plan<C> p, const C *__restrict__ rt, int T,
                                                         int per_group, const double *__restrict__ wa,
                                                         const double *__restrict__ wb, double *__restrict__ rho_part,
                                                         int CTs, int add) {
@@ -251,16 +370,20 @@ __global__ void __launch_bounds__(PNT) k_pencil_density(PencilGeom pg, Plan<C> p
   constexpr int N1 = fft_n1(N), N2 = N / N1, NP = N + 1;
   extern __shared__ unsigned char smraw[];
   const int nz = pg.nz;
-  Rl *acc = reinterpret_cast<Rl *>(smraw);  // [q][k'], row stride N+1
-  C *P = reinterpret_cast<C *>(acc + N * NP);
-  C *S = P + nz * NP;
-  C *tw = S + CTs * NP;
-  int *zinv = reinterpret_cast<int *>(tw + N);
+  PencilSmem<C, N> sm(smraw, nz, CTs);
+  C *P = sm.P, *S = sm.S, *tw = sm.tw;
+  const int *zinv = sm.zinv;
   load_tw<C, N>(tw, p);
-  for (int i = threadIdx.x; i < N; i += blockDim.x) zinv[i] = pg.zinv[i];
-  for (int idx = threadIdx.x; idx < N * NP; idx += blockDim.x) acc[idx] = (Rl)0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) sm.zinv[i] = pg.zinv[i];
   const int kx = blockIdx.x, grp = blockIdx.y;
   const int t0 = grp * per_group, t1 = min(T, t0 + per_group);
+  const int ntiles = (N + CTs - 1) / CTs;
+  const int reps = NS / ntiles;  // the launch guarantees ntiles * reps == NS and CTs N1 <= reps PNT
+  Rl acc[NS][N2];
+#pragma unroll
+  for (int s = 0; s < NS; ++s)
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) acc[s][k2] = (Rl)0;
   // the next pair's rays are loaded into registers while this pair is
   // transformed (planes of up to PREF * blockDim rays; else loaded in turn)
   constexpr int PREF = 4;
@@ -274,6 +397,7 @@ __global__ void __launch_bounds__(PNT) k_pencil_density(PencilGeom pg, Plan<C> p
       nxt[i] = r < pg.nray ? pl[r] : czero<C>();
     }
   };
+  const DivMod dz(nz);
   if (pre && t0 < t1) fetch(t0);
   for (int t = t0; t < t1; ++t) {
     if (pre) {
@@ -289,16 +413,22 @@ __global__ void __launch_bounds__(PNT) k_pencil_density(PencilGeom pg, Plan<C> p
     } else {
       pencil_scatter<C, N>(P, rt + ((long)t * pg.n1 + kx) * pg.nray, pg);
     }
-    rows_nat_to_perm<C, N, 1>(P, nz, NP, tw);
+    rows_nat_to_perm<C, N, 1>(P, nz, dz, tw);
     const Rl fa = (Rl)wa[t], fb = (Rl)wb[t];
-    for (int q0 = 0; q0 < N; q0 += CTs) {
-      const int ct = min(CTs, N - q0);
-      zcols_phase_a<C, N>(P, S, zinv, q0, ct, tw);
-      __syncthreads();
-      for (int idx = threadIdx.x; idx < ct * N1; idx += blockDim.x) {
-        const int qq = idx % ct, k1 = idx / ct;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const int ti = s / reps, rr = s - ti * reps;
+      const int q0 = ti * CTs, ct = min(CTs, N - q0);
+      const DivMod dq(ct);
+      if (rr == 0) {
+        zcols_phase_a<C, N>(P, S, zinv, q0, ct, dq, tw);
+        __syncthreads();
+      }
+      const int idx = threadIdx.x + rr * PNT;
+      if (idx < ct * N1) {
+        int k1, qq;
+        dq(idx, k1, qq);
         const C *row = S + qq * NP + k1 * N2;
-        Rl *ar = acc + (q0 + qq) * NP + k1 * N2;
         C u[N2];
 #pragma unroll
         for (int j2 = 0; j2 < N2; ++j2) u[j2] = row[j2];
@@ -306,17 +436,34 @@ __global__ void __launch_bounds__(PNT) k_pencil_density(PencilGeom pg, Plan<C> p
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2) {
           const Rl re = u[k2].x, im = u[k2].y;
-          ar[k2] += fa * re * re + fb * im * im;
+          acc[s][k2] += fa * re * re + fb * im * im;
         }
       }
-      __syncthreads();
+      if (rr == reps - 1) __syncthreads();
     }
   }
-  __syncthreads();  // a group without pairs has seen no barrier since the clearing
+  __syncthreads();  // a group without pairs has seen no barrier since the tables
+  // group sums -> shared memory [q][k'] (row stride N+1) -> the partial grid
+  Rl *stage = reinterpret_cast<Rl *>(smraw);
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int ti = s / reps, rr = s - ti * reps;
+    const int q0 = ti * CTs, ct = min(CTs, N - q0);
+    const int idx = threadIdx.x + rr * PNT;
+    if (idx < ct * N1) {
+      int k1, qq;
+      const DivMod dq(ct);
+      dq(idx, k1, qq);
+      Rl *ar = stage + (q0 + qq) * NP + k1 * N2;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) ar[k2] = acc[s][k2];
+    }
+  }
+  __syncthreads();
   double *out = rho_part + ((long)grp * pg.n1 + kx) * N * N;
   for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
     const int q = idx / N, k = idx % N;
-    const double v = (double)acc[q * NP + k];
+    const double v = (double)stage[q * NP + k];
     out[idx] = add ? out[idx] + v : v;
   }
 }

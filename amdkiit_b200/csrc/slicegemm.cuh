@@ -34,9 +34,12 @@
 // bands' sigma): persistent CTAs over 128-row tiles of the long index, the
 // epilogue writes (or subtracts from) FP64 output.
 //
-// Every wait is bounded (SG_SPIN polls): on expiry the kernel records a code
-// in *err, writes NaN where its result would go, waits (bounded) for its own
-// copies in flight, frees its tensor memory and returns.
+// Every wait is bounded: on expiry the kernel records a code in *err, writes
+// NaN where its result would go, waits for its own copies and MMAs in flight,
+// frees its tensor memory and returns.  The pipeline waits (a stage's data,
+// a free stage, the accumulators of a tile) give up after plim polls (a
+// kernel argument, SG_SPIN normally, smaller to test the expiry path); the
+// drains of a block's own copies and MMAs always allow SG_SPIN polls.
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -78,9 +81,10 @@ __device__ __forceinline__ bool sg_bar_try(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// bounded wait for the phase of the given parity; false (and *err = code) on expiry
-__device__ __forceinline__ bool sg_bar_wait(uint32_t bar, uint32_t parity, int *err, int code) {
-  for (long it = 0; it < SG_SPIN; ++it) {
+// bounded wait for the phase of the given parity; false (and *err = code)
+// after limit polls (limit <= 0: at once, without polling)
+__device__ __forceinline__ bool sg_bar_wait(uint32_t bar, uint32_t parity, int *err, int code, long limit = SG_SPIN) {
+  for (long it = 0; it < limit; ++it) {
     if (sg_bar_try(bar, parity)) return true;
     if (it > 32) __nanosleep(64);
   }
@@ -304,8 +308,10 @@ constexpr int SG_TN_THREADS = 256;
 template <int S>
 __global__ void __launch_bounds__(SG_TN_THREADS, 1) k_sgemm_tn(const __grid_constant__ CUtensorMap ta,
                                                      const __grid_constant__ CUtensorMap tb, int same, int ktiles,
-                                                     int per_cta, double *__restrict__ partial, int *err) {
+                                                     int per_cta, double *__restrict__ partial, int *err,
+                                                     long plim) {
   using G = SgTn<S>;
+  __shared__ int aborted;  // a pipeline wait of this block expired
   extern __shared__ unsigned char sg_raw[];
   unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sg_raw) + 1023) & ~uintptr_t(1023));
   // a Gram product (same) stages A alone, so twice as many stages fit
@@ -318,6 +324,7 @@ __global__ void __launch_bounds__(SG_TN_THREADS, 1) k_sgemm_tn(const __grid_cons
   const int nt = max(0, min(per_cta, ktiles - kt0));
   const uint32_t full0 = sg_smem(bars), empty0 = sg_smem(bars + 2 * SG_TN_ST), done = sg_smem(bars + 4 * SG_TN_ST);
   if (threadIdx.x == 0) {
+    aborted = 0;
     for (int i = 0; i < 2 * SG_TN_ST; ++i) {
       sg_bar_init(full0 + 8 * i, 1);
       sg_bar_init(empty0 + 8 * i, 1);
@@ -336,7 +343,10 @@ __global__ void __launch_bounds__(SG_TN_THREADS, 1) k_sgemm_tn(const __grid_cons
     int issued = 0;
     for (int i = 0; i < nt; ++i) {
       const int s = i % nst;
-      if (i >= nst && !sg_bar_wait(empty0 + 8 * s, ((i / nst) - 1) & 1, err, 1)) break;
+      if (i >= nst && !sg_bar_wait(empty0 + 8 * s, ((i / nst) - 1) & 1, err, 1, plim)) {
+        aborted = 1;
+        break;
+      }
       const uint32_t fb = full0 + 8 * s;
       sg_bar_expect_tx(fb, bytes);
       const uint32_t dA = sg_smem(base + s * sbytes), dB = dA + S * G::PLANE;
@@ -355,7 +365,10 @@ __global__ void __launch_bounds__(SG_TN_THREADS, 1) k_sgemm_tn(const __grid_cons
     constexpr uint32_t idesc = sg_idesc(false);
     for (int i = 0; i < nt; ++i) {
       const int s = i % nst;
-      if (!sg_bar_wait(full0 + 8 * s, (i / nst) & 1, err, 2)) break;
+      if (!sg_bar_wait(full0 + 8 * s, (i / nst) & 1, err, 2, plim)) {
+        aborted = 1;
+        break;
+      }
       sg_fence_after();
       const uint32_t aA = sg_smem(base + s * sbytes), aB = same ? aA : aA + S * G::PLANE;
 #pragma unroll
@@ -373,9 +386,9 @@ __global__ void __launch_bounds__(SG_TN_THREADS, 1) k_sgemm_tn(const __grid_cons
     sg_commit(done);
     sg_bar_wait(done, 0, err, 5);  // every MMA of this block has finished
   }
-  __syncwarp();
+  __syncthreads();  // the producer's copies and the issuer's MMAs have drained; `aborted` is final
   // epilogue: lane m of warp w holds row m = 32 (w % 4) + lane of every accumulator
-  const bool ok = __all_sync(0xffffffffu, nt > 0 && sg_bar_wait(done, 0, err, 3));
+  const bool ok = __all_sync(0xffffffffu, nt > 0 && !aborted && sg_bar_wait(done, 0, err, 3));
   sg_fence_after();
   const int ew = warp & 3, half = warp >> 2;
   const int m = 32 * ew + lane;
@@ -467,7 +480,7 @@ __global__ void __launch_bounds__(SG_NN_THREADS, 1) k_sgemm_nn(const __grid_cons
                                                      const __grid_constant__ CUtensorMap tb, int mtiles, long mreal,
                                                      double *__restrict__ out, long ldo, int nn,
                                                      const double *__restrict__ colscale,
-                                                     int8_t *__restrict__ dig, long kpad, int *err) {
+                                                     int8_t *__restrict__ dig, long kpad, int *err, long plim) {
   using G = SgNn<S>;
   extern __shared__ unsigned char sg_raw[];
   unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sg_raw) + 1023) & ~uintptr_t(1023));
@@ -506,7 +519,7 @@ __global__ void __launch_bounds__(SG_NN_THREADS, 1) k_sgemm_nn(const __grid_cons
     int issued = 0;
     for (int q = 0; q < nq; ++q) {
       const int s = q % SG_NN_ST;
-      if (q >= SG_NN_ST && !sg_bar_wait(empty0 + 8 * s, ((q / SG_NN_ST) - 1) & 1, err, 11)) break;
+      if (q >= SG_NN_ST && !sg_bar_wait(empty0 + 8 * s, ((q / SG_NN_ST) - 1) & 1, err, 11, plim)) break;
       const uint32_t fb = full0 + 8 * s;
       sg_bar_expect_tx(fb, S * G::PLANE);
       const int m0 = (blockIdx.x + q * gridDim.x) * SG_M;
@@ -519,11 +532,11 @@ __global__ void __launch_bounds__(SG_NN_THREADS, 1) k_sgemm_nn(const __grid_cons
       sg_bar_wait(full0 + 8 * (q % SG_NN_ST), (q / SG_NN_ST) & 1, err, 14);
   } else if (threadIdx.x == 32 && nq > 0) {
     constexpr uint32_t idesc = sg_idesc(true);
-    bool ok = sg_bar_wait(bfull, 0, err, 12);
+    bool ok = sg_bar_wait(bfull, 0, err, 12, plim);
     for (int q = 0; q < nq && ok; ++q) {
       const int s = q % SG_NN_ST;
-      if (!sg_bar_wait(full0 + 8 * s, (q / SG_NN_ST) & 1, err, 12)) break;
-      if (q > 0 && !sg_bar_wait(tfree, (q - 1) & 1, err, 13)) break;
+      if (!sg_bar_wait(full0 + 8 * s, (q / SG_NN_ST) & 1, err, 12, plim)) break;
+      if (q > 0 && !sg_bar_wait(tfree, (q - 1) & 1, err, 13, plim)) break;
       sg_fence_after();
       const uint32_t aA = sg_smem(sA + s * S * G::PLANE), aB = sg_smem(sB);
 #pragma unroll
@@ -546,7 +559,7 @@ __global__ void __launch_bounds__(SG_NN_THREADS, 1) k_sgemm_nn(const __grid_cons
     const int ew = warp & 3, cg = (warp - 2) >> 2;
     const int m = 32 * ew + lane;
     for (int q = 0; q < nq; ++q) {
-      const bool ok = __all_sync(0xffffffffu, sg_bar_wait(tfull, q & 1, err, 15));
+      const bool ok = __all_sync(0xffffffffu, sg_bar_wait(tfull, q & 1, err, 15, plim));
       sg_fence_after();
       const long gm = (long)(blockIdx.x + q * gridDim.x) * SG_M + m;
       const bool row_ok = gm < mreal;

@@ -100,6 +100,11 @@ def load_library(path: str = LIBPATH):
     lib.amdk_profile.argtypes = [P, C.c_int]
     lib.amdk_launch_count.argtypes = [P, C.POINTER(C.c_long)]
     lib.amdk_profile_get.argtypes = [P, C.c_int, C.POINTER(C.c_long), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.amdk_ensemble_create.argtypes = [C.POINTER(P), C.c_int, C.POINTER(P)]
+    lib.amdk_ensemble_iteration.argtypes = [P, C.POINTER(C.c_int), C.c_double, C.POINTER(Energies),
+                                            C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    lib.amdk_ensemble_last_ms.argtypes = [P, C.POINTER(C.c_double)]
+    lib.amdk_ensemble_destroy.argtypes = [P]
     _LIB = lib
     return lib
 
@@ -200,12 +205,17 @@ MIXED_STALL_ZONE = 10.0
 class Engine:
     """One system resident on one GPU."""
 
-    def __init__(self, system: System, precision: int = FP64, pair_batch: int = 0, device: int = 0):
+    def __init__(self, system: System, precision: int = FP64, pair_batch: int = 0, device: int = 0,
+                 wait_limit: int = 0):
+        """wait_limit != 0 (tests of the failure path only): the pipeline
+        waits of the tensor-core kernels give up after max(wait_limit, 0)
+        polls (amdk_options.reserved[0])."""
         self.lib = load_library()
         self.system = system
         s, self._keep = system_struct(system)
         opt = _Options()
         opt.device, opt.precision, opt.pair_batch = device, precision, pair_batch
+        opt.reserved[0] = wait_limit
         h = C.c_void_p()
         _check(self.lib.amdk_create(C.byref(s), C.byref(opt), C.byref(h)), "amdk_create")
         self.h = h
@@ -295,6 +305,7 @@ class Engine:
             "eigrxvps": ((self.ngrho,), np.complex128), "eigrxrhos": ((self.ngrho,), np.complex128),
             "vpp": ((self.ngpw,), np.float64),
             "force": ((nsp, self.system.na_max, 3), np.float64),
+            "overlap": ((self.nstate, self.nstate), np.float64),
         }
         del nproj
         shape, dt = shapes[name]
@@ -430,3 +441,43 @@ class Engine:
         finally:
             if refining:
                 self.set_precision(self.precision)
+
+
+class Ensemble:
+    """Several engines (independent systems on one GPU) iterated together
+    through amdk_ensemble_iteration: each CG segment of all members is one
+    CUDA graph launch once every member has run its first iteration."""
+
+    def __init__(self, engines):
+        self.lib = load_library()
+        self.engines = list(engines)
+        n = len(self.engines)
+        arr = (C.c_void_p * n)(*[e.h.value for e in self.engines])
+        h = C.c_void_p()
+        _check(self.lib.amdk_ensemble_create(arr, n, C.byref(h)), "amdk_ensemble_create")
+        self.h = h
+
+    def iteration(self, isteps, gcut: float):
+        n = len(self.engines)
+        st = (C.c_int * n)(*[int(i) for i in isteps])
+        en = (Energies * n)()
+        gm = (C.c_double * n)()
+        cv = (C.c_int * n)()
+        _check(self.lib.amdk_ensemble_iteration(self.h, st, gcut, en, gm, cv), "amdk_ensemble_iteration")
+        return [x.asdict() for x in en], np.array(gm[:]), np.array(cv[:], dtype=bool)
+
+    def last_ms(self) -> float:
+        m = C.c_double()
+        self.lib.amdk_ensemble_last_ms(self.h, C.byref(m))
+        return m.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.amdk_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -82,7 +82,9 @@ typedef struct {
   int device;             /* CUDA device ordinal */
   int precision;          /* AMDK_FP64 or AMDK_MIXED */
   int pair_batch;         /* band pairs per FFT batch (0: automatic) */
-  int reserved[8];
+  int reserved[8];        /* zero; reserved[0] != 0 (tests of the failure path only): the
+                             pipeline waits of the tensor-core kernels give up after
+                             max(reserved[0], 0) polls and the call returns AMDK_ERR_TIMEOUT */
 } amdk_options;
 
 typedef struct {
@@ -184,7 +186,8 @@ int amdk_wfn_history_clear(amdk_ctx *ctx);
 /* Copy a named device array to host memory (parity tests and drivers).
  * Names: "rho","v_pot" (nr3*nr2*nr1 real, x fastest), "rho_g" (ngrho complex),
  * "c2" (ngpw*nstate complex), "nl" (nat*nghmax*nstate), "vps","rhos"
- * (nsp*ngrho), "twnl" (ngpw*nghmax*nsp), "eigrxvps","eigrxrhos" (ngrho complex). */
+ * (nsp*ngrho), "twnl" (ngpw*nghmax*nsp), "eigrxvps","eigrxrhos" (ngrho complex),
+ * "overlap" (nstate*nstate: the last Gram matrix, S of ortho_gs or Lambda). */
 int amdk_get_array(amdk_ctx *ctx, const char *name, void *dst, size_t bytes);
 
 /* Raw pruned 3D FFT on the density sphere (fft_interface.f90:6-29):
@@ -223,6 +226,26 @@ int amdk_fft_sphere_noalloc(amdk_ctx *ctx, int sign, double *coef, double *grid)
 
 /* Elapsed device time of the last amdk_scf_iteration, milliseconds. */
 int amdk_last_iteration_ms(amdk_ctx *ctx, double *ms);
+
+/* Several systems on one GPU advanced together, e.g. an ensemble of small
+ * clusters (no reference counterpart: the reference runs one system per
+ * process).  The contexts stay owned by the caller and must outlive the
+ * ensemble.  amdk_ensemble_iteration runs one CG iteration, as
+ * amdk_scf_iteration does, of every member (istep[i]: member i's CG step
+ * number): from every member's second iteration on, segment A of all members
+ * (density, potential, energies, H|psi>, gradient) is one CUDA graph launch
+ * whose children are the members' own segment graphs, then one host read of
+ * all the GEMAX values decides CHK_TFOR per member, then segment B (forces,
+ * PCG, ortho) is a second launch.  Results equal per-context
+ * amdk_scf_iteration calls.  e, gemax, converged: arrays of n entries (any may
+ * be NULL).  amdk_ensemble_last_ms: device time of the last iteration of all
+ * members together. */
+typedef struct amdk_ensemble amdk_ensemble;
+int amdk_ensemble_create(amdk_ctx **ctx, int n, amdk_ensemble **out);
+int amdk_ensemble_iteration(amdk_ensemble *ens, const int *istep, double gcut, amdk_energies *e, double *gemax,
+                            int *converged);
+int amdk_ensemble_last_ms(amdk_ensemble *ens, double *ms);
+int amdk_ensemble_destroy(amdk_ensemble *ens);
 
 #ifdef __cplusplus
 }

@@ -5,7 +5,12 @@ that stays usable after each of them.
 - a band of zeros makes the overlap singular: ortho_gs's Cholesky meets a
   zero pivot (UINV STOPs there, wfn_initialize.f90:514-528) -> NOT_SPD;
 - a NaN coefficient reaches the total energy -> NONFINITE;
-- a CG step number below 1 -> BADARG."""
+- a CG step number below 1 -> BADARG;
+- the int8 tensor-core kernels' pipeline waits made to give up at once (a
+  test-only limit, amdk_options.reserved[0]; the waits that drain a block's
+  own copies and MMAs keep their full limit) -> TIMEOUT, NaN in the Gram
+  product, C0 left as it was, and the context goes on with the FP64
+  products."""
 import numpy as np
 import pytest
 
@@ -63,4 +68,22 @@ def test_step_below_one_is_badarg():
     e.ortho()
     with pytest.raises(AmdkError, match=r"\(-1\)"):
         e.scf_iteration(0, 1e-6)
+    _usable(e, c)
+
+
+def test_slice_pipeline_wait_expiry_is_timeout():
+    """64 bands (16 waters): the orthonormalisation's Gram and rotation run
+    on the int8 slice kernels, whose pipeline waits give up at once here."""
+    s = configs.cluster(16, 18.0, 916, ecut=20.0)
+    e = Engine(s, MIXED, wait_limit=-1)
+    g = e.gvectors()
+    c = start_coefficients(g["hg"][: e.ngpw], 2 * np.pi / s.alat, e.nstate)
+    e.set_wfn(c)
+    with pytest.raises(AmdkError, match=r"\(-6\)"):
+        e.ortho()
+    # the Gram product wrote NaN; the call stopped before rotating C0
+    assert np.isnan(e.get("overlap")).any()
+    assert np.array_equal(e.get_wfn(), c)
+    # the same context with FP64 products (no slice kernel) runs normally
+    e.set_precision(FP64)
     _usable(e, c)
