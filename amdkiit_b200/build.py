@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libamdk.so")
 SOURCES = ["capi.cu", "setup.cpp"]
-HEADERS = ["amdk_internal.h", "fft.cuh", "kernels.cuh", "pencil.cuh", "slicegemm.cuh", os.path.join("..", "..", "include", "amdk.h")]
+HEADERS = ["amdk_internal.h", "fft.cuh", "kernels.cuh", "pencil.cuh", "slicegemm.cuh", "dgemm.cuh", os.path.join("..", "..", "include", "amdk.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -61,7 +61,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         subprocess.check_call(cmd)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    cmd = [_nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcublas", "-lcusolver"]
+    cmd = [_nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcusolver"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)

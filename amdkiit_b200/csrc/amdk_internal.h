@@ -1,6 +1,5 @@
 // Internal declarations of libamdk (host setup, device context, kernels).
 #pragma once
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>

@@ -1,5 +1,4 @@
 // libamdk: device context and the extern "C" entry points of include/amdk.h.
-#include <cublas_v2.h>
 #include <cusolverDn.h>
 #include <cuda_runtime.h>
 
@@ -21,6 +20,7 @@
 #include "kernels.cuh"
 #include "pencil.cuh"
 #include "slicegemm.cuh"
+#include "dgemm.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -35,15 +35,6 @@ void set_error(const std::string &m) { g_err = m; }
     if (e_ != cudaSuccess) {                                                                      \
       set_error(std::string("CUDA: ") + cudaGetErrorString(e_) + " at " + __FILE__ + ":" +        \
                 std::to_string(__LINE__));                                                        \
-      return AMDK_ERR_CUDA;                                                                       \
-    }                                                                                             \
-  } while (0)
-#define CB(x)                                                                                     \
-  do {                                                                                            \
-    cublasStatus_t s_ = (x);                                                                      \
-    if (s_ != CUBLAS_STATUS_SUCCESS) {                                                            \
-      set_error(std::string("cuBLAS status ") + std::to_string((int)s_) + " at " + __FILE__ +    \
-                ":" + std::to_string(__LINE__));                                                  \
       return AMDK_ERR_CUDA;                                                                       \
     }                                                                                             \
   } while (0)
@@ -62,9 +53,15 @@ template <typename T> static int dalloc(T **p, size_t n) {
   }
   return 0;
 }
+// setup upload; a pageable-source cudaMemcpy may return before its DMA has
+// landed, and the context's streams do not wait for the legacy stream, so the
+// copy is waited for here
 template <typename T> static int upload(T **p, const std::vector<T> &v) {
   RC(dalloc(p, v.size()));
-  if (!v.empty()) CK(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  if (!v.empty()) {
+    CK(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    CK(cudaStreamSynchronize(0));
+  }
   return 0;
 }
 
@@ -83,7 +80,6 @@ struct amdk_ctx {
   HostSetup hs;
   int device = 0, precision = AMDK_FP64, batch = 4;
   cudaStream_t st = nullptr;
-  cublasHandle_t cb = nullptr;
   // cuSOLVER for the Cholesky/inverse of overlaps too large for one SM
   cusolverDnHandle_t cs = nullptr;
   double *d_potrf_ws = nullptr;
@@ -107,8 +103,11 @@ struct amdk_ctx {
   // side stream for the work that needs only C0 (projections, E_kin, C2
   // clearing), overlapped with the density and the potential
   cudaStream_t st2 = nullptr;
-  cublasHandle_t cb2 = nullptr;
   double *d_part2 = nullptr;
+  // FP64 tensor-core GEMMs: split-K partial tiles (one buffer per stream)
+  // and the poll limit of their pipeline waits (options.reserved[1])
+  double *d_dgpart = nullptr, *d_dgpart2 = nullptr;
+  long dg_plim = SG_SPIN;
   cudaEvent_t ev_fork = nullptr, ev_side_done = nullptr;
   size_t fftbuf_bytes = 0;
   // tables
@@ -157,6 +156,8 @@ struct amdk_ctx {
   double *d_sgA = nullptr, *d_sgB = nullptr, *d_sgS = nullptr;  // their row (column) scales
   double *d_sgpart = nullptr;
   unsigned long long *d_sgmax = nullptr;  // per-band max |x| of the slicing pass
+  unsigned long long *d_c2max = nullptr;  // per-band max |x| of C2, recorded by the H|psi> unpack
+  bool c2max_ok = false;                  // d_c2max belongs to the current C2
   double *d_sgnsq = nullptr;               // per-band sums of squares (by segment) of the slicing pass
   int *d_sgerr = nullptr;
   long sg_kpad = 0;
@@ -172,7 +173,6 @@ struct amdk_ctx {
   CUtensorMap tm_a_tn, tm_b_tn, tm_a_nn, tm_s_nn;
   bool warm[2] = {false, false};  // an eager iteration has run at this pair precision
   void *c0_first = nullptr;       // the buffer that held C0 at creation
-  void *cb_ws = nullptr;          // cuBLAS workspace (fixed, for capture)
   // BOMD predictor: converged C0 of earlier steps, most recent first
   static constexpr int MAX_PRED = 8;
   double2 *d_hist[MAX_PRED] = {};
@@ -434,9 +434,10 @@ static int grid_to_rays(amdk_ctx *c, int T, const double2 *cgrid, const double *
 
 // ------------------------------------------------------------------ pencil path
 // shared memory of a pencil block: slab plane, column tile of ct columns,
-// the twiddle tables (2n) and the kz -> slab index table
+// the twiddle tables (2n, from a 16-byte boundary) and the packed slab-plane
+// table (16 bytes for each of at most 16 j2)
 template <typename C> static size_t pencil_smem(int n, int nz, int ct) {
-  return ((size_t)(nz + ct) * (n + 1) + 2 * n) * sizeof(C) + n * sizeof(int);
+  return (((size_t)(nz + ct) * (n + 1) * sizeof(C) + 15) & ~(size_t)15) + 2 * (size_t)n * sizeof(C) + 16 * 16;
 }
 // widest column tile with the block within `budget` bytes (0: none fits)
 template <typename C> static int pencil_tile(int n, int nz, size_t extra, size_t budget) {
@@ -459,7 +460,7 @@ static void density_tiles(int n, int nz, size_t csize, size_t lim, int *ct, int 
   for (size_t budget : {lim / 2, lim})
     for (int tiles : {1, 2, 4}) {
       const int w = (n + tiles - 1) / tiles;
-      const size_t smem = ((size_t)(nz + w) * (n + 1) + 2 * n) * csize + n * sizeof(int);
+      const size_t smem = (((size_t)(nz + w) * (n + 1) * csize + 15) & ~(size_t)15) + 2 * (size_t)n * csize + 16 * 16;
       const int reps = (w * n1f + PNT - 1) / PNT;
       const int slots = tiles * reps;
       const bool stage_ok = (size_t)n * (n + 1) * (csize / 2) <= (size_t)(nz + w) * (n + 1) * csize;
@@ -875,6 +876,7 @@ static int do_potential(amdk_ctx *c) {
   return potential_t<double2>(c);
 }
 
+static bool use_slice(const amdk_ctx *c);
 // The unpack of pairs [p0, p0+T) (kinetic term, occupation scaling) fused
 // with fnonloc for the first UNPACK_NPJ projectors; further projectors are
 // added in chunks (k_fnonloc_add).  pp/pm: +G/-G positions in the ray buffer.
@@ -885,12 +887,17 @@ template <typename C> static void unpack_h(amdk_ctx *c, int p0, int T, const int
   const double scale = 1.0 / ((double)g.n1 * g.n2 * g.n3);
   const int npj0 = std::min(c->nproj, UNPACK_NPJ);
   const int nb = std::min(2 * T, c->nstate - 2 * p0);
+  // per-band maxima of C2 for its slicing (int8 products of the mixed path)
+  unsigned long long *bmax = use_slice(c) ? c->d_c2max + 2 * p0 : nullptr;
+  if (bmax && p0 == 0) cudaMemsetAsync(c->d_c2max, 0, sizeof(unsigned long long) * SG_M, c->st);
   ++c->nlaunch;
   constexpr int PAIRS = unpack_pairs<C>();
   const dim3 gu(nblk(h.ngpw, 128), (T + PAIRS - 1) / PAIRS);
   k_unpack_fnonloc<C><<<gu, 128, (size_t)2 * PAIRS * npj0 * sizeof(Rl), c->st>>>(
       h.ngpw, c->nstate, 2 * p0, T, npj0, pp, pm, (const C *)c->d_rb, rstride(c, 0), scale, c->d_hg, h.tpiba2,
-      c->d_occ, c->d_P, c->d_D, c->nproj, c->d_c0, c->d_c2);
+      c->d_occ, c->d_P, c->d_D, c->nproj, c->d_c0, c->d_c2, c->nproj > npj0 ? nullptr : bmax);
+  // with projector chunks still to add, C2 is sliced from scratch
+  c->c2max_ok = bmax != nullptr && c->nproj <= npj0;
   for (int j0 = npj0; j0 < c->nproj; j0 += UNPACK_NPJ) {
     const int npj = std::min(UNPACK_NPJ, c->nproj - j0);
     smem_opt_in<k_fnonloc_add<UNPACK_NPJ>>();
@@ -941,8 +948,8 @@ template <typename C> static int apply_h_t(amdk_ctx *c) {
 // Mixed path with at most 128 bands: Lambda, S, C2 -= C0 Lambda and C0 U^{-1}
 // on the int8 tensor cores (slicegemm.cuh) instead of DGEMM/DTRMM.
 static bool use_slice(const amdk_ctx *c) { return c->sg_ready && c->slice_gemm && c->precision == AMDK_MIXED; }
-// 2D map of S digit planes (kdim bytes per row, S*128 rows): box box_x x 128
-static int sg_encode(CUtensorMap *m, void *base, long kdim, int box_x, CUtensorMapSwizzle sw) {
+// the driver's tensor-map encoder (nullptr, with the error set, if absent)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
   if (!enc) {
     void *fn = nullptr;
@@ -950,10 +957,16 @@ static int sg_encode(CUtensorMap *m, void *base, long kdim, int box_x, CUtensorM
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
         q != cudaDriverEntryPointSuccess || !fn) {
       set_error("cuTensorMapEncodeTiled not available");
-      return AMDK_ERR_CUDA;
+      return nullptr;
     }
     enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
   }
+  return enc;
+}
+// 2D map of S digit planes (kdim bytes per row, S*128 rows): box box_x x 128
+static int sg_encode(CUtensorMap *m, void *base, long kdim, int box_x, CUtensorMapSwizzle sw) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return AMDK_ERR_CUDA;
   cuuint64_t dims[2] = {(cuuint64_t)kdim, (cuuint64_t)SG_S * SG_M};
   cuuint64_t strides[1] = {(cuuint64_t)kdim};
   cuuint32_t box[2] = {(cuuint32_t)box_x, (cuuint32_t)SG_M};
@@ -987,6 +1000,7 @@ static int sg_setup(amdk_ctx *c) {
   RC(c->alloc(&c->d_sgS, SG_M));
   RC(c->alloc(&c->d_sgpart, (size_t)c->sg_chunks * SG_M * SG_M));
   RC(c->alloc(&c->d_sgmax, SG_M));
+  RC(c->alloc(&c->d_c2max, SG_M));
   RC(c->alloc(&c->d_sgnsq, (size_t)SG_M * SG_SEG));
   c->d_sgerr = c->d_info + 1;
   RC(sg_encode(&c->tm_a_tn, c->d_plA, c->sg_kpad, SG_TN_KT, CU_TENSOR_MAP_SWIZZLE_64B));
@@ -1067,21 +1081,82 @@ static void sg_nn(amdk_ctx *c, const double *B, double2 *out, int sub, bool digi
   }
 }
 
+// ------------------------------------------------- FP64 tensor-core GEMMs
+// 2D map of a column-major FP64 matrix, dim0 x dim1 (dim0 contiguous, the
+// leading dimension), box box0 x box1
+static int dg_encode(CUtensorMap *m, const void *base, long dim0, long dim1, int box0, int box1, CUtensorMapSwizzle sw) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return AMDK_ERR_CUDA;
+  cuuint64_t dims[2] = {(cuuint64_t)dim0, (cuuint64_t)dim1};
+  cuuint64_t strides[1] = {(cuuint64_t)dim0 * sizeof(double)};
+  cuuint32_t box[2] = {(cuuint32_t)box0, (cuuint32_t)box1};
+  cuuint32_t es[2] = {1, 1};
+  if (enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void *>(base), dims, strides, box, es,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled (FP64) failed");
+    return AMDK_ERR_CUDA;
+  }
+  return 0;
+}
+// split-K partial tiles a TN product of m x n needs at most (buffer size)
+static size_t dg_part_doubles(const amdk_ctx *c, int m, int n) {
+  const size_t ntile = (size_t)((m + DG_T - 1) / DG_T) * ((n + DG_T - 1) / DG_T);
+  return (2 * (size_t)c->nsm + ntile) * DG_T * DG_T;
+}
+// out (m x n, leading dimension ldo) = alpha A^T B over the real index
+// K = 2 ngpw; A (K x m) and B (K x n) are the real views of complex band or
+// projector arrays.  sym: B = A, only the upper tiles are formed and the
+// result is mirrored.
+static int dg_tn(amdk_ctx *c, const void *A, int m, const void *B, int n, double alpha, double *out, int ldo,
+                 bool sym = false) {
+  const long K = 2L * c->hs.ngpw;
+  CUtensorMap ta, tb;
+  RC(dg_encode(&ta, A, K, m, DG_KT, DG_T, CU_TENSOR_MAP_SWIZZLE_128B));
+  if (sym)
+    tb = ta;
+  else
+    RC(dg_encode(&tb, B, K, n, DG_KT, DG_T, CU_TENSOR_MAP_SWIZZLE_128B));
+  const int mt = (m + DG_T - 1) / DG_T, nt = (n + DG_T - 1) / DG_T;
+  const int ntile = sym ? mt * (mt + 1) / 2 : mt * nt;
+  const int ktiles = (int)((K + DG_KT - 1) / DG_KT);
+  int nsplit = std::max(1, std::min(ktiles, (2 * c->nsm + ntile - 1) / ntile));
+  const int per = (ktiles + nsplit - 1) / nsplit;
+  nsplit = (ktiles + per - 1) / per;
+  c->nlaunch += 2;
+  k_dgemm_tn<<<dim3(ntile, nsplit), DG_THREADS, DG_TN_SMEM, c->st>>>(ta, tb, mt, sym ? 1 : 0, ktiles, per, c->d_dgpart,
+                                                                     c->d_info + 1, c->dg_plim);
+  k_dgemm_tn_sum<<<(int)std::min<long>((long)ntile * (DG_T * DG_T / 32), 8L * c->nsm), 256, 0, c->st>>>(
+      c->d_dgpart, nsplit, ntile, mt, sym ? 1 : 0, m, n, alpha, out, ldo);
+  CK(cudaGetLastError());
+  return 0;
+}
+// out (K x n, the real view of a complex band array) = alpha A G + beta out,
+// A the real view of n1 bands, G n1 x n (leading dimension n1); upper: G is
+// upper triangular (its lower part is not read)
+static int dg_nn(amdk_ctx *c, const void *A, int n1, const double *G, int n, double alpha, double beta, bool upper,
+                 void *out) {
+  const long K = 2L * c->hs.ngpw;
+  CUtensorMap ta;
+  RC(dg_encode(&ta, A, K, n1, 16, DG_NN_BS, CU_TENSOR_MAP_SWIZZLE_NONE));
+  const long items = ((K + DG_NN_R - 1) / DG_NN_R) * ((n + DG_NN_J - 1) / DG_NN_J);
+  ++c->nlaunch;
+  k_dgemm_nn<<<(int)std::min<long>(items, c->nsm), DG_NN_THREADS, DG_NN_SMEM, c->st>>>(
+      ta, G, n1, K, n1, n, alpha, beta, upper ? 1 : 0, (double *)out, K, c->d_info + 1, c->dg_plim);
+  CK(cudaGetLastError());
+  return 0;
+}
+
 // On the mixed path with the projector planes and C0's current planes: the
 // int8 tensor-core slice product (nl = 2 P^T C0, FP32-level accuracy);
-// otherwise DGEMM.
+// otherwise the FP64 tensor-core product.
 static int do_fnl(amdk_ctx *c) {
-  const HostSetup &h = c->hs;
   if (c->nproj == 0) return 0;
   if (use_slice(c) && c->sg_proj && c0_planes_current(c)) {
     sg_tn(c, c->tm_p_tn, c->tm_a_tn, 0, c->d_sgP, c->d_sgA, 2.0, c->d_nl, c->nproj, c->nproj);
     return 0;
   }
-  const double two = 2.0, zero = 0.0;
-  int n = c->nstate, K = 2 * h.ngpw;
-  CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, c->nproj, n, K, &two, (const double *)c->d_P, K,
-                 (const double *)c->d_c0, K, &zero, c->d_nl, c->nproj));
-  return 0;
+  return dg_tn(c, c->d_P, c->nproj, c->d_c0, c->nstate, 2.0, c->d_nl, c->nproj);
 }
 
 // energies from the device scalar slots (copied to the host)
@@ -1156,27 +1231,33 @@ static void gmax_precon(amdk_ctx *c) {
 
 static int do_gradient(amdk_ctx *c) {
   const HostSetup &h = c->hs;
-  int n = c->nstate, K = 2 * h.ngpw;
-  const double two = 2.0, one = 1.0, mone = -1.0, zero = 0.0;
+  const int n = c->nstate;
   const bool sl = use_slice(c);
   if (sl) {
-    sg_slice(c, c->d_c2, c->d_plB, c->d_sgB);
+    if (c->c2max_ok) {
+      // the unpack recorded C2's band maxima: only the digit pass
+      const long K = 2L * c->hs.ngpw;
+      ++c->nlaunch;
+      k_slice_rows<SG_S><<<dim3(SG_SEG, SG_M), 256, 0, c->st>>>((const double *)c->d_c2, K, K, c->nstate, c->d_c2max,
+                                                                c->d_plB, c->sg_kpad, c->d_sgB);
+    } else {
+      sg_slice(c, c->d_c2, c->d_plB, c->d_sgB);
+    }
     // C0's planes are those the last orthonormalisation wrote, if C0 has not changed since
     if (c->sg_c0_buf != (void *)c->d_c0) sg_slice(c, c->d_c0, c->d_plA, c->d_sgA);
     sg_tn(c, c->tm_b_tn, c->tm_a_tn, 0, c->d_sgB, c->d_sgA, 2.0, c->d_gam);
   } else {
-    CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, (const double *)c->d_c2, K,
-                   (const double *)c->d_c0, K, &zero, c->d_gam, n));
+    RC(dg_tn(c, c->d_c2, n, c->d_c0, n, 2.0, c->d_gam, n));
   }
   ++c->nlaunch;
   k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c2, c->d_c0, c->d_gam, c->d_occ, 1, 0);
   if (sl)
     sg_nn(c, c->d_gam, c->d_c2, 1, false);
   else
-    CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &mone, (const double *)c->d_c0, K, c->d_gam, n, &one,
-                   (double *)c->d_c2, K));
+    RC(dg_nn(c, c->d_c0, n, c->d_gam, n, -1.0, 1.0, false, c->d_c2));
   ++c->nlaunch;
   k_zclean<<<nblk(n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c2);
+  c->c2max_ok = false;  // C2 is the projected gradient now
   gmax_precon(c);
   CK(cudaGetLastError());
   return 0;
@@ -1208,7 +1289,7 @@ static int check_ortho(amdk_ctx *c) {
   // an expired wait comes first: its NaN results reach the overlap, whose
   // Cholesky then fails too; the recorded code is cleared once reported
   if (c->h_info[1]) {
-    set_error("tensor-core slice GEMM: a pipeline wait expired (code " + std::to_string(c->h_info[1]) + ")");
+    set_error("tensor-core GEMM: a pipeline wait expired (code " + std::to_string(c->h_info[1]) + ")");
     c->h_info[1] = 0;
     CK(cudaMemset(c->d_info + 1, 0, sizeof(int)));
     return AMDK_ERR_TIMEOUT;
@@ -1222,16 +1303,14 @@ static int check_ortho(amdk_ctx *c) {
 }
 static int do_ortho(amdk_ctx *c, bool check = true, bool swap = true) {
   const HostSetup &h = c->hs;
-  int n = c->nstate, K = 2 * h.ngpw;
-  const double two = 2.0, zero = 0.0, one = 1.0;
+  const int n = c->nstate;
   // S = 2 Re C0^T C0 - Re c0(0) Re c0(0)^T  (DSYRK + DGER, wfn_initialize.f90:481-482)
   const bool sl = use_slice(c);
   if (sl) {
     sg_slice(c, c->d_c0, c->d_plA, c->d_sgA);
     sg_tn(c, c->tm_a_tn, c->tm_a_tn, 1, c->d_sgA, c->d_sgA, 2.0, c->d_gam);
   } else {
-    CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, (const double *)c->d_c0, K,
-                   (const double *)c->d_c0, K, &zero, c->d_gam, n));
+    RC(dg_tn(c, c->d_c0, n, c->d_c0, n, 2.0, c->d_gam, n, true));
   }
   ++c->nlaunch;
   k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c0, c->d_c0, c->d_gam, c->d_occ, 0, 1);
@@ -1262,8 +1341,7 @@ static int do_ortho(amdk_ctx *c, bool check = true, bool swap = true) {
   if (sl)
     sg_nn(c, c->d_uinv, c->d_cp, 0, true);
   else
-    CB(cublasDtrmm(c->cb, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, K, n, &one,
-                   c->d_uinv, n, (const double *)c->d_c0, K, (double *)c->d_cp, K));
+    RC(dg_nn(c, c->d_c0, n, c->d_uinv, n, 1.0, 0.0, true, c->d_cp));
   ++c->nlaunch;
   k_zclean<<<nblk(n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_cp);
   if (swap) std::swap(c->d_c0, c->d_cp);
@@ -1332,14 +1410,12 @@ static int do_ionic_forces(amdk_ctx *c) {
                                                  c->d_rhog, c->d_erhos, c->d_vps, c->d_rhos, omtp, c->d_part);
   if (c->nproj) {
     // dfnl = 2 tpiba Q^T C0: the int8 slice product on the mixed path (C0's
-    // planes current), DGEMM otherwise
-    const double tfac = 2.0 * h.tpiba, zero = 0.0;
+    // planes current), the FP64 tensor-core product otherwise
+    const double tfac = 2.0 * h.tpiba;
     if (use_slice(c) && c->sg_dproj && c0_planes_current(c)) {
       sg_tn(c, c->tm_q_tn, c->tm_a_tn, 0, c->d_sgQ, c->d_sgA, tfac, c->d_dfnl, 3 * c->nproj, 3 * c->nproj);
     } else {
-      int K = 2 * h.ngpw;
-      CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, 3 * c->nproj, c->nstate, K, &tfac, (const double *)c->d_Q, K,
-                     (const double *)c->d_c0, K, &zero, c->d_dfnl, 3 * c->nproj));
+      RC(dg_tn(c, c->d_Q, 3 * c->nproj, c->d_c0, c->nstate, tfac, c->d_dfnl, 3 * c->nproj));
     }
   }
   ++c->nlaunch;
@@ -1456,18 +1532,6 @@ static int build_device(amdk_ctx *c) {
   CK(cudaMemset(c->d_c0, 0, cw * sizeof(double2)));
   c->c0_first = c->d_c0;
   {
-    // fixed cuBLAS workspace so that captured GEMMs allocate nothing
-    const size_t ws = 32u << 20;
-    char *w;
-    RC(c->alloc(&w, ws));
-    c->cb_ws = w;
-    char *w2;
-    RC(c->alloc(&w2, ws));
-    if (cublasSetWorkspace(c->cb, c->cb_ws, ws) != CUBLAS_STATUS_SUCCESS ||
-        cublasSetWorkspace(c->cb2, w2, ws) != CUBLAS_STATUS_SUCCESS) {
-      set_error("cublasSetWorkspace failed");
-      return AMDK_ERR_CUDA;
-    }
     RC(c->alloc(&c->d_part2, (size_t)RED_BLOCKS * 4));
     const char *env = getenv("AMDK_NO_GRAPHS");
     c->use_graphs = !(env && env[0] == '1');
@@ -1540,7 +1604,7 @@ static int build_device(amdk_ctx *c) {
   {
     bool known = false;
     with_n(n1, [&](auto NC) { known = decltype(NC)::value > 0; });
-    const bool ok = (n1 == n2 && n2 == n3) && known;
+    const bool ok = (n1 == n2 && n2 == n3) && known && g.nz[0] < 255;  // slab planes fit the packed table
     const size_t lim = 227 * 1024;
     const int nz0 = g.nz[0];
     const char *env = getenv("AMDK_NO_PENCIL");
@@ -1711,6 +1775,16 @@ static int build_device(amdk_ctx *c) {
     RC(c->up(&c->d_H, H));
     RC(sg_proj_setup(c));
   }
+  {
+    // FP64 tensor-core GEMM partials: the largest TN product is the overlap,
+    // nl (nproj rows) or dfnl (3 nproj rows) against the bands
+    const int rows = std::max(h.nstate, 3 * c->nproj);
+    const size_t np = dg_part_doubles(c, rows, h.nstate);
+    RC(c->alloc(&c->d_dgpart, np));
+    RC(c->alloc(&c->d_dgpart2, np));
+    CK(cudaFuncSetAttribute(k_dgemm_tn, cudaFuncAttributeMaxDynamicSharedMemorySize, DG_TN_SMEM));
+    CK(cudaFuncSetAttribute(k_dgemm_nn, cudaFuncAttributeMaxDynamicSharedMemorySize, DG_NN_SMEM));
+  }
   double es = 0.0;
   for (int is = 0; is < h.nsp; is++) es = es + (double)h.na[is] * h.zv[is] * h.zv[is] / RAGGIO;
   c->eself = es / std::sqrt(2.0 * (4.0 * std::atan(1.0)));
@@ -1720,21 +1794,20 @@ static int build_device(amdk_ctx *c) {
 
 // ------------------------------------------------------------------ C ABI
 // Launches inside its scope go to the side stream, with the side stream's
-// cuBLAS handle and reduction partials.
+// reduction and GEMM partials.
 struct OnSideStream {
   amdk_ctx *c;
   cudaStream_t s;
-  cublasHandle_t b;
-  double *p;
-  explicit OnSideStream(amdk_ctx *cc) : c(cc), s(cc->st), b(cc->cb), p(cc->d_part) {
+  double *p, *q;
+  explicit OnSideStream(amdk_ctx *cc) : c(cc), s(cc->st), p(cc->d_part), q(cc->d_dgpart) {
     c->st = c->st2;
-    c->cb = c->cb2;
     c->d_part = c->d_part2;
+    c->d_dgpart = c->d_dgpart2;
   }
   ~OnSideStream() {
     c->st = s;
-    c->cb = b;
     c->d_part = p;
+    c->d_dgpart = q;
   }
 };
 
@@ -1934,6 +2007,7 @@ int amdk_create(const amdk_system *sys, const amdk_options *opt, amdk_ctx **out)
     c->precision = opt->precision;
     c->batch = opt->pair_batch;
     if (opt->reserved[0] != 0) c->sg_plim = std::max(opt->reserved[0], 0);
+    if (opt->reserved[1] != 0) c->dg_plim = std::max(opt->reserved[1], 0);
   }
   int rc = host_setup(sys, c->hs);
   if (rc) {
@@ -1946,19 +2020,17 @@ int amdk_create(const amdk_system *sys, const amdk_options *opt, amdk_ctx **out)
     delete c;
     return AMDK_ERR_CUDA;
   }
-  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
-      cublasCreate(&c->cb) != CUBLAS_STATUS_SUCCESS || cublasSetStream(c->cb, c->st) != CUBLAS_STATUS_SUCCESS) {
-    set_error("stream / cuBLAS handle creation failed");
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error("stream creation failed");
     amdk_destroy(c);
     return AMDK_ERR_CUDA;
   }
   cudaEventCreate(&c->ev0);
   cudaEventCreate(&c->ev1);
   if (cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess ||
-      cublasCreate(&c->cb2) != CUBLAS_STATUS_SUCCESS || cublasSetStream(c->cb2, c->st2) != CUBLAS_STATUS_SUCCESS ||
       cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_side_done, cudaEventDisableTiming) != cudaSuccess) {
-    set_error("side stream / cuBLAS handle creation failed");
+    set_error("side stream creation failed");
     amdk_destroy(c);
     return AMDK_ERR_CUDA;
   }
@@ -1989,8 +2061,6 @@ int amdk_destroy(amdk_ctx *c) {
     cudaEventDestroy(e.first);
     cudaEventDestroy(e.second);
   }
-  if (c->cb) cublasDestroy(c->cb);
-  if (c->cb2) cublasDestroy(c->cb2);
   if (c->st2) {
     cudaStreamSynchronize(c->st2);
     cudaStreamDestroy(c->st2);
@@ -2070,7 +2140,10 @@ int amdk_set_positions(amdk_ctx *c, const double *atco) {
 int amdk_set_wfn(amdk_ctx *c, const double *c0) {
   if (!c || !c0) return AMDK_ERR_BADARG;
   cudaSetDevice(c->device);
-  CK(cudaMemcpy(c->d_c0, c0, sizeof(double2) * (size_t)c->hs.ngpw * c->nstate, cudaMemcpyHostToDevice));
+  // on the context stream (after any kernel still reading or writing C0, e.g.
+  // the rotation of an ortho that returned), and complete before returning
+  CK(cudaMemcpyAsync(c->d_c0, c0, sizeof(double2) * (size_t)c->hs.ngpw * c->nstate, cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
   c->sg_c0_buf = nullptr;
   return 0;
 }
@@ -2300,18 +2373,15 @@ int amdk_wfn_extrapolate(amdk_ctx *c) {
   else
     amdk::aspc_coefficients(np, w);
   if (np > 1) {
-    const int n = c->nstate, K = 2 * h.ngpw;
-    const double two = 2.0, one = 1.0, zero = 0.0;
+    const int n = c->nstate;
     for (int j = 1; j < np; ++j) {
       const double2 *hj = c->d_hist[j - 1];
       // M = 2 Re C_j^T C0 - Re c_j(0) Re c0(0)^T aligns step j's occupied
       // subspace with the current one; cp (+)= w_j C_j M
-      CB(cublasDgemm(c->cb, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, (const double *)hj, K, (const double *)c->d_c0, K,
-                     &zero, c->d_gam, n));
+      RC(dg_tn(c, hj, n, c->d_c0, n, 2.0, c->d_gam, n));
       ++c->nlaunch;
       k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, hj, c->d_c0, c->d_gam, c->d_occ, 0, 0);
-      CB(cublasDgemm(c->cb, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &w[j], (const double *)hj, K, c->d_gam, n,
-                     j == 1 ? &zero : &one, (double *)c->d_cp, K));
+      RC(dg_nn(c, hj, n, c->d_gam, n, w[j], j == 1 ? 0.0 : 1.0, false, c->d_cp));
     }
     ++c->nlaunch;
     k_axpy_c<<<RED_BLOCKS * 4, NTHR, 0, c->st>>>((long)cw, w[0], c->d_c0, c->d_cp);

@@ -267,15 +267,32 @@ template <typename C, int N> __device__ __forceinline__ void load_tw(C *tw, cons
   }
 }
 // v[k] *= W_N^(SG j k), k = 1..R-1, from row j of twiddle table TAB (table 0
-// for R = N1, j = j2; table 1 for R = N2, j = k1)
-template <typename C, int N, int R, int SG, int TAB>
+// for R = N1, j = j2; table 1 for R = N2, j = k1).  VEC: the table starts on a
+// 16-byte boundary (the caller guarantees it), so FP32 rows of even length are
+// read two twiddles per load.
+template <typename C, int N, int R, int SG, int TAB, bool VEC = false>
 __device__ __forceinline__ void twiddle_tab(C (&v)[R], int j, const C *tw) {
   const C *row = tw + TAB * N + j * R;
+  if constexpr (VEC && sizeof(C) == 8 && R % 2 == 0 && N % 2 == 0) {
+    const float4 *r4 = reinterpret_cast<const float4 *>(row);
 #pragma unroll
-  for (int k = 1; k < R; ++k) {
-    C w = row[k];
-    if (SG > 0) w.y = -w.y;
-    v[k] = cmul(v[k], w);
+    for (int k2 = 0; k2 < R / 2; ++k2) {
+      const float4 q = r4[k2];
+      C wa, wb;
+      wa.x = q.x;
+      wa.y = SG > 0 ? -q.y : q.y;
+      wb.x = q.z;
+      wb.y = SG > 0 ? -q.w : q.w;
+      if (k2 > 0) v[2 * k2] = cmul(v[2 * k2], wa);
+      v[2 * k2 + 1] = cmul(v[2 * k2 + 1], wb);
+    }
+  } else {
+#pragma unroll
+    for (int k = 1; k < R; ++k) {
+      C w = row[k];
+      if (SG > 0) w.y = -w.y;
+      v[k] = cmul(v[k], w);
+    }
   }
 }
 

@@ -446,7 +446,10 @@ __global__ void k_xc_combine(int ngrho, int gga, const int *pos_p, const int *po
 // L2-resident; the chunk's rows of D in shared memory), then unpacks, so C2
 // is written once.  P holds P_j(0)/2 at G = 0 (the convention of fnl's real
 // dot products); the full value is used here.  The projector sums run in the
-// transform's precision (FP32 with packed FMAs on the mixed path).
+// transform's precision (FP32 with packed FMAs on the mixed path).  With bmax
+// (the int8 slice products of the mixed path) the kernel also records each
+// band's max |Re|, |Im| of C2 (atomic max of the FP64 bits, non-negative
+// values), which the slicing of C2 needs, so C2 is not read once more for it.
 constexpr int UNPACK_NPJ = 32;
 template <typename C> __host__ __device__ constexpr int unpack_pairs() { return sizeof(C) == sizeof(float2) ? 8 : 4; }
 template <typename C>
@@ -456,9 +459,11 @@ __global__ void __launch_bounds__(128) k_unpack_fnonloc(int ngpw, int nstate, in
                                                         const double *__restrict__ hg, double tpiba2,
                                                         const double *__restrict__ occ, const double2 *__restrict__ P,
                                                         const double *__restrict__ D, int nproj,
-                                                        const double2 *__restrict__ c0, double2 *__restrict__ c2) {
+                                                        const double2 *__restrict__ c0, double2 *__restrict__ c2,
+                                                        unsigned long long *__restrict__ bmax) {
   typedef decltype(C().x) Rl;
   constexpr int PAIRS = unpack_pairs<C>(), NB = 2 * PAIRS;
+  __shared__ double red[4][NB];  // per-warp band maxima (128 threads)
   extern __shared__ unsigned char smraw[];
   Rl *Ds = reinterpret_cast<Rl *>(smraw);  // [j][band - b0]
   const int t0 = blockIdx.y * PAIRS, t1 = min(T, t0 + PAIRS);
@@ -469,8 +474,9 @@ __global__ void __launch_bounds__(128) k_unpack_fnonloc(int ngpw, int nstate, in
     Ds[i] = b < nb ? (Rl)D[j + (long)nproj * (b0 + b)] : (Rl)0;
   }
   __syncthreads();
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= ngpw) return;
+  const int g0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = g0 < ngpw;
+  const int g = valid ? g0 : 0;  // lanes past the sphere follow along for the reductions
   C acc[NB];
 #pragma unroll
   for (int b = 0; b < NB; ++b) acc[b] = czero<C>();
@@ -485,6 +491,7 @@ __global__ void __launch_bounds__(128) k_unpack_fnonloc(int ngpw, int nstate, in
   }
   const int pp = pos_p[g], pm = pos_m[g];
   const double kin = tpiba2 * hg[g];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int tt = 0; tt < PAIRS; ++tt) {
     const int t = t0 + tt;
@@ -498,15 +505,37 @@ __global__ void __launch_bounds__(128) k_unpack_fnonloc(int ngpw, int nstate, in
     if (fi == 0.0) fi = 1.0;
     const double2 ca = c0[(long)ba * ngpw + g];
     const C na = acc[2 * tt];
-    c2[(long)ba * ngpw + g] =
-        make_double2(-fi * (kin * ca.x + fpx) + (double)na.x, -fi * (kin * ca.y + fmy) + (double)na.y);
+    const double2 xa = make_double2(-fi * (kin * ca.x + fpx) + (double)na.x, -fi * (kin * ca.y + fmy) + (double)na.y);
+    if (valid) c2[(long)ba * ngpw + g] = xa;
+    double ma = valid ? fmax(fabs(xa.x), fabs(xa.y)) : 0.0, mb = 0.0;
     if (bb < nstate) {
       const C nbv = acc[2 * tt + 1];
       double fb = occ[bb] * 0.5;
       if (fb == 0.0) fb = 1.0;
       const double2 cb = c0[(long)bb * ngpw + g];
-      c2[(long)bb * ngpw + g] =
+      const double2 xb =
           make_double2(-fb * (kin * cb.x + fpy) + (double)nbv.x, -fb * (kin * cb.y - fmx) + (double)nbv.y);
+      if (valid) c2[(long)bb * ngpw + g] = xb;
+      mb = valid ? fmax(fabs(xb.x), fabs(xb.y)) : 0.0;
+    }
+    if (bmax) {
+      for (int o = 16; o > 0; o >>= 1) {
+        ma = fmax(ma, __shfl_xor_sync(0xffffffffu, ma, o));
+        mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+      }
+      if (lane == 0) {
+        red[warp][2 * tt] = ma;
+        red[warp][2 * tt + 1] = mb;
+      }
+    }
+  }
+  if (bmax) {
+    __syncthreads();
+    if (threadIdx.x < nb) {
+      double m = 0.0;
+#pragma unroll
+      for (int w = 0; w < 4; ++w) m = fmax(m, red[w][threadIdx.x]);
+      atomicMax(bmax + b0 - band0 + threadIdx.x, (unsigned long long)__double_as_longlong(m));
     }
   }
 }
@@ -963,7 +992,6 @@ __global__ void k_nl_energy_d(int nproj, int nstate, const double *H, const doub
 // F(3,na_max,nsp) zeroed first as in the reference; esr -> out[0].
 __global__ void k_esr(int nsp, const int *na, int na_max, const int *zv, const double *atco, double alat, int sym,
                       int tfor, double *F, double *out) {
-  __shared__ double sh[32];
   const double pi = 4.0 * atan(1.0);
   const double rckj = sqrt(1.2 * 1.2 + 1.2 * 1.2);
   double esr = 0;
@@ -1015,7 +1043,6 @@ __global__ void k_esr(int nsp, const int *na, int na_max, const int *zv, const d
       }
     out[0] = esr;
   }
-  (void)sh;
 }
 
 // POTFOR (nuclear_grad.f90:4-50): per atom and block partial sums of

@@ -171,7 +171,7 @@ __device__ __forceinline__ void rows_nat_to_perm(C *P, int nrow, const DivMod &d
 #pragma unroll
     for (int j1 = 0; j1 < N1; ++j1) v[j1] = row[j2 + N2 * j1];
     Dft<C, N1, SG>::run(v);
-    twiddle_tab<C, N, N1, SG, 0>(v, j2, tw);
+    twiddle_tab<C, N, N1, SG, 0, true>(v, j2, tw);
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) row[k1 * N2 + j2] = v[k1];
   }
@@ -200,7 +200,7 @@ __device__ __forceinline__ void rows_perm_to_nat(C *P, int nrow, const DivMod &d
 #pragma unroll
     for (int k2 = 0; k2 < N2; ++k2) u[k2] = row[k2];
     Dft<C, N2, SG>::run(u);
-    twiddle_tab<C, N, N2, SG, 1>(u, k1, tw);
+    twiddle_tab<C, N, N2, SG, 1, true>(u, k1, tw);
 #pragma unroll
     for (int n2 = 0; n2 < N2; ++n2) row[n2] = u[n2];
   }
@@ -228,40 +228,65 @@ __device__ __forceinline__ void pencil_scatter(C *P, const C *__restrict__ rt_pl
   __syncthreads();
 }
 
+// slab plane of kz = j2 + N2*j1 from the packed table zp (one 16-byte entry
+// per j2, byte j1; 0xFF where the slab has no plane)
+__device__ __forceinline__ int zp_plane(const uint4 &e, int j1) {
+  const unsigned w = (j1 < 4) ? e.x : (j1 < 8) ? e.y : (j1 < 12) ? e.z : e.w;
+  const int b = (int)((w >> (8 * (j1 & 3))) & 0xFFu);
+  return b == 0xFF ? -1 : b;
+}
 // Backward z transform of the column tile q0 .. q0+ct-1 of P, first phase:
 // thread (column, j2) takes the slab planes at kz = j2 + N2*j1 (zero where
 // the slab has no plane) and leaves W_N^(j2 k1) DFT_N1 in S[col][k1*N2 + j2].
 template <typename C, int N>
-__device__ __forceinline__ void zcols_phase_a(const C *P, C *S, const int *zinv, int q0, int ct, const DivMod &dq,
+__device__ __forceinline__ void zcols_phase_a(const C *P, C *S, const uint4 *zp, int q0, int ct, const DivMod &dq,
                                               const C *tw) {
   constexpr int N1 = fft_n1(N), N2 = N / N1, NP = N + 1;
   for (int idx = threadIdx.x; idx < ct * N2; idx += blockDim.x) {
     int j2, qq;
     dq(idx, j2, qq);
+    const uint4 e = zp[j2];
     C v[N1];
 #pragma unroll
     for (int j1 = 0; j1 < N1; ++j1) {
-      const int zi = zinv[j2 + N2 * j1];
+      const int zi = zp_plane(e, j1);
       v[j1] = (zi >= 0) ? P[zi * NP + q0 + qq] : czero<C>();
     }
     Dft<C, N1, 1>::run(v);
-    twiddle_tab<C, N, N1, 1, 0>(v, j2, tw);
+    twiddle_tab<C, N, N1, 1, 0, true>(v, j2, tw);
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) S[qq * NP + k1 * N2 + j2] = v[k1];
   }
 }
 
 // shared memory of a pencil block: P[nz][N+1], S[CTs][N+1], the twiddle
-// tables (2N) and the kz -> slab index table zinv[N]
+// tables (2N, from a 16-byte boundary) and the packed slab-plane table zp
+// (one 16-byte entry per j2 < N2: the slab plane of kz = j2 + N2*j1 in byte
+// j1, 0xFF for none; the slab has fewer than 255 planes)
 template <typename C, int N> struct PencilSmem {
   C *P, *S, *tw;
-  int *zinv;
+  uint4 *zp;
   __device__ __forceinline__ PencilSmem(unsigned char *raw, int nz, int CTs) {
     constexpr int NP = N + 1;
     P = reinterpret_cast<C *>(raw);
     S = P + nz * NP;
-    tw = S + CTs * NP;
-    zinv = reinterpret_cast<int *>(tw + 2 * N);
+    const size_t off = ((size_t)(nz + CTs) * NP * sizeof(C) + 15) & ~(size_t)15;
+    tw = reinterpret_cast<C *>(raw + off);
+    zp = reinterpret_cast<uint4 *>(tw + 2 * N);
+  }
+  // twiddles, and zp from the kz -> slab plane table zinv (global)
+  __device__ __forceinline__ void load(const Plan<C> &p, const int *zinv) {
+    constexpr int N1 = fft_n1(N), N2 = N / N1;
+    load_tw<C, N>(tw, p);
+    for (int j2 = threadIdx.x; j2 < N2; j2 += blockDim.x) {
+      unsigned w[4] = {~0u, ~0u, ~0u, ~0u};
+      for (int j1 = 0; j1 < N1; ++j1) {
+        const int zi = zinv[j2 + N2 * j1];
+        const unsigned b = zi >= 0 ? (unsigned)zi : 0xFFu;
+        w[j1 >> 2] = (w[j1 >> 2] & ~(0xFFu << (8 * (j1 & 3)))) | (b << (8 * (j1 & 3)));
+      }
+      zp[j2] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
   }
 };
 
@@ -281,9 +306,8 @@ __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C
   const int nz = pg.nz;
   PencilSmem<C, N> sm(smraw, nz, CTs);
   C *P = sm.P, *S = sm.S, *tw = sm.tw;
-  const int *zinv = sm.zinv;
-  load_tw<C, N>(tw, p);
-  for (int i = threadIdx.x; i < N; i += blockDim.x) sm.zinv[i] = pg.zinv[i];
+  const uint4 *zp = sm.zp;
+  sm.load(p, pg.zinv);
   const int kx = blockIdx.x, t = blockIdx.y;
   C *plane = rt + ((long)t * pg.n1 + kx) * pg.nray;
   pencil_scatter<C, N>(P, plane, pg);
@@ -303,7 +327,7 @@ __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C
 #pragma unroll
       for (int k2 = 0; k2 < N2; ++k2) v0[k2] = has0 ? vv[k2] : (Rl)0;
     }
-    zcols_phase_a<C, N>(P, S, zinv, q0, ct, dq, tw);
+    zcols_phase_a<C, N>(P, S, zp, q0, ct, dq, tw);
     __syncthreads();
     // DFT_N2 -> psi(kz = k1 + N1*k2), times V, then the first phase of the
     // forward z transform, in registers
@@ -327,7 +351,7 @@ __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C
 #pragma unroll
       for (int k2 = 0; k2 < N2; ++k2) u[k2] = cscale(u[k2], vv[k2]);
       Dft<C, N2, -1>::run(u);
-      twiddle_tab<C, N, N2, -1, 1>(u, k1, tw);
+      twiddle_tab<C, N, N2, -1, 1, true>(u, k1, tw);
 #pragma unroll
       for (int n2 = 0; n2 < N2; ++n2) row[n2] = u[n2];
     }
@@ -336,13 +360,14 @@ __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C
     for (int idx = threadIdx.x; idx < ct * N2; idx += blockDim.x) {
       int n2, qq;
       dq(idx, n2, qq);
+      const uint4 e = zp[n2];
       C w[N1];
 #pragma unroll
       for (int k1 = 0; k1 < N1; ++k1) w[k1] = S[qq * NP + k1 * N2 + n2];
       Dft<C, N1, -1>::run(w);
 #pragma unroll
       for (int n1 = 0; n1 < N1; ++n1) {
-        const int zi = zinv[n2 + N2 * n1];
+        const int zi = zp_plane(e, n1);
         if (zi >= 0) P[zi * NP + q0 + qq] = w[n1];
       }
     }
@@ -372,9 +397,8 @@ __global__ void __launch_bounds__(PNT, sizeof(C) == 8 ? 2 : 1) k_pencil_density(
   const int nz = pg.nz;
   PencilSmem<C, N> sm(smraw, nz, CTs);
   C *P = sm.P, *S = sm.S, *tw = sm.tw;
-  const int *zinv = sm.zinv;
-  load_tw<C, N>(tw, p);
-  for (int i = threadIdx.x; i < N; i += blockDim.x) sm.zinv[i] = pg.zinv[i];
+  const uint4 *zp = sm.zp;
+  sm.load(p, pg.zinv);
   const int kx = blockIdx.x, grp = blockIdx.y;
   const int t0 = grp * per_group, t1 = min(T, t0 + per_group);
   const int ntiles = (N + CTs - 1) / CTs;
@@ -421,7 +445,7 @@ __global__ void __launch_bounds__(PNT, sizeof(C) == 8 ? 2 : 1) k_pencil_density(
       const int q0 = ti * CTs, ct = min(CTs, N - q0);
       const DivMod dq(ct);
       if (rr == 0) {
-        zcols_phase_a<C, N>(P, S, zinv, q0, ct, dq, tw);
+        zcols_phase_a<C, N>(P, S, zp, q0, ct, dq, tw);
         __syncthreads();
       }
       const int idx = threadIdx.x + rr * PNT;

@@ -206,16 +206,17 @@ class Engine:
     """One system resident on one GPU."""
 
     def __init__(self, system: System, precision: int = FP64, pair_batch: int = 0, device: int = 0,
-                 wait_limit: int = 0):
-        """wait_limit != 0 (tests of the failure path only): the pipeline
-        waits of the tensor-core kernels give up after max(wait_limit, 0)
-        polls (amdk_options.reserved[0])."""
+                 wait_limit: int = 0, fp64_wait_limit: int = 0):
+        """wait_limit / fp64_wait_limit != 0 (tests of the failure path
+        only): the pipeline waits of the int8 / FP64 tensor-core kernels give
+        up after max(limit, 0) polls (amdk_options.reserved[0] / [1])."""
         self.lib = load_library()
         self.system = system
         s, self._keep = system_struct(system)
         opt = _Options()
         opt.device, opt.precision, opt.pair_batch = device, precision, pair_batch
         opt.reserved[0] = wait_limit
+        opt.reserved[1] = fp64_wait_limit
         h = C.c_void_p()
         _check(self.lib.amdk_create(C.byref(s), C.byref(opt), C.byref(h)), "amdk_create")
         self.h = h

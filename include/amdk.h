@@ -82,9 +82,11 @@ typedef struct {
   int device;             /* CUDA device ordinal */
   int precision;          /* AMDK_FP64 or AMDK_MIXED */
   int pair_batch;         /* band pairs per FFT batch (0: automatic) */
-  int reserved[8];        /* zero; reserved[0] != 0 (tests of the failure path only): the
-                             pipeline waits of the tensor-core kernels give up after
-                             max(reserved[0], 0) polls and the call returns AMDK_ERR_TIMEOUT */
+  int reserved[8];        /* zero; tests of the failure path only: reserved[0] != 0, the
+                             pipeline waits of the int8 tensor-core kernels (mixed path)
+                             give up after max(reserved[0], 0) polls; reserved[1] != 0, the
+                             same for the FP64 tensor-core kernels; the call then returns
+                             AMDK_ERR_TIMEOUT */
 } amdk_options;
 
 typedef struct {

@@ -10,7 +10,10 @@ that stays usable after each of them.
   test-only limit, amdk_options.reserved[0]; the waits that drain a block's
   own copies and MMAs keep their full limit) -> TIMEOUT, NaN in the Gram
   product, C0 left as it was, and the context goes on with the FP64
-  products."""
+  products;
+- the same for the FP64 tensor-core kernels (amdk_options.reserved[1]): the
+  density and potential computed afterwards in that context equal those of
+  a fresh context."""
 import numpy as np
 import pytest
 
@@ -87,3 +90,24 @@ def test_slice_pipeline_wait_expiry_is_timeout():
     # the same context with FP64 products (no slice kernel) runs normally
     e.set_precision(FP64)
     _usable(e, c)
+
+
+def test_fp64_pipeline_wait_expiry_is_timeout():
+    s = configs.small_water()
+    e = Engine(s, FP64, fp64_wait_limit=-1)
+    g = e.gvectors()
+    c = start_coefficients(g["hg"][: e.ngpw], 2 * np.pi / s.alat, e.nstate)
+    e.set_wfn(c)
+    with pytest.raises(AmdkError, match=r"\(-6\)"):
+        e.ortho()
+    assert np.isnan(e.get("overlap")).any()
+    assert np.array_equal(e.get_wfn(), c)
+    # kernels other than the products still run and give the same results
+    e.density()
+    e.potential()
+    ref = Engine(s, FP64)
+    ref.set_wfn(c)
+    ref.density()
+    ref.potential()
+    for name in ("rho", "v_pot"):
+        assert np.array_equal(e.get(name), ref.get(name)), name
