@@ -229,6 +229,27 @@ __global__ void __launch_bounds__(256) k_dgemm_tn_sum(const double *part, int ns
   }
 }
 
+// the MMAs of one band block for the column tiles c >= C0 of a warp; the two
+// steps one after the other, so that 16 independent MMAs separate the two
+// that update one accumulator
+template <int C0>
+__device__ __forceinline__ void dg_nn_cols(double (&acc)[2][2][4][2], const double2 (&a)[2][2], const double2 (&b)[4]) {
+#pragma unroll
+  for (int c = C0; c < 4; ++c)
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      dg_mma(acc[p][0][c], a[p][0].x, b[c].x);
+      dg_mma(acc[p][1][c], a[p][0].y, b[c].x);
+    }
+#pragma unroll
+  for (int c = C0; c < 4; ++c)
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      dg_mma(acc[p][0][c], a[p][1].x, b[c].y);
+      dg_mma(acc[p][1][c], a[p][1].y, b[c].y);
+    }
+}
+
 // out (K x n, leading dimension ldo) = alpha A G + beta out (beta 0: out is
 // only written).  ta maps A (K x n1, boxes of 16 rows x 64 bands); G is
 // n1 x n with leading dimension ldg.  Thread 0 also issues the copies: the
@@ -314,6 +335,7 @@ __global__ void __launch_bounds__(DG_NN_THREADS, 1) k_dgemm_nn(const __grid_cons
       if (jt != staged_jt || bc != staged_bc) {
         // the G chunk (bands 128 bc.., columns 128 jt..) as Gs[column][band]
         __syncthreads();
+#pragma unroll 16
         for (int e = threadIdx.x; e < DG_NN_J * DG_NN_B; e += DG_NN_THREADS) {
           const int jl = e / DG_NN_B, bl = e % DG_NN_B;
           const int b = bc * DG_NN_B + bl, j = jt * DG_NN_J + jl;
@@ -344,25 +366,16 @@ __global__ void __launch_bounds__(DG_NN_THREADS, 1) k_dgemm_nn(const __grid_cons
             for (int c = 0; c < 4; ++c)
               b[c] = *reinterpret_cast<const double2 *>(Gs + (8 * (wc + 4 * c) + g) * DG_NN_GLD + hf * DG_NN_BS +
                                                         8 * kb + 2 * t);
-            // the two steps one after the other: 16 independent MMAs between
-            // the two that update one accumulator
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-              if (upper && gkb > jt * (DG_NN_J / 8) + wc + 4 * c) continue;
-#pragma unroll
-              for (int p = 0; p < 2; ++p) {
-                dg_mma(acc[p][0][c], a[p][0].x, b[c].x);
-                dg_mma(acc[p][1][c], a[p][0].y, b[c].x);
-              }
-            }
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-              if (upper && gkb > jt * (DG_NN_J / 8) + wc + 4 * c) continue;
-#pragma unroll
-              for (int p = 0; p < 2; ++p) {
-                dg_mma(acc[p][0][c], a[p][1].x, b[c].y);
-                dg_mma(acc[p][1][c], a[p][1].y, b[c].y);
-              }
+            // with upper, column tile c takes this band block when its column
+            // block jt*16 + wc + 4c is not below it: the tiles c >= cmin
+            int cmin = 0;
+            if (upper) cmin = min(4, max(0, (gkb - jt * (DG_NN_J / 8) - wc + 3) / 4));
+            switch (cmin) {
+              case 0: dg_nn_cols<0>(acc, a, b); break;
+              case 1: dg_nn_cols<1>(acc, a, b); break;
+              case 2: dg_nn_cols<2>(acc, a, b); break;
+              case 3: dg_nn_cols<3>(acc, a, b); break;
+              default: break;
             }
           }
         }
