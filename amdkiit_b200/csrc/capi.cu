@@ -1138,7 +1138,7 @@ static int dg_nn(amdk_ctx *c, const void *A, int n1, const double *G, int n, dou
                  void *out) {
   const long K = 2L * c->hs.ngpw;
   CUtensorMap ta;
-  RC(dg_encode(&ta, A, K, n1, 16, DG_NN_BS, CU_TENSOR_MAP_SWIZZLE_NONE));
+  RC(dg_encode(&ta, A, K, n1, 16, DG_NN_BS, CU_TENSOR_MAP_SWIZZLE_128B));
   const long items = ((K + DG_NN_R - 1) / DG_NN_R) * ((n + DG_NN_J - 1) / DG_NN_J);
   ++c->nlaunch;
   k_dgemm_nn<<<(int)std::min<long>(items, c->nsm), DG_NN_THREADS, DG_NN_SMEM, c->st>>>(

@@ -31,9 +31,11 @@
 // per thread at row lane/4, column lane%4; B (4 x 8, col) row lane%4, column
 // lane/4; C (8 x 8) two values at row lane/4, columns 2 (lane%4) + {0, 1}.
 // Each thread reads 16 bytes of shared memory at a time: in TN the two values
-// are consecutive k and serve two MMA steps (step s takes k = 8 kb + 2 t + s,
-// the same set for A and B); in NN they are consecutive rows of the long
-// index and serve two row tiles (rows 2 g and 2 g + 1).
+// are consecutive k and serve two MMA steps (step s of half kb takes
+// k = 4 t + 2 kb + s, the same set for A and B, so that the eight lanes of a
+// quarter warp read eight different 16-byte bank groups of the swizzled
+// rows); in NN they are consecutive rows of the long index and serve two row
+// tiles (rows 2 g and 2 g + 1), from 128-byte-swizzled boxes as well.
 //
 // Waits are bounded as in the integer-slice kernels: a pipeline wait gives up
 // after plim polls, sets *err and the shared abort flag; the block then runs
@@ -59,7 +61,8 @@ constexpr int DG_NN_R = 64;    // rows of the long index per work item
 constexpr int DG_NN_B = 128;   // bands per staged G chunk
 constexpr int DG_NN_BS = 64;   // bands per A stage
 constexpr int DG_NN_J = 128;   // output columns per work item
-constexpr int DG_NN_GLD = DG_NN_B + 2;  // padded row of the staged G chunk (doubles)
+constexpr int DG_NN_GLD = DG_NN_B + 8;  // padded row of the staged G chunk (doubles): rows
+                                        // g and g + 1 half a bank line apart
 constexpr int DG_NN_ST = 2;
 constexpr int DG_NN_THREADS = 256;  // 8 MMA warps (thread 0 also issues the copies)
 constexpr int DG_NN_BOX = 16 * DG_NN_BS * 8;   // one TMA box, 16 rows x 64 bands, 8 KB
@@ -152,9 +155,9 @@ __global__ void __launch_bounds__(DG_THREADS) k_dgemm_tn(const __grid_constant__
         for (int kb = 0; kb < 2; ++kb) {
           double2 a[4], b[4];
 #pragma unroll
-          for (int i = 0; i < 4; ++i) a[i] = dg_ld_sw(A, wr * 32 + i * 8 + g, kb * 4 + t);
+          for (int i = 0; i < 4; ++i) a[i] = dg_ld_sw(A, wr * 32 + i * 8 + g, 2 * t + kb);
 #pragma unroll
-          for (int j = 0; j < 4; ++j) b[j] = dg_ld_sw(B, wc * 32 + j * 8 + g, kb * 4 + t);
+          for (int j = 0; j < 4; ++j) b[j] = dg_ld_sw(B, wc * 32 + j * 8 + g, 2 * t + kb);
           // the two steps one after the other: 16 independent MMAs between
           // the two that update one accumulator
 #pragma unroll
@@ -252,7 +255,9 @@ __device__ __forceinline__ void dg_nn_cols(double (&acc)[2][2][4][2], const doub
 
 // out (K x n, leading dimension ldo) = alpha A G + beta out (beta 0: out is
 // only written).  ta maps A (K x n1, boxes of 16 rows x 64 bands); G is
-// n1 x n with leading dimension ldg.  Thread 0 also issues the copies: the
+// n1 x n with leading dimension ldg; the boxes are 128-byte swizzled (the
+// 16-byte chunk of rows 2g, 2g + 1 of band b sits at chunk g ^ (b & 7)).
+// Thread 0 also issues the copies: the
 // first two stages up front, then each next one as soon as every warp has
 // released the stage it goes to (so all eight warps multiply, and a thread
 // may use up to 255 registers).
@@ -360,8 +365,10 @@ __global__ void __launch_bounds__(DG_NN_THREADS, 1) k_dgemm_nn(const __grid_cons
 #pragma unroll
             for (int p = 0; p < 2; ++p)
 #pragma unroll
-              for (int s2 = 0; s2 < 2; ++s2)
-                a[p][s2] = *reinterpret_cast<const double2 *>(A + p * DG_NN_BOX + (8 * kb + 2 * t + s2) * 128 + g * 16);
+              for (int s2 = 0; s2 < 2; ++s2) {
+                const int band = 8 * kb + 2 * t + s2;
+                a[p][s2] = *reinterpret_cast<const double2 *>(A + p * DG_NN_BOX + band * 128 + ((g ^ (band & 7)) << 4));
+              }
 #pragma unroll
             for (int c = 0; c < 4; ++c)
               b[c] = *reinterpret_cast<const double2 *>(Gs + (8 * (wc + 4 * c) + g) * DG_NN_GLD + hf * DG_NN_BS +
