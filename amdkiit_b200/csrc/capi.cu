@@ -1120,11 +1120,13 @@ static int dg_tn(amdk_ctx *c, const void *A, int m, const void *B, int n, double
   const int mt = (m + DG_T - 1) / DG_T, nt = (n + DG_T - 1) / DG_T;
   const int ntile = sym ? mt * (mt + 1) / 2 : mt * nt;
   const int ktiles = (int)((K + DG_KT - 1) / DG_KT);
-  int nsplit = std::max(1, std::min(ktiles, (2 * c->nsm + ntile - 1) / ntile));
+  // enough blocks to fill the GPU twice, but at least 8 k tiles each (a short
+  // block costs its pipeline fill, and every split is a partial tile to add)
+  int nsplit = std::max(1, std::min((ktiles + 7) / 8, (2 * c->nsm + ntile - 1) / ntile));
   const int per = (ktiles + nsplit - 1) / nsplit;
   nsplit = (ktiles + per - 1) / per;
   c->nlaunch += 2;
-  k_dgemm_tn<<<dim3(ntile, nsplit), DG_THREADS, DG_TN_SMEM, c->st>>>(ta, tb, mt, sym ? 1 : 0, ktiles, per, c->d_dgpart,
+  k_dgemm_tn<<<dim3(ntile, nsplit), DG_THREADS, DG_TN_SMEM, c->st>>>(ta, tb, m, n, mt, sym ? 1 : 0, ktiles, per, c->d_dgpart,
                                                                      c->d_info + 1, c->dg_plim);
   k_dgemm_tn_sum<<<(int)std::min<long>((long)ntile * (DG_T * DG_T / 32), 8L * c->nsm), 256, 0, c->st>>>(
       c->d_dgpart, nsplit, ntile, mt, sym ? 1 : 0, m, n, alpha, out, ldo);

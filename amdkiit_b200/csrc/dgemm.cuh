@@ -21,9 +21,10 @@
 // NN (out = alpha A G + beta out; A is K x n1 column-major, G is n1 x n
 // column-major): persistent blocks over work items of 64 rows of the long
 // index x 128 output columns, eight warps each owning 32 rows x 32
-// columns; G is staged in shared memory in chunks of 128 x 128 (kept for the
-// whole kernel when it fits in one chunk), A arrives in TMA boxes of 16 rows x
-// 64 bands, four per stage, through a 2-stage pipeline.  With upper, G is
+// columns; per 64-band half chunk, A arrives in four TMA boxes of 16 rows x
+// 64 bands through a 2-stage pipeline and the 64 x 128 slice of G by cp.async
+// into one of two buffers (kept for the whole kernel when G is at most
+// 128 x 128).  With upper, G is
 // upper triangular (U^{-1}): band blocks below a column block are skipped and
 // the lower part of G is read as zero.
 //
@@ -61,13 +62,13 @@ constexpr int DG_NN_R = 64;    // rows of the long index per work item
 constexpr int DG_NN_B = 128;   // bands per staged G chunk
 constexpr int DG_NN_BS = 64;   // bands per A stage
 constexpr int DG_NN_J = 128;   // output columns per work item
-constexpr int DG_NN_GLD = DG_NN_B + 8;  // padded row of the staged G chunk (doubles): rows
-                                        // g and g + 1 half a bank line apart
+constexpr int DG_NN_GLD = DG_NN_BS + 8;  // padded row of a staged G slice (doubles): rows
+                                         // g and g + 1 half a bank line apart
 constexpr int DG_NN_ST = 2;
 constexpr int DG_NN_THREADS = 256;  // 8 MMA warps (thread 0 also issues the copies)
 constexpr int DG_NN_BOX = 16 * DG_NN_BS * 8;   // one TMA box, 16 rows x 64 bands, 8 KB
 constexpr int DG_NN_STAGE = 4 * DG_NN_BOX;     // 64 rows, 32 KB
-constexpr int DG_NN_SMEM = DG_NN_ST * DG_NN_STAGE + DG_NN_J * DG_NN_GLD * 8 + 1024 + 2 * DG_NN_ST * 8;
+constexpr int DG_NN_SMEM = DG_NN_ST * DG_NN_STAGE + 2 * DG_NN_J * DG_NN_GLD * 8 + 1024 + 2 * DG_NN_ST * 8;
 
 __device__ __forceinline__ void dg_mma(double (&d)[2], double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
@@ -101,8 +102,9 @@ __host__ __device__ inline void dg_tile(int tile, int mt, int sym, int &it, int 
 // partial tiles: part[(split * ntile + tile) * 4096 + i + 64 j] =
 // sum over the split's k tiles of A[k][64 it + i] B[k][64 jt + j]
 __global__ void __launch_bounds__(DG_THREADS) k_dgemm_tn(const __grid_constant__ CUtensorMap ta,
-                                                         const __grid_constant__ CUtensorMap tb, int mt, int sym,
-                                                         int ktiles, int per, double *part, int *err, long plim) {
+                                                         const __grid_constant__ CUtensorMap tb, int m, int n, int mt,
+                                                         int sym, int ktiles, int per, double *part, int *err,
+                                                         long plim) {
   extern __shared__ unsigned char dg_raw[];
   unsigned char *sm = dg_align1k(dg_raw);
   uint64_t *full = reinterpret_cast<uint64_t *>(sm + DG_ST * DG_TN_STAGE);
@@ -146,10 +148,12 @@ __global__ void __launch_bounds__(DG_THREADS) k_dgemm_tn(const __grid_constant__
     }
   } else {
     const int wr = warp & 1, wc = warp >> 1, g = lane >> 2, t = lane & 3;
+    // a 32 x 32 quarter entirely outside m x n (few bands or projectors) has nothing to form
+    const bool live = it * DG_T + wr * 32 < m && jt * DG_T + wc * 32 < n;
     for (int q = 0; q < nk; ++q) {
       const int s = q % DG_ST;
       if (!*ab && !sg_bar_wait(sg_smem(full + s), (q / DG_ST) & 1, err, 33, plim)) *ab = 1;
-      if (!*ab) {
+      if (!*ab && live) {
         const unsigned char *A = sm + s * DG_TN_STAGE, *B = A + DG_TN_STAGE / 2;
 #pragma unroll
         for (int kb = 0; kb < 2; ++kb) {
@@ -204,7 +208,14 @@ __global__ void __launch_bounds__(256) k_dgemm_tn_sum(const double *part, int ns
   for (long base = (long)blockIdx.x * 32; base < tot; base += (long)gridDim.x * 32) {
     const long e = base + lane;
     double s0 = 0.0, s1 = 0.0;
+    int i = m, j = n, it = 0, jt = 0;
     if (e < tot) {
+      const int tile = (int)(e / (DG_T * DG_T)), loc = (int)(e % (DG_T * DG_T));
+      dg_tile(tile, mt, sym, it, jt);
+      i = it * DG_T + loc % DG_T;
+      j = jt * DG_T + loc / DG_T;
+    }
+    if (i < m && j < n) {
       const double *p = part + e;
       int q = q0;
       for (; q + 1 < q1; q += 2) {
@@ -215,37 +226,31 @@ __global__ void __launch_bounds__(256) k_dgemm_tn_sum(const double *part, int ns
     }
     red[grp][lane] = s0 + s1;
     __syncthreads();
-    if (grp == 0 && e < tot) {
+    if (grp == 0 && i < m && j < n) {
       double v = red[0][lane];
 #pragma unroll
       for (int k = 1; k < 8; ++k) v += red[k][lane];
-      const int tile = (int)(e / (DG_T * DG_T)), loc = (int)(e % (DG_T * DG_T));
-      int it, jt;
-      dg_tile(tile, mt, sym, it, jt);
-      const int i = it * DG_T + loc % DG_T, j = jt * DG_T + loc / DG_T;
-      if (i < m && j < n) {
-        out[i + (long)ldo * j] = alpha * v;
-        if (sym && it != jt) out[j + (long)ldo * i] = alpha * v;
-      }
+      out[i + (long)ldo * j] = alpha * v;
+      if (sym && it != jt) out[j + (long)ldo * i] = alpha * v;
     }
     __syncthreads();
   }
 }
 
-// the MMAs of one band block for the column tiles c >= C0 of a warp; the two
-// steps one after the other, so that 16 independent MMAs separate the two
-// that update one accumulator
-template <int C0>
+// the MMAs of one band block for the column tiles C0 <= c < C1 of a warp; the
+// two steps one after the other, so that up to 16 independent MMAs separate
+// the two that update one accumulator
+template <int C0, int C1>
 __device__ __forceinline__ void dg_nn_cols(double (&acc)[2][2][4][2], const double2 (&a)[2][2], const double2 (&b)[4]) {
 #pragma unroll
-  for (int c = C0; c < 4; ++c)
+  for (int c = C0; c < C1; ++c)
 #pragma unroll
     for (int p = 0; p < 2; ++p) {
       dg_mma(acc[p][0][c], a[p][0].x, b[c].x);
       dg_mma(acc[p][1][c], a[p][0].y, b[c].x);
     }
 #pragma unroll
-  for (int c = C0; c < 4; ++c)
+  for (int c = C0; c < C1; ++c)
 #pragma unroll
     for (int p = 0; p < 2; ++p) {
       dg_mma(acc[p][0][c], a[p][1].x, b[c].y);
@@ -253,22 +258,30 @@ __device__ __forceinline__ void dg_nn_cols(double (&acc)[2][2][4][2], const doub
     }
 }
 
+__device__ __forceinline__ void dg_cp8(uint32_t dst, const double *src, int bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void dg_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void dg_cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // out (K x n, leading dimension ldo) = alpha A G + beta out (beta 0: out is
 // only written).  ta maps A (K x n1, boxes of 16 rows x 64 bands); G is
 // n1 x n with leading dimension ldg; the boxes are 128-byte swizzled (the
 // 16-byte chunk of rows 2g, 2g + 1 of band b sits at chunk g ^ (b & 7)).
-// Thread 0 also issues the copies: the
-// first two stages up front, then each next one as soon as every warp has
-// released the stage it goes to (so all eight warps multiply, and a thread
-// may use up to 255 registers).
+// The work of a block is a sequence of units (work item, 64-band half chunk);
+// the A half chunk of a unit comes by TMA (thread 0 issues each load as soon
+// as every warp has released the stage it goes to), the matching 64 x 128
+// slice of G by cp.async into one of two buffers, the next unit's slice
+// copied while this unit multiplies.  When G has at most 128 rows and columns
+// both of its halves stay in the two buffers for the whole kernel.
 __global__ void __launch_bounds__(DG_NN_THREADS, 1) k_dgemm_nn(const __grid_constant__ CUtensorMap ta, const double *G,
                                                                int ldg, long K, int n1, int n, double alpha,
                                                                double beta, int upper, double *out, long ldo, int *err,
                                                                long plim) {
   extern __shared__ unsigned char dg_raw[];
   unsigned char *sm = dg_align1k(dg_raw);
-  double *Gs = reinterpret_cast<double *>(sm + DG_NN_ST * DG_NN_STAGE);
-  uint64_t *full = reinterpret_cast<uint64_t *>(sm + DG_NN_ST * DG_NN_STAGE + DG_NN_J * DG_NN_GLD * 8);
+  double *Gb = reinterpret_cast<double *>(sm + DG_NN_ST * DG_NN_STAGE);  // [2][128 columns][DG_NN_GLD]
+  uint64_t *full = reinterpret_cast<uint64_t *>(sm + DG_NN_ST * DG_NN_STAGE + 2 * DG_NN_J * DG_NN_GLD * 8);
   uint64_t *empty = full + DG_NN_ST;
   __shared__ int aborted;
   volatile int *ab = &aborted;
@@ -276,30 +289,53 @@ __global__ void __launch_bounds__(DG_NN_THREADS, 1) k_dgemm_nn(const __grid_cons
   const int nrt = (int)((K + DG_NN_R - 1) / DG_NN_R), njt = (n + DG_NN_J - 1) / DG_NN_J;
   const int nbc = (n1 + DG_NN_B - 1) / DG_NN_B;
   const long items = (long)nrt * njt;
+  const bool resident = njt == 1 && nbc == 1;
   // G chunks of work item column tile jt (with upper only those at or above
-  // its column block), and the 64-band A stages of chunk bc
+  // its column block), and the 64-band halves of chunk bc
   auto chunks = [&](int jt) { return upper ? min(nbc, jt + 1) : nbc; };
   auto halves = [&](int bc) { return min(2, (n1 - bc * DG_NN_B + DG_NN_BS - 1) / DG_NN_BS); };
-  // copy cursor (thread 0): work item, chunk and half of the next stage load
-  long cw = blockIdx.x;
-  int cbc = 0, chf = 0, issued = 0;
+  // a cursor over the block's units
+  struct Cur {
+    long w;
+    int bc, hf;
+  };
+  auto next = [&](Cur &u) {
+    if (++u.hf >= halves(u.bc)) {
+      u.hf = 0;
+      if (++u.bc >= chunks((int)(u.w % njt))) {
+        u.bc = 0;
+        u.w += gridDim.x;
+      }
+    }
+  };
+  // G slice of unit u into buffer buf (zero outside n1 x n and, with upper,
+  // below the diagonal); only whole 8-blocks that the products read
+  auto stage_g = [&](const Cur &u, int buf) {
+    const int jt = (int)(u.w % njt), b0 = u.bc * DG_NN_B + u.hf * DG_NN_BS;
+    const int jv = min(DG_NN_J, (n - jt * DG_NN_J + 7) / 8 * 8), bv = min(DG_NN_BS, (n1 - b0 + 7) / 8 * 8);
+    double *dst = Gb + (size_t)buf * DG_NN_J * DG_NN_GLD;
+    for (int e = threadIdx.x; e < jv * bv; e += DG_NN_THREADS) {
+      const int jl = e / bv, bl = e % bv;
+      const int b = b0 + bl, j = jt * DG_NN_J + jl;
+      const bool on = b < n1 && j < n && !(upper && b > j);
+      dg_cp8(sg_smem(dst + jl * DG_NN_GLD + bl), on ? G + b + (long)ldg * j : G, on ? 8 : 0);
+    }
+    dg_cp_commit();
+  };
+  // copy cursor (thread 0): the unit of the next A load
+  Cur cp{(long)blockIdx.x, 0, 0};
+  int issued = 0;
   auto issue = [&]() {
     const int s = issued % DG_NN_ST;
     unsigned char *st = sm + s * DG_NN_STAGE;
-    const int rt = (int)(cw / njt);
+    const int rt = (int)(cp.w / njt);
     sg_bar_expect_tx(sg_smem(full + s), DG_NN_STAGE);
 #pragma unroll
     for (int b4 = 0; b4 < 4; ++b4)
-      sg_tma_2d(sg_smem(st + b4 * DG_NN_BOX), &ta, rt * DG_NN_R + 16 * b4, cbc * DG_NN_B + chf * DG_NN_BS,
+      sg_tma_2d(sg_smem(st + b4 * DG_NN_BOX), &ta, rt * DG_NN_R + 16 * b4, cp.bc * DG_NN_B + cp.hf * DG_NN_BS,
                 sg_smem(full + s));
     ++issued;
-    if (++chf >= halves(cbc)) {
-      chf = 0;
-      if (++cbc >= chunks((int)(cw % njt))) {
-        cbc = 0;
-        cw += gridDim.x;
-      }
-    }
+    next(cp);
   };
   if (threadIdx.x == 0) {
     aborted = 0;
@@ -308,13 +344,25 @@ __global__ void __launch_bounds__(DG_NN_THREADS, 1) k_dgemm_nn(const __grid_cons
       sg_bar_init(sg_smem(empty + s), DG_NN_THREADS / 32);
     }
     sg_bar_fence_init();
-    for (int k = 0; k < DG_NN_ST && cw < items; ++k) issue();
+    for (int k = 0; k < DG_NN_ST && cp.w < items; ++k) issue();
   }
-  __syncthreads();
+  // G for the first unit (resident: both halves, for good)
+  Cur gu{(long)blockIdx.x, 0, 0};
+  if (gu.w < items) {
+    if (resident) {
+      for (int h = 0; h < halves(0); ++h) stage_g(Cur{gu.w, 0, h}, h);
+    } else {
+      stage_g(gu, 0);
+    }
+  }
   const int wr = warp >> 2, wc = warp & 3, g = lane >> 2, t = lane & 3;
-  int q = 0, staged_jt = -1, staged_bc = -1;
+  int q = 0;
+  Cur gn = gu;  // the unit whose G slice is copied next (streaming)
+  if (!resident) next(gn);
   for (long w = blockIdx.x; w < items; w += gridDim.x) {
     const int rt = (int)(w / njt), jt = (int)(w % njt);
+    // column tiles of this warp with a column below n
+    const int clive = min(4, max(0, (n - jt * DG_NN_J - 8 * wc + 31) / 32));
     double acc[2][2][4][2];
 #pragma unroll
     for (int p = 0; p < 2; ++p)
@@ -337,28 +385,23 @@ __global__ void __launch_bounds__(DG_NN_THREADS, 1) k_dgemm_nn(const __grid_cons
                                                          : make_double2(0.0, 0.0);
         }
     for (int bc = 0; bc < chunks(jt); ++bc) {
-      if (jt != staged_jt || bc != staged_bc) {
-        // the G chunk (bands 128 bc.., columns 128 jt..) as Gs[column][band]
-        __syncthreads();
-#pragma unroll 16
-        for (int e = threadIdx.x; e < DG_NN_J * DG_NN_B; e += DG_NN_THREADS) {
-          const int jl = e / DG_NN_B, bl = e % DG_NN_B;
-          const int b = bc * DG_NN_B + bl, j = jt * DG_NN_J + jl;
-          double v = 0.0;
-          if (b < n1 && j < n && !(upper && b > j)) v = G[b + (long)ldg * j];
-          Gs[jl * DG_NN_GLD + bl] = v;
-        }
-        __syncthreads();
-        staged_jt = jt;
-        staged_bc = bc;
-      }
       for (int hf = 0; hf < halves(bc); ++hf, ++q) {
+        // this unit's G slice has landed (every thread's copies), and every
+        // warp is done with the previous unit, whose buffer the next copy reuses
+        dg_cp_wait_all();
+        __syncthreads();
+        if (!resident && gn.w < items) {
+          stage_g(gn, (q + 1) & 1);
+          next(gn);
+        }
+        const double *Gs = Gb + (size_t)(resident ? hf : (q & 1)) * DG_NN_J * DG_NN_GLD;
         const int s = q % DG_NN_ST;
         if (!*ab && !sg_bar_wait(sg_smem(full + s), (q / DG_NN_ST) & 1, err, 36, plim)) *ab = 1;
         if (!*ab) {
           const unsigned char *A = sm + s * DG_NN_STAGE + 2 * wr * DG_NN_BOX;
-#pragma unroll 1
-          for (int kb = 0; kb < DG_NN_BS / 8; ++kb) {
+          const int nkb = min(DG_NN_BS / 8, (n1 - bc * DG_NN_B - hf * DG_NN_BS + 7) / 8);
+#pragma unroll 2
+          for (int kb = 0; kb < nkb; ++kb) {
             // band block of 8 (global index) against the column blocks of this warp
             const int gkb = bc * (DG_NN_B / 8) + hf * (DG_NN_BS / 8) + kb;
             double2 a[2][2], b[4];
@@ -371,24 +414,30 @@ __global__ void __launch_bounds__(DG_NN_THREADS, 1) k_dgemm_nn(const __grid_cons
               }
 #pragma unroll
             for (int c = 0; c < 4; ++c)
-              b[c] = *reinterpret_cast<const double2 *>(Gs + (8 * (wc + 4 * c) + g) * DG_NN_GLD + hf * DG_NN_BS +
-                                                        8 * kb + 2 * t);
+              b[c] = *reinterpret_cast<const double2 *>(Gs + (8 * (wc + 4 * c) + g) * DG_NN_GLD + 8 * kb + 2 * t);
             // with upper, column tile c takes this band block when its column
-            // block jt*16 + wc + 4c is not below it: the tiles c >= cmin
+            // block jt*16 + wc + 4c is not below it: the tiles c >= cmin;
+            // and the tiles c >= clive hold no column below n
             int cmin = 0;
             if (upper) cmin = min(4, max(0, (gkb - jt * (DG_NN_J / 8) - wc + 3) / 4));
-            switch (cmin) {
-              case 0: dg_nn_cols<0>(acc, a, b); break;
-              case 1: dg_nn_cols<1>(acc, a, b); break;
-              case 2: dg_nn_cols<2>(acc, a, b); break;
-              case 3: dg_nn_cols<3>(acc, a, b); break;
-              default: break;
+            switch (cmin * 5 + clive) {
+              case 1: dg_nn_cols<0, 1>(acc, a, b); break;
+              case 2: dg_nn_cols<0, 2>(acc, a, b); break;
+              case 3: dg_nn_cols<0, 3>(acc, a, b); break;
+              case 4: dg_nn_cols<0, 4>(acc, a, b); break;
+              case 7: dg_nn_cols<1, 2>(acc, a, b); break;
+              case 8: dg_nn_cols<1, 3>(acc, a, b); break;
+              case 9: dg_nn_cols<1, 4>(acc, a, b); break;
+              case 13: dg_nn_cols<2, 3>(acc, a, b); break;
+              case 14: dg_nn_cols<2, 4>(acc, a, b); break;
+              case 19: dg_nn_cols<3, 4>(acc, a, b); break;
+              default: break;  // no tile of this warp takes the block
             }
           }
         }
         __syncwarp();
         if (lane == 0) sg_bar_arrive(sg_smem(empty + s));
-        if (threadIdx.x == 0 && cw < items && !*ab) {
+        if (threadIdx.x == 0 && cp.w < items && !*ab) {
           // the next load goes to this stage once every warp has released
           // it and this load has landed (no stage ever holds two copies)
           if (!sg_bar_wait(sg_smem(empty + s), (q / DG_NN_ST) & 1, err, 34, plim) ||
@@ -421,6 +470,7 @@ __global__ void __launch_bounds__(DG_NN_THREADS, 1) k_dgemm_nn(const __grid_cons
         }
     }
   }
+  dg_cp_wait_all();
   // no copy of this block may land after it exits
   if (threadIdx.x == 0)
     for (int p = max(0, issued - DG_NN_ST); p < issued; ++p)
