@@ -44,6 +44,9 @@ struct HostSetup {
   std::vector<double> wns[AMDK_MAXSP];            // projector tables on ggng (ngh*NSPLN)
   int nstate;
   std::vector<double> occ;
+  // open shell (LSD): bands [0, nel_up) spin 1, [nel_up, nstate) spin 2
+  bool lsd = false;
+  int nel_up = 0;
 };
 
 // Host setup entry: returns 0 or an AMDK_ERR code (message via set_error).

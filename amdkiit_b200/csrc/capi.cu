@@ -125,6 +125,9 @@ struct amdk_ctx {
   // electronic state
   int nstate = 0, npairs = 0;
   double *d_occ = nullptr, *d_wa = nullptr, *d_wb = nullptr;
+  // open shell (LSD): the spin-2 pair weights, density and potentials
+  double *d_wa2 = nullptr, *d_wb2 = nullptr, *d_rho2 = nullptr, *d_vpot2 = nullptr;
+  void *d_vt2 = nullptr;
   double2 *d_c0 = nullptr, *d_c2 = nullptr, *d_cp = nullptr, *d_hnm1 = nullptr;
   double *d_rho = nullptr, *d_vpot = nullptr;
   double2 *d_rhog = nullptr, *d_vg = nullptr, *d_vxg = nullptr, *d_fp = nullptr, *d_fm = nullptr, *d_cgrid = nullptr;
@@ -600,12 +603,22 @@ static std::string pencil_key(const amdk_ctx *c, const char *what, int T) {
          std::to_string(g.n2) + "x" + std::to_string(g.n3) + "/nz" + std::to_string(c->pg.nz) + "/T" + std::to_string(T);
 }
 
-template <typename C, int N> static void launch_pencil_vpsi(amdk_ctx *c, int T, int ct, C *rb) {
+// pairs [p0, p0 + T) of the ray buffer rb; open shell: each pair with its
+// spin's potential (the pair straddling the spins with both)
+template <typename C, int N> static void launch_pencil_vpsi(amdk_ctx *c, int T, int ct, C *rb, int p0 = 0) {
   typedef decltype(C().x) Rl;
-  smem_opt_in<k_pencil_vpsi<C, N>>();
+  const size_t sm = pencil_smem<C>(N, c->pg.nz, ct);
   ++c->nlaunch;
-  k_pencil_vpsi<C, N><<<dim3(c->geom.n1, T), PNT, pencil_smem<C>(N, c->pg.nz, ct), c->st>>>(
-      c->pg, plan<C>(c, 1), rb, (const Rl *)c->d_vt, ct);
+  if (c->hs.lsd) {
+    const int nu = c->hs.nel_up, psplit = (nu + 1) / 2, pstr = (nu & 1) ? nu / 2 : -1;
+    smem_opt_in<k_pencil_vpsi<C, N, true>>();
+    k_pencil_vpsi<C, N, true><<<dim3(c->geom.n1, T), PNT, sm, c->st>>>(
+        c->pg, plan<C>(c, 1), rb, (const Rl *)c->d_vt, ct, (const Rl *)c->d_vt2, p0, psplit, pstr);
+  } else {
+    smem_opt_in<k_pencil_vpsi<C, N>>();
+    k_pencil_vpsi<C, N><<<dim3(c->geom.n1, T), PNT, sm, c->st>>>(c->pg, plan<C>(c, 1), rb, (const Rl *)c->d_vt, ct,
+                                                                nullptr, 0, 0, -1);
+  }
 }
 // Column-tile width of the V(r)psi pencil kernel for T pairs: measured once
 // per shape (every width ceil(N/t), t = 1..6, whose block fits, launched on a
@@ -664,7 +677,7 @@ template <typename C, int N> static int vpsi_tile(amdk_ctx *c, int T) {
   c->vpsi_tuned[q] = T;
   return best;
 }
-template <typename C> static void pencil_vpsi(amdk_ctx *c, int T) {
+template <typename C> static void pencil_vpsi(amdk_ctx *c, int T, int p0 = 0) {
   const Geom &g = c->geom;
   typedef decltype(C().x) Rl;
   const double npt = (double)g.n1 * g.n2 * g.n3;
@@ -673,7 +686,7 @@ template <typename C> static void pencil_vpsi(amdk_ctx *c, int T) {
     if constexpr (N > 0) {
       const int ct = vpsi_tile<C, N>(c, T);
       prof_begin(c, KT_ZVPSI, 2.0 * T * rstride(c, 0) * sizeof(C) + npt * sizeof(Rl));
-      launch_pencil_vpsi<C, N>(c, T, ct, (C *)c->d_rb);
+      launch_pencil_vpsi<C, N>(c, T, ct, (C *)c->d_rb, p0);
       prof_end(c);
     }
   });
@@ -783,6 +796,25 @@ template <typename C> static int density_pairs_t(amdk_ctx *c) {
     ++c->nlaunch;
     k_rho_reduce_p<<<dim3((g.n1 + 31) / 32, (g.n1 + 31) / 32, g.n1), dim3(32, 8), 0, c->st>>>(
         g.n1, c->pn1, c->pn2, ng, c->d_rhopart, c->d_rho);
+    if (h.lsd) {
+      // open shell: the spin-2 density from the same pair transforms, weighted
+      // by the spin-2 bands only (density.f90:64-76); with all pairs in one
+      // batch the ray buffer still holds them
+      if (ng > ng_first)
+        CK(cudaMemsetAsync(c->d_rhopart + (size_t)ng_first * npt, 0, sizeof(double) * (ng - ng_first) * npt, c->st));
+      std::swap(c->d_wa, c->d_wa2);
+      std::swap(c->d_wb, c->d_wb2);
+      for (int p0 = 0; p0 < c->npairs; p0 += c->batch) {
+        int T = std::min(c->batch, c->npairs - p0);
+        if (c->batch < c->npairs) xt_bwd_pair<C>(c, p0, T);
+        pencil_density<C>(c, p0, T);
+      }
+      std::swap(c->d_wa, c->d_wa2);
+      std::swap(c->d_wb, c->d_wb2);
+      ++c->nlaunch;
+      k_rho_reduce_p<<<dim3((g.n1 + 31) / 32, (g.n1 + 31) / 32, g.n1), dim3(32, 8), 0, c->st>>>(
+          g.n1, c->pn1, c->pn2, ng, c->d_rhopart, c->d_rho2);
+    }
   } else {
   CK(cudaMemsetAsync(c->d_rho, 0, sizeof(double) * (size_t)g.n1 * g.n2 * g.n3, c->st));
   for (int p0 = 0; p0 < c->npairs; p0 += c->batch) {
@@ -823,6 +855,60 @@ static int do_density(amdk_ctx *c) {
   return density_t<double2>(c);
 }
 
+// V(r) (real part of a complex grid) into vpot and, on the pencil path, its
+// permuted copy vt for the V(r)psi kernel
+static int store_potential(amdk_ctx *c, const double2 *grid, double *vpot, void *vt) {
+  const Geom &g = c->geom;
+  const long npt = (long)g.n1 * g.n2 * g.n3;
+  CK(cudaMemcpy2DAsync(vpot, sizeof(double), grid, sizeof(double2), sizeof(double), npt, cudaMemcpyDeviceToDevice,
+                       c->st));
+  if (c->pencil_vpsi) {
+    dim3 gt((g.n1 + 31) / 32, (g.n1 + 31) / 32, g.n1);
+    ++c->nlaunch;
+    if (c->precision == AMDK_MIXED)
+      k_v_permute<float><<<gt, dim3(32, 8), 0, c->st>>>(g.n1, c->pn1, c->pn2, vpot, (float *)vt);
+    else
+      k_v_permute<double><<<gt, dim3(32, 8), 0, c->st>>>(g.n1, c->pn1, c->pn2, vpot, (double *)vt);
+  }
+  return 0;
+}
+
+// Open shell (LDA): both spins start from V_H + V_loc of the total density
+// (potential.f90:43); the polarized XC of rho_a = rho - rho2, rho_b = rho2
+// (xc.f90:135-246) gives v1a, v1b, and each spin's potential is band limited
+// through the density sphere as the closed-shell one (xc.f90:302-425).
+template <typename C> static int potential_lsd_t(amdk_ctx *c) {
+  const HostSetup &h = c->hs;
+  const Geom &g = c->geom;
+  const long npt = (long)g.n1 * g.n2 * g.n3;
+  double2 *g0 = c->d_cgrid, *g1 = c->d_cgrid + npt;
+  ++c->nlaunch;
+  if (sizeof(C) == sizeof(float2))
+    k_xc_lsd<float><<<RED_BLOCKS, NTHR, 0, c->st>>>(npt, c->d_rho, c->d_rho2, g0, g1, c->d_part, c->d_scal + S_EXC,
+                                                   c->d_ticket + TK_XC);
+  else
+    k_xc_lsd<double><<<RED_BLOCKS, NTHR, 0, c->st>>>(npt, c->d_rho, c->d_rho2, g0, g1, c->d_part,
+                                                    c->d_scal + S_EXC, c->d_ticket + TK_XC);
+  RC(grid_to_rays<C>(c, 2, c->d_cgrid, nullptr));
+  const double scale = 1.0 / (double)npt;
+  // both spins' G-space potentials first (the ray buffer holds both fields)
+  double2 *vx[2] = {c->d_vxg, c->d_fp + h.ngrho}, *vm[2] = {c->d_fm, c->d_fm + h.ngrho};
+  for (int sp = 0; sp < 2; ++sp) {
+    ++c->nlaunch;
+    k_xc_combine<C><<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, 0, c->d_posp, c->d_posm,
+                                                       (const C *)c->d_rbf + (size_t)sp * rstride(c, 1), rstride(c, 1),
+                                                       scale, c->d_gvec, h.tpiba, c->d_vg, vx[sp]);
+    ++c->nlaunch;
+    k_conj_field<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, vx[sp], vm[sp]);
+  }
+  for (int sp = 0; sp < 2; ++sp) {
+    RC(field_to_grid<C>(c, 1, vx[sp], vm[sp], c->d_cgrid));
+    RC(store_potential(c, c->d_cgrid, sp ? c->d_vpot2 : c->d_vpot, sp ? c->d_vt2 : c->d_vt));
+  }
+  CK(cudaGetLastError());
+  return 0;
+}
+
 // eval_pot + cal_vpot_ex; the density-sphere transforms run in the pair
 // transforms' precision (FP32 on the mixed path, which ends on FP64)
 template <typename C> static int potential_t(amdk_ctx *c) {
@@ -835,6 +921,7 @@ template <typename C> static int potential_t(amdk_ctx *c) {
                                            c->d_part, c->d_scal + S_EH, c->d_ticket + TK_VLOC);
   int gga = (h.xc == AMDK_XC_PBE);
   double2 *g0 = c->d_cgrid, *g1 = c->d_cgrid + npt;
+  if (h.lsd) return potential_lsd_t<C>(c);
   if (gga) {
     ++c->nlaunch;
     k_grad_fields<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_gvec, h.tpiba, c->d_rhog, c->d_fp, c->d_fm);
@@ -856,18 +943,9 @@ template <typename C> static int potential_t(amdk_ctx *c) {
   ++c->nlaunch;
   k_conj_field<<<nblk(h.ngrho), NTHR, 0, c->st>>>(h.ngrho, c->d_vxg, c->d_fm);
   RC(field_to_grid<C>(c, 1, c->d_vxg, c->d_fm, c->d_cgrid));
-  // V(r) = Re of the backward transform (xc.f90:299-301)
-  CK(cudaMemcpy2DAsync(c->d_vpot, sizeof(double), c->d_cgrid, sizeof(double2), sizeof(double), npt,
-                       cudaMemcpyDeviceToDevice, c->st));
-  if (c->pencil_vpsi) {
-    // V in the x-plane-major layout the pencil kernel reads
-    dim3 gt((g.n1 + 31) / 32, (g.n1 + 31) / 32, g.n1);
-    ++c->nlaunch;
-    if (c->precision == AMDK_MIXED)
-      k_v_permute<float><<<gt, dim3(32, 8), 0, c->st>>>(g.n1, c->pn1, c->pn2, c->d_vpot, (float *)c->d_vt);
-    else
-      k_v_permute<double><<<gt, dim3(32, 8), 0, c->st>>>(g.n1, c->pn1, c->pn2, c->d_vpot, (double *)c->d_vt);
-  }
+  // V(r) = Re of the backward transform (xc.f90:299-301), and V in the
+  // x-plane-major layout the pencil kernel reads
+  RC(store_potential(c, c->d_cgrid, c->d_vpot, c->d_vt));
   CK(cudaGetLastError());
   return 0;
 }
@@ -916,7 +994,7 @@ template <typename C> static int apply_h_t(amdk_ctx *c) {
     for (int p0 = 0; p0 < c->npairs; p0 += c->batch) {
       int T = std::min(c->batch, c->npairs - p0);
       xt_bwd_pair<C>(c, p0, T);
-      pencil_vpsi<C>(c, T);
+      pencil_vpsi<C>(c, T, p0);
       xt_fwd<C>(c, T);
       unpack_h<C>(c, p0, T, c->d_postp, c->d_postm);
     }
@@ -1231,6 +1309,15 @@ static void gmax_precon(amdk_ctx *c) {
                                                 c->d_scal + S_GMAX, c->d_ticket + TK_GRAD);
 }
 
+// open shell: zero the entries of an nstate x nstate band matrix that couple
+// the two spins (the reference forms the spin blocks separately)
+static void spin_mask(amdk_ctx *c, double *A) {
+  if (!c->hs.lsd) return;
+  const int n = c->nstate;
+  ++c->nlaunch;
+  k_spin_mask<<<nblk((long)n * n), NTHR, 0, c->st>>>(n, c->hs.nel_up, A);
+}
+
 static int do_gradient(amdk_ctx *c) {
   const HostSetup &h = c->hs;
   const int n = c->nstate;
@@ -1253,6 +1340,7 @@ static int do_gradient(amdk_ctx *c) {
   }
   ++c->nlaunch;
   k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c2, c->d_c0, c->d_gam, c->d_occ, 1, 0);
+  spin_mask(c, c->d_gam);
   if (sl)
     sg_nn(c, c->d_gam, c->d_c2, 1, false);
   else
@@ -1316,6 +1404,7 @@ static int do_ortho(amdk_ctx *c, bool check = true, bool swap = true) {
   }
   ++c->nlaunch;
   k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c0, c->d_c0, c->d_gam, c->d_occ, 0, 1);
+  spin_mask(c, c->d_gam);
   const int np = (n + CHOL_B - 1) / CHOL_B * CHOL_B;
   const size_t sm = ((size_t)np * (np + 1) + (size_t)CHOL_B * np) * sizeof(double);
   ++c->nlaunch;
@@ -1576,10 +1665,23 @@ static int build_device(amdk_ctx *c) {
     }
     RC(c->up(&c->d_wa, wa));
     RC(c->up(&c->d_wb, wb));
+    if (h.lsd) {
+      // the spin-2 bands' weights (bands nel_up.. are spin 2)
+      for (int p = 0; p < c->npairs; p++) {
+        if (2 * p < h.nel_up) wa[p] = 0.0;
+        if (2 * p + 1 < h.nel_up) wb[p] = 0.0;
+      }
+      RC(c->up(&c->d_wa2, wa));
+      RC(c->up(&c->d_wb2, wb));
+    }
   }
   long npt = (long)n1 * n2 * n3;
   RC(c->alloc(&c->d_rho, npt));
   RC(c->alloc(&c->d_vpot, npt));
+  if (h.lsd) {
+    RC(c->alloc(&c->d_rho2, npt));
+    RC(c->alloc(&c->d_vpot2, npt));
+  }
   RC(c->alloc(&c->d_cgrid, 2 * npt));
   RC(c->alloc(&c->d_rhog, h.ngrho));
   RC(c->alloc(&c->d_vg, h.ngrho));
@@ -1634,6 +1736,10 @@ static int build_device(amdk_ctx *c) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
   }
+  if (h.lsd && !(c->pv_p[0] && c->pd_p[0] && c->pv_p[1] && c->pd_p[1])) {
+    set_error("the open-shell branch needs the pencil transforms in both precisions (this grid has none)");
+    return AMDK_ERR_UNSUPPORTED;
+  }
   RC(sg_setup(c));
   const int q0 = (c->precision == AMDK_MIXED) ? 1 : 0;
   const bool pencil_all = c->pv_p[q0] && c->pd_p[q0];
@@ -1675,6 +1781,10 @@ static int build_device(amdk_ctx *c) {
       char *vt;
       RC(c->alloc(&vt, (size_t)npt * sizeof(double)));
       c->d_vt = vt;
+      if (h.lsd) {
+        RC(c->alloc(&vt, (size_t)npt * sizeof(double)));
+        c->d_vt2 = vt;
+      }
     }
   }
   // pseudopotential tables on the device
@@ -2383,6 +2493,7 @@ int amdk_wfn_extrapolate(amdk_ctx *c) {
       RC(dg_tn(c, hj, n, c->d_c0, n, 2.0, c->d_gam, n));
       ++c->nlaunch;
       k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, hj, c->d_c0, c->d_gam, c->d_occ, 0, 0);
+      spin_mask(c, c->d_gam);
       RC(dg_nn(c, hj, n, c->d_gam, n, w[j], j == 1 ? 0.0 : 1.0, false, c->d_cp));
     }
     ++c->nlaunch;
@@ -2444,6 +2555,8 @@ int amdk_get_array(amdk_ctx *c, const char *name, void *dst, size_t bytes) {
   std::string k(name);
   if (k == "rho") { src = c->d_rho; n = npt * sizeof(double); }
   else if (k == "v_pot") { src = c->d_vpot; n = npt * sizeof(double); }
+  else if (k == "rho2" && c->d_rho2) { src = c->d_rho2; n = npt * sizeof(double); }
+  else if (k == "v_pot2" && c->d_vpot2) { src = c->d_vpot2; n = npt * sizeof(double); }
   else if (k == "rho_g") { src = c->d_rhog; n = h.ngrho * sizeof(double2); }
   else if (k == "c2") { src = c->d_c2; n = (size_t)h.ngpw * c->nstate * sizeof(double2); }
   else if (k == "c0") { src = c->d_c0; n = (size_t)h.ngpw * c->nstate * sizeof(double2); }

@@ -406,6 +406,89 @@ __global__ void k_xc(long npt, int xc, const double *rho, double2 *g0, double2 *
   reduce_and_finish<1>(vv, part, out, ticket);
 }
 
+// Teter93 spin polarized (libxc XC_LDA_XC_TETER93 with two spin densities;
+// Goedecker, Teter and Hutter, Phys. Rev. B 54, 1703 (1996)): every Pade
+// coefficient c = c(unpolarized) + f(zeta) dc with
+// f(zeta) = ((1+zeta)^(4/3) + (1-zeta)^(4/3) - 2) / (2^(4/3) - 2);
+// e = rho eps, va / vb = d(rho eps) / d rho_a / rho_b.
+template <typename R> __device__ void xc_teter93_pol(R ra, R rb, R &e, R &va, R &vb) {
+  const R a0 = (R)0.4581652932831429, a1 = (R)2.217058676663745, a2 = (R)0.7405551735357053,
+          a3 = (R)0.01968227878617998;
+  const R b1 = (R)1.0, b2 = (R)4.504130959426697, b3 = (R)1.110667363742916, b4 = (R)0.02359291751427506;
+  const R da0 = (R)0.119086804055547, da1 = (R)0.6157402568883345, da2 = (R)0.1574201515892867,
+          da3 = (R)0.003532336663397157;
+  const R db1 = (R)0.0, db2 = (R)0.2673612973836267, db3 = (R)0.2052004607777787, db4 = (R)0.004200005045691381;
+  const R fp = (R)12.566370614359172954;  // 4 pi
+  const R rho = ra + rb;
+  R z = (ra - rb) / rho;
+  z = z > (R)1 ? (R)1 : (z < (R)-1 ? (R)-1 : z);
+  const R fden = cbrt((R)16) - (R)2;  // 2^(4/3) - 2
+  const R cp = cbrt((R)1 + z), cm = cbrt((R)1 - z);
+  const R f = (((R)1 + z) * cp + ((R)1 - z) * cm - (R)2) / fden;
+  const R dfz = (R)4 / (R)3 * (cp - cm) / fden;
+  const R A0 = a0 + f * da0, A1 = a1 + f * da1, A2 = a2 + f * da2, A3 = a3 + f * da3;
+  const R B1 = b1 + f * db1, B2 = b2 + f * db2, B3 = b3 + f * db3, B4 = b4 + f * db4;
+  const R rs = cbrt((R)3 / (fp * rho));
+  const R num = A0 + rs * (A1 + rs * (A2 + rs * A3));
+  const R den = rs * (B1 + rs * (B2 + rs * (B3 + rs * B4)));
+  const R dnum = A1 + rs * ((R)2 * A2 + rs * (R)3 * A3);
+  const R dden = B1 + rs * ((R)2 * B2 + rs * ((R)3 * B3 + rs * (R)4 * B4));
+  const R nf = da0 + rs * (da1 + rs * (da2 + rs * da3));
+  const R dfden = rs * (db1 + rs * (db2 + rs * (db3 + rs * db4)));
+  const R eps = -num / den;
+  const R deps_drs = -(dnum * den - num * dden) / (den * den);
+  const R deps_dz = -(nf * den - num * dfden) / (den * den) * dfz;
+  e = rho * eps;
+  va = eps - rs / (R)3 * deps_drs + deps_dz * ((R)1 - z);
+  vb = eps - rs / (R)3 * deps_drs - deps_dz * ((R)1 + z);
+}
+
+// Open-shell XC (xc.f90:135-246, LDA): rho_a = rho - rho2, rho_b = rho2 (the
+// reference subtracts the spin-2 density from the total, :46-50), the
+// polarized functional with the smoothing of the total (:196-236);
+// g0 = (v1a, 0), g1 = (v1b, 0); E_xc partial sums finished into out.
+template <typename R>
+__global__ void k_xc_lsd(long npt, const double *rho, const double *rho2, double2 *g0, double2 *g1, double *part,
+                         double *out, unsigned *ticket) {
+  const double gc = 1.0e-8;
+  double sm = 0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < npt; i += (long)gridDim.x * blockDim.x) {
+    const double ra = rho[i] - rho2[i], rb = rho2[i];
+    const double pa = ra > 0.0 ? ra : 0.0, pb = rb > 0.0 ? rb : 0.0;
+    R e = 0, va = 0, vb = 0;
+    if (pa + pb > 1e-30) xc_teter93_pol<R>((R)pa, (R)pb, e, va, vb);
+    const double rt = pa + pb;
+    double v1a = 0, v1b = 0;
+    if (rt > 0.1 * gc) {
+      double smoo, dsmoo;
+      if (rt > 4.0 * gc) { smoo = 1.0; dsmoo = 0.0; }
+      else {
+        double texp = exp(3.0 * (1.0 - rt / gc));
+        smoo = 1.0 / (1.0 + texp);
+        dsmoo = 3.0 / gc * texp * smoo * smoo;
+      }
+      sm += smoo * (double)e;
+      v1a = dsmoo * (double)e + smoo * (double)va;
+      v1b = dsmoo * (double)e + smoo * (double)vb;
+    }
+    g0[i] = make_double2(v1a, 0.0);
+    g1[i] = make_double2(v1b, 0.0);
+  }
+  const double vv[1] = {sm};
+  reduce_and_finish<1>(vv, part, out, ticket);
+}
+
+// Open shell: band-space matrices are block diagonal by spin (OVLAP_D and
+// ortho_gs take the spin-1 and spin-2 blocks separately,
+// wfn_initialize.f90:245-253,458-477): entries coupling the two spins are zeroed
+__global__ void k_spin_mask(int n, int nel_up, double *A) {
+  const long tot = (long)n * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < tot; e += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % n), j = (int)(e / n);
+    if ((i < nel_up) != (j < nel_up)) A[e] = 0.0;
+  }
+}
+
 // G-space assembly of the XC potential (xc.f90:257-297): from the forward
 // transforms of g0 (and g1 for GGA) in the ray buffer (t stride) build
 // vpotg = V_H+V_loc + v1(G) - i G.(v2 grad rho)(G)

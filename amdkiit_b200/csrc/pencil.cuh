@@ -297,9 +297,15 @@ template <typename C, int N> struct PencilSmem {
 // kz = k'/N2 + N1*(k'%N2), the order in which the z transform leaves psi.
 // The column tiles are CTs wide (the last may be narrower); the V values of a
 // thread's first task of a tile are loaded before the tile's first phase.
-template <typename C, int N>
+// LSD (open shell): pair gp0 + blockIdx.y takes the spin-2 potential vp2 from
+// pair psplit on, and the pair pstraddle (whose first band is the last of
+// spin 1) multiplies its real part by V_1 and its imaginary part by V_2
+// (wfn_initialize.f90:313-326).
+template <typename C, int N, bool LSD = false>
 __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C *__restrict__ rt,
-                                                     const decltype(C().x) *__restrict__ vp, int CTs) {
+                                                     const decltype(C().x) *__restrict__ vp, int CTs,
+                                                     const decltype(C().x) *__restrict__ vp2, int gp0, int psplit,
+                                                     int pstraddle) {
   typedef decltype(C().x) Rl;
   constexpr int N1 = fft_n1(N), N2 = N / N1, NP = N + 1;
   extern __shared__ unsigned char smraw[];
@@ -314,6 +320,17 @@ __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C
   const DivMod dz(nz);
   rows_nat_to_perm<C, N, 1>(P, nz, dz, tw);
   const Rl *V = vp + (long)kx * N * N;
+  const Rl *V2 = nullptr;
+  bool straddle = false;
+  if constexpr (LSD) {
+    const int gp = gp0 + t;
+    if (gp == pstraddle) {
+      straddle = true;
+      V2 = vp2 + (long)kx * N * N;
+    } else if (gp >= psplit) {
+      V = vp2 + (long)kx * N * N;
+    }
+  }
   for (int q0 = 0; q0 < N; q0 += CTs) {
     const int ct = min(CTs, N - q0);
     const DivMod dq(ct);
@@ -348,8 +365,17 @@ __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C
 #pragma unroll
       for (int j2 = 0; j2 < N2; ++j2) u[j2] = row[j2];
       Dft<C, N2, 1>::run(u);
+      if (LSD && straddle) {
+        const Rl *vg2 = V2 + (long)(q0 + qq) * N + k1 * N2;
 #pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) u[k2] = cscale(u[k2], vv[k2]);
+        for (int k2 = 0; k2 < N2; ++k2) {
+          u[k2].x = u[k2].x * vv[k2];
+          u[k2].y = u[k2].y * vg2[k2];
+        }
+      } else {
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) u[k2] = cscale(u[k2], vv[k2]);
+      }
       Dft<C, N2, -1>::run(u);
       twiddle_tab<C, N, N2, -1, 1, true>(u, k1, tw);
 #pragma unroll

@@ -582,20 +582,41 @@ int host_setup(const amdk_system *in, HostSetup &s, bool gvectors_only) {
       }
     }
   }
-  // ---- occupations (atomic_basis.f90:49-71, closed shell)
+  // ---- occupations (atomic_basis.f90:49-79): closed shell two electrons per
+  // orbital; open shell one orbital per valence electron, occupation 1
+  s.lsd = in->multiplicity > 0;
   int nst = in->nstate;
   if (nst <= 0) {
     nst = 0;
     for (int is = 0; is < s.nsp; is++) {
-      nst = nst + (int)((double)(s.na[is] * s.zv[is]) / 2.0);
-      if (2.0 * (double)nst < (double)(s.na[is] * s.zv[is])) {
-        nst++;
-        break;
+      if (s.lsd) {
+        nst = nst + s.na[is] * s.zv[is];
+      } else {
+        nst = nst + (int)((double)(s.na[is] * s.zv[is]) / 2.0);
+        if (2.0 * (double)nst < (double)(s.na[is] * s.zv[is])) {
+          nst++;
+          break;
+        }
       }
     }
   }
   s.nstate = nst;
-  s.occ.assign(nst, 2.0);
+  s.occ.assign(nst, s.lsd ? 1.0 : 2.0);
+  if (s.lsd) {
+    // NSPIN unpaired electrons; NEL_UP = INT((NSTATE-NSPIN)/2) bands of spin 1,
+    // NEL_DOWN = INT((NSTATE+NSPIN)/2) of spin 2 (init_module.f90:122-131)
+    const int nspin = in->multiplicity - 1;
+    const int up = (int)((double)(nst - nspin) / 2.0), down = (int)((double)(nst + nspin) / 2.0);
+    if (up + down != nst || up < 0 || down < 0) {
+      set_error("incorrect multiplicity for the number of bands");
+      return AMDK_ERR_BADARG;
+    }
+    if (in->xc != AMDK_XC_TETER93) {
+      set_error("the open-shell branch supports Teter93 only");
+      return AMDK_ERR_UNSUPPORTED;
+    }
+    s.nel_up = up;
+  }
   return 0;
 }
 

@@ -36,7 +36,7 @@ class _Species(C.Structure):
 class _System(C.Structure):
     _fields_ = [("a_cell", C.c_double * 9), ("alat", C.c_double), ("symmetry", C.c_int), ("ecut", C.c_double),
                 ("nsp", C.c_int), ("na", C.c_int * MAXSP), ("na_max", C.c_int), ("atco", C.POINTER(C.c_double)),
-                ("xc", C.c_int), ("nstate", C.c_int), ("sp", _Species * MAXSP)]
+                ("xc", C.c_int), ("nstate", C.c_int), ("sp", _Species * MAXSP), ("multiplicity", C.c_int)]
 
 
 class _Options(C.Structure):
@@ -132,6 +132,7 @@ def system_struct(system: System):
     s.atco = _dp(atco)
     s.xc = system.xc
     s.nstate = system.nstate
+    s.multiplicity = getattr(system, "multiplicity", 0)
     for i, sp in enumerate(system.species):
         o = s.sp[i]
         o.type, o.z, o.zv, o.mesh = sp.kind, sp.z, sp.zv, sp.mesh
@@ -299,6 +300,7 @@ class Engine:
         nproj = sum(n * 0 for n in self.system.na)
         shapes = {
             "rho": ((n3, n2, n1), np.float64), "v_pot": ((n3, n2, n1), np.float64),
+            "rho2": ((n3, n2, n1), np.float64), "v_pot2": ((n3, n2, n1), np.float64),
             "rho_g": ((self.ngrho,), np.complex128), "c2": ((self.nstate, self.ngpw), np.complex128),
             "c0": ((self.nstate, self.ngpw), np.complex128),
             "vps": ((nsp, self.ngrho), np.float64), "rhos": ((nsp, self.ngrho), np.float64),
@@ -338,12 +340,19 @@ class Engine:
         on the GPU; C2 = -f_i H|psi_i> with f_i = 2 (the pair unpack of
         wfn_initialize.f90:342-361 scales by f_i/2 and the pair transform
         doubles V psi), so H|psi_i> = -C2_i / 2.  The nstate x nstate
-        matrix is formed and diagonalised on the host.  Overwrites C2."""
+        matrix is formed and diagonalised on the host.  Open shell: f_i = 1,
+        and each spin's block separately (spin 1 first).  Overwrites C2."""
         self.density()
         self.potential()
         self.energy()
         self.apply_h()
-        return subspace_eigenvalues(self.get_wfn(), -0.5 * self.get("c2"))
+        c = self.get_wfn()
+        mult = getattr(self.system, "multiplicity", 0)
+        if mult > 0:
+            hc = -self.get("c2")
+            nu = (self.nstate - (mult - 1)) // 2
+            return np.concatenate([subspace_eigenvalues(c[:nu], hc[:nu]), subspace_eigenvalues(c[nu:], hc[nu:])])
+        return subspace_eigenvalues(c, -0.5 * self.get("c2"))
 
     def gradient(self) -> float:
         g = C.c_double()

@@ -86,6 +86,7 @@ class System:
     xc: int
     nstate: int = 0                  # 0: derived from the valence charge
     name: str = ""
+    multiplicity: int = 0            # 0: closed shell; m >= 1: open shell (LSD) of multiplicity m
 
     @property
     def na(self) -> List[int]:
@@ -109,7 +110,7 @@ class System:
     def with_positions(self, atco: np.ndarray) -> "System":
         pos = [np.array(atco[i, :n, :]) for i, n in enumerate(self.na)]
         return System(self.a_cell.copy(), self.alat, self.symmetry, self.ecut,
-                      self.species, pos, self.xc, self.nstate, self.name)
+                      self.species, pos, self.xc, self.nstate, self.name, self.multiplicity)
 
 
 # --------------------------------------------------------------------------
@@ -312,5 +313,9 @@ def load_reference_input(directory: str, yaml_name: str = "input.yaml") -> Syste
         xc = XC_PBE
     else:
         xc = XC_PZ
+    # INITIALIZATION: OPEN_SHELL (Fortran logical) and MULTIPLICITY (yamlread.f90:70-73)
+    init = cfg.get("INITIALIZATION") or {}
+    open_shell = str(init.get("OPEN_SHELL", ".FALSE.")).strip().upper() in (".TRUE.", "TRUE", "T", ".T.")
+    mult = int(init.get("MULTIPLICITY", 1)) if open_shell else 0
     return System(a_cell=a_cell, alat=dims[0], symmetry=_SYM_ID[sym], ecut=ecut, species=species,
-                  positions=pos, xc=xc, name=os.path.basename(os.path.normpath(directory)))
+                  positions=pos, xc=xc, name=os.path.basename(os.path.normpath(directory)), multiplicity=mult)

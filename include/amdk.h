@@ -76,6 +76,10 @@ typedef struct {
   int xc;                 /* AMDK_XC_* */
   int nstate;             /* 0: from the valence charge (atomic_basis.f90:49-71) */
   amdk_species sp[AMDK_MAXSP];
+  int multiplicity;       /* 0: closed shell; m >= 1: OPEN_SHELL with MULTIPLICITY m, the LSD
+                             branch (init_module.f90:122-160): one orbital per valence electron,
+                             occupation 1, bands 1..NEL_UP = INT((NSTATE-m+1)/2) of spin 1,
+                             the rest of spin 2; Teter93 only, pencil transforms only */
 } amdk_system;
 
 typedef struct {

@@ -169,6 +169,10 @@ struct orc_sys {
   /* electronic state */
   int nstate;
   double *occ;
+  /* open shell (LSD): bands 1..nel_up are spin 1, the rest spin 2 (init_module.f90:122-131);
+     rho = total density, rho2 = spin-2 density, v_pot / v_pot2 the potentials of spins 1 / 2 */
+  int lsd, nel_up;
+  double *rho2, *v_pot2;
   zc *c0, *c2, *hnm1, *c2p;
   double *rho, *v_pot;
   zc *rho_g;
@@ -1003,6 +1007,7 @@ void orc_eval_density(orc_sys *s) {
   long nnr1 = s->nnr1;
   int n = s->nstate, ngpw = s->ngpw;
   memset(s->rho, 0, sizeof(double) * nnr1);
+  if (s->lsd) memset(s->rho2, 0, sizeof(double) * nnr1);
   for (int id = 1; id <= n; id += 2) {
     int tfcal = 0;
     int ilast = id + 1 <= n ? id + 1 : n;
@@ -1028,11 +1033,15 @@ void orc_eval_density(orc_sys *s) {
     do_fft(s, -1, work);
     double coef3 = s->occ[is1 - 1] / s->omega;
     double coef4 = (is2 > n) ? 0.0 : s->occ[is2 - 1] / s->omega;
+    /* open shell: each band also adds to the spin-2 density when it is a
+       spin-2 band (density.f90:64-76; the total is rho1 + rho2, :94-98) */
+    const double w3 = (s->lsd && is1 > s->nel_up) ? 1.0 : 0.0, w4 = (s->lsd && is2 > s->nel_up) ? 1.0 : 0.0;
 #pragma omp parallel for schedule(static)
     for (long l = 0; l < nnr1; l++) {
       double r1 = creal(work[l]), r2 = cimag(work[l]);
       double tt = coef3 * r1 * r1 + coef4 * r2 * r2;
       s->rho[l] = s->rho[l] + tt;
+      if (s->lsd) s->rho2[l] = s->rho2[l] + (w3 * (coef3 * r1 * r1) + w4 * (coef4 * r2 * r2));
     }
   }
 }
@@ -1064,6 +1073,8 @@ void orc_eval_pot(orc_sys *s) {
   work[s->mapp[0] - 1] = vt[0];
   do_fft(s, -1, work);
   for (long l = 0; l < s->nnr1; l++) s->v_pot[l] = creal(work[l]);
+  /* open shell: both spins start from the same Hartree + local potential (potential.f90:43) */
+  if (s->lsd) memcpy(s->v_pot2, s->v_pot, sizeof(double) * s->nnr1);
   free(vt);
 }
 
@@ -1082,6 +1093,41 @@ static void lda_teter93(double rho, double *e, double *v) {
   double deps = -(dnum * den - num * dden) / (den * den);
   *e = rho * eps;
   *v = eps - rs / 3.0 * deps;
+}
+/* libxc XC_LDA_XC_TETER93 spin polarized (Goedecker, Teter and Hutter,
+   Phys. Rev. B 54, 1703 (1996)): the Pade form above with every coefficient
+   c = c(unpolarized) + f(zeta) dc, f(zeta) = ((1+zeta)^(4/3) + (1-zeta)^(4/3)
+   - 2) / (2^(4/3) - 2).  e = rho eps, va = d(rho eps)/d rho_a,
+   vb = d(rho eps)/d rho_b (d zeta/d rho_a = (1 - zeta)/rho, d zeta/d rho_b =
+   -(1 + zeta)/rho). */
+static void lda_teter93_pol(double ra, double rb, double *e, double *va, double *vb) {
+  const double a[4] = {0.4581652932831429, 2.217058676663745, 0.7405551735357053, 0.01968227878617998};
+  const double b[4] = {1.0, 4.504130959426697, 1.110667363742916, 0.02359291751427506};
+  const double da[4] = {0.119086804055547, 0.6157402568883345, 0.1574201515892867, 0.003532336663397157};
+  const double db[4] = {0.0, 0.2673612973836267, 0.2052004607777787, 0.004200005045691381};
+  double rho = ra + rb;
+  double z = (ra - rb) / rho;
+  if (z > 1.0) z = 1.0;
+  if (z < -1.0) z = -1.0;
+  const double fden = cbrt(16.0) - 2.0; /* 2^(4/3) - 2 */
+  double cp = cbrt(1.0 + z), cm = cbrt(1.0 - z);
+  double f = ((1.0 + z) * cp + (1.0 - z) * cm - 2.0) / fden;
+  double df = 4.0 / 3.0 * (cp - cm) / fden;
+  double A[4], B[4];
+  for (int i = 0; i < 4; i++) { A[i] = a[i] + f * da[i]; B[i] = b[i] + f * db[i]; }
+  double rs = cbrt(3.0 / (FOURPI_ * rho));
+  double num = A[0] + rs * (A[1] + rs * (A[2] + rs * A[3]));
+  double den = rs * (B[0] + rs * (B[1] + rs * (B[2] + rs * B[3])));
+  double dnum = A[1] + rs * (2.0 * A[2] + rs * 3.0 * A[3]);
+  double dden = B[0] + rs * (2.0 * B[1] + rs * (3.0 * B[2] + rs * 4.0 * B[3]));
+  double nf = da[0] + rs * (da[1] + rs * (da[2] + rs * da[3]));
+  double df_den = rs * (db[0] + rs * (db[1] + rs * (db[2] + rs * db[3])));
+  double eps = -num / den;
+  double deps_drs = -(dnum * den - num * dden) / (den * den);
+  double deps_dz = -(nf * den - num * df_den) / (den * den) * df;
+  *e = rho * eps;
+  *va = eps - rs / 3.0 * deps_drs + deps_dz * (1.0 - z);
+  *vb = eps - rs / 3.0 * deps_drs - deps_dz * (1.0 + z);
 }
 static void lda_slater(double rho, double *e, double *v) {
   double ex = -0.75 * cbrt(3.0 / PI_) * cbrt(rho);
@@ -1207,44 +1253,16 @@ static void grad_cal(orc_sys *s, const double *ro, double *grad) {
   free(tmp);
 }
 
-/* xc.f90:4-131,252-301 cal_vpot_ex (closed shell) */
-void orc_cal_vpot_ex(orc_sys *s) {
+/* the G-space assembly of one potential (xc.f90:252-301 closed shell,
+   :302-425 per spin): vp = band limit of [vp + v1 - i G.(v2 grad rho)] */
+static void assemble_v(orc_sys *s, double *vp, const double *v1, const double *v2, const double *grad) {
   long nnr1 = s->nnr1;
   int ngrho = s->ngrho;
-  int gga = (s->xc == ORC_XC_PBE);
-  double *grad = s->grad;
-  if (gga) grad_cal(s, s->rho, grad);
-  double *v1 = (double *)xcalloc(nnr1, sizeof(double)), *v2 = (double *)xcalloc(nnr1, sizeof(double));
-  double sgcx = 0.0;
-  double *sxa = (double *)xcalloc(nnr1, sizeof(double));
-#pragma omp parallel for schedule(static)
-  for (long i = 0; i < nnr1; i++) {
-    double e, v, vs;
-    orc_xc_point(s->xc, s->rho[i], gga ? grad[i] : 0.0, &e, &v, &vs);
-    double rt = s->rho[i] > 0.0 ? s->rho[i] : 0.0;
-    double v1_ = 0, v2_ = 0, sm = 0;
-    if (rt > 0.1 * GC_CUTOFF) {
-      double smoo, dsmoo;
-      if (rt > 4.0 * GC_CUTOFF) { smoo = 1.0; dsmoo = 0.0; }
-      else {
-        double texp = exp(3.0 * (1.0 - rt / GC_CUTOFF));
-        smoo = 1.0 / (1.0 + texp);
-        dsmoo = 3.0 / GC_CUTOFF * texp * smoo * smoo;
-      }
-      sm = smoo * e;
-      v1_ = dsmoo * e + smoo * v;
-      v2_ = smoo * (2.0 * vs);
-    }
-    sxa[i] = sm;
-    v1[i] = v1_;
-    v2[i] = v2_;
-  }
-  for (long i = 0; i < nnr1; i++) sgcx = sgcx + sxa[i];
-  s->etxc = sgcx;
+  int gga = v2 != NULL;
   zc *work = s->wk;
   zc *vpotg = (zc *)xcalloc(ngrho, sizeof(zc));
   memset(work, 0, sizeof(zc) * s->max_fft);
-  for (long l = 0; l < nnr1; l++) work[l] = s->v_pot[l];
+  for (long l = 0; l < nnr1; l++) work[l] = vp[l];
   do_fft(s, +1, work);
   for (int g = 0; g < ngrho; g++) vpotg[g] = work[s->mapp[g] - 1];
   memset(work, 0, sizeof(zc) * s->max_fft);
@@ -1277,8 +1295,69 @@ void orc_cal_vpot_ex(orc_sys *s) {
     work[s->mapm[g] - 1] = conj(vpotg[g]);
   }
   do_fft(s, -1, work);
-  for (long l = 0; l < nnr1; l++) s->v_pot[l] = creal(work[l]);
-  free(v1); free(v2); free(sxa); free(vpotg);
+  for (long l = 0; l < nnr1; l++) vp[l] = creal(work[l]);
+  free(vpotg);
+}
+
+/* smoothing of the functional near zero density (xc.f90:100-130, :196-236) */
+static void smoothing(double rt, double *smoo, double *dsmoo) {
+  if (rt > 4.0 * GC_CUTOFF) { *smoo = 1.0; *dsmoo = 0.0; return; }
+  double texp = exp(3.0 * (1.0 - rt / GC_CUTOFF));
+  *smoo = 1.0 / (1.0 + texp);
+  *dsmoo = 3.0 / GC_CUTOFF * texp * (*smoo) * (*smoo);
+}
+
+/* xc.f90:4-434 cal_vpot_ex: closed shell (:64-131) or, open shell, the
+   polarized LDA branch (:135-246) with rho_a = rho - rho2, rho_b = rho2 */
+void orc_cal_vpot_ex(orc_sys *s) {
+  long nnr1 = s->nnr1;
+  int gga = (s->xc == ORC_XC_PBE) && !s->lsd;
+  double *grad = s->grad;
+  if (gga) grad_cal(s, s->rho, grad);
+  double *v1 = (double *)xcalloc(nnr1, sizeof(double)), *v2 = (double *)xcalloc(nnr1, sizeof(double));
+  double *v1b = s->lsd ? (double *)xcalloc(nnr1, sizeof(double)) : NULL;
+  double *sxa = (double *)xcalloc(nnr1, sizeof(double));
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < nnr1; i++) {
+    if (s->lsd) {
+      double ra = s->rho[i] - s->rho2[i], rb = s->rho2[i];
+      double pa = ra > 0.0 ? ra : 0.0, pb = rb > 0.0 ? rb : 0.0;
+      double e = 0, va = 0, vb = 0;
+      if (pa + pb > 1e-30) lda_teter93_pol(pa, pb, &e, &va, &vb);
+      double rt = pa + pb, sm = 0, a = 0, b = 0;
+      if (rt > 0.1 * GC_CUTOFF) {
+        double smoo, dsmoo;
+        smoothing(rt, &smoo, &dsmoo);
+        sm = smoo * e;
+        a = dsmoo * e + smoo * va;
+        b = dsmoo * e + smoo * vb;
+      }
+      sxa[i] = sm;
+      v1[i] = a;
+      v1b[i] = b;
+      continue;
+    }
+    double e, v, vs;
+    orc_xc_point(s->xc, s->rho[i], gga ? grad[i] : 0.0, &e, &v, &vs);
+    double rt = s->rho[i] > 0.0 ? s->rho[i] : 0.0;
+    double v1_ = 0, v2_ = 0, sm = 0;
+    if (rt > 0.1 * GC_CUTOFF) {
+      double smoo, dsmoo;
+      smoothing(rt, &smoo, &dsmoo);
+      sm = smoo * e;
+      v1_ = dsmoo * e + smoo * v;
+      v2_ = smoo * (2.0 * vs);
+    }
+    sxa[i] = sm;
+    v1[i] = v1_;
+    v2[i] = v2_;
+  }
+  double sgcx = 0.0;
+  for (long i = 0; i < nnr1; i++) sgcx = sgcx + sxa[i];
+  s->etxc = sgcx;
+  assemble_v(s, s->v_pot, v1, gga ? v2 : NULL, grad);
+  if (s->lsd) assemble_v(s, s->v_pot2, v1b, NULL, grad);
+  free(v1); free(v2); free(v1b); free(sxa);
 }
 
 /* ------------------------------------------------------------------ */
@@ -1502,8 +1581,18 @@ void orc_vpsi(orc_sys *s) {
       psy[s->mapp[0] - 1] = ca[0] + I * cb[0];
     }
     do_fft(s, -1, psy);
+    if (s->lsd) {
+      /* open shell (wfn_initialize.f90:313-326): each band of the pair with
+         its own spin's potential (V_1 on Re, V_2 on Im for the pair that
+         straddles the spins) */
+      const double *va = is1 > s->nel_up ? s->v_pot2 : s->v_pot;
+      const double *vb = is2 > s->nel_up ? s->v_pot2 : s->v_pot;
 #pragma omp parallel for schedule(static)
-    for (long l = 0; l < nnr1; l++) psy[l] = s->v_pot[l] * psy[l];
+      for (long l = 0; l < nnr1; l++) psy[l] = va[l] * creal(psy[l]) + I * (vb[l] * cimag(psy[l]));
+    } else {
+#pragma omp parallel for schedule(static)
+      for (long l = 0; l < nnr1; l++) psy[l] = s->v_pot[l] * psy[l];
+    }
     do_fft(s, +1, psy);
     double fi = s->occ[is1 - 1] * 0.5;
     if (fi == 0.0) fi = 1.0;
@@ -1595,6 +1684,17 @@ static void ovlap_d(orc_sys *s, const zc *ca, const zc *cb, double *A) {
     }
 }
 
+/* open shell: the overlap matrices are block diagonal by spin (OVLAP_D and
+   ortho_gs each take the spin-1 and spin-2 blocks separately,
+   wfn_initialize.f90:245-253,458-477) */
+static void spin_mask(orc_sys *s, double *A) {
+  if (!s->lsd) return;
+  int n = s->nstate;
+  for (int j = 0; j < n; j++)
+    for (int i = 0; i < n; i++)
+      if ((i < s->nel_up) != (j < s->nel_up)) A[i + (long)n * j] = 0.0;
+}
+
 static void eval_gmax(orc_sys *s, double gcut) {
   int nocc = 0;
   for (int i = 0; i < s->nstate; i++) if (s->occ[i] > 1e-5) nocc++;
@@ -1611,6 +1711,7 @@ void orc_forces(orc_sys *s) {
   int n = s->nstate, ngpw = s->ngpw;
   double *gam = (double *)xcalloc((long)n * n, sizeof(double));
   ovlap_d(s, s->c2, s->c0, gam);
+  spin_mask(s, gam);
   for (int j = 0; j < n; j++)
     for (int i = 0; i < n; i++) {
       double fi = s->occ[i] == 0.0 ? 0.0 : 1.0, fj = s->occ[j] == 0.0 ? 0.0 : 1.0;
@@ -1811,7 +1912,9 @@ int orc_ortho(orc_sys *s) {
   int n = s->nstate, ngpw = s->ngpw;
   double *S = (double *)xcalloc((long)n * n, sizeof(double));
   ovlap_d(s, s->c0, s->c0, S);
-  /* DPOTRF('U'): S = U^T U, U stored in the upper triangle */
+  spin_mask(s, S);
+  /* DPOTRF('U'): S = U^T U, U stored in the upper triangle; block diagonal
+     by spin when open shell, so the blocks factor separately */
   for (int j = 0; j < n; j++) {
     double d = S[j + (long)n * j];
     for (int k = 0; k < j; k++) d -= S[k + (long)n * j] * S[k + (long)n * j];
@@ -1971,18 +2074,39 @@ orc_sys *orc_create(const orc_input *in, int nthreads) {
   nlppgrid(s);
   nlpro(s);
   exp_igrxfactor(s);
-  /* occupations (atomic_basis.f90:49-71, closed shell) */
+  /* occupations (atomic_basis.f90:49-79): closed shell two electrons per
+     orbital; open shell one orbital per valence electron, occupation 1 */
+  s->lsd = in->multiplicity > 0;
   int nst = in->nstate;
   if (nst <= 0) {
     nst = 0;
     for (int is = 0; is < s->nsp; is++) {
-      nst = nst + (int)((double)(s->na[is] * s->zv[is]) / 2.0);
-      if (2.0 * (double)nst < (double)(s->na[is] * s->zv[is])) { nst++; break; }
+      if (s->lsd) {
+        nst = nst + s->na[is] * s->zv[is];
+      } else {
+        nst = nst + (int)((double)(s->na[is] * s->zv[is]) / 2.0);
+        if (2.0 * (double)nst < (double)(s->na[is] * s->zv[is])) { nst++; break; }
+      }
     }
   }
   s->nstate = nst;
   s->occ = (double *)xcalloc(nst, sizeof(double));
-  for (int i = 0; i < nst; i++) s->occ[i] = 2.0;
+  for (int i = 0; i < nst; i++) s->occ[i] = s->lsd ? 1.0 : 2.0;
+  if (s->lsd) {
+    /* NSPIN unpaired electrons; NEL_UP = INT((NSTATE-NSPIN)/2) bands of spin 1,
+       NEL_DOWN = INT((NSTATE+NSPIN)/2) of spin 2 (init_module.f90:122-131) */
+    int nspin = in->multiplicity - 1;
+    int up = (int)((double)(nst - nspin) / 2.0), down = (int)((double)(nst + nspin) / 2.0);
+    if (up + down != nst || up < 0 || down < 0) {
+      fprintf(stderr, "oracle: incorrect multiplicity\n");
+      abort();
+    }
+    if (in->xc != ORC_XC_TETER93) {
+      fprintf(stderr, "oracle: the open-shell branch is restated for Teter93 only\n");
+      abort();
+    }
+    s->nel_up = up;
+  }
   long tot = (long)s->ngpw * nst;
   s->c0 = (zc *)xcalloc(tot, sizeof(zc));
   s->c2 = (zc *)xcalloc(tot, sizeof(zc));
@@ -1990,6 +2114,8 @@ orc_sys *orc_create(const orc_input *in, int nthreads) {
   s->hnm1 = (zc *)xcalloc(tot, sizeof(zc));
   s->rho = (double *)xcalloc(s->nnr1, sizeof(double));
   s->v_pot = (double *)xcalloc(s->nnr1, sizeof(double));
+  s->rho2 = (double *)xcalloc(s->nnr1, sizeof(double));
+  s->v_pot2 = (double *)xcalloc(s->nnr1, sizeof(double));
   s->grad = (double *)xcalloc(4 * s->nnr1, sizeof(double));
   s->rho_g = (zc *)xcalloc(s->ngrho, sizeof(zc));
   s->nl = (double *)xcalloc((long)s->nat * s->nghmax * nst, sizeof(double));
@@ -2012,7 +2138,7 @@ void orc_destroy(orc_sys *s) {
   free(s->isa_is); free(s->isa_ia); free(s->atco);
   free(s->vps); free(s->rhos); free(s->twnl); free(s->eigr); free(s->eigrxvps); free(s->eigrxrhos);
   free(s->occ); free(s->c0); free(s->c2); free(s->c2p); free(s->hnm1);
-  free(s->rho); free(s->v_pot); free(s->grad); free(s->rho_g); free(s->nl); free(s->dfnl); free(s->force);
+  free(s->rho); free(s->v_pot); free(s->rho2); free(s->v_pot2); free(s->grad); free(s->rho_g); free(s->nl); free(s->dfnl); free(s->force);
   free(s->w1); free(s->w2); free(s->wk);
   free(s);
 }
@@ -2087,6 +2213,8 @@ void *orc_get_ptr(orc_sys *s, const char *k) {
   if (!strcmp(k, "c2")) return s->c2;
   if (!strcmp(k, "rho")) return s->rho;
   if (!strcmp(k, "v_pot")) return s->v_pot;
+  if (!strcmp(k, "rho2")) return s->rho2;
+  if (!strcmp(k, "v_pot2")) return s->v_pot2;
   if (!strcmp(k, "rho_g")) return s->rho_g;
   if (!strcmp(k, "nl")) return s->nl;
   if (!strcmp(k, "dfnl")) return s->dfnl;

@@ -74,6 +74,8 @@ typedef struct {
   int xc;
   int nstate;              /* 0: derived as in setbasis (atomic_basis.f90:49-71) */
   orc_species sp[ORC_MAXSP];
+  int multiplicity;        /* 0: closed shell; m >= 1: OPEN_SHELL with MULTIPLICITY m (LSD,
+                              init_module.f90:122-160; Teter93 only) */
 } orc_input;
 
 typedef struct orc_sys orc_sys;

@@ -28,7 +28,7 @@ class OrcSpecies(C.Structure):
 class OrcInput(C.Structure):
     _fields_ = [("a_cell", C.c_double * 9), ("alat", C.c_double), ("symmetry", C.c_int), ("ecut", C.c_double),
                 ("nsp", C.c_int), ("na", C.c_int * MAXSP), ("na_max", C.c_int), ("atco", C.POINTER(C.c_double)),
-                ("xc", C.c_int), ("nstate", C.c_int), ("sp", OrcSpecies * MAXSP)]
+                ("xc", C.c_int), ("nstate", C.c_int), ("sp", OrcSpecies * MAXSP), ("multiplicity", C.c_int)]
 
 
 def build():
@@ -103,6 +103,7 @@ class Oracle:
         inp.atco = _dp(atco)
         inp.xc = system.xc
         inp.nstate = system.nstate
+        inp.multiplicity = getattr(system, "multiplicity", 0)
         for i, sp in enumerate(system.species):
             o = inp.sp[i]
             o.type = sp.kind

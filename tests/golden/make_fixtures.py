@@ -26,6 +26,9 @@ CASES = {
     "water2_mt": "tests/2_water/wf_opt",
     "water32_mt": "tests/32_water/wf_opt",
     "si_fcc_mt": "tests/bulk_si/single_point",
+    # open shell (LSD): O2 singlet and triplet, MT psp, Teter93
+    "o2_singlet": "tests/O2/singlet_sp_cube",
+    "o2_triplet": "tests/O2/triplet_sp_cube",
 }
 KEYS = {"TOTAL ENERGY": "etotal", "KINETIC ENERGY": "eke", "ELECTROSTATIC ENERGY": "estat",
         "SELF ENERGY CONTRIBUTION": "eself", "OVERLAP ENERGY CONTRIBUTION": "esr", "LOCAL PP ENERGY": "eloc",
@@ -79,9 +82,8 @@ def parse_sp_energy(path):
     return float(last.split()[1])
 
 
-# open-shell runs (the LSD branch is outside the path): only the system and
-# the G-sphere / ray counts of the rank table are kept, not the energies
-GSPHERE_ONLY = {"o2_singlet": "tests/O2/singlet_sp_cube"}
+# G-sphere / ray counts only (none at present)
+GSPHERE_ONLY = {}
 
 MD_FORCES = {"water32_mt": "tests/32_water/md", "water1_mt": "tests/1_water/md"}
 GEO_GRADIENTS = {"water1_mt": "tests/1_water/geo_opt/atom_force.dat",
@@ -101,7 +103,8 @@ def parse_first_gradient(path):
 
 
 def save_system(path, s):
-    d = dict(a_cell=s.a_cell, alat=s.alat, symmetry=s.symmetry, ecut=s.ecut, xc=s.xc, nsp=len(s.species))
+    d = dict(a_cell=s.a_cell, alat=s.alat, symmetry=s.symmetry, ecut=s.ecut, xc=s.xc, nsp=len(s.species),
+             multiplicity=s.multiplicity)
     for i, (sp, pos) in enumerate(zip(s.species, s.positions)):
         d[f"pos{i}"] = pos
         d[f"sp{i}_meta"] = np.array([sp.z, sp.zv, sp.kind, sp.lmax, sp.l_local, sp.skip, int(sp.tkb), sp.upf_lmax])

@@ -11,6 +11,8 @@ written to oracle_<name>.json.  Systems:
               bands), 1e-6; about an hour on 8 cores
   water1      the single-water benchmark system (GTH, LDA-PZ, 70 Ry, 64^3,
               4 bands), CG to 1e-7 then forces; a minute
+  o2_triplet  the reference's open-shell O2 triplet (MT psp, Teter93, 80 Ry,
+              60^3, 5 + 7 bands), 1e-7; a minute
 Run from the repository root:
     python tests/golden/make_oracle_fixtures.py <name>
 """
@@ -30,13 +32,13 @@ from oracle.oracle import Oracle  # noqa: E402
 from amdkiit_b200 import configs  # noqa: E402
 from tests.helpers import load_fixture, oracle_eigenvalues, start_coefficients  # noqa: E402
 
-GCUT = {"water32_mt": 1e-6, "water2_mt": 1e-7, "water32": 1e-6, "water1": 1e-7}
+GCUT = {"water32_mt": 1e-6, "water2_mt": 1e-7, "water32": 1e-6, "water1": 1e-7, "o2_triplet": 1e-7}
 
 
 def system(name):
     """The reference runs come from their npz fixtures, the benchmark systems
     from amdkiit_b200.configs."""
-    if name.endswith("_mt"):
+    if name.endswith("_mt") or name.startswith("o2_"):
         return load_fixture(name)
     return configs.BY_NAME[name]()
 
@@ -56,7 +58,7 @@ def main(name="water32_mt"):
     assert conv == 1, "no convergence"
     out = dict(system=name, gcut=GCUT[name], iterations=it, energies=o.energies(),
                forces=np.concatenate([o.force()[i, :k] for i, k in enumerate(s.na)]).tolist())
-    out["eigenvalues"] = oracle_eigenvalues(o).tolist()
+    out["eigenvalues"] = oracle_eigenvalues(o, s.multiplicity).tolist()
     with open(os.path.join(HERE, f"oracle_{name}.json"), "w") as f:
         json.dump(out, f, indent=1)
     print("energy", out["energies"]["etotal"], "iterations", it)

@@ -30,8 +30,9 @@ def load_fixture(name: str) -> System:
                                lmax=int(lmax), l_local=int(l_local), skip=int(skip), tkb=bool(tkb),
                                upf_lmax=int(upf_lmax), **kw))
         pos.append(d[f"pos{i}"])
+    mult = int(d["multiplicity"]) if "multiplicity" in d else 0
     return System(a_cell=d["a_cell"], alat=float(d["alat"]), symmetry=int(d["symmetry"]), ecut=float(d["ecut"]),
-                  species=species, positions=pos, xc=int(d["xc"]), name=name)
+                  species=species, positions=pos, xc=int(d["xc"]), name=name, multiplicity=mult)
 
 
 def start_coefficients(hg_pw: np.ndarray, tpiba: float, nstate: int, seed: int = 1234) -> np.ndarray:
@@ -63,13 +64,18 @@ class OracleEngine:
         return self.o.force()
 
 
-def oracle_eigenvalues(o) -> np.ndarray:
+def oracle_eigenvalues(o, multiplicity: int = 0) -> np.ndarray:
     """Subspace eigenvalues (Ha) at the oracle's current C0: the stages of one
-    iteration up to H|psi> (C2 = -f_i H|psi_i>, f_i = 2), then the same
-    nstate x nstate diagonalisation the engine uses."""
+    iteration up to H|psi> (C2 = -f_i H|psi_i>, f_i = 2, or 1 open shell),
+    then the same diagonalisation the engine uses (per spin block when open
+    shell, spin 1 first)."""
     from amdkiit_b200.engine import subspace_eigenvalues
     for r in ("eval_density", "rhor2g", "eval_pot", "cal_vpot_ex", "pp_energy", "vpsi", "fnonloc"):
         o.call(r)
+    if multiplicity > 0:
+        nu = (o.nstate - (multiplicity - 1)) // 2
+        c, hc = o.c0(), -o.c2()
+        return np.concatenate([subspace_eigenvalues(c[:nu], hc[:nu]), subspace_eigenvalues(c[nu:], hc[nu:])])
     return subspace_eigenvalues(o.c0(), -0.5 * o.c2())
 
 

@@ -138,3 +138,43 @@ def test_reference_upf_energy():
     ref = golden()["h2_upf"]
     tol = 0.5 * 10.0 ** -ref["energy_decimals"] + E_TOL_PER_ATOM * s.nat
     assert abs(o.d("etotal") - ref["energies"]["etotal"]) < tol
+
+
+def test_reference_open_shell_triplet():
+    """tests/O2/triplet_sp_cube: O2, MULTIPLICITY 3 (5 bands of spin 1, 7 of
+    spin 2), MT psp, Teter93 polarized, GRAD_CUTOFF 1e-7: the LSD branch
+    (density per spin, polarized XC, a potential per spin, spin-block overlap
+    and orthonormalisation).  Measured: 1.4e-8 Ha total."""
+    s, o = _converge("o2_triplet", 1e-7, 800)
+    ref = golden()["o2_triplet"]["energies"]
+    e = o.energies()
+    assert abs(e["etotal"] - ref["etotal"]) < E_TOL_PER_ATOM * s.nat
+    for k in ("eself", "esr"):
+        assert abs(e[k] - ref[k]) < 1e-9, k
+    for k in ("eke", "estat", "eloc", "enl", "exc"):
+        assert abs(e[k] - ref[k]) < COMP_TOL, k
+
+
+def test_reference_open_shell_singlet():
+    """tests/O2/singlet_sp_cube: O2 with OPEN_SHELL and MULTIPLICITY 1 (6 + 6
+    bands), GRAD_CUTOFF 1e-5.  The reference's atomic guess gives both spins
+    the same orbitals and the iteration keeps them equal (the spin-restricted
+    solution); a start with the same coefficients for both spins does the
+    same.  A start that differs between the spins ends lower, on a
+    broken-symmetry solution (-31.709 Ha from the seeded start, measured).
+    The reference stopped at GEMAX < 1e-5, so its energy carries that run's
+    convergence error (measured 1.0e-5 Ha total)."""
+    s = load_fixture("o2_singlet")
+    o = Oracle(s, 0)
+    g = o.gvectors()
+    c = start_coefficients(g["hg"][: o.ngpw], o.d("tpiba"), o.nstate)
+    h = o.nstate // 2
+    c[h:] = c[:h]
+    o.set_wfn(c)
+    assert o.ortho() == 0
+    n = o.wfn_opt(800, 1e-5)
+    assert 0 < n < 800
+    ref = golden()["o2_singlet"]["energies"]
+    assert abs(o.d("etotal") - ref["etotal"]) < 1e-5 * s.nat
+    rho, rho2 = o.real_grid("rho"), o.real_grid("rho2")
+    assert np.max(np.abs(rho - 2.0 * rho2)) < 1e-8 * np.max(rho)  # equal spin densities
