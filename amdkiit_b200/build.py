@@ -61,7 +61,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         subprocess.check_call(cmd)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    cmd = [_nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcusolver"]
+    cmd = [_nvcc(), *ARCH, "-shared", "-o", tmp, *objs]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)

@@ -1,5 +1,4 @@
 // libamdk: device context and the extern "C" entry points of include/amdk.h.
-#include <cusolverDn.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -80,13 +79,8 @@ struct amdk_ctx {
   HostSetup hs;
   int device = 0, precision = AMDK_FP64, batch = 4;
   cudaStream_t st = nullptr;
-  // cuSOLVER for the Cholesky/inverse of overlaps too large for one SM
-  cusolverDnHandle_t cs = nullptr;
-  double *d_potrf_ws = nullptr;
-  int potrf_lw = 0;
-  void *d_trtri_ws = nullptr, *h_trtri_ws = nullptr;
-  size_t trtri_dws = 0, trtri_hws = 0;
-  int *d_info2 = nullptr;
+  // the blocked Cholesky of overlaps too large for one SM: work copy, block row
+  double *d_cholw = nullptr, *d_cholt = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
   // geometry / FFT
@@ -306,7 +300,7 @@ template <typename F> static void with_n(int n, F &&f) {
   switch (n) {
 #define AMDK_NCASE(v) \
   case v: f(std::integral_constant<int, v>{}); break;
-    AMDK_NCASE(36) AMDK_NCASE(48) AMDK_NCASE(64) AMDK_NCASE(72) AMDK_NCASE(80) AMDK_NCASE(90) AMDK_NCASE(96)
+    AMDK_NCASE(36) AMDK_NCASE(48) AMDK_NCASE(60) AMDK_NCASE(64) AMDK_NCASE(72) AMDK_NCASE(80) AMDK_NCASE(90) AMDK_NCASE(96)
     AMDK_NCASE(100) AMDK_NCASE(108) AMDK_NCASE(120) AMDK_NCASE(128) AMDK_NCASE(144) AMDK_NCASE(160)
 #undef AMDK_NCASE
     default: f(std::integral_constant<int, 0>{}); break;
@@ -1391,6 +1385,56 @@ static int check_ortho(amdk_ctx *c) {
   }
   return 0;
 }
+// C (m x n, ldc) = alpha op(A) op(B) + beta C for the blocked factorisation
+static void small_dgemm(amdk_ctx *c, int ta, int tb, int m, int n, int k, double alpha, const double *A, int lda,
+                        const double *B, int ldb, double beta, double *Cm, int ldc) {
+  if (m <= 0 || n <= 0) return;
+  ++c->nlaunch;
+  k_small_dgemm<<<dim3((m + 63) / 64, (n + 63) / 64), 256, 0, c->st>>>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm,
+                                                                      ldc);
+}
+// Cholesky factor and inverse of the overlap above CHOL_NMAX bands (UINV,
+// DPOTRF + DTRTRI, wfn_initialize.f90:504-530), blocked by 128:
+// right-looking over a work copy W of S, each diagonal block factored and
+// inverted by k_chol_inv_s (X_kk = U_kk^-1 into U^-1's diagonal block), the
+// block row U_k,j = X_kk^T S_k,j (j > k) and the trailing update
+// S_j,l -= U_k,j^T U_k,l as small products; then the inverse's off-diagonal
+// blocks column by column from the bottom, X_i,j = -X_i,i sum_{k=i+1..j}
+// U_i,k X_k,j.  All on the context stream (capturable).
+static int chol_inv_blocked(amdk_ctx *c, int n) {
+  constexpr int BK = 128;
+  double *W = c->d_cholw, *T = c->d_cholt, *X = c->d_uinv;
+  CK(cudaMemcpyAsync(W, c->d_gam, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)n * n, c->st));
+  const int nb = (n + BK - 1) / BK;
+  const size_t sm = ((size_t)BK * (BK + 1) + (size_t)CHOL_B * BK) * sizeof(double);
+  for (int kb = 0; kb < nb; ++kb) {
+    const int k0 = kb * BK, kn = std::min(BK, n - k0), k1 = k0 + kn, rest = n - k1;
+    ++c->nlaunch;
+    k_chol_inv_s<<<1, CHOL_NT, sm, c->st>>>(kn, W + k0 + (size_t)n * k0, n, X + k0 + (size_t)n * k0, n, c->d_info, k0,
+                                            kb == 0);
+    if (rest <= 0) break;
+    // block row: T = X_kk^T W[k0:k1, k1:n], then back into W
+    small_dgemm(c, 1, 0, kn, rest, kn, 1.0, X + k0 + (size_t)n * k0, n, W + k0 + (size_t)n * k1, n, 0.0, T, kn);
+    CK(cudaMemcpy2DAsync(W + k0 + (size_t)n * k1, sizeof(double) * n, T, sizeof(double) * kn, sizeof(double) * kn,
+                         rest, cudaMemcpyDeviceToDevice, c->st));
+    // trailing matrix (the whole square; only its upper triangle is read later)
+    small_dgemm(c, 1, 0, rest, rest, kn, -1.0, W + k0 + (size_t)n * k1, n, W + k0 + (size_t)n * k1, n, 1.0,
+                W + k1 + (size_t)n * k1, n);
+  }
+  for (int jb = 1; jb < nb; ++jb) {
+    const int j0 = jb * BK, jn = std::min(BK, n - j0), j1 = j0 + jn;
+    for (int ib = jb - 1; ib >= 0; --ib) {
+      const int i0 = ib * BK, in = BK, i1 = i0 + in;
+      // T = U[i0:i1, i1:j1] X[i1:j1, j0:j1], then X[i0:i1, j0:j1] = -X_ii T
+      small_dgemm(c, 0, 0, in, jn, j1 - i1, 1.0, W + i0 + (size_t)n * i1, n, X + i1 + (size_t)n * j0, n, 0.0, T, in);
+      small_dgemm(c, 0, 0, in, jn, in, -1.0, X + i0 + (size_t)n * i0, n, T, in, 0.0, X + i0 + (size_t)n * j0, n);
+    }
+  }
+  CK(cudaGetLastError());
+  return 0;
+}
+
 static int do_ortho(amdk_ctx *c, bool check = true, bool swap = true) {
   const HostSetup &h = c->hs;
   const int n = c->nstate;
@@ -1405,22 +1449,13 @@ static int do_ortho(amdk_ctx *c, bool check = true, bool swap = true) {
   ++c->nlaunch;
   k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, c->st>>>(n, h.ngpw, c->d_c0, c->d_c0, c->d_gam, c->d_occ, 0, 1);
   spin_mask(c, c->d_gam);
-  const int np = (n + CHOL_B - 1) / CHOL_B * CHOL_B;
-  const size_t sm = ((size_t)np * (np + 1) + (size_t)CHOL_B * np) * sizeof(double);
-  ++c->nlaunch;
   if (n <= CHOL_NMAX) {
-    k_chol_inv_s<<<1, CHOL_NT, sm, c->st>>>(n, c->d_gam, c->d_uinv, c->d_info);
+    const int np = (n + CHOL_B - 1) / CHOL_B * CHOL_B;
+    const size_t sm = ((size_t)np * (np + 1) + (size_t)CHOL_B * np) * sizeof(double);
+    ++c->nlaunch;
+    k_chol_inv_s<<<1, CHOL_NT, sm, c->st>>>(n, c->d_gam, n, c->d_uinv, n, c->d_info, 0, 1);
   } else {
-    // DPOTRF + DTRTRI as the reference (wfn_initialize.f90:513,524), in place
-    // in a copy of S (the lower triangle is never read by the DTRMM below)
-    CK(cudaMemcpyAsync(c->d_uinv, c->d_gam, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, c->st));
-    if (cusolverDnDpotrf(c->cs, CUBLAS_FILL_MODE_UPPER, n, c->d_uinv, n, c->d_potrf_ws, c->potrf_lw, c->d_info) !=
-            CUSOLVER_STATUS_SUCCESS ||
-        cusolverDnXtrtri(c->cs, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, n, CUDA_R_64F, c->d_uinv, n,
-                         c->d_trtri_ws, c->trtri_dws, c->h_trtri_ws, c->trtri_hws, c->d_info2) != CUSOLVER_STATUS_SUCCESS) {
-      set_error("cuSOLVER Cholesky/inverse failed");
-      return AMDK_ERR_CUDA;
-    }
+    RC(chol_inv_blocked(c, n));
   }
   CK(cudaMemcpyAsync(c->h_info, c->d_info, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
   if (check) {
@@ -1632,28 +1667,9 @@ static int build_device(amdk_ctx *c) {
     c->overlap = !(no && no[0] == '1');
   }
   if (h.nstate > CHOL_NMAX) {
-    // large overlaps: cuSOLVER (its DTRTRI keeps a host workspace, so the
-    // iteration is not graph-captured)
-    if (cusolverDnCreate(&c->cs) != CUSOLVER_STATUS_SUCCESS || cusolverDnSetStream(c->cs, c->st) != CUSOLVER_STATUS_SUCCESS) {
-      set_error("cusolverDnCreate failed");
-      return AMDK_ERR_CUDA;
-    }
-    const int n = h.nstate;
-    double *tmp;
-    RC(c->alloc(&tmp, (size_t)n * n));
-    if (cusolverDnDpotrf_bufferSize(c->cs, CUBLAS_FILL_MODE_UPPER, n, tmp, n, &c->potrf_lw) != CUSOLVER_STATUS_SUCCESS ||
-        cusolverDnXtrtri_bufferSize(c->cs, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, n, CUDA_R_64F, tmp, n,
-                                    &c->trtri_dws, &c->trtri_hws) != CUSOLVER_STATUS_SUCCESS) {
-      set_error("cuSOLVER workspace query failed");
-      return AMDK_ERR_CUDA;
-    }
-    RC(c->alloc(&c->d_potrf_ws, (size_t)std::max(c->potrf_lw, 1)));
-    char *tw;
-    RC(c->alloc(&tw, std::max<size_t>(c->trtri_dws, 16)));
-    c->d_trtri_ws = tw;
-    c->h_trtri_ws = std::malloc(std::max<size_t>(c->trtri_hws, 16));
-    RC(c->alloc(&c->d_info2, 4));
-    c->use_graphs = false;
+    // large overlaps: the blocked factorisation's work copy and block row
+    RC(c->alloc(&c->d_cholw, (size_t)h.nstate * h.nstate));
+    RC(c->alloc(&c->d_cholt, (size_t)128 * h.nstate));
   }
   RC(c->up(&c->d_occ, h.occ));
   {
@@ -2166,8 +2182,6 @@ int amdk_destroy(amdk_ctx *c) {
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
   }
   if (c->h_pin) cudaFreeHost(c->h_pin);
-  if (c->cs) cusolverDnDestroy(c->cs);
-  if (c->h_trtri_ws) std::free(c->h_trtri_ws);
   if (c->h_info) cudaFreeHost(c->h_info);
   for (auto &e : c->evpool) {
     cudaEventDestroy(e.first);

@@ -874,7 +874,11 @@ __device__ __forceinline__ void warp_chol_inv16(double *D, int ld, int base, int
   }
 }
 
-__global__ void __launch_bounds__(CHOL_NT) k_chol_inv_s(int n, const double *A, double *Ui, int *info) {
+// A (leading dimension lda) in, U^-1 into Ui (leading dimension ldu); a
+// non-positive pivot j sets *info = base + j + 1 (first: the status is also
+// cleared on success; otherwise an earlier failure is kept)
+__global__ void __launch_bounds__(CHOL_NT) k_chol_inv_s(int n, const double *A, int lda, double *Ui, int ldu, int *info,
+                                                        int base, int first) {
   extern __shared__ double M[];
   __shared__ int bad;
   const int np = (n + CHOL_B - 1) / CHOL_B * CHOL_B, ld = np + 1, nb = np / CHOL_B;
@@ -884,7 +888,7 @@ __global__ void __launch_bounds__(CHOL_NT) k_chol_inv_s(int n, const double *A, 
   if (tid == 0) bad = 0;
   for (int b = w; b < np; b += nw)
     for (int a = lane; a < np; a += 32)
-      M[a + ld * b] = (a < n && b < n) ? A[a + (long)n * b] : (a == b ? 1.0 : 0.0);
+      M[a + ld * b] = (a < n && b < n) ? A[a + (long)lda * b] : (a == b ? 1.0 : 0.0);
   __syncthreads();
   if (w == 0) warp_chol_inv16(M, ld, 0, &bad);
   __syncthreads();
@@ -982,12 +986,58 @@ __global__ void __launch_bounds__(CHOL_NT) k_chol_inv_s(int n, const double *A, 
     __syncthreads();
   }
   if (bad) {
-    if (tid == 0) *info = bad;
+    if (tid == 0 && (first || *info == 0)) *info = base + bad;
     return;
   }
   for (int b = w; b < n; b += nw)
-    for (int a = lane; a < n; a += 32) Ui[a + (long)n * b] = (a <= b) ? M[a + ld * b] : 0.0;
-  if (tid == 0) *info = 0;
+    for (int a = lane; a < n; a += 32) Ui[a + (long)ldu * b] = (a <= b) ? M[a + ld * b] : 0.0;
+  if (tid == 0 && first) *info = 0;
+}
+
+// Small dense FP64 product for the blocked Cholesky above 144 bands:
+// C (m x n, ldc) = alpha op(A) op(B) + beta C, column-major operands, op = the
+// matrix (0) or its transpose (1); 64 x 64 tiles, 256 threads of 4 x 4
+// outputs, k in steps of 16 through shared memory
+__global__ void __launch_bounds__(256) k_small_dgemm(int ta, int tb, int m, int n, int k, double alpha, const double *A,
+                                                    int lda, const double *B, int ldb, double beta, double *C,
+                                                    int ldc) {
+  __shared__ double As[16][64 + 1], Bs[16][64 + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int i0 = blockIdx.x * 64, j0 = blockIdx.y * 64;
+  double acc[4][4] = {};
+  for (int k0 = 0; k0 < k; k0 += 16) {
+    for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+      const int kk = e / 64, r = e % 64;
+      const int i = i0 + r, j = j0 + r, q = k0 + kk;
+      As[kk][r] = (i < m && q < k) ? (ta ? A[q + (long)lda * i] : A[i + (long)lda * q]) : 0.0;
+      Bs[kk][r] = (j < n && q < k) ? (tb ? B[j + (long)ldb * q] : B[q + (long)ldb * j]) : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        a[u] = As[kk][tx + 16 * u];
+        b[u] = Bs[kk][ty + 16 * u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = i0 + tx + 16 * u, j = j0 + ty + 16 * v;
+      if (i < m && j < n) {
+        double *c = C + i + (long)ldc * j;
+        *c = alpha * acc[u][v] + (beta != 0.0 ? beta * *c : 0.0);
+      }
+    }
 }
 
 // e_sr (total_energy.f90:133-239) with minimum image: one thread per atom

@@ -1,6 +1,8 @@
-"""The FP64 tensor-core products (csrc/dgemm.cuh) against numpy in FP64, on
-band counts that cover one and several 64 x 64 output tiles, partial tiles,
-band chunks of 128 in the rotation and the symmetric (upper-tile) Gram:
+"""The FP64 tensor-core products (csrc/dgemm.cuh) and the Cholesky against
+numpy in FP64, on band counts that cover one and several 64 x 64 output
+tiles, partial tiles, band chunks of 128 in the rotation, the symmetric
+(upper-tile) Gram, and above 144 bands the blocked factorisation (160 and
+300 bands: two and three blocks of 128):
 
 - the overlap S = 2 Re C0^T C0 - Re c0(0) Re c0(0)^T of ortho_gs
   (wfn_initialize.f90:481-482), read back with amdk_get_array("overlap");
@@ -32,7 +34,9 @@ def _check_overlap(e, c):
 
 
 CASES = [(1, 12.0, 501, 30.0, FP64), (3, 13.5, 503, 30.0, FP64), (2, 14.0, 502, 30.0, FP64), (5, 15.2, 705, 16.0, MIXED),
-         (16, 18.1, 716, 16.0, FP64), (18, 18.4, 718, 16.0, FP64), (33, 20.5, 733, 16.0, FP64)]
+         (16, 18.1, 716, 16.0, FP64), (18, 18.4, 718, 16.0, FP64), (33, 20.5, 733, 16.0, FP64),
+         # above 144 bands: the blocked Cholesky and inverse (blocks of 128)
+         (40, 22.0, 740, 16.0, FP64), (75, 26.0, 775, 14.0, MIXED)]
 
 
 @pytest.mark.parametrize("nwat,box,seed,ecut,prec", CASES)
