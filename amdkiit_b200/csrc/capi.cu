@@ -720,8 +720,8 @@ template <typename C> static int density_groups(amdk_ctx *c, int T) {
                                    c->pencil_groups);
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(c->st, &cap);
-  const std::string tkey = pencil_key(c, "pencil_density_groups", T) + "/ct" + std::to_string(c->ct_dens) + "/ns" +
-                           std::to_string(c->ns_dens);
+  const std::string tkey = pencil_key(c, "pencil_density_groups_with_reduce", T) + "/ct" +
+                           std::to_string(c->ct_dens) + "/ns" + std::to_string(c->ns_dens);
   int cached = 0;
   if (cap == cudaStreamCaptureStatusNone && c->tune && tune_get(tkey, &cached) && cached >= 1 &&
       cached <= std::min(c->pencil_groups, T)) {
@@ -732,13 +732,20 @@ template <typename C> static int density_groups(amdk_ctx *c, int T) {
     cudaEventCreate(&e1);
     const long nl = c->nlaunch;
     float best_ms = 1e30f;
+    // each candidate timed with the reduction of its partial grids: more
+    // groups spread the blocks better but leave more grids to add
+    auto run = [&](int grp) {
+      launch_pencil_density<C>(c, 0, T, grp, 0);
+      k_rho_reduce_p<<<dim3((g.n1 + 31) / 32, (g.n1 + 31) / 32, g.n1), dim3(32, 8), 0, c->st>>>(
+          g.n1, c->pn1, c->pn2, grp, c->d_rhopart, c->d_rho);
+    };
     const int cands[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16};
     for (int grp : cands) {
       if (grp > c->pencil_groups || grp > T || (grp - 1) * ((T + grp - 1) / grp) >= T) continue;  // no empty group
-      launch_pencil_density<C>(c, 0, T, grp, 0);  // warm
+      run(grp);  // warm
       cudaEventRecord(e0, c->st);
-      launch_pencil_density<C>(c, 0, T, grp, 0);
-      launch_pencil_density<C>(c, 0, T, grp, 0);
+      run(grp);
+      run(grp);
       cudaEventRecord(e1, c->st);
       cudaEventSynchronize(e1);
       float ms = 0;

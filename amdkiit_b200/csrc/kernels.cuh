@@ -688,14 +688,35 @@ struct BandWalk {
   }
 };
 
+// A block's contiguous chunk of the (band, G) index space (as BandWalk), read
+// STREAM_U elements per thread per round with all loads issued first, so
+// that enough of them are in flight to stream at the copy rate.
+constexpr int STREAM_U = 4;
+__device__ __forceinline__ void stream_chunk(long tot, long &k0, long &k1) {
+  const long per = (tot + gridDim.x - 1) / gridDim.x;
+  const long chunk = (per + blockDim.x - 1) / blockDim.x * blockDim.x;
+  k0 = blockIdx.x * chunk;
+  k1 = min(tot, k0 + chunk);
+}
 __global__ void k_ekin(int ngpw, int nstate, const double2 *c0, const double *hg, const double *occ, double *part,
                        double *out, unsigned *ticket) {
   double s = 0;
-  BandWalk w((long)ngpw * nstate, ngpw);
-#pragma unroll 4
-  for (; w.k < w.k1; w.next(ngpw)) {
-    const double2 c = c0[w.k];
-    s += occ[w.b] * hg[w.g] * (c.x * c.x + c.y * c.y);
+  long k0, k1;
+  stream_chunk((long)ngpw * nstate, k0, k1);
+  for (long kb = k0 + threadIdx.x; kb < k1; kb += STREAM_U * (long)blockDim.x) {
+    double2 c[STREAM_U];
+#pragma unroll
+    for (int u = 0; u < STREAM_U; ++u) {
+      const long k = kb + u * (long)blockDim.x;
+      c[u] = k < k1 ? c0[k] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < STREAM_U; ++u) {
+      const long k = kb + u * (long)blockDim.x;
+      if (k >= k1) break;
+      const unsigned b = (unsigned)k / (unsigned)ngpw, g = (unsigned)k - b * (unsigned)ngpw;
+      s += occ[b] * hg[g] * (c[u].x * c[u].x + c[u].y * c[u].y);
+    }
   }
   const double v[1] = {s};
   reduce_and_finish<1>(v, part, out, ticket);
@@ -751,22 +772,26 @@ __global__ void k_zclean(int n, int ngpw, double2 *c) {
 __global__ void k_gmax_precon(int ngpw, int nocc, const double *vpp, const double *occ, const double2 *c2,
                               double *part, double *out, unsigned *ticket) {
   double m = 0.0, s = 0.0;
-  BandWalk w((long)ngpw * nocc, ngpw);
-  int bf = -1;
-  double fi = 1.0;
-#pragma unroll 4
-  for (; w.k < w.k1; w.next(ngpw)) {
-    const int b = w.b, g = w.g;
-    if (b != bf) {  // 1/f_i once per band
-      bf = b;
-      fi = occ[b] > 0.01 ? 1.0 / occ[b] : 1.0;
+  long k0, k1;
+  stream_chunk((long)ngpw * nocc, k0, k1);
+  for (long kb = k0 + threadIdx.x; kb < k1; kb += STREAM_U * (long)blockDim.x) {
+    double2 c[STREAM_U];
+#pragma unroll
+    for (int u = 0; u < STREAM_U; ++u) {
+      const long k = kb + u * (long)blockDim.x;
+      c[u] = k < k1 ? c2[k] : make_double2(0.0, 0.0);
     }
-    const double2 c = c2[w.k];
-    const double a2 = c.x * c.x + c.y * c.y;
-    m = fmax(m, a2);
-    const double f = fi * vpp[g];
-    const double2 v = make_double2(f * c.x, f * c.y);
-    s += (g == 0) ? v.x * v.x : 2.0 * (v.x * v.x + v.y * v.y);
+#pragma unroll
+    for (int u = 0; u < STREAM_U; ++u) {
+      const long k = kb + u * (long)blockDim.x;
+      if (k >= k1) break;
+      const unsigned b = (unsigned)k / (unsigned)ngpw, g = (unsigned)k - b * (unsigned)ngpw;
+      const double fi = occ[b] > 0.01 ? 1.0 / occ[b] : 1.0;  // 1/f_i
+      m = fmax(m, c[u].x * c[u].x + c[u].y * c[u].y);
+      const double f = fi * vpp[g];
+      const double2 v = make_double2(f * c[u].x, f * c[u].y);
+      s += (g == 0) ? v.x * v.x : 2.0 * (v.x * v.x + v.y * v.y);
+    }
   }
   const double vals[2] = {sqrt(m), s};  // sqrt is monotonic: the max of the roots is the root of the max
   reduce_and_finish<2, 1u>(vals, part, out, ticket);
