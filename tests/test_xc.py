@@ -1,6 +1,8 @@
 """The restated functionals (libxc is not vendored by the reference): the
 potentials must be the derivatives of the energy density, checked by central
-finite differences, and limiting values must match the closed forms."""
+finite differences; limiting values must match the closed forms; and PZ81,
+PW92 and PBE are pinned to their papers' constants and limits (the GPU's
+k_xc matches this restatement to 1e-10 in the stage tests)."""
 import math
 
 import numpy as np
@@ -53,3 +55,73 @@ def test_pbe_reduces_to_lda_exchange_plus_pw92():
 def test_teter93_matches_pz_at_moderate_density():
     for rho in (0.01, 0.1, 1.0):
         assert abs(xc_point(0, rho, 0)[0] - xc_point(1, rho, 0)[0]) < 3e-3 * abs(xc_point(1, rho, 0)[0])
+
+
+# ----------------------------------------------------------------------------
+# Pins to the published parameterisations (values that follow from the papers'
+# constants and limits, evaluated here independently of the oracle's code):
+#   PZ81 (Perdew & Zunger, PRB 23, 5048): eps_c(rs) = gamma/(1 + beta1 sqrt(rs)
+#     + beta2 rs) for rs >= 1 (gamma = -0.1423, beta1 = 1.0529, beta2 = 0.3334),
+#     A ln rs + B + C rs ln rs + D rs below, which tends to B + D = -0.0596 at
+#     rs = 1 (the rounded constants leave a 3e-5 Ha step there);
+#   PW92 (Perdew & Wang, PRB 45, 13244), the LDA correlation inside PBE, from
+#     its published constants;
+#   PBE (Perdew, Burke & Ernzerhof, PRL 77, 3865): F_x(s) = 1 + kappa -
+#     kappa/(1 + mu s^2/kappa), kappa = 0.804, mu = 0.21951, reached where the
+#     gradient correction H cancels eps_c (high density, large t), 1 + kappa as
+#     s -> infinity; and mu = beta pi^2/3 (beta = 0.066725), which makes the
+#     second-order gradient terms of exchange and correlation cancel.
+def _rho_of_rs(rs):
+    return 3.0 / (4.0 * math.pi * rs ** 3)
+
+
+def _ex_lda(rho):
+    return -0.75 * (3 / math.pi) ** (1 / 3) * rho ** (4 / 3)
+
+
+def _eps_c(xc, rs):
+    rho = _rho_of_rs(rs)
+    return (xc_point(xc, rho, 0.0)[0] - _ex_lda(rho)) / rho
+
+
+def test_pz81_correlation_at_rs1():
+    assert abs(_eps_c(1, 1.0) - (-0.1423 / (1.0 + 1.0529 + 0.3334))) < 1e-7
+    assert abs(_eps_c(1, 1.0 - 1e-7) - (-0.048 - 0.0116)) < 1e-6
+    # high density: A ln rs + B + C rs ln rs + D rs, A = 0.0311, C = 0.0020
+    rs = 0.01
+    assert abs(_eps_c(1, rs) - (0.0311 * math.log(rs) - 0.048 + 0.0020 * rs * math.log(rs) - 0.0116 * rs)) < 1e-7
+
+
+@pytest.mark.parametrize("rs", [0.5, 1.0, 4.0])
+def test_pw92_correlation(rs):
+    a, a1, b1, b2, b3, b4 = 0.031091, 0.21370, 7.5957, 3.5876, 1.6382, 0.49294
+    q = 2 * a * (b1 * rs ** 0.5 + b2 * rs + b3 * rs ** 1.5 + b4 * rs ** 2)
+    assert abs(_eps_c(2, rs) - (-2 * a * (1 + a1 * rs) * math.log(1 + 1 / q))) < 1e-6
+
+
+@pytest.mark.parametrize("rho", [0.01, 0.1, 1.0])
+def test_pbe_large_gradient_limit(rho):
+    kf = (3 * math.pi ** 2 * rho) ** (1 / 3)
+    s = 1e4
+    sigma = (2 * kf * rho * s) ** 2
+    assert abs(xc_point(2, rho, sigma)[0] / _ex_lda(rho) - 1.804) < 1e-4
+
+
+@pytest.mark.parametrize("s", [0.5, 1.0, 2.0])
+def test_pbe_exchange_enhancement(s):
+    rho = 1e8  # t >> s: H cancels eps_c, and eps_c << eps_x
+    kf = (3 * math.pi ** 2 * rho) ** (1 / 3)
+    fx = 1.804 - 0.804 / (1 + 0.2195149727645171 * s * s / 0.804)
+    assert abs(xc_point(2, rho, (2 * kf * rho * s) ** 2)[0] / _ex_lda(rho) - fx) < 3e-4
+
+
+@pytest.mark.parametrize("rho", [0.01, 0.1, 1.0])
+def test_pbe_gradient_terms_cancel_at_second_order(rho):
+    kf = (3 * math.pi ** 2 * rho) ** (1 / 3)
+    ks = math.sqrt(4 * kf / math.pi)
+    exch = _ex_lda(rho) * 0.2195149727645171 / (4 * kf * kf * rho * rho)  # mu s^2
+    corr = 0.06672455060314922 / (4 * ks * ks * rho)  # rho beta t^2
+    assert abs(exch + corr) < 1e-6 * abs(exch)
+    sigma = 1e-8 * (2 * kf * rho) ** 2
+    got = (xc_point(2, rho, sigma)[0] - xc_point(2, rho, 0.0)[0]) / sigma
+    assert abs(got) < 1e-4 * abs(exch)
