@@ -737,7 +737,7 @@ template <typename C> static int density_groups(amdk_ctx *c, int T) {
     auto run = [&](int grp) {
       launch_pencil_density<C>(c, 0, T, grp, 0);
       k_rho_reduce_p<<<dim3((g.n1 + 31) / 32, (g.n1 + 31) / 32, g.n1), dim3(32, 8), 0, c->st>>>(
-          g.n1, c->pn1, c->pn2, grp, c->d_rhopart, c->d_rho);
+          g.n1, g.n1, c->pn1, c->pn2, grp, c->d_rhopart, c->d_rho, 0);
     };
     const int cands[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16};
     for (int grp : cands) {
@@ -796,7 +796,7 @@ template <typename C> static int density_pairs_t(amdk_ctx *c) {
     }
     ++c->nlaunch;
     k_rho_reduce_p<<<dim3((g.n1 + 31) / 32, (g.n1 + 31) / 32, g.n1), dim3(32, 8), 0, c->st>>>(
-        g.n1, c->pn1, c->pn2, ng, c->d_rhopart, c->d_rho);
+        g.n1, g.n1, c->pn1, c->pn2, ng, c->d_rhopart, c->d_rho, 0);
     if (h.lsd) {
       // open shell: the spin-2 density from the same pair transforms, weighted
       // by the spin-2 bands only (density.f90:64-76); with all pairs in one
@@ -814,7 +814,7 @@ template <typename C> static int density_pairs_t(amdk_ctx *c) {
       std::swap(c->d_wb, c->d_wb2);
       ++c->nlaunch;
       k_rho_reduce_p<<<dim3((g.n1 + 31) / 32, (g.n1 + 31) / 32, g.n1), dim3(32, 8), 0, c->st>>>(
-          g.n1, c->pn1, c->pn2, ng, c->d_rhopart, c->d_rho2);
+          g.n1, g.n1, c->pn1, c->pn2, ng, c->d_rhopart, c->d_rho2, 0);
     }
   } else {
   CK(cudaMemsetAsync(c->d_rho, 0, sizeof(double) * (size_t)g.n1 * g.n2 * g.n3, c->st));
@@ -867,9 +867,9 @@ static int store_potential(amdk_ctx *c, const double2 *grid, double *vpot, void 
     dim3 gt((g.n1 + 31) / 32, (g.n1 + 31) / 32, g.n1);
     ++c->nlaunch;
     if (c->precision == AMDK_MIXED)
-      k_v_permute<float><<<gt, dim3(32, 8), 0, c->st>>>(g.n1, c->pn1, c->pn2, vpot, (float *)vt);
+      k_v_permute<float><<<gt, dim3(32, 8), 0, c->st>>>(g.n1, g.n1, c->pn1, c->pn2, vpot, (float *)vt);
     else
-      k_v_permute<double><<<gt, dim3(32, 8), 0, c->st>>>(g.n1, c->pn1, c->pn2, vpot, (double *)vt);
+      k_v_permute<double><<<gt, dim3(32, 8), 0, c->st>>>(g.n1, g.n1, c->pn1, c->pn2, vpot, (double *)vt);
   }
   return 0;
 }
@@ -974,7 +974,7 @@ template <typename C> static void unpack_h(amdk_ctx *c, int p0, int T, const int
   const dim3 gu(nblk(h.ngpw, 128), (T + PAIRS - 1) / PAIRS);
   k_unpack_fnonloc<C><<<gu, 128, (size_t)2 * PAIRS * npj0 * sizeof(Rl), c->st>>>(
       h.ngpw, c->nstate, 2 * p0, T, npj0, pp, pm, (const C *)c->d_rb, rstride(c, 0), scale, c->d_hg, h.tpiba2,
-      c->d_occ, c->d_P, c->d_D, c->nproj, c->d_c0, c->d_c2, c->nproj > npj0 ? nullptr : bmax);
+      c->d_occ, c->d_P, c->d_D, c->nproj, c->d_c0, c->d_c2, c->nproj > npj0 ? nullptr : bmax, 0);
   // with projector chunks still to add, C2 is sliced from scratch
   c->c2max_ok = bmax != nullptr && c->nproj <= npj0;
   for (int j0 = npj0; j0 < c->nproj; j0 += UNPACK_NPJ) {
@@ -1570,6 +1570,36 @@ static void set_pair_precision(amdk_ctx *c, int prec) {
   c->ns_dens = c->nsd_p[q];
 }
 
+// Ray coordinates (ky, kz) of the density-sphere x-rays in the reference's
+// ray numbering (the wavefunction sphere's rays first), and per G vector of
+// the density half sphere the position ray*n1 + kx of +G and of -G
+// (prepare_fft, fft_interface.f90:262-293).
+static void ray_tables(const HostSetup &h, std::vector<int> &ray_ky, std::vector<int> &ray_kz, std::vector<int> &posp,
+                       std::vector<int> &posm) {
+  const int n1 = h.nr[0], n2 = h.nr[1], n3 = h.nr[2];
+  const int nh1 = n1 / 2 + 1, nh2 = n2 / 2 + 1, nh3 = n3 / 2 + 1;
+  ray_ky.assign(h.nhrays, 0);
+  ray_kz.assign(h.nhrays, 0);
+  for (int r = 0; r < h.nhrays; r++) {
+    int m = h.msp[r] - 1;
+    int i = m % h.nrl[1] + 1, j = m / h.nrl[1] + 1;
+    int iy = i - nh2, iz = j - nh3;
+    ray_ky[r] = ((iy % n2) + n2) % n2;
+    ray_kz[r] = ((iz % n3) + n3) % n3;
+  }
+  posp.assign(h.ngrho, 0);
+  posm.assign(h.ngrho, 0);
+  for (int ig = 0; ig < h.ngrho; ig++) {
+    int i1 = h.inyh[3L * ig], i2 = h.inyh[3L * ig + 1], i3 = h.inyh[3L * ig + 2];
+    int ix = i1 - nh1;
+    int rp = h.xrays[(i2 - 1) + (size_t)h.nrl[1] * (i3 - 1)] - 1;
+    int rm = h.xrays[(-i2 + 2 * nh2 - 1) + (size_t)h.nrl[1] * (-i3 + 2 * nh3 - 1)] - 1;
+    int kxp = ((ix % n1) + n1) % n1, kxm = ((-ix % n1) + n1) % n1;
+    posp[ig] = rp * n1 + kxp;
+    posm[ig] = rm * n1 + kxm;
+  }
+}
+
 static int build_device(amdk_ctx *c) {
   HostSetup &h = c->hs;
   Geom &g = c->geom;
@@ -1581,25 +1611,10 @@ static int build_device(amdk_ctx *c) {
   g.nray[0] = h.ngrays;
   g.nray[1] = h.nhrays;
   int n1 = g.n1, n2 = g.n2, n3 = g.n3;
-  int nh1 = n1 / 2 + 1, nh2 = n2 / 2 + 1, nh3 = n3 / 2 + 1;
-  // ray coordinates from the reference's ray numbering
-  std::vector<int> ray_ky(h.nhrays), ray_kz(h.nhrays);
-  for (int r = 0; r < h.nhrays; r++) {
-    int m = h.msp[r] - 1;
-    int i = m % h.nrl[1] + 1, j = m / h.nrl[1] + 1;
-    int iy = i - nh2, iz = j - nh3;
-    ray_ky[r] = ((iy % n2) + n2) % n2;
-    ray_kz[r] = ((iz % n3) + n3) % n3;
-  }
-  std::vector<int> gmap((size_t)h.nhrays * n1, 0), posp(h.ngrho), posm(h.ngrho);
+  std::vector<int> ray_ky, ray_kz, posp, posm;
+  ray_tables(h, ray_ky, ray_kz, posp, posm);
+  std::vector<int> gmap((size_t)h.nhrays * n1, 0);
   for (int ig = 0; ig < h.ngrho; ig++) {
-    int i1 = h.inyh[3L * ig], i2 = h.inyh[3L * ig + 1], i3 = h.inyh[3L * ig + 2];
-    int ix = i1 - nh1;
-    int rp = h.xrays[(i2 - 1) + (size_t)h.nrl[1] * (i3 - 1)] - 1;
-    int rm = h.xrays[(-i2 + 2 * nh2 - 1) + (size_t)h.nrl[1] * (-i3 + 2 * nh3 - 1)] - 1;
-    int kxp = ((ix % n1) + n1) % n1, kxm = ((-ix % n1) + n1) % n1;
-    posp[ig] = rp * n1 + kxp;
-    posm[ig] = rm * n1 + kxm;
     if (ig != 0) gmap[(size_t)posm[ig]] = -(ig + 1);
     gmap[(size_t)posp[ig]] = ig + 1;
   }
@@ -1797,7 +1812,7 @@ static int build_device(amdk_ctx *c) {
     for (int r = 0; r < h.ngrays; r++)
       for (int k = 0; k < n1; k++) gmapt[(size_t)k * h.ngrays + r] = gmap[(size_t)r * n1 + k];
     RC(c->up(&c->d_gmapt, gmapt));
-    c->pg = PencilGeom{n1, n2, n3, h.ngrays, g.nz[0], c->d_rpos, c->d_zinv, c->d_zlist[0], c->d_gmapt};
+    c->pg = pencil_geom_1gpu(n1, n2, n3, h.ngrays, g.nz[0], c->d_rpos, c->d_zinv, c->d_zlist[0], c->d_gmapt);
     c->pencil_groups = std::max(1, std::min(c->batch, 16));
     if (c->pd_p[0] || c->pd_p[1]) RC(c->alloc(&c->d_rhopart, (size_t)c->pencil_groups * npt));
     if (c->pv_p[0] || c->pv_p[1]) {
@@ -2123,6 +2138,314 @@ static int ensemble_parent(amdk_ensemble *E, const std::vector<std::array<int, 4
   CK(e);
   E->parents.emplace(keys, exec);
   *out = exec;
+  return 0;
+}
+
+// ------------------------------------------------------------------ slab decomposition
+// The band-pair transforms distributed over nranks processes as the
+// reference distributes its FFTs (fft_interface.f90:109-137: x-rays in G
+// space per rank, an all-to-all, contiguous x planes per rank in real space).
+// G vectors go to ranks with their x-ray, the rays in mirror pairs
+// {(ky, kz), (-ky, -kz)} so that +G and -G of every owned G lie on the rank's
+// rays (the pair pack and unpack then need no remote coefficient); pairs are
+// placed largest first on the rank with the fewest G vectors so far (ties:
+// fewer rays, then the lower rank).  The x planes are split into contiguous
+// ranges of n1/nranks (rounded down at each boundary).
+static int slab_partition(const HostSetup &h, int nranks, const std::vector<int> &ray_ky,
+                          const std::vector<int> &ray_kz, const std::vector<int> &posp, std::vector<int> &ray_owner,
+                          std::vector<int> &plane0) {
+  const int n1 = h.nr[0], n2 = h.nr[1], n3 = h.nr[2], R = h.ngrays;
+  if (nranks < 1 || nranks > PG_MAXSEG || nranks > n1) {
+    set_error("slab decomposition: nranks must be 1.." + std::to_string(std::min(PG_MAXSEG, n1)));
+    return AMDK_ERR_BADARG;
+  }
+  std::vector<long> ng(R, 0);
+  for (int ig = 0; ig < h.ngpw; ig++) ng[posp[ig] / n1]++;
+  std::vector<int> at((size_t)n2 * n3, -1);
+  for (int r = 0; r < R; r++) at[(size_t)ray_kz[r] * n2 + ray_ky[r]] = r;
+  struct Cls {
+    int r, m;
+    long g;
+  };
+  std::vector<Cls> cls;
+  for (int r = 0; r < R; r++) {
+    const int m = at[(size_t)((n3 - ray_kz[r]) % n3) * n2 + (n2 - ray_ky[r]) % n2];
+    if (m < 0) {
+      set_error("slab decomposition: the wavefunction rays are not closed under G -> -G");
+      return AMDK_ERR_UNSUPPORTED;
+    }
+    if (r <= m) cls.push_back({r, m, ng[r] + (m != r ? ng[m] : 0)});
+  }
+  if ((int)cls.size() < nranks) {
+    set_error("slab decomposition: fewer ray pairs than ranks");
+    return AMDK_ERR_BADARG;
+  }
+  std::stable_sort(cls.begin(), cls.end(), [](const Cls &a, const Cls &b) { return a.g > b.g; });
+  std::vector<long> gl(nranks, 0), rl(nranks, 0);
+  ray_owner.assign(R, -1);
+  for (const Cls &k : cls) {
+    int best = 0;
+    for (int q = 1; q < nranks; q++)
+      if (gl[q] < gl[best] || (gl[q] == gl[best] && rl[q] < rl[best])) best = q;
+    ray_owner[k.r] = best;
+    ray_owner[k.m] = best;
+    gl[best] += k.g;
+    rl[best] += (k.m != k.r) ? 2 : 1;
+  }
+  plane0.assign(nranks + 1, 0);
+  for (int q = 0; q <= nranks; q++) plane0[q] = (int)((long)q * n1 / nranks);
+  return 0;
+}
+
+struct amdk_slab {
+  amdk_ctx *c = nullptr;
+  int nranks = 1, rank = 0, precision = AMDK_FP64;
+  int ng = 0, nray_loc = 0, gzero = -1, nplane = 0, nray = 0;
+  std::vector<int> plane0, seg_r0, local_g;
+  // sender side: local G code of (kx, local ray), planes and local rays of
+  // each local G's +G / -G position, |G|^2; receiver side: rpos of every ray
+  // in owner order
+  int *d_gmapt = nullptr, *d_kxp = nullptr, *d_rlp = nullptr, *d_kxm = nullptr, *d_rlm = nullptr;
+  int *d_pp = nullptr, *d_pm = nullptr, *d_rpos = nullptr;
+  double *d_hg = nullptr, *d_rhopart = nullptr;
+  void *d_vp = nullptr;
+  int pos_T = -1, groups_max = 8;
+  std::vector<void *> allocs;
+  template <typename T> int alloc(T **p, size_t n) {
+    RC(dalloc(p, n));
+    allocs.push_back((void *)*p);
+    return 0;
+  }
+  template <typename T> int up(T **p, const std::vector<T> &v) {
+    RC(amdk::upload(p, v));
+    allocs.push_back((void *)*p);
+    return 0;
+  }
+  ~amdk_slab() {
+    for (void *p : allocs) cudaFree(p);
+  }
+};
+
+static int slab_create(amdk_ctx *c, int nranks, int rank, amdk_slab *s) {
+  const HostSetup &h = c->hs;
+  const int q = (c->precision == AMDK_MIXED) ? 1 : 0;
+  if (h.lsd) {
+    set_error("slab decomposition: the open-shell branch is not distributed");
+    return AMDK_ERR_UNSUPPORTED;
+  }
+  if (!(c->pv_p[q] && c->pd_p[q])) {
+    set_error("slab decomposition: needs the pencil transforms of this grid at the context's precision");
+    return AMDK_ERR_UNSUPPORTED;
+  }
+  if (rank < 0 || rank >= nranks) {
+    set_error("slab decomposition: rank out of range");
+    return AMDK_ERR_BADARG;
+  }
+  const int n1 = h.nr[0], n2 = h.nr[1];
+  std::vector<int> ray_ky, ray_kz, posp, posm, owner;
+  ray_tables(h, ray_ky, ray_kz, posp, posm);
+  RC(slab_partition(h, nranks, ray_ky, ray_kz, posp, owner, s->plane0));
+  s->c = c;
+  s->nranks = nranks;
+  s->rank = rank;
+  s->precision = c->precision;
+  s->nray = h.ngrays;
+  s->nplane = s->plane0[rank + 1] - s->plane0[rank];
+  // rays in owner order (increasing ray number within an owner): the
+  // receiver's segments, and the sender's local ray numbering
+  std::vector<int> order, rloc(h.ngrays, -1);
+  s->seg_r0.assign(nranks + 1, 0);
+  for (int o = 0; o < nranks; o++) {
+    s->seg_r0[o] = (int)order.size();
+    int k = 0;
+    for (int r = 0; r < h.ngrays; r++)
+      if (owner[r] == o) {
+        order.push_back(r);
+        rloc[r] = k++;
+      }
+  }
+  s->seg_r0[nranks] = (int)order.size();
+  s->nray_loc = s->seg_r0[rank + 1] - s->seg_r0[rank];
+  // the ray's plane position, as in the one-GPU pencil tables
+  std::vector<int> zl0(c->geom.nz[0]), zinv(h.nr[2], -1), rpos(h.ngrays);
+  CK(cudaMemcpy(zl0.data(), c->d_zlist[0], sizeof(int) * zl0.size(), cudaMemcpyDeviceToHost));
+  for (int zi = 0; zi < (int)zl0.size(); zi++) zinv[zl0[zi]] = zi;
+  for (int j = 0; j < h.ngrays; j++) rpos[j] = zinv[ray_kz[order[j]]] * (n2 + 1) + ray_ky[order[j]];
+  RC(s->up(&s->d_rpos, rpos));
+  // local G vectors (increasing global index) and their tables
+  const int R = s->nray_loc;
+  std::vector<int> gmapt((size_t)n1 * std::max(R, 1), 0), kxp, rlp, kxm, rlm;
+  std::vector<double> hg;
+  for (int ig = 0; ig < h.ngpw; ig++) {
+    const int rp = posp[ig] / n1;
+    if (owner[rp] != rank) continue;
+    const int il = (int)s->local_g.size(), rm = posm[ig] / n1;
+    s->local_g.push_back(ig);
+    kxp.push_back(posp[ig] % n1);
+    rlp.push_back(rloc[rp]);
+    kxm.push_back(posm[ig] % n1);
+    rlm.push_back(rloc[rm]);
+    hg.push_back(h.hg[ig]);
+    if (ig == 0) s->gzero = il;
+    if (ig != 0) gmapt[(size_t)(posm[ig] % n1) * R + rloc[rm]] = -(il + 1);
+    gmapt[(size_t)(posp[ig] % n1) * R + rloc[rp]] = il + 1;
+  }
+  s->ng = (int)s->local_g.size();
+  RC(s->up(&s->d_gmapt, gmapt));
+  RC(s->up(&s->d_kxp, kxp));
+  RC(s->up(&s->d_rlp, rlp));
+  RC(s->up(&s->d_kxm, kxm));
+  RC(s->up(&s->d_rlm, rlm));
+  RC(s->up(&s->d_hg, hg));
+  RC(s->alloc(&s->d_pp, std::max(s->ng, 1)));
+  RC(s->alloc(&s->d_pm, std::max(s->ng, 1)));
+  const size_t pl = (size_t)s->nplane * n1 * n1;  // cubic grid (pencil path)
+  RC(s->alloc(&s->d_rhopart, (size_t)s->groups_max * pl));
+  char *vp;
+  RC(s->alloc(&vp, pl * sizeof(double)));
+  s->d_vp = vp;
+  return 0;
+}
+
+static cudaStream_t slab_stream(const amdk_slab *s, void *stream) {
+  return stream ? (cudaStream_t)stream : s->c->st;
+}
+static int slab_check_pairs(const amdk_slab *s, int band0, int npairs) {
+  const int nst = s->c->nstate;
+  if (band0 < 0 || (band0 & 1) || npairs < 1 || band0 + 2 * (npairs - 1) >= nst) {
+    set_error("slab transform: band0 must be even and the pairs within the bands");
+    return AMDK_ERR_BADARG;
+  }
+  if (npairs > 65535 || (long)npairs * s->nray * s->c->hs.nr[0] > (long)INT32_MAX) {
+    set_error("slab transform: too many pairs in one call for 32-bit positions");
+    return AMDK_ERR_BADARG;
+  }
+  return 0;
+}
+// sender side: local rays, layout [kx][t][ray] (rank-major send order)
+static PencilGeom slab_xgeom(const amdk_slab *s, int T) {
+  const HostSetup &h = s->c->hs;
+  PencilGeom g = pencil_geom_1gpu(h.nr[0], h.nr[1], h.nr[2], s->nray_loc, s->c->geom.nz[0], nullptr, nullptr, nullptr,
+                                  s->d_gmapt);
+  g.xt_t = s->nray_loc;
+  g.xt_x = (long)T * s->nray_loc;
+  return g;
+}
+// receiver side: this rank's planes, every ray, one segment per source rank
+static PencilGeom slab_pgeom(const amdk_slab *s, int T) {
+  const HostSetup &h = s->c->hs;
+  PencilGeom g = pencil_geom_1gpu(s->nplane, h.nr[1], h.nr[2], s->nray, s->c->geom.nz[0], s->d_rpos, s->c->d_zinv,
+                                  s->c->d_zlist[0], nullptr);
+  g.pr_t = 1;
+  g.pr_x = T;
+  g.nseg = s->nranks;
+  g.seg_mul = (long)s->nplane * T;
+  for (int o = 0; o <= s->nranks; o++) g.seg_r0[o] = s->seg_r0[o];
+  return g;
+}
+
+template <typename C>
+static int slab_pairs_out_t(amdk_slab *s, const double2 *c0, int band0, int T, C *send, cudaStream_t st) {
+  amdk_ctx *c = s->c;
+  const PencilGeom gx = slab_xgeom(s, T);
+  const long lines = (long)T * s->nray_loc;
+  if (lines == 0) return 0;
+  with_n(c->hs.nr[0], [&](auto NC) {
+    constexpr int N = decltype(NC)::value;
+    if constexpr (N > 0) {
+      smem_opt_in<k_xt_bwd_pair<C, N>>();
+      ++c->nlaunch;
+      constexpr int N2 = N / fft_n1(N);
+      k_xt_bwd_pair<C, N><<<nblk(lines, XL), XL * N2, xt_smem<C>(N), st>>>(c0, s->ng, c->nstate, band0, T, gx,
+                                                                          plan<C>(c, 0), send);
+    }
+  });
+  CK(cudaGetLastError());
+  return 0;
+}
+template <typename C> static int slab_vpsi_t(amdk_slab *s, C *recv, int T, const double *v, cudaStream_t st) {
+  typedef decltype(C().x) Rl;
+  amdk_ctx *c = s->c;
+  const int n = c->hs.nr[1], q = (s->precision == AMDK_MIXED) ? 1 : 0;
+  ++c->nlaunch;
+  k_v_permute<Rl><<<dim3((s->nplane + 31) / 32, (n + 31) / 32, n), dim3(32, 8), 0, st>>>(n, s->nplane, c->pn1, c->pn2,
+                                                                                      v, (Rl *)s->d_vp);
+  const PencilGeom gp = slab_pgeom(s, T);
+  const int ct = c->ctv_p[q];
+  with_n(n, [&](auto NC) {
+    constexpr int N = decltype(NC)::value;
+    if constexpr (N > 0) {
+      smem_opt_in<k_pencil_vpsi<C, N>>();
+      ++c->nlaunch;
+      k_pencil_vpsi<C, N><<<dim3(s->nplane, T), PNT, pencil_smem<C>(N, gp.nz, ct), st>>>(
+          gp, plan<C>(c, 1), recv, (const Rl *)s->d_vp, ct, nullptr, 0, 0, -1);
+    }
+  });
+  CK(cudaGetLastError());
+  return 0;
+}
+template <typename C, int N, int NS>
+static void slab_density_launch(amdk_slab *s, const C *recv, int band0, int T, int grp, int ct, cudaStream_t st) {
+  amdk_ctx *c = s->c;
+  const PencilGeom gp = slab_pgeom(s, T);
+  const int per = (T + grp - 1) / grp;
+  smem_opt_in<k_pencil_density<C, N, NS>>();
+  ++c->nlaunch;
+  k_pencil_density<C, N, NS><<<dim3(s->nplane, grp), PNT, pencil_smem<C>(N, gp.nz, ct), st>>>(
+      gp, plan<C>(c, 1), recv, T, per, c->d_wa + band0 / 2, c->d_wb + band0 / 2, s->d_rhopart, ct, 0);
+}
+template <typename C>
+static int slab_density_t(amdk_slab *s, const C *recv, int band0, int T, double *rho, int add, cudaStream_t st) {
+  amdk_ctx *c = s->c;
+  const int n = c->hs.nr[1], q = (s->precision == AMDK_MIXED) ? 1 : 0;
+  const int ct = c->ctd_p[q], ns = c->nsd_p[q];
+  // pair groups: enough blocks for two waves, at most groups_max grids
+  int grp = std::max(1, std::min({T, s->groups_max, (2 * c->nsm + s->nplane - 1) / s->nplane}));
+  const int per = (T + grp - 1) / grp;
+  grp = (T + per - 1) / per;  // no empty group
+  with_n(n, [&](auto NC) {
+    constexpr int N = decltype(NC)::value;
+    if constexpr (N > 0) {
+      if (ns == 1) slab_density_launch<C, N, 1>(s, recv, band0, T, grp, ct, st);
+      else if (ns == 2) slab_density_launch<C, N, 2>(s, recv, band0, T, grp, ct, st);
+      else slab_density_launch<C, N, 4>(s, recv, band0, T, grp, ct, st);
+    }
+  });
+  ++c->nlaunch;
+  k_rho_reduce_p<<<dim3((n + 31) / 32, (s->nplane + 31) / 32, n), dim3(32, 8), 0, st>>>(
+      n, s->nplane, c->pn1, c->pn2, grp, s->d_rhopart, rho, add);
+  CK(cudaGetLastError());
+  return 0;
+}
+template <typename C>
+static int slab_pairs_in_t(amdk_slab *s, C *back, const double2 *c0, int band0, int T, double2 *c2, cudaStream_t st) {
+  amdk_ctx *c = s->c;
+  const HostSetup &h = c->hs;
+  const long lines = (long)T * s->nray_loc;
+  if (lines == 0 || s->ng == 0) return 0;
+  if (s->pos_T != T) {
+    ++c->nlaunch;
+    k_slab_pos<<<nblk(s->ng), NTHR, 0, st>>>(s->ng, s->d_kxp, s->d_rlp, s->d_kxm, s->d_rlm, (long)T * s->nray_loc,
+                                             s->d_pp, s->d_pm);
+    s->pos_T = T;
+  }
+  const PencilGeom gx = slab_xgeom(s, T);
+  with_n(h.nr[0], [&](auto NC) {
+    constexpr int N = decltype(NC)::value;
+    if constexpr (N > 0) {
+      smem_opt_in<k_xt_fwd<C, N>>();
+      ++c->nlaunch;
+      constexpr int N2 = N / fft_n1(N);
+      k_xt_fwd<C, N><<<nblk(lines, XL), XL * N2, xt_smem<C>(N), st>>>(T, gx, plan<C>(c, 0), back);
+    }
+  });
+  const double scale = 1.0 / ((double)h.nr[0] * h.nr[1] * h.nr[2]);
+  constexpr int PAIRS = unpack_pairs<C>();
+  ++c->nlaunch;
+  k_unpack_fnonloc<C><<<dim3(nblk(s->ng, 128), (T + PAIRS - 1) / PAIRS), 128, 0, st>>>(
+      s->ng, c->nstate, band0, T, 0, s->d_pp, s->d_pm, back, s->nray_loc, scale, s->d_hg, h.tpiba2, c->d_occ, nullptr,
+      nullptr, 0, c0, c2, nullptr, s->gzero);
+  CK(cudaGetLastError());
   return 0;
 }
 
@@ -2735,6 +3058,121 @@ int amdk_launch_count(amdk_ctx *c, long *n) {
 int amdk_last_iteration_ms(amdk_ctx *c, double *ms) {
   if (!c || !ms) return AMDK_ERR_BADARG;
   *ms = c->last_ms;
+  return 0;
+}
+
+// ------------------------------------------------------------------ slab decomposition entries
+int amdk_slab_layout(const amdk_system *sys, int nranks, int *g_owner, int *plane0) {
+  if (!sys) {
+    set_error("amdk_slab_layout: null system");
+    return AMDK_ERR_BADARG;
+  }
+  HostSetup h;
+  RC(host_setup(sys, h, true));
+  std::vector<int> ray_ky, ray_kz, posp, posm, owner, p0;
+  ray_tables(h, ray_ky, ray_kz, posp, posm);
+  RC(slab_partition(h, nranks, ray_ky, ray_kz, posp, owner, p0));
+  if (g_owner)
+    for (int ig = 0; ig < h.ngpw; ig++) g_owner[ig] = owner[posp[ig] / h.nr[0]];
+  if (plane0) std::memcpy(plane0, p0.data(), sizeof(int) * p0.size());
+  return 0;
+}
+
+int amdk_slab_create(amdk_ctx *c, int nranks, int rank, amdk_slab **out) {
+  if (!c || !out) {
+    set_error("amdk_slab_create: null argument");
+    return AMDK_ERR_BADARG;
+  }
+  *out = nullptr;
+  CK(cudaSetDevice(c->device));
+  amdk_slab *s = new (std::nothrow) amdk_slab();
+  if (!s) return AMDK_ERR_ALLOC;
+  const int rc = slab_create(c, nranks, rank, s);
+  if (rc) {
+    delete s;
+    return rc;
+  }
+  *out = s;
+  return 0;
+}
+
+int amdk_slab_info_get(amdk_slab *s, amdk_slab_info *info) {
+  if (!s || !info) return AMDK_ERR_BADARG;
+  std::memset(info, 0, sizeof(*info));
+  info->nranks = s->nranks;
+  info->rank = s->rank;
+  info->ngpw_local = s->ng;
+  info->nray_local = s->nray_loc;
+  info->plane0 = s->plane0[s->rank];
+  info->nplane = s->nplane;
+  info->gzero_local = s->gzero;
+  info->elem_bytes = (s->precision == AMDK_MIXED) ? (int)sizeof(float2) : (int)sizeof(double2);
+  for (int o = 0; o < s->nranks; o++) {
+    info->send_elems[o] = (long)(s->plane0[o + 1] - s->plane0[o]) * s->nray_loc;
+    info->recv_elems[o] = (long)s->nplane * (s->seg_r0[o + 1] - s->seg_r0[o]);
+  }
+  return 0;
+}
+
+int amdk_slab_local_g(amdk_slab *s, int *ig) {
+  if (!s || !ig) return AMDK_ERR_BADARG;
+  if (s->ng) std::memcpy(ig, s->local_g.data(), sizeof(int) * s->ng);
+  return 0;
+}
+
+// the call's stream, or the context's stream with the call waited for
+static int slab_finish(amdk_slab *s, void *stream) {
+  if (!stream) CK(cudaStreamSynchronize(s->c->st));
+  return 0;
+}
+
+int amdk_slab_pairs_out(amdk_slab *s, const double *c0, int band0, int npairs, void *send, void *stream) {
+  if (!s || !c0 || !send) return AMDK_ERR_BADARG;
+  RC(slab_check_pairs(s, band0, npairs));
+  CK(cudaSetDevice(s->c->device));
+  const cudaStream_t st = slab_stream(s, stream);
+  if (s->precision == AMDK_MIXED) RC(slab_pairs_out_t<float2>(s, (const double2 *)c0, band0, npairs, (float2 *)send, st));
+  else RC(slab_pairs_out_t<double2>(s, (const double2 *)c0, band0, npairs, (double2 *)send, st));
+  return slab_finish(s, stream);
+}
+
+int amdk_slab_planes_vpsi(amdk_slab *s, void *recv, int npairs, const double *v, void *stream) {
+  if (!s || !recv || !v) return AMDK_ERR_BADARG;
+  RC(slab_check_pairs(s, 0, npairs));
+  CK(cudaSetDevice(s->c->device));
+  const cudaStream_t st = slab_stream(s, stream);
+  if (s->precision == AMDK_MIXED) RC(slab_vpsi_t<float2>(s, (float2 *)recv, npairs, v, st));
+  else RC(slab_vpsi_t<double2>(s, (double2 *)recv, npairs, v, st));
+  return slab_finish(s, stream);
+}
+
+int amdk_slab_planes_density(amdk_slab *s, const void *recv, int band0, int npairs, double *rho, int accumulate,
+                             void *stream) {
+  if (!s || !recv || !rho) return AMDK_ERR_BADARG;
+  RC(slab_check_pairs(s, band0, npairs));
+  CK(cudaSetDevice(s->c->device));
+  const cudaStream_t st = slab_stream(s, stream);
+  if (s->precision == AMDK_MIXED) RC(slab_density_t<float2>(s, (const float2 *)recv, band0, npairs, rho, accumulate, st));
+  else RC(slab_density_t<double2>(s, (const double2 *)recv, band0, npairs, rho, accumulate, st));
+  return slab_finish(s, stream);
+}
+
+int amdk_slab_pairs_in(amdk_slab *s, void *back, const double *c0, int band0, int npairs, double *c2, void *stream) {
+  if (!s || !back || !c0 || !c2) return AMDK_ERR_BADARG;
+  RC(slab_check_pairs(s, band0, npairs));
+  CK(cudaSetDevice(s->c->device));
+  const cudaStream_t st = slab_stream(s, stream);
+  if (s->precision == AMDK_MIXED)
+    RC(slab_pairs_in_t<float2>(s, (float2 *)back, (const double2 *)c0, band0, npairs, (double2 *)c2, st));
+  else RC(slab_pairs_in_t<double2>(s, (double2 *)back, (const double2 *)c0, band0, npairs, (double2 *)c2, st));
+  return slab_finish(s, stream);
+}
+
+int amdk_slab_destroy(amdk_slab *s) {
+  if (!s) return 0;
+  cudaSetDevice(s->c->device);
+  cudaDeviceSynchronize();
+  delete s;
   return 0;
 }
 

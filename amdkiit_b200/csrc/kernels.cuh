@@ -533,6 +533,8 @@ __global__ void k_xc_combine(int ngrho, int gga, const int *pos_p, const int *po
 // (the int8 slice products of the mixed path) the kernel also records each
 // band's max |Re|, |Im| of C2 (atomic max of the FP64 bits, non-negative
 // values), which the slicing of C2 needs, so C2 is not read once more for it.
+// gzero: index of G = 0 among the ngpw G vectors (0; -1 for a rank of the
+// slab decomposition that does not own it).
 constexpr int UNPACK_NPJ = 32;
 template <typename C> __host__ __device__ constexpr int unpack_pairs() { return sizeof(C) == sizeof(float2) ? 8 : 4; }
 template <typename C>
@@ -543,7 +545,7 @@ __global__ void __launch_bounds__(128) k_unpack_fnonloc(int ngpw, int nstate, in
                                                         const double *__restrict__ occ, const double2 *__restrict__ P,
                                                         const double *__restrict__ D, int nproj,
                                                         const double2 *__restrict__ c0, double2 *__restrict__ c2,
-                                                        unsigned long long *__restrict__ bmax) {
+                                                        unsigned long long *__restrict__ bmax, int gzero) {
   typedef decltype(C().x) Rl;
   constexpr int PAIRS = unpack_pairs<C>(), NB = 2 * PAIRS;
   __shared__ double red[4][NB];  // per-warp band maxima (128 threads)
@@ -563,7 +565,7 @@ __global__ void __launch_bounds__(128) k_unpack_fnonloc(int ngpw, int nstate, in
   C acc[NB];
 #pragma unroll
   for (int b = 0; b < NB; ++b) acc[b] = czero<C>();
-  const double gw = (g == 0) ? 2.0 : 1.0;
+  const double gw = (g == gzero) ? 2.0 : 1.0;
 #pragma unroll 4
   for (int j = 0; j < npj; ++j) {
     const double2 v = P[(long)j * ngpw + g];

@@ -17,13 +17,54 @@
 
 namespace amdk {
 
+constexpr int PG_MAXSEG = 16;  // source ranks of a slab-decomposed plane buffer
 struct PencilGeom {
-  int n1, n2, n3, nray, nz;
+  int n1, n2, n3, nray, nz;  // n1: x planes of the buffers the plane kernels read
   const int *rpos;   // [nray] zi*(n2+1) + ky of the ray in the padded plane
   const int *zinv;   // [n3] slab index of kz, -1 outside the slab
   const int *zlist;  // [nz] kz of slab plane
   const int *gmapt;  // [n1][nray] G code of (ray, kx): +(ig+1) at +G, -(ig+1) at -G, 0 empty
+  // x passes: element kx of the line (pair t, ray r) at t*xt_t + kx*xt_x + r
+  long xt_t, xt_x;
+  // plane kernels: the rays of plane kx of pair t form row pr = t*pr_t +
+  // kx*pr_x of nseg segments; segment s holds rays seg_r0[s] .. seg_r0[s+1]-1
+  // (in rpos order), its row pr at seg_mul*seg_r0[s] + pr*(its ray count).
+  // One GPU: one segment, row pr = t*n1 + kx of nray rays.  Slab
+  // decomposition: one segment per source rank, as the all-to-all leaves them.
+  int pr_t, pr_x, nseg;
+  long seg_mul;
+  int seg_r0[PG_MAXSEG + 1];
 };
+// the one-GPU layout RT[t][kx][ray]
+inline PencilGeom pencil_geom_1gpu(int n1, int n2, int n3, int nray, int nz, const int *rpos, const int *zinv,
+                                   const int *zlist, const int *gmapt) {
+  PencilGeom g{};
+  g.n1 = n1;
+  g.n2 = n2;
+  g.n3 = n3;
+  g.nray = nray;
+  g.nz = nz;
+  g.rpos = rpos;
+  g.zinv = zinv;
+  g.zlist = zlist;
+  g.gmapt = gmapt;
+  g.xt_t = (long)n1 * nray;
+  g.xt_x = nray;
+  g.pr_t = n1;
+  g.pr_x = 1;
+  g.nseg = 1;
+  g.seg_mul = 0;
+  g.seg_r0[0] = 0;
+  g.seg_r0[1] = nray;
+  return g;
+}
+// position of ray r of row pr in the plane kernels' buffer
+__device__ __forceinline__ long ray_at(const PencilGeom &pg, long pr, int r) {
+  int s = 0;
+  while (s + 1 < pg.nseg && r >= pg.seg_r0[s + 1]) ++s;
+  const int r0 = pg.seg_r0[s];
+  return pg.seg_mul * r0 + pr * (pg.seg_r0[s + 1] - r0) + (r - r0);
+}
 
 constexpr int PNT = 512;  // threads per pencil block
 // Shared-memory rows (slab plane P, column tile S, density accumulator) have
@@ -31,7 +72,8 @@ constexpr int PNT = 512;  // threads per pencil block
 
 constexpr int XL = 32;  // lines per x-pass block
 // Backward x pass with the band-pair pack (psi_a + i psi_b, the pack of
-// vpsi and eval_density), output transposed: RT[t][kx][r].  Block = XL lines
+// vpsi and eval_density), output transposed: RT[t][kx][r] on one GPU, the
+// slab decomposition's send layout [kx][t][r] (strides xt_t, xt_x).  Block = XL lines
 // (consecutive rays) x N2 threads; thread (l, j2) gathers the N1 elements
 // kx = j2 + N2*j1 of its ray straight from the coefficients, the second
 // phase writes kx = k1 + N1*k2 back with consecutive threads on consecutive
@@ -88,9 +130,9 @@ __global__ void __launch_bounds__(512) k_xt_bwd_pair(const double2 *__restrict__
     Dft<C, N2, 1>::run(u);
     if (line < nlines) {
       const int t = (int)(line / R), r = (int)(line % R);
-      C *o = rt + (long)t * pg.n1 * R + r;
+      C *o = rt + t * pg.xt_t + r;
 #pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) o[(long)(k1 + N1 * k2) * R] = u[k2];
+      for (int k2 = 0; k2 < N2; ++k2) o[(long)(k1 + N1 * k2) * pg.xt_x] = u[k2];
     }
   }
 }
@@ -113,9 +155,9 @@ __global__ void __launch_bounds__(512) k_xt_fwd(int T, PencilGeom pg, Plan<C> p,
     C v[N1];
     if (line < nlines) {
       const int t = (int)(line / R), r = (int)(line % R);
-      const C *in = rt + (long)t * pg.n1 * R + r;
+      const C *in = rt + t * pg.xt_t + r;
 #pragma unroll
-      for (int j1 = 0; j1 < N1; ++j1) v[j1] = in[(long)(j2 + N2 * j1) * R];
+      for (int j1 = 0; j1 < N1; ++j1) v[j1] = in[(long)(j2 + N2 * j1) * pg.xt_x];
     } else {
 #pragma unroll
       for (int j1 = 0; j1 < N1; ++j1) v[j1] = czero<C>();
@@ -135,9 +177,9 @@ __global__ void __launch_bounds__(512) k_xt_fwd(int T, PencilGeom pg, Plan<C> p,
     Dft<C, N2, -1>::run(u);
     if (line < nlines) {
       const int t = (int)(line / R), r = (int)(line % R);
-      C *o = rt + (long)t * pg.n1 * R + r;
+      C *o = rt + t * pg.xt_t + r;
 #pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) o[(long)(k1 + N1 * k2) * R] = u[k2];
+      for (int k2 = 0; k2 < N2; ++k2) o[(long)(k1 + N1 * k2) * pg.xt_x] = u[k2];
     }
   }
 }
@@ -219,12 +261,16 @@ __device__ __forceinline__ void rows_perm_to_nat(C *P, int nrow, const DivMod &d
   __syncthreads();
 }
 
-// scatter the rays of one x-plane into P (zero elsewhere)
+// scatter the rays of row pr (one x-plane of one pair) into P (zero elsewhere)
 template <typename C, int N>
-__device__ __forceinline__ void pencil_scatter(C *P, const C *__restrict__ rt_plane, const PencilGeom &pg) {
+__device__ __forceinline__ void pencil_scatter(C *P, const C *__restrict__ rt, long pr, const PencilGeom &pg) {
   for (int idx = threadIdx.x; idx < pg.nz * (N + 1); idx += blockDim.x) P[idx] = czero<C>();
   __syncthreads();
-  for (int r = threadIdx.x; r < pg.nray; r += blockDim.x) P[pg.rpos[r]] = rt_plane[r];
+  for (int s = 0; s < pg.nseg; ++s) {
+    const int r0 = pg.seg_r0[s], nr = pg.seg_r0[s + 1] - r0;
+    const C *src = rt + pg.seg_mul * r0 + pr * nr;
+    for (int j = threadIdx.x; j < nr; j += blockDim.x) P[pg.rpos[r0 + j]] = src[j];
+  }
   __syncthreads();
 }
 
@@ -315,8 +361,8 @@ __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C
   const uint4 *zp = sm.zp;
   sm.load(p, pg.zinv);
   const int kx = blockIdx.x, t = blockIdx.y;
-  C *plane = rt + ((long)t * pg.n1 + kx) * pg.nray;
-  pencil_scatter<C, N>(P, plane, pg);
+  const long pr = (long)t * pg.pr_t + (long)kx * pg.pr_x;
+  pencil_scatter<C, N>(P, rt, pr, pg);
   const DivMod dz(nz);
   rows_nat_to_perm<C, N, 1>(P, nz, dz, tw);
   const Rl *V = vp + (long)kx * N * N;
@@ -400,7 +446,11 @@ __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C
     __syncthreads();
   }
   rows_perm_to_nat<C, N, -1>(P, nz, dz, tw);
-  for (int r = threadIdx.x; r < pg.nray; r += blockDim.x) plane[r] = P[pg.rpos[r]];
+  for (int sg = 0; sg < pg.nseg; ++sg) {
+    const int r0 = pg.seg_r0[sg], nr = pg.seg_r0[sg + 1] - r0;
+    C *dst = rt + pg.seg_mul * r0 + pr * nr;
+    for (int j = threadIdx.x; j < nr; j += blockDim.x) dst[j] = P[pg.rpos[r0 + j]];
+  }
 }
 
 // Density: one x-plane for a group of band pairs (density.f90:49-86);
@@ -440,11 +490,11 @@ __global__ void __launch_bounds__(PNT, sizeof(C) == 8 ? 2 : 1) k_pencil_density(
   const bool pre = pg.nray <= PREF * (int)blockDim.x;
   C nxt[PREF];
   auto fetch = [&](int t) {
-    const C *pl = rt + ((long)t * pg.n1 + kx) * pg.nray;
+    const long pr = (long)t * pg.pr_t + (long)kx * pg.pr_x;
 #pragma unroll
     for (int i = 0; i < PREF; ++i) {
       const int r = threadIdx.x + i * blockDim.x;
-      nxt[i] = r < pg.nray ? pl[r] : czero<C>();
+      nxt[i] = r < pg.nray ? rt[ray_at(pg, pr, r)] : czero<C>();
     }
   };
   const DivMod dz(nz);
@@ -461,7 +511,7 @@ __global__ void __launch_bounds__(PNT, sizeof(C) == 8 ? 2 : 1) k_pencil_density(
       __syncthreads();
       if (t + 1 < t1) fetch(t + 1);
     } else {
-      pencil_scatter<C, N>(P, rt + ((long)t * pg.n1 + kx) * pg.nray, pg);
+      pencil_scatter<C, N>(P, rt, (long)t * pg.pr_t + (long)kx * pg.pr_x, pg);
     }
     rows_nat_to_perm<C, N, 1>(P, nz, dz, tw);
     const Rl fa = (Rl)wa[t], fb = (Rl)wb[t];
@@ -522,17 +572,18 @@ __global__ void __launch_bounds__(PNT, sizeof(C) == 8 ? 2 : 1) k_pencil_density(
 // index a + N1*b
 __device__ __forceinline__ int perm_index(int pos, int n1f, int n2f) { return pos / n2f + n1f * (pos % n2f); }
 
-// rho[kz][ky][kx] = sum over groups of rho_part[g][kx][q][k']
-__global__ void k_rho_reduce_p(int n, int n1f, int n2f, int ngroups, const double *__restrict__ part,
-                               double *__restrict__ rho) {
+// rho[kz][ky][kx] (=, or += with add) sum over groups of rho_part[g][kx][q][k'],
+// for nx x planes (n on one GPU, a rank's planes in the slab decomposition)
+__global__ void k_rho_reduce_p(int n, int nx, int n1f, int n2f, int ngroups, const double *__restrict__ part,
+                               double *__restrict__ rho, int add) {
   __shared__ double tile[32][33];
   const int q = blockIdx.z;
   const int k0 = blockIdx.x * 32, kx0 = blockIdx.y * 32;
-  const long gstride = (long)n * n * n;
+  const long gstride = (long)nx * n * n;
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
     const int kx = kx0 + j, k = k0 + threadIdx.x;
     double s = 0.0;
-    if (kx < n && k < n) {
+    if (kx < nx && k < n) {
       const double *pp = part + ((long)kx * n + q) * n + k;
       // the loads are independent: unrolled, several are in flight while the
       // sum keeps its group order
@@ -545,25 +596,42 @@ __global__ void k_rho_reduce_p(int n, int n1f, int n2f, int ngroups, const doubl
   const int ky = perm_index(q, n1f, n2f);
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
     const int k = k0 + j, kx = kx0 + threadIdx.x;
-    if (kx < n && k < n) rho[((long)perm_index(k, n1f, n2f) * n + ky) * n + kx] = tile[threadIdx.x][j];
+    if (kx < nx && k < n) {
+      double *o = rho + ((long)perm_index(k, n1f, n2f) * n + ky) * nx + kx;
+      *o = add ? *o + tile[threadIdx.x][j] : tile[threadIdx.x][j];
+    }
   }
 }
 
-// vp[kx][q][k'] (working precision) from V[kz][ky][kx] (FP64), permuted order
+// vp[kx][q][k'] (working precision) from V[kz][ky][kx] (FP64), permuted
+// order, for nx x planes
 template <typename Rl>
-__global__ void k_v_permute(int n, int n1f, int n2f, const double *__restrict__ v, Rl *__restrict__ vp) {
+__global__ void k_v_permute(int n, int nx, int n1f, int n2f, const double *__restrict__ v, Rl *__restrict__ vp) {
   __shared__ double tile[32][33];
   const int q = blockIdx.z;
   const int ky = perm_index(q, n1f, n2f);
   const int kx0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
     const int k = k0 + j, kx = kx0 + threadIdx.x;
-    tile[j][threadIdx.x] = (kx < n && k < n) ? v[((long)perm_index(k, n1f, n2f) * n + ky) * n + kx] : 0.0;
+    tile[j][threadIdx.x] = (kx < nx && k < n) ? v[((long)perm_index(k, n1f, n2f) * n + ky) * nx + kx] : 0.0;
   }
   __syncthreads();
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
     const int kx = kx0 + j, k = k0 + threadIdx.x;
-    if (kx < n && k < n) vp[((long)kx * n + q) * n + k] = (Rl)tile[threadIdx.x][j];
+    if (kx < nx && k < n) vp[((long)kx * n + q) * n + k] = (Rl)tile[threadIdx.x][j];
+  }
+}
+
+// Slab decomposition: the +G / -G positions of a rank's G vectors in its
+// send/return buffer [kx][t][local ray] for T pairs (row = T * local rays),
+// from the planes and local rays of the two positions
+__global__ void k_slab_pos(int ng, const int *__restrict__ kxp, const int *__restrict__ rlp,
+                           const int *__restrict__ kxm, const int *__restrict__ rlm, long row, int *__restrict__ pp,
+                           int *__restrict__ pm) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < ng) {
+    pp[g] = (int)(kxp[g] * row + rlp[g]);
+    pm[g] = (int)(kxm[g] * row + rlm[g]);
   }
 }
 

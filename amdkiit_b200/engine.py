@@ -189,7 +189,7 @@ def host_gvectors(system: System) -> dict:
     _check(lib.amdk_host_gvectors(C.byref(s), C.byref(info), inyh.ctypes.data, hg.ctypes.data, gvec.ctypes.data,
                                   mp.ctypes.data, mm.ctypes.data), "amdk_host_gvectors")
     return dict(inyh=inyh, hg=hg, gvec=gvec, mapp=mp, mapm=mm, ngpw=info.ngpw, ngrho=ng, ngrays=info.ngrays,
-                nhrays=info.nhrays, nr=tuple(info.nr))
+                nhrays=info.nhrays, nr=tuple(info.nr), omega=info.omega)
 
 
 # mixed-precision CG hands over to FP64 at this GEMAX: below it the FP32 pair

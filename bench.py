@@ -16,9 +16,15 @@ The default runs both precisions: `value` is the mixed-precision path
 numbers, the speed-ups and the energy/force differences of the two paths at
 the converged MD start (the metric's 1e-6 Ha/atom condition).
 
-Multi-GPU: the single-system path is not sharded (its only split is the
-reference's slab all-to-all, not built); N ranks run N independent replicas
-(weak scaling), value = total iterations of all ranks / max rank time.
+Multi-GPU: N ranks run N independent replicas of the CG iteration (weak
+scaling), value = total iterations of all ranks / max rank time.  The
+slab decomposition of the band-pair transforms (the reference's x-ray /
+x-plane split with an all-to-all inside each FFT) is measured by
+`--slab R,...`: under torchrun every rank holds its own slab and the
+all-to-alls are NCCL's; on one GPU the R ranks are emulated in one process
+(their launches one after the other, the exchange as copies) and the line
+reports the largest rank's kernel time per phase with the bytes each rank
+would send over NVLink.
 """
 from __future__ import annotations
 
@@ -482,6 +488,97 @@ def cufft_compare(args, local):
     return 0
 
 
+def slab_report(args, local, rank, world):
+    """Band-pair transforms of water32 (64 pairs, one pass each of V(r)psi
+    and the density) in the slab decomposition: per phase the largest
+    rank's device time (CUDA events, median of the timed passes), the
+    bytes each rank sends per pass, and the exchange time (NCCL under
+    torchrun; on one GPU the emulation's copies, which are not NVLink)."""
+    import torch
+    from amdkiit_b200.engine import FP64, MIXED
+    from amdkiit_b200.slab import LocalExchange, Slab, TorchExchange
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    out = {"metric": "slab-decomposed band-pair transforms, water32 (64 pairs, 100^3)", "unit": "ms per pass",
+           "report": "slab decomposition", "mode": "nccl" if world > 1 else "emulated ranks on one GPU",
+           "steps": args.steps, "warmup": args.warmup}
+    rlist = [world] if world > 1 else [int(x) for x in args.slab.split(",")]
+    for name, prec in (("fp64", FP64), ("mixed", MIXED)):
+        s, e = setup_engine(prec, local)
+        e.density()
+        e.potential()
+        c0 = e.get_wfn()
+        n1 = e.nr[0]
+        v = e.get("v_pot").reshape(n1, n1, n1)
+        T = (e.nstate + 1) // 2
+        res = {}
+        for R in rlist:
+            mine = [rank] if world > 1 else list(range(R))
+            slabs = [Slab(e, R, r) for r in mine]
+            ex = TorchExchange() if world > 1 else LocalExchange()
+            c0s = [torch.from_numpy(np.ascontiguousarray(c0[:, sl.local_g])).cuda() for sl in slabs]
+            vs = [torch.from_numpy(np.ascontiguousarray(v[:, :, sl.plane0:sl.plane0 + sl.nplane])).cuda()
+                  for sl in slabs]
+            c2s = [torch.zeros_like(c) for c in c0s]
+            rhos = [torch.zeros_like(x) for x in vs]
+            sends = [sl.new_send(T) for sl in slabs]
+            sc = [sl.send_counts(T) for sl in slabs]
+            rc = [sl.recv_counts(T) for sl in slabs]
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+            def timed(fn):
+                ev[0].record()
+                fn()
+                ev[1].record()
+                torch.cuda.synchronize()
+                return ev[0].elapsed_time(ev[1])
+
+            t = {k: [] for k in ("pairs_out", "exchange", "planes_density", "planes_vpsi", "exchange_back",
+                                 "pairs_in")}
+            for it in range(args.warmup + args.steps):
+                if dist is not None:
+                    dist.barrier()
+                pt = {k: 0.0 for k in t}
+                for i, sl in enumerate(slabs):
+                    pt["pairs_out"] = max(pt["pairs_out"], timed(lambda: sl.pairs_out(c0s[i], 0, T, sends[i])))
+                box = {}
+                pt["exchange"] = timed(lambda: box.update(r=ex(sends, sc, rc)))
+                recvs = box["r"]
+                dens_in = [x.clone() for x in recvs]
+                for i, sl in enumerate(slabs):
+                    pt["planes_density"] = max(pt["planes_density"],
+                                               timed(lambda: sl.planes_density(dens_in[i], 0, T, rhos[i], False)))
+                    pt["planes_vpsi"] = max(pt["planes_vpsi"], timed(lambda: sl.planes_vpsi(recvs[i], T, vs[i])))
+                pt["exchange_back"] = timed(lambda: box.update(b=ex(recvs, rc, sc)))
+                for i, sl in enumerate(slabs):
+                    pt["pairs_in"] = max(pt["pairs_in"], timed(lambda: sl.pairs_in(box["b"][i], c0s[i], 0, T, c2s[i])))
+                if it >= args.warmup:
+                    for k in t:
+                        t[k].append(max_over_ranks(pt[k], dist) if dist is not None else pt[k])
+            eb = slabs[0].elem_bytes
+            send_bytes = max(sum(c for r, c in enumerate(sc[i]) if r != sl.rank) * eb // 2
+                             for i, sl in enumerate(slabs))
+            res[str(R)] = {k: round(float(np.median(x)), 4) for k, x in t.items()}
+            res[str(R)]["nvlink_bytes_per_rank_each_way"] = int(send_bytes)
+            res[str(R)]["largest_rank_g"] = max(sl.ngpw_local for sl in slabs)
+            res[str(R)]["largest_rank_planes"] = max(sl.nplane for sl in slabs)
+            for sl in slabs:
+                sl.close()
+            del c0s, vs, c2s, rhos, sends
+        out[name] = res
+        e.close()
+        torch.cuda.empty_cache()
+    if rank == 0:
+        print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 def oracle_fixture():
     """The oracle's converged water32 energy and forces (a committed JSON
     fixture; the oracle itself does not run here), or None."""
@@ -545,6 +642,9 @@ def main():
     ap.add_argument("--relax", action="store_true",
                     help="cfg4: LBFGS relaxation of water128 (GRAD_CUTOFF 5e-4), one JSON line")
     ap.add_argument("--relax-steps", type=int, default=100)
+    ap.add_argument("--slab", default="",
+                    help="R,R,...: the slab-decomposed band-pair transforms with R ranks (emulated on one GPU; "
+                         "under torchrun the world size, exchanged by NCCL)")
     ap.add_argument("--cufft", action="store_true",
                     help="compare the library's H|psi> with cuFFT full-grid transforms of the same pairs")
     args = ap.parse_args()
@@ -558,6 +658,8 @@ def main():
         return config_report(args, local) if rank == 0 else 0
     if args.cufft:
         return cufft_compare(args, local) if rank == 0 else 0
+    if args.slab:
+        return slab_report(args, local, rank, world)
     if args.relax:
         return relax_report(args, local) if rank == 0 else 0
 

@@ -253,6 +253,71 @@ int amdk_ensemble_iteration(amdk_ensemble *ens, const int *istep, double gcut, a
 int amdk_ensemble_last_ms(amdk_ensemble *ens, double *ms);
 int amdk_ensemble_destroy(amdk_ensemble *ens);
 
+/* Slab decomposition of the band-pair transforms over nranks processes, as
+ * the reference distributes its FFTs (do_fft, fft_interface.f90:109-137):
+ * G space by x-rays, real space by contiguous x planes
+ * (distribute_YZplanes, gvectors.f90:80-108), an all-to-all in between
+ * (FFT_COMM -> MPI_trans, fft_interface.f90:500-511).  The library does the
+ * compute on each side of the exchange and writes/reads the exchange
+ * buffers in place; the caller moves them (one all-to-all, e.g. NCCL's, per
+ * direction), so no collective library is linked here.
+ *
+ * Ownership: rays go to ranks in mirror pairs {(ky,kz), (-ky,-kz)} (the rank
+ * holds +G and -G of every G it owns), largest first onto the rank with the
+ * fewest G vectors; rank r holds x planes [plane0[r], plane0[r+1]) with
+ * plane0[r] = floor(r n1 / nranks).  A rank's coefficients are C0/C2 arrays
+ * [nstate][ngpw_local] (complex FP64, its G vectors in increasing global
+ * order, amdk_slab_local_g); its real-space arrays are [nr3][nr2][nplane]
+ * FP64 (x fastest, over its planes).
+ *
+ * Exchange buffers (complex, elem_bytes each: the context's precision at
+ * amdk_slab_create): for npairs pairs the send buffer holds npairs *
+ * send_elems[r] elements for each rank r, in rank order; the receive buffer
+ * npairs * recv_elems[s] elements from each source s, in rank order (what an
+ * all-to-all with those counts produces).  The reverse exchange uses the
+ * same counts swapped and returns the blocks to where they came from.
+ *
+ * Per pass over pairs [band0/2, band0/2 + npairs) (band0 even):
+ *   amdk_slab_pairs_out      pack + backward x pass of the rank's rays -> send
+ *   (all-to-all send -> recv)
+ *   amdk_slab_planes_vpsi    y/z passes, V(r) psi, inverse (recv in place);
+ *                            v: this rank's slab of V(r), FP64
+ *   amdk_slab_planes_density rho(r) (=, or += with accumulate) sum of f/Omega
+ *                            |psi|^2 over the pairs' bands on this rank's slab
+ *   (all-to-all recv -> back, after planes_vpsi)
+ *   amdk_slab_pairs_in       forward x pass + unpack: C2 = -f (|G|^2/2 C0 +
+ *                            FFT(V psi)) on the rank's G vectors (vpsi,
+ *                            wfn_initialize.f90:283-362, without fnonloc)
+ * Pointers are device pointers; stream: a cudaStream_t to launch on
+ * (asynchronous), or NULL for the context's stream with the call waited for.
+ * A slab object serves one call at a time.  Closed-shell systems on grids
+ * with the pencil transforms only; nranks <= 16. */
+#define AMDK_SLAB_MAXRANKS 16
+typedef struct amdk_slab amdk_slab;
+typedef struct {
+  int nranks, rank;
+  int ngpw_local;         /* plane-wave G vectors of this rank */
+  int nray_local;         /* wavefunction x-rays of this rank */
+  int plane0, nplane;     /* x planes [plane0, plane0 + nplane) */
+  int gzero_local;        /* local index of G = 0, -1 on the other ranks */
+  int elem_bytes;         /* bytes per complex element of the exchange buffers */
+  long send_elems[AMDK_SLAB_MAXRANKS];  /* per pair, to each rank */
+  long recv_elems[AMDK_SLAB_MAXRANKS];  /* per pair, from each rank */
+} amdk_slab_info;
+/* Host only (no GPU): the owner of every plane-wave G vector (g_owner[ngpw])
+ * and the plane ranges (plane0[nranks+1]); either may be NULL. */
+int amdk_slab_layout(const amdk_system *sys, int nranks, int *g_owner, int *plane0);
+int amdk_slab_create(amdk_ctx *ctx, int nranks, int rank, amdk_slab **out);
+int amdk_slab_info_get(amdk_slab *slab, amdk_slab_info *info);
+int amdk_slab_local_g(amdk_slab *slab, int *ig);
+int amdk_slab_pairs_out(amdk_slab *slab, const double *c0, int band0, int npairs, void *send, void *stream);
+int amdk_slab_planes_vpsi(amdk_slab *slab, void *recv, int npairs, const double *v, void *stream);
+int amdk_slab_planes_density(amdk_slab *slab, const void *recv, int band0, int npairs, double *rho, int accumulate,
+                             void *stream);
+int amdk_slab_pairs_in(amdk_slab *slab, void *back, const double *c0, int band0, int npairs, double *c2,
+                       void *stream);
+int amdk_slab_destroy(amdk_slab *slab);
+
 #ifdef __cplusplus
 }
 #endif

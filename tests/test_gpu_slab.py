@@ -1,0 +1,98 @@
+"""The slab decomposition's kernels on the GPU (amdk_slab_*): nranks ranks
+held by one process (slab.LocalExchange moves the exchange buffers; every
+rank's launches run one after the other on one stream, none waits on
+another), against the oracle's vpsi and eval_density on the whole grid
+(wfn_initialize.f90:283-362, density.f90:19-90).
+
+Bars: FP64 1e-10 relative to the array's max, mixed (FP32 transforms) 1e-5."""
+import numpy as np
+import pytest
+
+from amdkiit_b200 import configs
+from amdkiit_b200.engine import FP64, MIXED, AmdkError, Engine
+from amdkiit_b200.slab import LocalExchange, Slab, SlabLayout, apply_local_h, density
+from oracle.oracle import Oracle
+from tests.helpers import start_coefficients
+
+pytestmark = pytest.mark.gpu
+
+_REF = {}
+
+
+def _reference(name):
+    """Oracle C0 (orthonormal), V(r), vpsi's C2 and rho(r) of the system."""
+    if name not in _REF:
+        s = configs.small_water() if name == "small_water" else configs.water32()
+        o = Oracle(s, 0)
+        g = o.gvectors()
+        o.set_wfn(start_coefficients(g["hg"][: o.ngpw], o.d("tpiba"), o.nstate, 21))
+        assert o.ortho() == 0
+        o.call("eval_density")
+        o.call("rhor2g")
+        o.call("eval_pot")
+        o.call("cal_vpot_ex")
+        o.call("vpsi")
+        _REF[name] = (s, o.c0(), o.real_grid("v_pot"), o.c2(), o.real_grid("rho"))
+    return _REF[name]
+
+
+def _run(name, prec, nranks):
+    import torch
+    s, c0, v, c2_ref, rho_ref = _reference(name)
+    e = Engine(s, prec)
+    slabs = [Slab(e, nranks, r) for r in range(nranks)]
+    lay = SlabLayout.of(s, nranks)
+    for r, sl in enumerate(slabs):
+        assert np.array_equal(sl.local_g, lay.local_g(r))
+        assert sl.plane0 == lay.plane0[r] and sl.nplane == lay.plane0[r + 1] - lay.plane0[r]
+    assert sum(sl.ngpw_local for sl in slabs) == e.ngpw
+    assert sum(sl.gzero_local >= 0 for sl in slabs) == 1
+    c0s = [torch.from_numpy(np.ascontiguousarray(c0[:, sl.local_g])).cuda() for sl in slabs]
+    vs = [torch.from_numpy(np.ascontiguousarray(v[:, :, sl.plane0:sl.plane0 + sl.nplane])).cuda() for sl in slabs]
+    c2s = [torch.zeros_like(c) for c in c0s]
+    rhos = [torch.zeros_like(x) for x in vs]
+    apply_local_h(slabs, LocalExchange(), c0s, vs, c2s)
+    density(slabs, LocalExchange(), c0s, rhos)
+    torch.cuda.synchronize()
+    c2 = np.zeros_like(c0)
+    rho = np.zeros_like(rho_ref)
+    for sl, c2l, rl in zip(slabs, c2s, rhos):
+        c2[:, sl.local_g] = c2l.cpu().numpy()
+        rho[:, :, sl.plane0:sl.plane0 + sl.nplane] = rl.cpu().numpy()
+    dc2 = np.abs(c2 - c2_ref).max() / np.abs(c2_ref).max()
+    drho = np.abs(rho - rho_ref).max() / np.abs(rho_ref).max()
+    for sl in slabs:
+        sl.close()
+    return dc2, drho
+
+
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+@pytest.mark.parametrize("nranks", [1, 2, 3, 4])
+def test_slab_small_water_matches_oracle(nranks, prec):
+    dc2, drho = _run("small_water", prec, nranks)
+    bar = 1e-10 if prec == FP64 else 1e-5
+    assert dc2 < bar and drho < bar, (dc2, drho)
+
+
+@pytest.mark.parametrize("prec,nranks", [(FP64, 2), (MIXED, 2), (MIXED, 8)])
+def test_slab_water32_matches_oracle(prec, nranks):
+    dc2, drho = _run("water32", prec, nranks)
+    bar = 1e-10 if prec == FP64 else 1e-5
+    print(prec, nranks, dc2, drho)
+    assert dc2 < bar and drho < bar, (dc2, drho)
+
+
+def test_slab_bad_arguments():
+    s = configs.small_water()
+    e = Engine(s, FP64)
+    with pytest.raises(AmdkError):
+        Slab(e, 2, 2)
+    with pytest.raises(AmdkError):
+        Slab(e, 17, 0)
+    sl = Slab(e, 2, 0)
+    import torch
+    buf = torch.zeros(8, dtype=torch.float64, device="cuda")
+    with pytest.raises(AmdkError):
+        sl.pairs_out(buf, 1, 1, buf)  # odd band0
+    with pytest.raises(AmdkError):
+        sl.pairs_out(buf, 0, e.nstate, buf)  # pairs beyond the bands
