@@ -691,8 +691,11 @@ struct BandWalk {
 };
 
 // A block's contiguous chunk of the (band, G) index space (as BandWalk), read
-// STREAM_U elements per thread per round with all loads issued first, so
-// that enough of them are in flight to stream at the copy rate.
+// STREAM_U elements per thread per round with every load of the round (the
+// coefficients and the per-G and per-band factors) issued first, so that
+// enough of them are in flight to stream at the copy rate; the (band, G)
+// position advances by additions, not a division per element.  The kernels
+// are launched with one wave of blocks (the resident count, not RED_BLOCKS).
 constexpr int STREAM_U = 4;
 __device__ __forceinline__ void stream_chunk(long tot, long &k0, long &k1) {
   const long per = (tot + gridDim.x - 1) / gridDim.x;
@@ -700,25 +703,36 @@ __device__ __forceinline__ void stream_chunk(long tot, long &k0, long &k1) {
   k0 = blockIdx.x * chunk;
   k1 = min(tot, k0 + chunk);
 }
+// (band, G) of element k + d from that of k (band-major, ngpw per band)
+__device__ __forceinline__ void band_step(int &b, int &g, int d, int ngpw) {
+  g += d;
+  while (g >= ngpw) {
+    g -= ngpw;
+    ++b;
+  }
+}
 __global__ void k_ekin(int ngpw, int nstate, const double2 *c0, const double *hg, const double *occ, double *part,
                        double *out, unsigned *ticket) {
   double s = 0;
   long k0, k1;
   stream_chunk((long)ngpw * nstate, k0, k1);
-  for (long kb = k0 + threadIdx.x; kb < k1; kb += STREAM_U * (long)blockDim.x) {
+  long k = k0 + threadIdx.x;
+  int b = (int)(k / ngpw), g = (int)(k - (long)b * ngpw);
+  const int step = blockDim.x;
+  while (k < k1) {
     double2 c[STREAM_U];
+    double h[STREAM_U], o[STREAM_U];
 #pragma unroll
     for (int u = 0; u < STREAM_U; ++u) {
-      const long k = kb + u * (long)blockDim.x;
-      c[u] = k < k1 ? c0[k] : make_double2(0.0, 0.0);
+      const bool v = k < k1;
+      c[u] = v ? c0[k] : make_double2(0.0, 0.0);
+      h[u] = v ? hg[g] : 0.0;
+      o[u] = v ? occ[b] : 0.0;
+      k += step;
+      band_step(b, g, step, ngpw);
     }
 #pragma unroll
-    for (int u = 0; u < STREAM_U; ++u) {
-      const long k = kb + u * (long)blockDim.x;
-      if (k >= k1) break;
-      const unsigned b = (unsigned)k / (unsigned)ngpw, g = (unsigned)k - b * (unsigned)ngpw;
-      s += occ[b] * hg[g] * (c[u].x * c[u].x + c[u].y * c[u].y);
-    }
+    for (int u = 0; u < STREAM_U; ++u) s += o[u] * h[u] * (c[u].x * c[u].x + c[u].y * c[u].y);
   }
   const double v[1] = {s};
   reduce_and_finish<1>(v, part, out, ticket);
@@ -776,23 +790,30 @@ __global__ void k_gmax_precon(int ngpw, int nocc, const double *vpp, const doubl
   double m = 0.0, s = 0.0;
   long k0, k1;
   stream_chunk((long)ngpw * nocc, k0, k1);
-  for (long kb = k0 + threadIdx.x; kb < k1; kb += STREAM_U * (long)blockDim.x) {
+  long k = k0 + threadIdx.x;
+  int b = (int)(k / ngpw), g = (int)(k - (long)b * ngpw);
+  const int step = blockDim.x;
+  while (k < k1) {
     double2 c[STREAM_U];
+    double kv[STREAM_U], o[STREAM_U];
+    bool g0[STREAM_U];
 #pragma unroll
     for (int u = 0; u < STREAM_U; ++u) {
-      const long k = kb + u * (long)blockDim.x;
-      c[u] = k < k1 ? c2[k] : make_double2(0.0, 0.0);
+      const bool v = k < k1;
+      c[u] = v ? c2[k] : make_double2(0.0, 0.0);
+      kv[u] = v ? vpp[g] : 0.0;
+      o[u] = v ? occ[b] : 1.0;
+      g0[u] = g == 0;
+      k += step;
+      band_step(b, g, step, ngpw);
     }
 #pragma unroll
     for (int u = 0; u < STREAM_U; ++u) {
-      const long k = kb + u * (long)blockDim.x;
-      if (k >= k1) break;
-      const unsigned b = (unsigned)k / (unsigned)ngpw, g = (unsigned)k - b * (unsigned)ngpw;
-      const double fi = occ[b] > 0.01 ? 1.0 / occ[b] : 1.0;  // 1/f_i
+      const double fi = o[u] > 0.01 ? 1.0 / o[u] : 1.0;  // 1/f_i
       m = fmax(m, c[u].x * c[u].x + c[u].y * c[u].y);
-      const double f = fi * vpp[g];
+      const double f = fi * kv[u];
       const double2 v = make_double2(f * c[u].x, f * c[u].y);
-      s += (g == 0) ? v.x * v.x : 2.0 * (v.x * v.x + v.y * v.y);
+      s += g0[u] ? v.x * v.x : 2.0 * (v.x * v.x + v.y * v.y);
     }
   }
   const double vals[2] = {sqrt(m), s};  // sqrt is monotonic: the max of the roots is the root of the max

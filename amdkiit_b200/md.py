@@ -15,12 +15,18 @@ restarting from C0(t) as molecular_dynamics.f90:106-109 does; the converged
 state and the trajectory are the same to the SCF tolerance, the number of
 SCF iterations per step drops.
 
-Deviations from the reference driver (both outside the hot path):
-- velocities are drawn per atom from a seeded Maxwell-Boltzmann
-  distribution (md_tools.f90:19-44 draws one random triple for every atom
-  and its seed is not applied, random.f90:15-17);
-- no centre-of-mass shift after the drift (md_tools.f90 shift_com divides
-  by na_max instead of the atom count); the linear momentum is removed once.
+Velocities and the centre-of-mass shift (outside the hot path):
+- by default velocities are drawn per atom from a seeded Maxwell-Boltzmann
+  distribution; md_tools.f90:19-44 instead draws one random triple w for
+  all atoms (v = sigma_s w for every atom of species s, then the linear
+  momentum is removed and the velocities rescaled to the temperature), and
+  its seed is not applied (random.f90:15-17), so its w cannot be
+  reproduced: `reference_velocities(w)` restates init_vel for a given w;
+- by default no centre-of-mass shift after the drift; com_shift=True
+  restates shift_com (md_tools.f90:116-149, called at
+  molecular_dynamics.f90:100): all atoms translated so that the sum of the
+  positions divided by na_max keeps its starting value (a uniform
+  translation, which changes no energy beyond the grid's egg-box effect).
 """
 from __future__ import annotations
 
@@ -37,7 +43,7 @@ KBOLTZ = 0.316681534e-5
 class BOMD:
     def __init__(self, engine, temperature: float = 300.0, dt_fs: float = 0.5, seed: int = 2024,
                  gcut: float = 1e-6, max_scf: int = 800, extrapolate: bool = False,
-                 predictor_points: int = 2):
+                 predictor_points: int = 2, com_shift: bool = False):
         self.e = engine
         self.extrapolate = extrapolate
         self.predictor_points = predictor_points
@@ -51,6 +57,8 @@ class BOMD:
             self.mass[i, : s.na[i]] = atomic_mass(sp.z) * AMU_AU
         self.mask = self.mass > 0
         self.pos = s.atco()
+        self.com_shift = com_shift
+        self.com0 = self._com(self.pos)
         self.ndof = 3 * s.nat - 3
         self.vel = self._init_velocities(temperature, seed)
         self.force = None
@@ -70,6 +78,26 @@ class BOMD:
         if t > 0:
             v *= np.sqrt(temperature / t)
         return v
+
+    def reference_velocities(self, w, temperature: float = 300.0):
+        """init_vel (md_tools.f90:19-48) with its random triple's vector w
+        given: every atom of species s gets sigma_s w, sigma_s =
+        sqrt(T k_B / m_s); then remove_lin_momentum (md_tools.f90:87-114)
+        and rescale_atvel to the temperature."""
+        w = np.asarray(w, dtype=np.float64)
+        v = np.zeros_like(self.pos)
+        sig = np.zeros_like(self.mass)
+        sig[self.mask] = np.sqrt(temperature * KBOLTZ / self.mass[self.mask])
+        v[self.mask] = sig[self.mask][:, None] * w[None, :]
+        p = (self.mass[..., None] * v).sum(axis=(0, 1)) / self.mass.sum()
+        v[self.mask] -= p
+        v *= np.sqrt(temperature / self.temperature(v))
+        return v
+
+    def _com(self, pos):
+        """get_com (md_tools.f90:116-131): the sum of the positions over all
+        atoms divided by na_max."""
+        return pos[self.mask].sum(axis=0) / self.system.na_max
 
     def kinetic(self, v=None):
         v = self.vel if v is None else v
@@ -105,6 +133,8 @@ class BOMD:
         a[self.mask] = self.force[self.mask] / self.mass[self.mask][:, None]
         self.vel += 0.5 * self.dt * a
         self.pos = self.pos + self.vel * self.dt
+        if self.com_shift:
+            self.pos[self.mask] -= self._com(self.pos) - self.com0
         self.e.set_positions(self.pos)
         if self.extrapolate:
             self.e.extrapolate()

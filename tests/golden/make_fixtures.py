@@ -3,8 +3,10 @@
 Reads AMDKIIT's tests/<case>/ directories (input.yaml, xyz, pseudopotential
 files and the amdkiit.out of the committed run) and writes, per case,
   <case>.npz   the parsed system (cell, positions, pseudopotential tables)
-  golden.json  the energies the reference printed (eprint.f90:1-14) and the
-               per-rank G-vector tables summed over ranks (gvectors.f90:315-325)
+  golden.json  the energies the reference printed (eprint.f90:1-14), the
+               per-rank G-vector tables summed over ranks (gvectors.f90:315-325),
+               and for the 32-water MD run every tenth frame of its trajectory
+               and its per-step energies
 Run from the repository root:  python tests/golden/make_fixtures.py /path/to/AMDKIIT
 """
 from __future__ import annotations
@@ -91,6 +93,36 @@ GEO_GRADIENTS = {"water1_mt": "tests/1_water/geo_opt/atom_force.dat",
                  "si_fcc_mt": "tests/bulk_si/geo_opt/atom_force.dat"}
 
 
+# the committed MD run whose trajectory the BOMD driver is compared with:
+# frames kept (every MD_FRAME_STRIDE-th, and frame 1, which with frame 0
+# fixes the initial velocities), all MD_ENERGY.dat rows
+MD_TRAJECTORY = {"water32_mt": "tests/32_water/md"}
+MD_FRAME_STRIDE = 10
+
+
+def parse_md_trajectory(dirname):
+    """MD_TRAJECTORY.xyz (write_md_trajectory, md_tools.f90:152-172: per
+    frame the atom count, 'MD STEP= n', then per atom the symbol, position
+    (Angstrom) and velocity (a.u.), 6 decimals) and MD_ENERGY.dat
+    (write_md_energy, md_tools.f90:174-184: step, temperature, KS energy,
+    KS + kinetic energy, CPU time)."""
+    lines = open(os.path.join(dirname, "MD_TRAJECTORY.xyz")).read().split("\n")
+    frames = {}
+    i = 0
+    while i < len(lines) and lines[i].strip():
+        nat = int(lines[i].split()[0])
+        step = int(lines[i + 1].split()[-1])
+        rows = [ln.split() for ln in lines[i + 2:i + 2 + nat]]
+        frames[step] = dict(symbols=[r[0] for r in rows], pos=[[float(v) for v in r[1:4]] for r in rows],
+                            vel=[[float(v) for v in r[4:7]] for r in rows])
+        i += 2 + nat
+    keep = sorted(k for k in frames if k % MD_FRAME_STRIDE == 0 or k == 1)
+    energy = [[float(v) for v in ln.split()[:4]]
+              for ln in open(os.path.join(dirname, "MD_ENERGY.dat")).read().split("\n") if ln.strip()]
+    return dict(symbols=frames[0]["symbols"], frames={str(k): frames[k]["pos"] for k in keep},
+                vel0=frames[0]["vel"], energy=energy, nsteps=max(frames))
+
+
 def parse_first_gradient(path):
     """The first block of a geometry optimisation's atom_force.dat: atom
     count, ENERGY= E step, then one line per atom with dE/dR (Ha/bohr, 16
@@ -130,6 +162,10 @@ def main(root):
             md = MD_FORCES[name] + "/amdkiit.out"
             pos, frc = parse_md_start_forces(os.path.join(root, md))
             golden[name]["md_start"] = dict(positions=pos.tolist(), forces=frc.tolist(), source=md)
+        if name in MD_TRAJECTORY:
+            tr = parse_md_trajectory(os.path.join(root, MD_TRAJECTORY[name]))
+            tr["source"] = MD_TRAJECTORY[name] + "/MD_TRAJECTORY.xyz, MD_ENERGY.dat"
+            golden[name]["md_trajectory"] = tr
         if name in GEO_GRADIENTS:
             # the geometry optimisation starts from the same input; its first
             # gradient is taken at the converged start geometry
