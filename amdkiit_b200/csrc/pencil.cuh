@@ -491,10 +491,19 @@ __global__ void __launch_bounds__(PNT, sizeof(C) == 8 ? 2 : 1) k_pencil_density(
   C nxt[PREF];
   auto fetch = [&](int t) {
     const long pr = (long)t * pg.pr_t + (long)kx * pg.pr_x;
+    if (pg.nseg == 1) {
+      const C *pl = rt + pr * pg.nray;
 #pragma unroll
-    for (int i = 0; i < PREF; ++i) {
-      const int r = threadIdx.x + i * blockDim.x;
-      nxt[i] = r < pg.nray ? rt[ray_at(pg, pr, r)] : czero<C>();
+      for (int i = 0; i < PREF; ++i) {
+        const int r = threadIdx.x + i * blockDim.x;
+        nxt[i] = r < pg.nray ? pl[r] : czero<C>();
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < PREF; ++i) {
+        const int r = threadIdx.x + i * blockDim.x;
+        nxt[i] = r < pg.nray ? rt[ray_at(pg, pr, r)] : czero<C>();
+      }
     }
   };
   const DivMod dz(nz);
@@ -573,32 +582,48 @@ __global__ void __launch_bounds__(PNT, sizeof(C) == 8 ? 2 : 1) k_pencil_density(
 __device__ __forceinline__ int perm_index(int pos, int n1f, int n2f) { return pos / n2f + n1f * (pos % n2f); }
 
 // rho[kz][ky][kx] (=, or += with add) sum over groups of rho_part[g][kx][q][k'],
-// for nx x planes (n on one GPU, a rank's planes in the slab decomposition)
+// for nx x planes (n on one GPU, a rank's planes in the slab decomposition).
+// grid ((n+31)/32, (nx+31)/32, n), block (32, 8): a 32 (k') x 32 (kx) tile of
+// plane q; a thread adds the groups of its four rows together (four loads
+// per group in flight; each element's sum keeps the group order), the tile
+// is transposed through shared memory.
 __global__ void k_rho_reduce_p(int n, int nx, int n1f, int n2f, int ngroups, const double *__restrict__ part,
                                double *__restrict__ rho, int add) {
   __shared__ double tile[32][33];
   const int q = blockIdx.z;
   const int k0 = blockIdx.x * 32, kx0 = blockIdx.y * 32;
   const long gstride = (long)nx * n * n;
-  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-    const int kx = kx0 + j, k = k0 + threadIdx.x;
-    double s = 0.0;
-    if (kx < nx && k < n) {
-      const double *pp = part + ((long)kx * n + q) * n + k;
-      // the loads are independent: unrolled, several are in flight while the
-      // sum keeps its group order
-#pragma unroll 8
-      for (int g = 0; g < ngroups; ++g) s += pp[g * gstride];
-    }
-    tile[j][threadIdx.x] = s;
+  const int k = k0 + threadIdx.x;
+  long off[4];
+  bool ok[4];
+  double s[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int kx = kx0 + threadIdx.y + 8 * i;
+    ok[i] = kx < nx && k < n;
+    off[i] = ok[i] ? ((long)kx * n + q) * n + k : 0;
+    s[i] = 0.0;
   }
+#pragma unroll 2
+  for (int g = 0; g < ngroups; ++g) {
+    const double *pg = part + g * gstride;
+    double v[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = ok[i] ? pg[off[i]] : 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) s[i] += v[i];
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) tile[threadIdx.y + 8 * i][threadIdx.x] = s[i];
   __syncthreads();
   const int ky = perm_index(q, n1f, n2f);
-  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-    const int k = k0 + j, kx = kx0 + threadIdx.x;
-    if (kx < nx && k < n) {
-      double *o = rho + ((long)perm_index(k, n1f, n2f) * n + ky) * nx + kx;
-      *o = add ? *o + tile[threadIdx.x][j] : tile[threadIdx.x][j];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int kk = k0 + threadIdx.y + 8 * i, kx = kx0 + threadIdx.x;
+    if (kx < nx && kk < n) {
+      double *o = rho + ((long)perm_index(kk, n1f, n2f) * n + ky) * nx + kx;
+      const double t = tile[threadIdx.x][threadIdx.y + 8 * i];
+      *o = add ? *o + t : t;
     }
   }
 }

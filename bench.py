@@ -416,6 +416,16 @@ def relax_report(args, local):
     e.set_wfn(initial_coefficients(g["hg"][: e.ngpw] * tp * tp, e.nstate))
     e.ortho()
     opt = GeometryOptimizer(e, gcut_wfn=1e-6, gcut_geo=5e-4, max_step=args.relax_steps)
+    evaluate = opt.energy_gradient
+
+    def logged(x):  # one progress line per geometry on stderr (energy, max force, SCF iterations)
+        out = evaluate(x)
+        en, fmax, nscf = opt.evaluations[-1]
+        print("relax evaluation %d: E %.8f Ha, max |F| %.3e Ha/bohr, %d SCF iterations, %.1f s"
+              % (len(opt.evaluations), en, fmax, nscf, time.perf_counter() - t0), file=sys.stderr, flush=True)
+        return out
+
+    opt.energy_gradient = logged
     t0 = time.perf_counter()
     res, atco = opt.run()
     wall = time.perf_counter() - t0
