@@ -690,9 +690,15 @@ template <typename C> static void pencil_vpsi(amdk_ctx *c, int T, int p0 = 0) {
 template <typename C, int N, int NS> static void launch_pencil_density_ns(amdk_ctx *c, int p0, int T, int grp, int add) {
   const Geom &g = c->geom;
   const size_t sm = pencil_smem<C>(N, c->pg.nz, c->ct_dens);
+  ++c->nlaunch;
+  if (grp < 0) {  // balanced schedule, -grp blocks (one batch of pairs)
+    smem_opt_in<k_pencil_density_bal<C, N, NS>>();
+    k_pencil_density_bal<C, N, NS><<<-grp, PNT, sm, c->st>>>(c->pg, plan<C>(c, 1), (const C *)c->d_rb, T, c->d_wa + p0,
+                                                             c->d_wb + p0, c->d_rhopart, c->ct_dens);
+    return;
+  }
   const int per = (T + grp - 1) / grp;
   smem_opt_in<k_pencil_density<C, N, NS>>();
-  ++c->nlaunch;
   k_pencil_density<C, N, NS><<<dim3(g.n1, grp), PNT, sm, c->st>>>(c->pg, plan<C>(c, 1), (const C *)c->d_rb, T, per,
                                                                   c->d_wa + p0, c->d_wb + p0, c->d_rhopart, c->ct_dens,
                                                                   add);
@@ -706,6 +712,20 @@ template <typename C> static void launch_pencil_density(amdk_ctx *c, int p0, int
       else launch_pencil_density_ns<C, N, 4>(c, p0, T, grp, add);
     }
   });
+}
+// rho (FP64 grid) from the partial grids of a density schedule (grp > 0
+// groups per plane, grp < 0 the balanced schedule of -grp blocks over T pairs)
+static void reduce_density(amdk_ctx *c, int grp, int T, double *rho) {
+  const Geom &g = c->geom;
+  ++c->nlaunch;
+  k_rho_reduce_p<<<dim3((g.n1 + 31) / 32, (g.n1 + 31) / 32, g.n1), dim3(32, 8), 0, c->st>>>(
+      g.n1, g.n1, c->pn1, c->pn2, grp > 0 ? grp : 0, c->d_rhopart, rho, 0, grp < 0 ? T : 0, grp < 0 ? -grp : 0);
+}
+// most partial grids a plane takes under the balanced schedule of nblk blocks
+static int bal_max_slots(int n1, int T, int nblk) {
+  int m = 0;
+  for (int kx = 0; kx < n1; ++kx) m = std::max(m, bal_slots(kx, T, (long)n1 * T, nblk));
+  return m;
 }
 // Pair groups of the density pencil kernel for T pairs at the current
 // precision: measured once (every candidate launched on the current buffers,
@@ -724,9 +744,15 @@ template <typename C> static int density_groups(amdk_ctx *c, int T) {
   cudaStreamIsCapturing(c->st, &cap);
   const std::string tkey = pencil_key(c, "pencil_density_groups_with_reduce", T) + "/ct" +
                            std::to_string(c->ct_dens) + "/ns" + std::to_string(c->ns_dens);
+  // the balanced schedule (negative values: -blocks) for a batch that holds
+  // every pair, with at most pencil_groups partial grids per plane
+  auto bal_ok = [&](int nblk) {
+    return T == c->npairs && nblk >= 1 && (long)nblk <= (long)g.n1 * T &&
+           bal_max_slots(g.n1, T, nblk) <= c->pencil_groups;
+  };
   int cached = 0;
-  if (cap == cudaStreamCaptureStatusNone && c->tune && tune_get(tkey, &cached) && cached >= 1 &&
-      cached <= std::min(c->pencil_groups, T)) {
+  if (cap == cudaStreamCaptureStatusNone && c->tune && tune_get(tkey, &cached) &&
+      ((cached >= 1 && cached <= std::min(c->pencil_groups, T)) || (cached < 0 && bal_ok(-cached)))) {
     best = cached;
   } else if (cap == cudaStreamCaptureStatusNone && c->tune) {
     cudaEvent_t e0, e1;
@@ -738,12 +764,18 @@ template <typename C> static int density_groups(amdk_ctx *c, int T) {
     // groups spread the blocks better but leave more grids to add
     auto run = [&](int grp) {
       launch_pencil_density<C>(c, 0, T, grp, 0);
-      k_rho_reduce_p<<<dim3((g.n1 + 31) / 32, (g.n1 + 31) / 32, g.n1), dim3(32, 8), 0, c->st>>>(
-          g.n1, g.n1, c->pn1, c->pn2, grp, c->d_rhopart, c->d_rho, 0);
+      reduce_density(c, grp, T, c->d_rho);
     };
-    const int cands[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16};
+    // (plane, pair group) blocks, then the balanced schedule with one, two or
+    // three waves of resident blocks
+    std::vector<int> cands = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16};
+    const int bps = (int)std::min<size_t>(sizeof(C) == sizeof(float2) ? 2 : 1,
+                                          std::max<size_t>(1, (228 * 1024) / (sm + 1024)));
+    for (int w = 1; w <= 3; ++w)
+      if (bal_ok(w * bps * c->nsm)) cands.push_back(-w * bps * c->nsm);
     for (int grp : cands) {
-      if (grp > c->pencil_groups || grp > T || (grp - 1) * ((T + grp - 1) / grp) >= T) continue;  // no empty group
+      if (grp > 0 && (grp > c->pencil_groups || grp > T || (grp - 1) * ((T + grp - 1) / grp) >= T))
+        continue;  // no empty group
       run(grp);  // warm
       float ms = 1e30f;
       for (int rep = 0; rep < 3; ++rep) {  // the fastest of three (another context may share the GPU)
@@ -773,7 +805,9 @@ template <typename C> static void pencil_density(amdk_ctx *c, int p0, int T) {
   const int grp = density_groups<C>(c, T);
   const double npt = (double)g.n1 * g.n2 * g.n3;
   const int add = p0 > 0;
-  prof_begin(c, KT_ZDENS, (double)T * rstride(c, 0) * sizeof(C) + (1.0 + add) * grp * npt * 8.0);
+  // partial grids written: groups per plane, or about one per block and plane boundary
+  const double grids = grp > 0 ? (double)grp : 1.0 + (double)(-grp) / g.n1;
+  prof_begin(c, KT_ZDENS, (double)T * rstride(c, 0) * sizeof(C) + (1.0 + add) * grids * npt * 8.0);
   launch_pencil_density<C>(c, p0, T, grp, add);
   prof_end(c);
 }
@@ -789,7 +823,9 @@ template <typename C> static int density_pairs_t(amdk_ctx *c) {
     // groups that only later batches use are cleared first
     const int ng_full = density_groups<C>(c, c->batch);
     const int ng_rem = (c->npairs % c->batch) ? density_groups<C>(c, c->npairs % c->batch) : 0;
-    const int ng = std::max(ng_full, ng_rem);
+    // the balanced schedule (ng_full < 0) runs only when one batch holds
+    // every pair: each plane's partial grids are all written, none cleared
+    const int ng = ng_full < 0 ? ng_full : std::max(ng_full, ng_rem);
     const int ng_first = c->npairs < c->batch ? ng_rem : ng_full;
     const size_t npt = (size_t)g.n1 * g.n2 * g.n3;
     if (ng > ng_first)
@@ -799,9 +835,7 @@ template <typename C> static int density_pairs_t(amdk_ctx *c) {
       xt_bwd_pair<C>(c, p0, T);
       pencil_density<C>(c, p0, T);
     }
-    ++c->nlaunch;
-    k_rho_reduce_p<<<dim3((g.n1 + 31) / 32, (g.n1 + 31) / 32, g.n1), dim3(32, 8), 0, c->st>>>(
-        g.n1, g.n1, c->pn1, c->pn2, ng, c->d_rhopart, c->d_rho, 0);
+    reduce_density(c, ng, c->npairs, c->d_rho);
     if (h.lsd) {
       // open shell: the spin-2 density from the same pair transforms, weighted
       // by the spin-2 bands only (density.f90:64-76); with all pairs in one
@@ -817,9 +851,7 @@ template <typename C> static int density_pairs_t(amdk_ctx *c) {
       }
       std::swap(c->d_wa, c->d_wa2);
       std::swap(c->d_wb, c->d_wb2);
-      ++c->nlaunch;
-      k_rho_reduce_p<<<dim3((g.n1 + 31) / 32, (g.n1 + 31) / 32, g.n1), dim3(32, 8), 0, c->st>>>(
-          g.n1, g.n1, c->pn1, c->pn2, ng, c->d_rhopart, c->d_rho2, 0);
+      reduce_density(c, ng, c->npairs, c->d_rho2);
     }
   } else {
   CK(cudaMemsetAsync(c->d_rho, 0, sizeof(double) * (size_t)g.n1 * g.n2 * g.n3, c->st));
@@ -2424,7 +2456,7 @@ static int slab_density_t(amdk_slab *s, const C *recv, int band0, int T, double 
   });
   ++c->nlaunch;
   k_rho_reduce_p<<<dim3((n + 31) / 32, (s->nplane + 31) / 32, n), dim3(32, 8), 0, st>>>(
-      n, s->nplane, c->pn1, c->pn2, grp, s->d_rhopart, rho, add);
+      n, s->nplane, c->pn1, c->pn2, grp, s->d_rhopart, rho, add, 0, 0);
   CK(cudaGetLastError());
   return 0;
 }

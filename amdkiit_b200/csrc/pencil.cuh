@@ -577,39 +577,171 @@ __global__ void __launch_bounds__(PNT, sizeof(C) == 8 ? 2 : 1) k_pencil_density(
   }
 }
 
+// Balanced schedule of the density sums over one batch of T pairs: the
+// n1 T (x-plane, pair) units, plane-major (unit u = plane u / T, pair u % T),
+// in nblk contiguous ranges, block b taking [b U / nblk, (b+1) U / nblk),
+// U = n1 T; one wave of blocks then has equal work to within one pair, where
+// (plane, pair-group) blocks leave a partial last wave.  A plane is shared by
+// the consecutive blocks bal_block(plane T) .. bal_block(plane T + T - 1); the
+// k-th of them stores its sums of that plane in partial grid k.
+__host__ __device__ __forceinline__ int bal_block(long u, long U, int nblk) {
+  return (int)(((u + 1) * nblk - 1) / U);  // the largest b with floor(b U / nblk) <= u
+}
+__host__ __device__ __forceinline__ int bal_slots(int kx, int T, long U, int nblk) {
+  return bal_block((long)kx * T + T - 1, U, nblk) - bal_block((long)kx * T, U, nblk) + 1;
+}
+template <typename C, int N, int NS>
+__global__ void __launch_bounds__(PNT, sizeof(C) == 8 ? 2 : 1)
+    k_pencil_density_bal(PencilGeom pg, Plan<C> p, const C *__restrict__ rt, int T, const double *__restrict__ wa,
+                         const double *__restrict__ wb, double *__restrict__ rho_part, int CTs) {
+  typedef decltype(C().x) Rl;
+  constexpr int N1 = fft_n1(N), N2 = N / N1, NP = N + 1;
+  extern __shared__ unsigned char smraw[];
+  const int nz = pg.nz;
+  PencilSmem<C, N> sm(smraw, nz, CTs);
+  C *P = sm.P, *S = sm.S, *tw = sm.tw;
+  const uint4 *zp = sm.zp;
+  sm.load(p, pg.zinv);
+  const long U = (long)pg.n1 * T;
+  const int nb = gridDim.x, b = blockIdx.x;
+  const long u0 = (long)b * U / nb, u1 = (long)(b + 1) * U / nb;
+  const int ntiles = (N + CTs - 1) / CTs;
+  const int reps = NS / ntiles;  // the launch guarantees ntiles * reps == NS and CTs N1 <= reps PNT
+  Rl acc[NS][N2];
+  constexpr int PREF = 4;
+  const bool pre = pg.nray <= PREF * (int)blockDim.x;
+  C nxt[PREF];
+  auto row_of = [&](long u) {
+    const long kx = u / T;
+    return (u - kx * T) * pg.pr_t + kx * pg.pr_x;
+  };
+  auto fetch = [&](long u) {
+    const C *pl = rt + row_of(u) * pg.nray;  // one ray segment (the one-GPU layout)
+#pragma unroll
+    for (int i = 0; i < PREF; ++i) {
+      const int r = threadIdx.x + i * blockDim.x;
+      nxt[i] = r < pg.nray ? pl[r] : czero<C>();
+    }
+  };
+  const DivMod dz(nz);
+  if (pre && u0 < u1) fetch(u0);
+  __syncthreads();  // the tables
+  for (long u = u0; u < u1;) {
+    const int kx = (int)(u / T);
+    const long ue = min(u1, (long)(kx + 1) * T);
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) acc[s][k2] = (Rl)0;
+    for (; u < ue; ++u) {
+      const int t = (int)(u - (long)kx * T);
+      if (pre) {
+        for (int idx = threadIdx.x; idx < nz * NP; idx += blockDim.x) P[idx] = czero<C>();
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < PREF; ++i) {
+          const int r = threadIdx.x + i * blockDim.x;
+          if (r < pg.nray) P[pg.rpos[r]] = nxt[i];
+        }
+        __syncthreads();
+        if (u + 1 < u1) fetch(u + 1);
+      } else {
+        pencil_scatter<C, N>(P, rt, row_of(u), pg);
+      }
+      rows_nat_to_perm<C, N, 1>(P, nz, dz, tw);
+      const Rl fa = (Rl)wa[t], fb = (Rl)wb[t];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const int ti = s / reps, rr = s - ti * reps;
+        const int q0 = ti * CTs, ct = min(CTs, N - q0);
+        const DivMod dq(ct);
+        if (rr == 0) {
+          zcols_phase_a<C, N>(P, S, zp, q0, ct, dq, tw);
+          __syncthreads();
+        }
+        const int idx = threadIdx.x + rr * PNT;
+        if (idx < ct * N1) {
+          int k1, qq;
+          dq(idx, k1, qq);
+          const C *row = S + qq * NP + k1 * N2;
+          C w[N2];
+#pragma unroll
+          for (int j2 = 0; j2 < N2; ++j2) w[j2] = row[j2];
+          Dft<C, N2, 1>::run(w);
+#pragma unroll
+          for (int k2 = 0; k2 < N2; ++k2) {
+            const Rl re = w[k2].x, im = w[k2].y;
+            acc[s][k2] += fa * re * re + fb * im * im;
+          }
+        }
+        if (rr == reps - 1) __syncthreads();
+      }
+    }
+    // this plane's sums -> shared memory [q][k'] (row stride N+1) -> its partial grid
+    Rl *stage = reinterpret_cast<Rl *>(smraw);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const int ti = s / reps, rr = s - ti * reps;
+      const int q0 = ti * CTs, ct = min(CTs, N - q0);
+      const int idx = threadIdx.x + rr * PNT;
+      if (idx < ct * N1) {
+        int k1, qq;
+        const DivMod dq(ct);
+        dq(idx, k1, qq);
+        Rl *ar = stage + (q0 + qq) * NP + k1 * N2;
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) ar[k2] = acc[s][k2];
+      }
+    }
+    __syncthreads();
+    const int slot = b - bal_block((long)kx * T, U, nb);
+    double *out = rho_part + ((long)slot * pg.n1 + kx) * N * N;
+    for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
+      const int q = idx / N, k = idx % N;
+      out[idx] = (double)stage[q * NP + k];
+    }
+    __syncthreads();  // the stage overlaps P, which the next plane's first pair fills
+  }
+}
+
 // position <-> index of the permuted (ky, kz) order: position a*N2 + b holds
 // index a + N1*b
 __device__ __forceinline__ int perm_index(int pos, int n1f, int n2f) { return pos / n2f + n1f * (pos % n2f); }
 
 // rho[kz][ky][kx] (=, or += with add) sum over groups of rho_part[g][kx][q][k'],
-// for nx x planes (n on one GPU, a rank's planes in the slab decomposition).
+// for nx x planes (n on one GPU, a rank's planes in the slab decomposition);
+// ngroups grids per plane, or with bal_nblk > 0 the balanced schedule's
+// bal_slots grids of each plane.
 // grid ((n+31)/32, (nx+31)/32, n), block (32, 8): a 32 (k') x 32 (kx) tile of
 // plane q; a thread adds the groups of its four rows together (four loads
 // per group in flight; each element's sum keeps the group order), the tile
 // is transposed through shared memory.
 __global__ void k_rho_reduce_p(int n, int nx, int n1f, int n2f, int ngroups, const double *__restrict__ part,
-                               double *__restrict__ rho, int add) {
+                               double *__restrict__ rho, int add, int bal_T, int bal_nblk) {
   __shared__ double tile[32][33];
   const int q = blockIdx.z;
   const int k0 = blockIdx.x * 32, kx0 = blockIdx.y * 32;
   const long gstride = (long)nx * n * n;
   const int k = k0 + threadIdx.x;
   long off[4];
-  bool ok[4];
+  int ng[4];
   double s[4];
+  int gmax = 0;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int kx = kx0 + threadIdx.y + 8 * i;
-    ok[i] = kx < nx && k < n;
-    off[i] = ok[i] ? ((long)kx * n + q) * n + k : 0;
+    const bool ok = kx < nx && k < n;
+    ng[i] = !ok ? 0 : (bal_nblk > 0 ? bal_slots(kx, bal_T, (long)nx * bal_T, bal_nblk) : ngroups);
+    gmax = max(gmax, ng[i]);
+    off[i] = ok ? ((long)kx * n + q) * n + k : 0;
     s[i] = 0.0;
   }
 #pragma unroll 2
-  for (int g = 0; g < ngroups; ++g) {
+  for (int g = 0; g < gmax; ++g) {
     const double *pg = part + g * gstride;
     double v[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) v[i] = ok[i] ? pg[off[i]] : 0.0;
+    for (int i = 0; i < 4; ++i) v[i] = g < ng[i] ? pg[off[i]] : 0.0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) s[i] += v[i];
   }
