@@ -1,7 +1,7 @@
-"""Seeded initial wavefunction used by every configuration of this build.
+"""Seeded initial wavefunction used by every configuration of the library.
 
 The reference starts from an atomic-orbital guess (wfn_initialize.f90:4);
-this build starts every run from seeded complex Gaussian coefficients damped
+the library starts every run from seeded complex Gaussian coefficients damped
 by 1/(1+|G|^2) (|G|^2 in bohr^-2), with Im c(G=0) = 0, which the caller then
 orthonormalises (ortho_gs, wfn_initialize.f90:448-499).
 """

@@ -123,7 +123,7 @@ def set_vec(a: float, b: float, c: float, symmetry: str) -> np.ndarray:
     if s == "FCC":
         cols = [[-a / 2.0, 0.0, a / 2.0], [0.0, a / 2.0, a / 2.0], [-a / 2.0, a / 2.0, 0.0]]
         return np.array(cols, dtype=float).T
-    raise ValueError(f"lattice {symmetry} is not supported by this build (cubic and fcc only)")
+    raise ValueError(f"lattice {symmetry} is not supported (cubic and fcc only)")
 
 
 _SYM_ID = {"CUBIC": 1, "FCC": 2}

@@ -91,7 +91,7 @@ void *orc_get_ptr(orc_sys *s, const char *name);
 /* geometry: new positions -> exp_igrxfactor (atco layout as orc_input) */
 void orc_set_positions(orc_sys *s, const double *atco);
 
-/* the seeded initial guess used by every configuration of this build:
+/* the seeded initial guess used by every configuration of the library:
  * complex Gaussian N(0,1) per real and imaginary part, damped by
  * 1/(1+|G|^2) with |G|^2 in bohr^-2, Im c(G=0)=0, then ortho_gs.
  * The random numbers come from the caller (so the product and the oracle

@@ -1,5 +1,5 @@
-"""Subspace eigenvalues (the north-star eigenvalue check is oracle vs GPU:
-the reference prints none).  CPU tests of the shared diagonalisation and of
+"""Subspace eigenvalues (the 1e-5 Ha eigenvalue check is oracle vs GPU: the
+reference prints none).  CPU tests of the shared diagonalisation and of
 the H|psi> scaling it assumes (C2 = -f_i H|psi_i>, f_i = 2)."""
 import numpy as np
 

@@ -1,7 +1,7 @@
 """The CPU restatement against the reference's committed runs (the oracle pin).
 
 The reference prints its converged energy breakdown (eprint.f90:1-14); the
-oracle, started from this build's seeded guess instead of the atomic guess,
+oracle, started from the library's seeded guess instead of the atomic guess,
 must reach the same total energy within 1e-6 Ha/atom (components within
 2e-5 Ha: they converge more slowly than the variational total)."""
 import os
