@@ -59,11 +59,17 @@ inline PencilGeom pencil_geom_1gpu(int n1, int n2, int n3, int nray, int nz, con
   return g;
 }
 // position of ray r of row pr in the plane kernels' buffer
+// (the segment tables are read with compile-time indices only, so they stay
+// in the kernel's parameter space)
 __device__ __forceinline__ long ray_at(const PencilGeom &pg, long pr, int r) {
-  int s = 0;
-  while (s + 1 < pg.nseg && r >= pg.seg_r0[s + 1]) ++s;
-  const int r0 = pg.seg_r0[s];
-  return pg.seg_mul * r0 + pr * (pg.seg_r0[s + 1] - r0) + (r - r0);
+  int r0 = 0, r1 = pg.seg_r0[1];
+#pragma unroll
+  for (int s = 1; s < PG_MAXSEG; ++s)
+    if (s < pg.nseg && r >= pg.seg_r0[s]) {
+      r0 = pg.seg_r0[s];
+      r1 = pg.seg_r0[s + 1];
+    }
+  return pg.seg_mul * r0 + pr * (r1 - r0) + (r - r0);
 }
 
 constexpr int PNT = 512;  // threads per pencil block
@@ -266,7 +272,9 @@ template <typename C, int N>
 __device__ __forceinline__ void pencil_scatter(C *P, const C *__restrict__ rt, long pr, const PencilGeom &pg) {
   for (int idx = threadIdx.x; idx < pg.nz * (N + 1); idx += blockDim.x) P[idx] = czero<C>();
   __syncthreads();
-  for (int s = 0; s < pg.nseg; ++s) {
+#pragma unroll
+  for (int s = 0; s < PG_MAXSEG; ++s) {
+    if (s >= pg.nseg) break;
     const int r0 = pg.seg_r0[s], nr = pg.seg_r0[s + 1] - r0;
     const C *src = rt + pg.seg_mul * r0 + pr * nr;
     for (int j = threadIdx.x; j < nr; j += blockDim.x) P[pg.rpos[r0 + j]] = src[j];
@@ -446,7 +454,9 @@ __global__ void __launch_bounds__(PNT) k_pencil_vpsi(PencilGeom pg, Plan<C> p, C
     __syncthreads();
   }
   rows_perm_to_nat<C, N, -1>(P, nz, dz, tw);
-  for (int sg = 0; sg < pg.nseg; ++sg) {
+#pragma unroll
+  for (int sg = 0; sg < PG_MAXSEG; ++sg) {
+    if (sg >= pg.nseg) break;
     const int r0 = pg.seg_r0[sg], nr = pg.seg_r0[sg + 1] - r0;
     C *dst = rt + pg.seg_mul * r0 + pr * nr;
     for (int j = threadIdx.x; j < nr; j += blockDim.x) dst[j] = P[pg.rpos[r0 + j]];
