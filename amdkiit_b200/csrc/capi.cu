@@ -2647,6 +2647,21 @@ int amdk_set_wfn(amdk_ctx *c, const double *c0) {
   return 0;
 }
 
+int amdk_set_density(amdk_ctx *c, const double *rho) {
+  if (!c || !rho) return AMDK_ERR_BADARG;
+  if (c->hs.lsd) {
+    set_error("amdk_set_density: the open-shell branch keeps a density per spin; not supported");
+    return AMDK_ERR_UNSUPPORTED;
+  }
+  cudaSetDevice(c->device);
+  const size_t npt = (size_t)c->hs.nr[0] * c->hs.nr[1] * c->hs.nr[2];
+  CK(cudaMemcpyAsync(c->d_rho, rho, sizeof(double) * npt, cudaMemcpyHostToDevice, c->st));
+  if (c->precision == AMDK_MIXED) RC(rhor2g_t<float2>(c));
+  else RC(rhor2g_t<double2>(c));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
 int amdk_get_wfn(amdk_ctx *c, double *c0) {
   if (!c || !c0) return AMDK_ERR_BADARG;
   cudaSetDevice(c->device);

@@ -84,6 +84,7 @@ def load_library(path: str = LIBPATH):
     lib.amdk_wfn_set_predictor.argtypes = [P, C.c_int, C.c_void_p]
     lib.amdk_wfn_history_clear.argtypes = [P]
     lib.amdk_set_wfn.argtypes = [P, C.POINTER(C.c_double)]
+    lib.amdk_set_density.argtypes = [P, C.POINTER(C.c_double)]
     lib.amdk_get_wfn.argtypes = [P, C.POINTER(C.c_double)]
     for f in ("amdk_ortho", "amdk_density", "amdk_potential", "amdk_apply_h"):
         getattr(lib, f).argtypes = [P]
@@ -278,6 +279,15 @@ class Engine:
         c = np.ascontiguousarray(c0, dtype=np.complex128)
         assert c.shape == (self.nstate, self.ngpw)
         _check(self.lib.amdk_set_wfn(self.h, c.ctypes.data_as(C.POINTER(C.c_double))), "amdk_set_wfn")
+
+    def set_density(self, rho: np.ndarray):
+        """rho(r) as (nr3, nr2, nr1) float64 in place of the density of C0
+        (rhor2g applied): the gathered density of a slab-decomposed system."""
+        r = np.ascontiguousarray(rho, dtype=np.float64)
+        n1, n2, n3 = self.nr
+        if r.size != n1 * n2 * n3:
+            raise ValueError("set_density: rho must have nr3 * nr2 * nr1 values")
+        _check(self.lib.amdk_set_density(self.h, _dp(r)), "amdk_set_density")
 
     def get_wfn(self, out: np.ndarray | None = None) -> np.ndarray:
         """C0 as (nstate, ngpw) complex128; with `out` (C-contiguous, that

@@ -29,7 +29,10 @@ all-to-alls:
                 283-362)
 
 so the exchange is fused with the pack and the unpack: no kernel copies the
-ray data into or out of a staging layout.  The band-space products that
+ray data into or out of a staging layout.  The potential between the two
+passes (`local_h_from_c0`) is computed on every rank from the gathered
+density (the slabs' planes all-gathered, 8 MB at water32): the density-sphere
+fields stay replicated.  The band-space products that
 follow (Gram matrices, projections, norms) are sums over G and take an
 all-reduce of the local sums, as the reference's are (mympi.f90).
 
@@ -203,6 +206,23 @@ class TorchExchange:
         return [out]
 
 
+def _gather_torch(self, parts, plane0):
+    """Every rank's [nr3][nr2][nplane] slab assembled along x into the full
+    grid (all_gather of slabs padded to the largest plane count)."""
+    import torch
+    import torch.distributed as dist
+    x = parts[0]
+    counts = np.diff(plane0)
+    pad = torch.zeros(x.shape[:2] + (int(counts.max()),), dtype=x.dtype, device=x.device)
+    pad[:, :, : x.shape[2]] = x
+    outs = [torch.empty_like(pad) for _ in counts]
+    dist.all_gather(outs, pad, group=self.group)
+    return [torch.cat([o[:, :, : int(c)] for o, c in zip(outs, counts)], dim=2)]
+
+
+TorchExchange.gather_planes = _gather_torch
+
+
 class LocalExchange:
     """The all-to-all among ranks held by one process: receive buffer r is
     the concatenation over sources s of the block s addressed to r."""
@@ -219,6 +239,12 @@ class LocalExchange:
                 raise ValueError("send and receive counts disagree")
             outs.append(out)
         return outs
+
+    def gather_planes(self, parts, plane0):
+        """The ranks' slabs assembled along x into the full grid, one copy per rank."""
+        import torch
+        full = torch.cat(list(parts), dim=2)
+        return [full for _ in parts]
 
 
 def _pair_range(nstate: int, band0: int, npairs):
@@ -261,3 +287,38 @@ def density(slabs: Sequence, exchange, c0s: Sequence, rhos: Sequence, band0: int
     recvs = exchange(sends, [s.send_counts(npairs) for s in slabs], [s.recv_counts(npairs) for s in slabs])
     for s, buf, rho in zip(slabs, recvs, rhos):
         s.planes_density(buf, band0, npairs, rho, accumulate)
+
+
+def potential_slabs(engine, slabs: Sequence, exchange, rhos: Sequence):
+    """V(r) on every rank's x planes from the ranks' density slabs: the slabs
+    gathered into rho(r), eval_pot + cal_vpot_ex (potential.f90:4-46,
+    xc.f90:4-434) on that full grid, each rank keeping its planes."""
+    import torch
+    fulls = exchange.gather_planes(rhos, plane_ranges(engine.nr[0], slabs[0].nranks))
+    vs = []
+    for s, full in zip(slabs, fulls):
+        engine.set_density(full.cpu().numpy())
+        engine.potential()
+        v = engine.get("v_pot")
+        vs.append(torch.from_numpy(np.ascontiguousarray(v[:, :, s.plane0:s.plane0 + s.nplane])).to(rhos[0].device))
+    return vs
+
+
+def plane_ranges(n1: int, nranks: int) -> np.ndarray:
+    """plane0[0..nranks] of the decomposition: rank r holds x planes
+    floor(r n1 / nranks) .. floor((r+1) n1 / nranks) - 1."""
+    return np.array([(r * n1) // nranks for r in range(nranks + 1)])
+
+
+def local_h_from_c0(engine, slabs: Sequence, exchange, c0s: Sequence, c2s: Sequence):
+    """The local part of H|psi> of a slab-decomposed wavefunction from C0
+    alone: rho(r) by the slab transforms, V(r) from the gathered density,
+    then C2 = -f (G^2/2 C0 + FFT(V psi)) by the slab transforms (eval_density,
+    eval_pot, cal_vpot_ex, vpsi of one CG iteration)."""
+    import torch
+    rhos = [torch.zeros(engine.nr[2], engine.nr[1], s.nplane, dtype=torch.float64, device=c.device)
+            for s, c in zip(slabs, c0s)]
+    density(slabs, exchange, c0s, rhos)
+    vs = potential_slabs(engine, slabs, exchange, rhos)
+    apply_local_h(slabs, exchange, c0s, vs, c2s)
+    return rhos, vs

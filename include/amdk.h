@@ -142,6 +142,13 @@ int amdk_set_precision(amdk_ctx *ctx, int precision);
 int amdk_set_wfn(amdk_ctx *ctx, const double *c0);
 int amdk_get_wfn(amdk_ctx *ctx, double *c0);
 
+/* rho(r) given instead of computed from C0 (nr3*nr2*nr1 FP64, host memory, x
+ * fastest), with rhor2g (density.f90:128-150) applied, so that amdk_potential
+ * and amdk_energy use it: the density of a system whose bands are spread over
+ * several processes, gathered from their slabs (amdk_slab_planes_density).
+ * Closed shell only. */
+int amdk_set_density(amdk_ctx *ctx, const double *rho);
+
 /* wfn_initialize.f90:448-499 ortho_gs (Cholesky of the overlap) */
 int amdk_ortho(amdk_ctx *ctx);
 /* density.f90:5-98 eval_density + density.f90:128-150 rhor2g */

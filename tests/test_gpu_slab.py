@@ -96,3 +96,34 @@ def test_slab_bad_arguments():
         sl.pairs_out(buf, 1, 1, buf)  # odd band0
     with pytest.raises(AmdkError):
         sl.pairs_out(buf, 0, e.nstate, buf)  # pairs beyond the bands
+
+
+@pytest.mark.parametrize("name,prec,nranks", [("small_water", FP64, 3), ("water32", MIXED, 4)])
+def test_slab_local_h_from_c0_matches_oracle(name, prec, nranks):
+    """The whole local part of H|psi> from a distributed C0 alone: rho(r) by
+    the slab transforms, the slabs gathered into rho, the potential of that
+    density (amdk_set_density + amdk_potential), each rank's V slab, then
+    V(r)psi by the slab transforms; against the oracle's eval_density,
+    eval_pot, cal_vpot_ex and vpsi from the same C0."""
+    import torch
+    from amdkiit_b200.slab import local_h_from_c0
+    s, c0, v_ref, c2_ref, rho_ref = _reference(name)
+    e = Engine(s, prec)
+    slabs = [Slab(e, nranks, r) for r in range(nranks)]
+    c0s = [torch.from_numpy(np.ascontiguousarray(c0[:, sl.local_g])).cuda() for sl in slabs]
+    c2s = [torch.zeros_like(c) for c in c0s]
+    rhos, vs = local_h_from_c0(e, slabs, LocalExchange(), c0s, c2s)
+    torch.cuda.synchronize()
+    c2 = np.zeros_like(c0)
+    rho = np.zeros_like(rho_ref)
+    v = np.zeros_like(v_ref)
+    for sl, c2l, rl, vl in zip(slabs, c2s, rhos, vs):
+        c2[:, sl.local_g] = c2l.cpu().numpy()
+        rho[:, :, sl.plane0:sl.plane0 + sl.nplane] = rl.cpu().numpy()
+        v[:, :, sl.plane0:sl.plane0 + sl.nplane] = vl.cpu().numpy()
+    bar = 1e-10 if prec == FP64 else 1e-5
+    errs = [np.abs(a - b).max() / np.abs(b).max() for a, b in ((rho, rho_ref), (v, v_ref), (c2, c2_ref))]
+    print(name, prec, nranks, errs)
+    assert max(errs) < bar, errs
+    for sl in slabs:
+        sl.close()

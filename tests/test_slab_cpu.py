@@ -313,3 +313,48 @@ def test_stand_in_matches_oracle_vpsi_and_density():
         rho[:, :, s.plane0:s.plane0 + s.nplane] = rl
     assert np.abs(c2 - c2_ref).max() < 1e-11 * np.abs(c2_ref).max()
     assert np.abs(rho - rho_ref).max() < 1e-11 * np.abs(rho_ref).max()
+
+
+def _gather_rank(rank, nranks, port, q):
+    import torch
+    import torch.distributed as dist
+    from amdkiit_b200.slab import plane_ranges
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=nranks)
+    try:
+        full = np.arange(5 * 4 * 9, dtype=np.float64).reshape(5, 4, 9)
+        p0 = plane_ranges(9, nranks)
+        mine = torch.from_numpy(np.ascontiguousarray(full[:, :, p0[rank]:p0[rank + 1]]))
+        got = TorchExchange().gather_planes([mine], p0)[0].numpy()
+        q.put((rank, bool(np.array_equal(got, full))))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_density_slabs_gathered_over_gloo():
+    """The all-gather of the ranks' x-plane slabs (uneven plane counts: 9
+    planes over 2 ranks) rebuilds the whole grid on every rank, as the
+    potential between the two passes of a distributed H|psi> needs."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gather_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert all(ok for _, ok in res), res
+
+
+def test_local_exchange_gathers_planes():
+    import torch
+    from amdkiit_b200.slab import plane_ranges
+    full = np.random.default_rng(3).normal(size=(6, 5, 11))
+    p0 = plane_ranges(11, 3)
+    parts = [torch.from_numpy(np.ascontiguousarray(full[:, :, p0[r]:p0[r + 1]])) for r in range(3)]
+    for got in LocalExchange().gather_planes(parts, p0):
+        assert np.array_equal(got.numpy(), full)
