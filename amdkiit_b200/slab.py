@@ -205,22 +205,18 @@ class TorchExchange:
         dist.all_to_all_single(out, sends[0], list(recv_counts[0]), list(send_counts[0]), group=self.group)
         return [out]
 
-
-def _gather_torch(self, parts, plane0):
-    """Every rank's [nr3][nr2][nplane] slab assembled along x into the full
-    grid (all_gather of slabs padded to the largest plane count)."""
-    import torch
-    import torch.distributed as dist
-    x = parts[0]
-    counts = np.diff(plane0)
-    pad = torch.zeros(x.shape[:2] + (int(counts.max()),), dtype=x.dtype, device=x.device)
-    pad[:, :, : x.shape[2]] = x
-    outs = [torch.empty_like(pad) for _ in counts]
-    dist.all_gather(outs, pad, group=self.group)
-    return [torch.cat([o[:, :, : int(c)] for o, c in zip(outs, counts)], dim=2)]
-
-
-TorchExchange.gather_planes = _gather_torch
+    def gather_planes(self, parts, plane0):
+        """Every rank's [nr3][nr2][nplane] slab assembled along x into the full
+        grid (all_gather of slabs padded to the largest plane count)."""
+        import torch
+        import torch.distributed as dist
+        x = parts[0]
+        counts = np.diff(plane0)
+        pad = torch.zeros(x.shape[:2] + (int(counts.max()),), dtype=x.dtype, device=x.device)
+        pad[:, :, : x.shape[2]] = x
+        outs = [torch.empty_like(pad) for _ in counts]
+        dist.all_gather(outs, pad, group=self.group)
+        return [torch.cat([o[:, :, : int(c)] for o, c in zip(outs, counts)], dim=2)]
 
 
 class LocalExchange:
