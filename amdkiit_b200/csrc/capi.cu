@@ -1225,8 +1225,10 @@ static size_t dg_part_doubles(const amdk_ctx *c, int m, int n) {
 // projector arrays.  sym: B = A, only the upper tiles are formed and the
 // result is mirrored.
 static int dg_tn(amdk_ctx *c, const void *A, int m, const void *B, int n, double alpha, double *out, int ldo,
-                 bool sym = false) {
-  const long K = 2L * c->hs.ngpw;
+                 bool sym = false, long Kin = 0, cudaStream_t sin = nullptr) {
+  // K: 2 ngpw unless given (a slab rank's 2 ngpw_local); stream: the context's unless given
+  const long K = Kin > 0 ? Kin : 2L * c->hs.ngpw;
+  cudaStream_t st = sin ? sin : c->st;
   CUtensorMap ta, tb;
   RC(dg_encode(&ta, A, K, m, DG_KT, DG_T, CU_TENSOR_MAP_SWIZZLE_128B));
   if (sym)
@@ -1242,9 +1244,9 @@ static int dg_tn(amdk_ctx *c, const void *A, int m, const void *B, int n, double
   const int per = (ktiles + nsplit - 1) / nsplit;
   nsplit = (ktiles + per - 1) / per;
   c->nlaunch += 2;
-  k_dgemm_tn<<<dim3(ntile, nsplit), DG_THREADS, DG_TN_SMEM, c->st>>>(ta, tb, m, n, mt, sym ? 1 : 0, ktiles, per, c->d_dgpart,
-                                                                     c->d_info + 1, c->dg_plim);
-  k_dgemm_tn_sum<<<(int)std::min<long>((long)ntile * (DG_T * DG_T / 32), 8L * c->nsm), 256, 0, c->st>>>(
+  k_dgemm_tn<<<dim3(ntile, nsplit), DG_THREADS, DG_TN_SMEM, st>>>(ta, tb, m, n, mt, sym ? 1 : 0, ktiles, per, c->d_dgpart,
+                                                                 c->d_info + 1, c->dg_plim);
+  k_dgemm_tn_sum<<<(int)std::min<long>((long)ntile * (DG_T * DG_T / 32), 8L * c->nsm), 256, 0, st>>>(
       c->d_dgpart, nsplit, ntile, mt, sym ? 1 : 0, m, n, alpha, out, ldo);
   CK(cudaGetLastError());
   return 0;
@@ -3224,6 +3226,38 @@ int amdk_slab_pairs_in(amdk_slab *s, void *back, const double *c0, int band0, in
     RC(slab_pairs_in_t<float2>(s, (float2 *)back, (const double2 *)c0, band0, npairs, (double2 *)c2, st));
   else RC(slab_pairs_in_t<double2>(s, (double2 *)back, (const double2 *)c0, band0, npairs, (double2 *)c2, st));
   return slab_finish(s, stream);
+}
+
+int amdk_slab_gram(amdk_slab *s, const double *a, const double *b, int n, double *out, void *stream) {
+  if (!s || !a || !b || !out || n < 1 || n > s->c->nstate) {
+    set_error("amdk_slab_gram: null pointer or band count outside 1..nstate");
+    return AMDK_ERR_BADARG;
+  }
+  amdk_ctx *c = s->c;
+  CK(cudaSetDevice(c->device));
+  const cudaStream_t st = slab_stream(s, stream);
+  if (s->ng == 0) {
+    CK(cudaMemsetAsync(out, 0, sizeof(double) * n * n, st));
+    CK(cudaStreamSynchronize(st));
+    return 0;
+  }
+  // the FP64 tensor-core product over the rank's 2 ngpw_local real components
+  RC(dg_tn(c, a, n, b, n, 2.0, out, n, a == b, 2L * s->ng, st));
+  if (s->gzero == 0) {  // the rank holding G = 0 (local index 0) removes its doubled term
+    ++c->nlaunch;
+    k_g0_correct<<<dim3(nblk(n), n), NTHR, 0, st>>>(n, s->ng, (const double2 *)a, (const double2 *)b, out, c->d_occ, 0,
+                                                    0);
+  }
+  CK(cudaGetLastError());
+  int expired = 0;
+  CK(cudaMemcpyAsync(&expired, c->d_info + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (expired) {
+    CK(cudaMemset(c->d_info + 1, 0, sizeof(int)));
+    set_error("amdk_slab_gram: a pipeline wait of the FP64 tensor-core product gave up");
+    return AMDK_ERR_TIMEOUT;
+  }
+  return 0;
 }
 
 int amdk_slab_destroy(amdk_slab *s) {

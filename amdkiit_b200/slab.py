@@ -76,6 +76,7 @@ def _bind(lib):
     lib.amdk_slab_planes_vpsi.argtypes = [P, P, C.c_int, P, P]
     lib.amdk_slab_planes_density.argtypes = [P, P, C.c_int, C.c_int, P, C.c_int, P]
     lib.amdk_slab_pairs_in.argtypes = [P, P, P, C.c_int, C.c_int, P, P]
+    lib.amdk_slab_gram.argtypes = [P, P, P, C.c_int, P, P]
     lib.amdk_slab_destroy.argtypes = [P]
     lib._slab_bound = True
     return lib
@@ -177,6 +178,11 @@ class Slab:
         _check(self.lib.amdk_slab_pairs_in(self.h, _ptr(back), _ptr(c0), band0, npairs, _ptr(c2), self._stream()),
                "amdk_slab_pairs_in")
 
+    def gram(self, a, b, n: int, out):
+        """out (n x n float64, column-major) = this rank's share of 2 Re a^H b
+        over its G vectors (the G = 0 term once, on its owner)."""
+        _check(self.lib.amdk_slab_gram(self.h, _ptr(a), _ptr(b), n, _ptr(out), self._stream()), "amdk_slab_gram")
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.amdk_slab_destroy(self.h)
@@ -203,6 +209,13 @@ class TorchExchange:
             raise ValueError("TorchExchange moves the buffers of one rank per process")
         out = torch.empty(sum(recv_counts[0]), dtype=sends[0].dtype, device=sends[0].device)
         dist.all_to_all_single(out, sends[0], list(recv_counts[0]), list(send_counts[0]), group=self.group)
+        return [out]
+
+    def all_reduce(self, parts):
+        """The sum over ranks of each rank's array (a band-space partial sum)."""
+        import torch.distributed as dist
+        out = parts[0].clone()
+        dist.all_reduce(out, group=self.group)
         return [out]
 
     def gather_planes(self, parts, plane0):
@@ -235,6 +248,13 @@ class LocalExchange:
                 raise ValueError("send and receive counts disagree")
             outs.append(out)
         return outs
+
+    def all_reduce(self, parts):
+        """The sum over the ranks' arrays (in rank order), one copy per rank."""
+        total = parts[0].clone()
+        for p in parts[1:]:
+            total += p
+        return [total for _ in parts]
 
     def gather_planes(self, parts, plane0):
         """The ranks' slabs assembled along x into the full grid, one copy per rank."""
@@ -318,3 +338,17 @@ def local_h_from_c0(engine, slabs: Sequence, exchange, c0s: Sequence, c2s: Seque
     vs = potential_slabs(engine, slabs, exchange, rhos)
     apply_local_h(slabs, exchange, c0s, vs, c2s)
     return rhos, vs
+
+
+def gram(slabs: Sequence, exchange, a_s: Sequence, b_s: Sequence, n: int):
+    """The band-space Gram matrix 2 Re A^H B - Re a(0) Re b(0)^T (n x n,
+    column-major) of a slab-decomposed pair of band arrays: each rank's share
+    over its G vectors, then an all-reduce (the overlap of ortho_gs,
+    wfn_initialize.f90:481-482, and Lambda of OVLAP_D are this product)."""
+    import torch
+    parts = []
+    for s, a, b in zip(slabs, a_s, b_s):
+        out = torch.empty(n * n, dtype=torch.float64, device=a.device)
+        s.gram(a, b, n, out)
+        parts.append(out)
+    return [x.reshape(n, n).T for x in exchange.all_reduce(parts)]

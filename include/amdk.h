@@ -323,6 +323,15 @@ int amdk_slab_planes_density(amdk_slab *slab, const void *recv, int band0, int n
                              void *stream);
 int amdk_slab_pairs_in(amdk_slab *slab, void *back, const double *c0, int band0, int npairs, double *c2,
                        void *stream);
+/* The rank's share of a band-space Gram matrix (the overlap S of ortho_gs,
+ * wfn_initialize.f90:481-482, or Lambda of OVLAP_D): out (n x n, column-major,
+ * device) = 2 Re sum over the rank's G of conj(a_i) b_j, less Re a_i(0) Re b_j(0)
+ * on the rank that holds G = 0, for bands 0..n-1 of the rank's arrays a and b
+ * ([nstate][ngpw_local] complex, device); the sum over ranks (an all-reduce) is
+ * the whole matrix.  FP64 tensor-core product; waits for its stream; uses the
+ * context's split buffer, so it does not run concurrently with the context's
+ * own calls.  AMDK_ERR_TIMEOUT if a pipeline wait gave up. */
+int amdk_slab_gram(amdk_slab *slab, const double *a, const double *b, int n, double *out, void *stream);
 int amdk_slab_destroy(amdk_slab *slab);
 
 #ifdef __cplusplus

@@ -358,3 +358,10 @@ def test_local_exchange_gathers_planes():
     parts = [torch.from_numpy(np.ascontiguousarray(full[:, :, p0[r]:p0[r + 1]])) for r in range(3)]
     for got in LocalExchange().gather_planes(parts, p0):
         assert np.array_equal(got.numpy(), full)
+
+
+def test_local_exchange_all_reduce():
+    import torch
+    parts = [torch.full((3, 3), float(r + 1)) for r in range(4)]
+    for got in LocalExchange().all_reduce(parts):
+        assert torch.equal(got, torch.full((3, 3), 10.0))
